@@ -1,0 +1,378 @@
+/*
+ * CPU oracle for the tet4 ADER-DG elastic / viscoelastic element update.
+ *
+ * TEST INFRASTRUCTURE ONLY. This file restates, in plain C and FP64, the reference's GTS element
+ * update so that tests, smoke() and the bench's CPU-baseline leg can check the CUDA path against
+ * it. Nothing in the product links, calls or ships this code.
+ *
+ * Layouts (runs fastest, row-major):
+ *   dofsE  [nEl][9][B][R]          dofsA [nEl][rm][6][B][R]        tDofs [nEl][9][B][R]
+ *   starE  [nEl][3][24]  (row-major non-zeros of the elastic star matrices, Elasticity.cpp:254-300)
+ *   starA  [nEl][3][9]   (row-major non-zeros of the 6x3 anelastic star, ViscoElasticity.cpp:295-316)
+ *   srcA   [nEl][rm][12] (row-major non-zeros of the 6x6 anelastic source, ViscoElasticity.h:460-508)
+ *   fsE    [2][nEl][4][81] (row-major 9x9 flux solvers; [0] local, [1] neighbour, AderDgInit.hpp:394-665)
+ *   fsA    [2][nEl][4][54] (row-major 6x9 anelastic flux solvers)
+ *   stiffT [3][B][B] = K_d^T M^-1 (NOT negated; negated on use like dg/TimePred.hpp:86)
+ *   stiffV [3][B][B] = K_d M^-1,  fluxL [4][B][F], fluxN [12][B][F] (id 4v+f), fluxT [4][F][B]
+ *
+ * Functions follow (reference file:line):
+ *   oracle_ck          TimePredVanilla::ck            src/impl/seismic/kernels/TimePredVanilla.hpp:200-306
+ *   oracle_eval_pred   TimePred::evalTimePrediction   src/impl/seismic/kernels/TimePred.hpp:130-156
+ *   oracle_volint      VolIntVanilla::apply           src/impl/seismic/kernels/VolIntVanilla.hpp:189-241
+ *   oracle_surf_local  SurfIntVanilla::local          src/impl/seismic/kernels/SurfIntVanilla.hpp:212-262
+ *   oracle_surf_neigh  SurfIntVanilla::neigh(+FluxInt) src/impl/seismic/kernels/SurfIntVanilla.hpp:274-357
+ *   oracle_series_int  Series<1>::integrate           src/linalg/Series.hpp:59-134
+ *   oracle_step        steps 0/1/2 of one GTS step    src/impl/seismic/steps.inc:24-77 with
+ *                      AderDg::local (AderDg.hpp:338-534), PointSources::apply (PointSources.hpp:887-931),
+ *                      AderDg::neigh (AderDg.hpp:553-722), Receivers (io/Receivers.cpp:235-290)
+ */
+#include <math.h>
+#include <stdlib.h>
+#include <string.h>
+
+/* sparsity patterns: row-major non-zeros (Elasticity.cpp:254-300, ViscoElasticity.cpp:295-316,
+ * ViscoElasticity.h:484-507) */
+static const int SE_R[24] = {0,0,0,1,1,1,2,2,2,3,3,4,4,5,5,6,6,6,7,7,7,8,8,8};
+static const int SE_C[24] = {6,7,8,6,7,8,6,7,8,6,7,7,8,6,8,0,3,5,1,3,4,2,4,5};
+static const int SA_R[9]  = {0,1,2,3,3,4,4,5,5};
+static const int SA_C[9]  = {0,1,2,0,1,1,2,0,2}; /* column within the velocities (6+c) */
+static const int SR_R[12] = {0,0,0,1,1,1,2,2,2,3,4,5};
+static const int SR_C[12] = {0,1,2,0,1,2,0,1,2,3,4,5};
+
+static int nmodes(int o) { return o <= 0 ? 0 : o * (o + 1) * (o + 2) / 6; }
+
+/* C[m][n][r] (+)= sum_k A[m][k][r] * B[k][n]   (MmVanilla fused-AC, Matrix.h:296-330) */
+static void mm_ac(int R, int M, int N, int K, int ldA, int ldB, int ldC, double beta,
+                  const double *A, const double *Bm, double *C) {
+  for (int m = 0; m < M; m++)
+    for (int n = 0; n < N; n++)
+      for (int r = 0; r < R; r++) {
+        double *c = &C[((size_t)m * ldC + n) * R + r];
+        *c = (beta != 0.0) ? *c * beta : 0.0;
+      }
+  for (int k = 0; k < K; k++)
+    for (int m = 0; m < M; m++)
+      for (int n = 0; n < N; n++) {
+        double b = Bm[(size_t)k * ldB + n];
+        if (b == 0.0) continue; /* exact: adding a zero product changes nothing */
+        for (int r = 0; r < R; r++)
+          C[((size_t)m * ldC + n) * R + r] += A[((size_t)m * ldA + k) * R + r] * b;
+      }
+}
+
+/* C[m][n][r] += sum_k A[m][k] * B[k][n][r] with A dense MxK (fused-BC, Matrix.h:332-378) */
+static void mm_bc(int R, int M, int N, int K, int ldB, int ldC, const double *A,
+                  const double *Bm, double *C) {
+  for (int k = 0; k < K; k++)
+    for (int m = 0; m < M; m++) {
+      double a = A[m * K + k];
+      if (a == 0.0) continue;
+      for (int n = 0; n < N; n++)
+        for (int r = 0; r < R; r++)
+          C[((size_t)m * ldC + n) * R + r] += a * Bm[((size_t)k * ldB + n) * R + r];
+    }
+}
+
+static void dense_star(const double *sp, double *d) {
+  memset(d, 0, 81 * sizeof(double));
+  for (int i = 0; i < 24; i++) d[SE_R[i] * 9 + SE_C[i]] = sp[i];
+}
+static void dense_starA(const double *sp, double *d) { /* 6x3 acting on velocities */
+  memset(d, 0, 18 * sizeof(double));
+  for (int i = 0; i < 9; i++) d[SA_R[i] * 3 + SA_C[i]] = sp[i];
+}
+static void dense_src(const double *sp, double *d) {
+  memset(d, 0, 36 * sizeof(double));
+  for (int i = 0; i < 12; i++) d[SR_R[i] * 6 + SR_C[i]] = sp[i];
+}
+
+void oracle_ck(int O, int R, int rm, double dt, const double *stiffT, const double *starE,
+               const double *starA, const double *srcA, const double *omega,
+               const double *dofsE, const double *dofsA, double *derE, double *tIntE,
+               double *tIntA) {
+  const int B = nmodes(O);
+  const size_t szE = (size_t)9 * B * R, szM = (size_t)6 * B * R;
+  double *scr = calloc(szE, sizeof(double));
+  double *scrA = calloc(szM, sizeof(double));
+  double *derA = rm ? calloc((size_t)rm * O * szM, sizeof(double)) : NULL;
+  double *kT = malloc((size_t)3 * B * B * sizeof(double));
+  double st[3][81], sa[3][18], sr[6 * 6];
+  for (size_t i = 0; i < (size_t)3 * B * B; i++) kT[i] = -stiffT[i];
+  for (int d = 0; d < 3; d++) {
+    dense_star(starE + 24 * d, st[d]);
+    if (rm) dense_starA(starA + 9 * d, sa[d]);
+  }
+  double sca = dt;
+  for (size_t i = 0; i < szE; i++) {
+    derE[i] = dofsE[i];
+    tIntE[i] = sca * dofsE[i];
+  }
+  for (int m = 0; m < rm; m++)
+    for (size_t i = 0; i < szM; i++) {
+      derA[(size_t)m * O * szM + i] = dofsA[m * szM + i];
+      tIntA[m * szM + i] = sca * dofsA[m * szM + i];
+    }
+  for (int de = 1; de < O; de++) {
+    const int re = rm == 0 ? de : 1;
+    const int nN = nmodes(O - re), nK = nmodes(O - re + 1);
+    double *dCur = derE + (size_t)de * szE, *dPrv = derE + (size_t)(de - 1) * szE;
+    memset(dCur, 0, szE * sizeof(double));
+    memset(scrA, 0, szM * sizeof(double));
+    for (int di = 0; di < 3; di++) {
+      mm_ac(R, 9, nN, nK, B, B, B, 0.0, dPrv, kT + (size_t)di * B * B, scr);
+      mm_bc(R, 9, nN, 9, B, B, st[di], scr, dCur);
+      if (rm) mm_bc(R, 6, nN, 3, B, B, sa[di], scr + (size_t)6 * B * R, scrA);
+    }
+    sca *= dt / (de + 1);
+    for (int m = 0; m < rm; m++) {
+      double *aPrv = derA + ((size_t)m * O + de - 1) * szM, *aCur = aPrv + szM;
+      dense_src(srcA + 12 * m, sr);
+      mm_bc(R, 6, B, 6, B, B, sr, aPrv, dCur);
+      for (size_t i = 0; i < szM; i++) {
+        aCur[i] = omega[m] * (scrA[i] + aPrv[i]);
+        tIntA[m * szM + i] += sca * aCur[i];
+      }
+    }
+    const int nCp = rm == 0 ? nmodes(O - de) : B;
+    for (int q = 0; q < 9; q++)
+      for (int md = 0; md < nCp; md++)
+        for (int r = 0; r < R; r++) {
+          size_t i = ((size_t)q * B + md) * R + r;
+          tIntE[i] += sca * dCur[i];
+        }
+  }
+  free(scr);
+  free(scrA);
+  free(derA);
+  free(kT);
+}
+
+void oracle_eval_pred(int O, int R, double tau, const double *derE, double *pred) {
+  const int B = nmodes(O);
+  const size_t szE = (size_t)9 * B * R;
+  memcpy(pred, derE, szE * sizeof(double));
+  double sca = 1.0;
+  for (int de = 1; de < O; de++) {
+    sca *= tau / de;
+    const int nCk = nmodes(O - de); /* CK modes even with anelasticity (TimePred.hpp:149) */
+    for (int q = 0; q < 9; q++)
+      for (int md = 0; md < nCk; md++)
+        for (int r = 0; r < R; r++) {
+          size_t i = ((size_t)q * B + md) * R + r;
+          pred[i] += sca * derE[(size_t)de * szE + i];
+        }
+  }
+}
+
+void oracle_volint(int O, int R, int rm, const double *stiffV, const double *starE,
+                   const double *starA, const double *srcA, const double *omega,
+                   const double *tIntE, const double *tIntA, double *dofsE, double *dofsA) {
+  const int B = nmodes(O), Bk = nmodes(O - 1);
+  const size_t szE = (size_t)9 * B * R, szM = (size_t)6 * B * R;
+  double *scr = malloc(szE * sizeof(double));
+  double *scrA = calloc(szM, sizeof(double));
+  double st[81], sa[18], sr[36];
+  for (int di = 0; di < 3; di++) {
+    mm_ac(R, 9, B, Bk, B, B, B, 0.0, tIntE, stiffV + (size_t)di * B * B, scr);
+    dense_star(starE + 24 * di, st);
+    mm_bc(R, 9, B, 9, B, B, st, scr, dofsE);
+    if (rm) {
+      dense_starA(starA + 9 * di, sa);
+      mm_bc(R, 6, B, 3, B, B, sa, scr + (size_t)6 * B * R, scrA);
+    }
+  }
+  for (int m = 0; m < rm; m++) {
+    dense_src(srcA + 12 * m, sr);
+    mm_bc(R, 6, B, 6, B, B, sr, tIntA + m * szM, dofsE);
+    for (size_t i = 0; i < szM; i++) dofsA[m * szM + i] += omega[m] * (scrA[i] - tIntA[m * szM + i]);
+  }
+  free(scr);
+  free(scrA);
+}
+
+/* one face of the surface integral: dofsE += fluxT_f^T-apply((fs * (tInt * flux)));  upA likewise */
+static void surf_face(int O, int R, int rm, const double *flux, const double *fluxTf,
+                      const double *fsE, const double *fsA, const double *tInt, double *dofsE,
+                      double *upA, double *s0, double *s1) {
+  const int B = nmodes(O), F = O * (O + 1) / 2;
+  mm_ac(R, 9, F, B, B, F, F, 0.0, tInt, flux, s0);
+  memset(s1, 0, (size_t)9 * F * R * sizeof(double));
+  mm_bc(R, 9, F, 9, F, F, fsE, s0, s1);
+  mm_ac(R, 9, B, F, F, B, B, 1.0, s1, fluxTf, dofsE);
+  if (rm) {
+    memset(s1, 0, (size_t)6 * F * R * sizeof(double));
+    mm_bc(R, 6, F, 9, F, F, fsA, s0, s1);
+    mm_ac(R, 6, B, F, F, B, B, 1.0, s1, fluxTf, upA);
+  }
+}
+
+static void scatter_upA(int B, int R, int rm, const double *omega, const double *upA,
+                        double *dofsA) {
+  const size_t szM = (size_t)6 * B * R;
+  for (int m = 0; m < rm; m++)
+    for (size_t i = 0; i < szM; i++) dofsA[m * szM + i] += omega[m] * upA[i];
+}
+
+void oracle_surf_local(int O, int R, int rm, const double *fluxL, const double *fluxT,
+                       const double *fsE4, const double *fsA4, const double *omega,
+                       const double *tIntE, double *dofsE, double *dofsA) {
+  const int B = nmodes(O), F = O * (O + 1) / 2;
+  double *s0 = malloc((size_t)9 * F * R * sizeof(double));
+  double *s1 = malloc((size_t)9 * F * R * sizeof(double));
+  double *upA = calloc((size_t)6 * B * R, sizeof(double));
+  for (int f = 0; f < 4; f++)
+    surf_face(O, R, rm, fluxL + (size_t)f * B * F, fluxT + (size_t)f * F * B, fsE4 + 81 * f,
+              rm ? fsA4 + 54 * f : NULL, tIntE, dofsE, upA, s0, s1);
+  if (rm) scatter_upA(B, R, rm, omega, upA, dofsA);
+  free(s0);
+  free(s1);
+  free(upA);
+}
+
+/* vId < 0 selects the local flux matrix of face fa (free surface); otherwise fluxN[4*vId+fId] */
+void oracle_surf_neigh(int O, int R, int rm, int fa, int vId, int fId, const double *fluxL,
+                       const double *fluxN, const double *fluxT, const double *fsE,
+                       const double *fsA, const double *tIntNe, double *dofsE, double *upA) {
+  const int B = nmodes(O), F = O * (O + 1) / 2;
+  double *s0 = malloc((size_t)9 * F * R * sizeof(double));
+  double *s1 = malloc((size_t)9 * F * R * sizeof(double));
+  const double *flux = vId < 0 ? fluxL + (size_t)fa * B * F : fluxN + (size_t)(4 * vId + fId) * B * F;
+  surf_face(O, R, rm, flux, fluxT + (size_t)fa * F * B, fsE, fsA, tIntNe, dofsE, upA, s0, s1);
+  free(s0);
+  free(s1);
+}
+
+double oracle_series_int(double dx, double xStart, long nPts, const double *vals, double x1,
+                         double x2, double na, double tol) {
+  const double dxH = dx * 0.5;
+  double out = 0;
+  double f = (x1 - xStart + dx) / dx, l = (x2 - xStart) / dx;
+  size_t first = (size_t)(f > 0 ? f : 0), last = (size_t)(l > 0 ? l : 0);
+  if (last > (size_t)(nPts - 1)) last = nPts - 1;
+  if (first > last) first = last;
+  for (size_t p = first + 1; p < last + 1; p++) {
+    out += dxH * (vals[p] - vals[p - 1]);
+    out += vals[p - 1] * dx;
+  }
+  int bL = 0, bR = 0;
+  double tEnd = xStart + (nPts - 1) * dx;
+  if (x1 + tol > xStart && x1 - tol < tEnd) bL = 1;
+  if (x2 + tol > xStart && x2 - tol < tEnd) bR = 1;
+  double diff = xStart + first * dx - x1;
+  if (first > 0 && bL) {
+    out += 0.5 * diff * (diff / dx) * (vals[first - 1] - vals[first]);
+    out += vals[first] * diff;
+  } else
+    out += na * diff;
+  diff = x2 - (xStart + last * dx);
+  if (last < (size_t)(nPts - 1) && bR) {
+    out += 0.5 * diff * (diff / dx) * (vals[last + 1] - vals[last]);
+    out += vals[last] * diff;
+  } else
+    out += na * diff;
+  return out;
+}
+
+/* face types of the per-element face table */
+enum { FT_INNER = 0, FT_FREE = 1, FT_OUTFLOW = 2 };
+
+/*
+ * One GTS time step over the whole mesh: local (CK, receivers, volume, local surface) ->
+ * point sources -> neighbour surface + anelastic scatter.
+ *
+ * Receivers: nRe receivers grouped by element (recvEl ascending, equal elements adjacent); each
+ * has basis values recvBasis[nRe][B] and its next output time recvTime[nRe] (updated). Output:
+ * recvBuf[nRe][maxBuf][9][R], recvBufTime[nRe][maxBuf], recvCount[nRe] (updated). A group of
+ * receivers in one element is evaluated at the first receiver's time (Receivers.cpp:250-290).
+ *
+ * Sources: nSrc point sources sorted by (element, run); source s adds
+ * int_{t}^{t+dt} series * srcScal[s][q] * srcBEval[s][md] to run srcRun[s] of element srcEl[s].
+ * Series s has srcNPts[s] samples at srcTsOff[s] in srcTs, start time srcT0[s], spacing srcDt[s].
+ */
+int oracle_step(int O, int R, int rm, long nEl, double t, double dt, const double *stiffT,
+                const double *stiffV, const double *fluxL, const double *fluxN,
+                const double *fluxT, const double *starE, const double *starA,
+                const double *srcA, const double *omega, const double *fsE, const double *fsA,
+                const int *elFaEl, const unsigned char *fIdElFaEl,
+                const unsigned char *vIdElFaEl, const unsigned char *faType, double *dofsE,
+                double *dofsA, double *tDofs,
+                /* receivers */ int nRe, const long *recvEl, const double *recvBasis,
+                double *recvTime, double period, int maxBuf, double *recvBuf,
+                double *recvBufTime, int *recvCount,
+                /* sources */ int nSrc, const long *srcEl, const int *srcRun,
+                const double *srcScal, const double *srcBEval, const double *srcT0,
+                const double *srcDt, const long *srcTsOff, const long *srcNPts,
+                const double *srcTs, double tolTime) {
+  const int B = nmodes(O);
+  const size_t szE = (size_t)9 * B * R, szM = (size_t)6 * B * R;
+  double *der = malloc((size_t)O * szE * sizeof(double));
+  double *tIntA = rm ? malloc((size_t)rm * szM * sizeof(double)) : NULL;
+  double *pred = malloc(szE * sizeof(double));
+  double *upA = rm ? malloc(szM * sizeof(double)) : NULL;
+  int re = 0;
+  /* step 0: local */
+  for (long el = 0; el < nEl; el++) {
+    double *dE = dofsE + el * szE, *dA = rm ? dofsA + el * rm * szM : NULL;
+    double *tD = tDofs + el * szE;
+    oracle_ck(O, R, rm, dt, stiffT, starE + el * 72, rm ? starA + el * 27 : NULL,
+              rm ? srcA + el * 12 * rm : NULL, omega, dE, dA, der, tD, tIntA);
+    while (re < nRe && recvEl[re] < el) re++;
+    if (re < nRe && recvEl[re] == el) {
+      for (;;) {
+        double tr = recvTime[re];
+        if (!(tr > t - tolTime && tr < t + dt - tolTime)) break;
+        oracle_eval_pred(O, R, fabs(tr - t), der, pred);
+        for (int r2 = re; r2 < nRe && recvEl[r2] == el; r2++) {
+          if (recvCount[r2] >= maxBuf) { free(der); free(tIntA); free(pred); free(upA); return -1; }
+          double *buf = recvBuf + ((size_t)r2 * maxBuf + recvCount[r2]) * 9 * R;
+          for (int q = 0; q < 9; q++) {
+            for (int r = 0; r < R; r++) buf[q * R + r] = 0;
+            for (int md = 0; md < B; md++)
+              for (int r = 0; r < R; r++)
+                buf[q * R + r] += recvBasis[(size_t)r2 * B + md] * pred[((size_t)q * B + md) * R + r];
+          }
+          recvBufTime[(size_t)r2 * maxBuf + recvCount[r2]] = recvTime[r2];
+          recvTime[r2] += period;
+          recvCount[r2]++;
+        }
+      }
+    }
+    oracle_volint(O, R, rm, stiffV, starE + el * 72, rm ? starA + el * 27 : NULL,
+                  rm ? srcA + el * 12 * rm : NULL, omega, tD, tIntA, dE, dA);
+    oracle_surf_local(O, R, rm, fluxL, fluxT, fsE + el * 4 * 81,
+                      rm ? fsA + el * 4 * 54 : NULL, omega, tD, dE, dA);
+  }
+  /* step 1: point sources */
+  for (int s = 0; s < nSrc; s++) {
+    double in = oracle_series_int(srcDt[s], srcT0[s], srcNPts[s], srcTs + srcTsOff[s], t, t + dt,
+                                  0.0, tolTime);
+    double *dE = dofsE + srcEl[s] * szE;
+    for (int q = 0; q < 9; q++) {
+      double sc = in * srcScal[(size_t)s * 9 + q];
+      for (int md = 0; md < B; md++)
+        dE[((size_t)q * B + md) * R + srcRun[s]] += sc * srcBEval[(size_t)s * B + md];
+    }
+  }
+  /* step 2: neighbour */
+  const double *fsE1 = fsE + (size_t)nEl * 4 * 81;
+  const double *fsA1 = rm ? fsA + (size_t)nEl * 4 * 54 : NULL;
+  for (long el = 0; el < nEl; el++) {
+    if (rm) memset(upA, 0, szM * sizeof(double));
+    for (int f = 0; f < 4; f++) {
+      int ty = faType[el * 4 + f];
+      if (ty == FT_OUTFLOW) continue;
+      long ne = ty == FT_FREE ? el : elFaEl[el * 4 + f];
+      int vId = ty == FT_FREE ? -1 : vIdElFaEl[el * 4 + f];
+      int fId = ty == FT_FREE ? -1 : fIdElFaEl[el * 4 + f];
+      oracle_surf_neigh(O, R, rm, f, vId, fId, fluxL, fluxN, fluxT, fsE1 + (el * 4 + f) * 81,
+                        rm ? fsA1 + (el * 4 + f) * 54 : NULL, tDofs + ne * szE,
+                        dofsE + el * szE, upA);
+    }
+    if (rm) scatter_upA(B, R, rm, omega, upA, dofsA + el * rm * szM);
+  }
+  free(der);
+  free(tIntA);
+  free(pred);
+  free(upA);
+  return 0;
+}

@@ -1,0 +1,127 @@
+"""ctypes bindings of the CPU oracle (test infrastructure only).
+
+Only ``tests/``, ``__graft_entry__.smoke()`` and the CPU-baseline leg of ``bench.py`` import this
+module, and only to check or time against it. It loads ``oracle/liboracle.so`` (built from
+``oracle.c`` by ``oracle/Makefile``).
+"""
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_LIB = None
+
+_dp = np.ctypeslib.ndpointer(dtype=np.float64, flags="C_CONTIGUOUS")
+
+
+def _opt(a, dtype):
+    if a is None:
+        return None
+    a = np.ascontiguousarray(a, dtype=dtype)
+    return a
+
+
+def _ptr(a):
+    return None if a is None else a.ctypes.data_as(C.c_void_p)
+
+
+def lib():
+    global _LIB
+    if _LIB is None:
+        path = os.path.join(_HERE, "liboracle.so")
+        src = os.path.join(_HERE, "oracle.c")
+        if not os.path.exists(path) or os.path.getmtime(path) < os.path.getmtime(src):
+            subprocess.check_call(["make", "-s", "-C", _HERE, "liboracle.so"])
+        _LIB = C.CDLL(path)
+        _LIB.oracle_step.restype = C.c_int
+        _LIB.oracle_series_int.restype = C.c_double
+        _LIB.oracle_series_int.argtypes = [C.c_double, C.c_double, C.c_long, C.c_void_p, C.c_double,
+                                           C.c_double, C.c_double, C.c_double]
+    return _LIB
+
+
+def nmodes(o):
+    return o * (o + 1) * (o + 2) // 6 if o > 0 else 0
+
+
+def ck(O, R, rm, dt, stiffT, starE, dofsE, starA=None, srcA=None, omega=None, dofsA=None):
+    B = nmodes(O)
+    der = np.zeros((O, 9, B, R))
+    tE = np.zeros((9, B, R))
+    tA = np.zeros((max(rm, 1), 6, B, R))
+    a = [_opt(x, np.float64) for x in (stiffT, starE, starA, srcA, omega, dofsE, dofsA)]
+    lib().oracle_ck(C.c_int(O), C.c_int(R), C.c_int(rm), C.c_double(dt), *[_ptr(x) for x in a],
+                    _ptr(der), _ptr(tE), _ptr(tA))
+    return der, tE, tA[:rm]
+
+
+def eval_pred(O, R, tau, der):
+    B = nmodes(O)
+    pred = np.zeros((9, B, R))
+    der = _opt(der, np.float64)
+    lib().oracle_eval_pred(C.c_int(O), C.c_int(R), C.c_double(tau), _ptr(der), _ptr(pred))
+    return pred
+
+
+def volint(O, R, rm, stiffV, starE, tE, dofsE, starA=None, srcA=None, omega=None, tA=None, dofsA=None):
+    dofsE = np.array(dofsE, dtype=np.float64, order="C")
+    dofsA = None if dofsA is None else np.array(dofsA, dtype=np.float64, order="C")
+    a = [_opt(x, np.float64) for x in (stiffV, starE, starA, srcA, omega, tE, tA)]
+    lib().oracle_volint(C.c_int(O), C.c_int(R), C.c_int(rm), *[_ptr(x) for x in a], _ptr(dofsE),
+                        _ptr(dofsA))
+    return dofsE, dofsA
+
+
+def surf_local(O, R, rm, fluxL, fluxT, fsE4, tE, dofsE, fsA4=None, omega=None, dofsA=None):
+    dofsE = np.array(dofsE, dtype=np.float64, order="C")
+    dofsA = None if dofsA is None else np.array(dofsA, dtype=np.float64, order="C")
+    a = [_opt(x, np.float64) for x in (fluxL, fluxT, fsE4, fsA4, omega, tE)]
+    lib().oracle_surf_local(C.c_int(O), C.c_int(R), C.c_int(rm), *[_ptr(x) for x in a],
+                            _ptr(dofsE), _ptr(dofsA))
+    return dofsE, dofsA
+
+
+def surf_neigh(O, R, rm, fa, vId, fId, fluxL, fluxN, fluxT, fsE, tNe, dofsE, fsA=None, upA=None):
+    dofsE = np.array(dofsE, dtype=np.float64, order="C")
+    B = nmodes(O)
+    upA = np.zeros((6, B, R)) if upA is None else np.array(upA, dtype=np.float64, order="C")
+    a = [_opt(x, np.float64) for x in (fluxL, fluxN, fluxT, fsE, fsA, tNe)]
+    lib().oracle_surf_neigh(C.c_int(O), C.c_int(R), C.c_int(rm), C.c_int(fa), C.c_int(vId),
+                            C.c_int(fId), *[_ptr(x) for x in a], _ptr(dofsE), _ptr(upA))
+    return dofsE, upA
+
+
+def series_int(dx, x0, vals, x1, x2, na=0.0, tol=1e-9):
+    vals = _opt(vals, np.float64)
+    return lib().oracle_series_int(dx, x0, len(vals), _ptr(vals), x1, x2, na, tol)
+
+
+def step(prob, state, t, dt, recv=None, src=None, tol_time=1e-9):
+    """One GTS step of the oracle. ``prob`` is a dict of the element data (see oracle.c),
+    ``state`` holds dofsE/dofsA/tDofs (updated in place), ``recv``/``src`` the optional
+    receiver and source tables (updated in place where the C code writes)."""
+    O, R, rm = prob["order"], prob["runs"], prob["rm"]
+    nEl = prob["nEl"]
+    L = lib()
+    f64 = lambda k: _ptr(prob[k]) if prob.get(k) is not None else None
+    if recv is None:
+        recv = dict(n=0, el=None, basis=None, time=None, period=1.0, maxbuf=0, buf=None,
+                    buftime=None, count=None)
+    if src is None:
+        src = dict(n=0)
+    rc = L.oracle_step(
+        C.c_int(O), C.c_int(R), C.c_int(rm), C.c_long(nEl), C.c_double(t), C.c_double(dt),
+        f64("stiffT"), f64("stiffV"), f64("fluxL"), f64("fluxN"), f64("fluxT"), f64("starE"),
+        f64("starA"), f64("srcA"), f64("omega"), f64("fsE"), f64("fsA"), _ptr(prob["elFaEl"]),
+        _ptr(prob["fIdElFaEl"]), _ptr(prob["vIdElFaEl"]), _ptr(prob["faType"]),
+        _ptr(state["dofsE"]), _ptr(state.get("dofsA")), _ptr(state["tDofs"]),
+        C.c_int(recv["n"]), _ptr(recv["el"]), _ptr(recv["basis"]), _ptr(recv["time"]),
+        C.c_double(recv["period"]), C.c_int(recv["maxbuf"]), _ptr(recv["buf"]),
+        _ptr(recv["buftime"]), _ptr(recv["count"]),
+        C.c_int(src.get("n", 0)), _ptr(src.get("el")), _ptr(src.get("run")), _ptr(src.get("scal")),
+        _ptr(src.get("bEval")), _ptr(src.get("t0")), _ptr(src.get("dt")), _ptr(src.get("tsOff")),
+        _ptr(src.get("nPts")), _ptr(src.get("ts")), C.c_double(tol_time))
+    if rc != 0:
+        raise RuntimeError("oracle_step failed (receiver buffer full?)")
