@@ -1,0 +1,87 @@
+"""Builds ``edge_b200/libedge_b200.so`` in-tree with nvcc for sm_100a.
+
+The library holds the host setup (host.cpp), the CUDA kernels and the C ABI declared in
+``include/edge_b200.h``. Objects are compiled in parallel into ``edge_b200/_build`` and relinked only
+when a source or header changed.
+
+Usage: python -m edge_b200.build [-j N] [--force]
+"""
+import argparse
+import concurrent.futures as cf
+import glob
+import os
+import shutil
+import subprocess
+import sys
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(HERE)
+CSRC = os.path.join(HERE, "csrc")
+BUILD = os.path.join(HERE, "_build")
+LIB = os.path.join(HERE, "libedge_b200.so")
+
+ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+NVCC_FLAGS = ARCH + ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-Xcompiler", "-O2",
+                     "--expt-relaxed-constexpr", "-I" + os.path.join(ROOT, "include"), "-I" + CSRC]
+
+
+def nvcc():
+    for c in (os.environ.get("NVCC"), "/usr/local/cuda/bin/nvcc", shutil.which("nvcc")):
+        if c and os.path.exists(c):
+            return c
+    raise RuntimeError("nvcc not found")
+
+
+def _deps_mtime():
+    hdrs = glob.glob(os.path.join(CSRC, "**", "*.h"), recursive=True)
+    hdrs += glob.glob(os.path.join(CSRC, "**", "*.cuh"), recursive=True)
+    hdrs += glob.glob(os.path.join(CSRC, "**", "*.inc"), recursive=True)
+    hdrs += [os.path.join(ROOT, "include", "edge_b200.h")]
+    return max(os.path.getmtime(h) for h in hdrs)
+
+
+def sources():
+    return sorted(glob.glob(os.path.join(CSRC, "*.cu")) + glob.glob(os.path.join(CSRC, "*.cpp")))
+
+
+def _compile(src, force, hdr_mtime):
+    obj = os.path.join(BUILD, os.path.basename(src) + ".o")
+    if (not force and os.path.exists(obj) and os.path.getmtime(obj) >= os.path.getmtime(src)
+            and os.path.getmtime(obj) >= hdr_mtime):
+        return obj, False
+    cmd = [nvcc()] + NVCC_FLAGS + ["-c", src, "-o", obj]
+    if src.endswith(".cpp"):
+        cmd = [nvcc(), "-x", "cu"] + NVCC_FLAGS + ["-c", src, "-o", obj]
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    if r.returncode != 0:
+        raise RuntimeError(f"nvcc failed for {src}:\n{r.stdout}\n{r.stderr}")
+    return obj, True
+
+
+def build(force=False, jobs=None, verbose=False):
+    os.makedirs(BUILD, exist_ok=True)
+    hdr = _deps_mtime()
+    srcs = sources()
+    jobs = jobs or min(len(srcs), os.cpu_count() or 4)
+    changed = False
+    objs = []
+    with cf.ThreadPoolExecutor(jobs) as ex:
+        for obj, ch in ex.map(lambda s: _compile(s, force, hdr), srcs):
+            objs.append(obj)
+            changed |= ch
+    if changed or force or not os.path.exists(LIB) or os.path.getmtime(LIB) < max(os.path.getmtime(o) for o in objs):
+        cmd = [nvcc()] + ARCH + ["-shared", "-o", LIB] + objs + ["-lcudart", "-lcuda"]
+        r = subprocess.run(cmd, capture_output=True, text=True)
+        if r.returncode != 0:
+            raise RuntimeError(f"link failed:\n{r.stdout}\n{r.stderr}")
+        if verbose:
+            print("linked", LIB)
+    return LIB
+
+
+if __name__ == "__main__":
+    ap = argparse.ArgumentParser()
+    ap.add_argument("-j", type=int, default=None)
+    ap.add_argument("--force", action="store_true")
+    a = ap.parse_args()
+    print(build(force=a.force, jobs=a.j, verbose=True))

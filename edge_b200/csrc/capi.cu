@@ -1,0 +1,442 @@
+// C ABI of the device element update (include/edge_b200.h): context, uploads, the GTS step loop.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <new>
+#include <string>
+#include <vector>
+
+#include "../../include/edge_b200.h"
+#include "kernel_set.h"
+#include "kernels.cuh"
+
+namespace edge_b200 {
+KernelSet *makeKernelSet_o2(int, int, int, int);
+KernelSet *makeKernelSet_o3(int, int, int, int);
+KernelSet *makeKernelSet_o4(int, int, int, int);
+KernelSet *makeKernelSet_o5(int, int, int, int);
+KernelSet *makeKernelSet_o6(int, int, int, int);
+
+KernelSet *makeKernelSet(int precision, int order, int runs, int rms) {
+  switch (order) {
+    case 2: return makeKernelSet_o2(precision, order, runs, rms);
+    case 3: return makeKernelSet_o3(precision, order, runs, rms);
+    case 4: return makeKernelSet_o4(precision, order, runs, rms);
+    case 5: return makeKernelSet_o5(precision, order, runs, rms);
+    case 6: return makeKernelSet_o6(precision, order, runs, rms);
+    default: return nullptr;
+  }
+}
+}  // namespace edge_b200
+
+using namespace edge_b200;
+
+namespace {
+constexpr double kTolTime = 1e-9;  // TOL.TIME of the FP64 build (src/constants.hpp:289-309)
+
+template <typename P>
+void dfree(P *&p) {
+  if (p) cudaFree((void *)p);
+  p = nullptr;
+}
+}  // namespace
+
+struct edge_b200_ctx {
+  edge_b200_cfg cfg{};
+  int64_t nEl = 0;
+  int B = 0, F = 0;
+  size_t realSize = 8;
+  cudaStream_t stream = nullptr;
+  KernelSet *ks = nullptr;
+  // resident device data
+  void *dofsE = nullptr, *dofsA = nullptr, *tDofs = nullptr, *face = nullptr;
+  double *starE = nullptr, *starA = nullptr, *srcA = nullptr, *fsE = nullptr, *fsA = nullptr;
+  int32_t *elFaEl = nullptr;
+  uint8_t *fId = nullptr, *vId = nullptr, *faType = nullptr;
+  double omega[3] = {0, 0, 0};
+  bool meshSet = false, dataSet = false;
+  // sources
+  SrcArgs src{};
+  void *srcMem[10] = {};
+  // receivers
+  int nRecv = 0, nRecvGrp = 0, maxBuf = 0;
+  double recvTime = 0, period = 0;
+  int32_t recvCount = 0;
+  int64_t *dGrpEl = nullptr;
+  int32_t *dGrpOff = nullptr;
+  double *dBasis = nullptr, *dBuf = nullptr, *dBufTime = nullptr;
+  std::vector<double> hBufTime;
+  double *dTau = nullptr;
+  int32_t *dSlot = nullptr;
+  size_t tauCap = 0;
+  int64_t launches = 0;
+  std::string err;
+
+  size_t dofsCount() const { return (size_t)nEl * 9 * B * cfg.n_runs; }
+  size_t dofsACount() const { return (size_t)nEl * cfg.n_rms * 6 * B * cfg.n_runs; }
+  size_t faceCount() const { return (size_t)nEl * 4 * 9 * F * cfg.n_runs; }
+
+  int fail(cudaError_t e, const char *what) {
+    err = std::string(what) + ": " + cudaGetErrorString(e);
+    return EDGE_B200_EDEVICE;
+  }
+  StepArgsRaw args(double dt) const {
+    StepArgsRaw a;
+    a.dofsE = dofsE;
+    a.dofsA = dofsA;
+    a.tDofs = tDofs;
+    a.face = face;
+    a.starE = starE;
+    a.starA = starA;
+    a.srcA = srcA;
+    a.fsE = fsE;
+    a.fsA = fsA;
+    a.elFaEl = elFaEl;
+    a.fId = fId;
+    a.vId = vId;
+    a.faType = faType;
+    a.nEl = nEl;
+    a.dt = dt;
+    for (int i = 0; i < 3; i++) a.omega[i] = omega[i];
+    return a;
+  }
+  ~edge_b200_ctx() {
+    dfree(dofsE); dfree(dofsA); dfree(tDofs); dfree(face);
+    dfree(starE); dfree(starA); dfree(srcA); dfree(fsE); dfree(fsA);
+    dfree(elFaEl); dfree(fId); dfree(vId); dfree(faType);
+    for (auto &p : srcMem) dfree(p);
+    dfree(dGrpEl); dfree(dGrpOff); dfree(dBasis); dfree(dBuf); dfree(dTau); dfree(dSlot);
+    delete ks;
+  }
+};
+
+#define EDGE_CUDA(call, what)                 \
+  do {                                        \
+    cudaError_t e_ = (call);                  \
+    if (e_ != cudaSuccess) return ctx->fail(e_, what); \
+  } while (0)
+
+template <typename P>
+static cudaError_t upload(P *&dst, const void *src, size_t bytes, cudaStream_t s) {
+  cudaError_t e;
+  if (!dst && (e = cudaMalloc((void **)&dst, bytes ? bytes : 1))) return e;
+  if (bytes && (e = cudaMemcpyAsync((void *)dst, src, bytes, cudaMemcpyHostToDevice, s))) return e;
+  return cudaSuccess;
+}
+
+extern "C" {
+
+int edge_b200_create(const edge_b200_cfg *cfg, int64_t n_el, edge_b200_ctx **out) {
+  if (!cfg || !out || n_el < 1) return EDGE_B200_EINVAL;
+  if (cfg->precision != 32 && cfg->precision != 64) return EDGE_B200_EINVAL;
+  if (cfg->n_rms < 0 || cfg->n_rms > 3 || cfg->n_runs < 1 || 32 % cfg->n_runs) return EDGE_B200_EINVAL;
+  KernelSet *ks = makeKernelSet(cfg->precision, cfg->order, cfg->n_runs, cfg->n_rms);
+  if (!ks) return EDGE_B200_ENOTSUP;
+  edge_b200_ctx *ctx = new (std::nothrow) edge_b200_ctx();
+  if (!ctx) {
+    delete ks;
+    return EDGE_B200_ENOMEM;
+  }
+  ctx->cfg = *cfg;
+  ctx->ks = ks;
+  ctx->nEl = n_el;
+  ctx->B = nModes(cfg->order);
+  ctx->F = nFaceModes(cfg->order);
+  ctx->realSize = cfg->precision == 64 ? 8 : 4;
+  ctx->stream = (cudaStream_t)cfg->stream;
+  cudaError_t e;
+  if ((e = cudaSetDevice(cfg->device)) != cudaSuccess || (e = ks->init(cfg->device)) != cudaSuccess) {
+    delete ctx;
+    return EDGE_B200_EDEVICE;
+  }
+  size_t rs = ctx->realSize;
+  if ((e = cudaMalloc(&ctx->dofsE, ctx->dofsCount() * rs)) ||
+      (cfg->n_rms && (e = cudaMalloc(&ctx->dofsA, ctx->dofsACount() * rs))) ||
+      (e = cudaMalloc(&ctx->tDofs, ctx->dofsCount() * rs)) ||
+      (e = cudaMalloc(&ctx->face, ctx->faceCount() * rs))) {
+    delete ctx;
+    return e == cudaErrorMemoryAllocation ? EDGE_B200_ENOMEM : EDGE_B200_EDEVICE;
+  }
+  cudaMemsetAsync(ctx->dofsE, 0, ctx->dofsCount() * rs, ctx->stream);
+  if (cfg->n_rms) cudaMemsetAsync(ctx->dofsA, 0, ctx->dofsACount() * rs, ctx->stream);
+  cudaMemsetAsync(ctx->face, 0, ctx->faceCount() * rs, ctx->stream);
+  *out = ctx;
+  return EDGE_B200_OK;
+}
+
+int edge_b200_destroy(edge_b200_ctx *ctx) {
+  if (!ctx) return EDGE_B200_EINVAL;
+  cudaStreamSynchronize(ctx->stream);
+  delete ctx;
+  return EDGE_B200_OK;
+}
+
+int edge_b200_upload_mesh(edge_b200_ctx *ctx, const int32_t *el_fa_el, const uint8_t *fid_el_fa_el,
+                          const uint8_t *vid_el_fa_el, const uint8_t *el_fa_type) {
+  if (!ctx || !el_fa_el || !fid_el_fa_el || !vid_el_fa_el || !el_fa_type) return EDGE_B200_EINVAL;
+  const int64_t n = ctx->nEl * 4;
+  for (int64_t i = 0; i < n; i++) {
+    const int ty = el_fa_type[i];
+    if (ty > EDGE_FACE_OUTFLOW) return EDGE_B200_EINVAL;
+    if (ty == EDGE_FACE_INNER &&
+        (el_fa_el[i] < 0 || el_fa_el[i] >= ctx->nEl || fid_el_fa_el[i] > 3 || vid_el_fa_el[i] > 2))
+      return EDGE_B200_EMESH;
+  }
+  cudaStream_t s = ctx->stream;
+  EDGE_CUDA(upload(ctx->elFaEl, el_fa_el, n * sizeof(int32_t), s), "upload elFaEl");
+  EDGE_CUDA(upload(ctx->fId, fid_el_fa_el, n, s), "upload fId");
+  EDGE_CUDA(upload(ctx->vId, vid_el_fa_el, n, s), "upload vId");
+  EDGE_CUDA(upload(ctx->faType, el_fa_type, n, s), "upload faType");
+  EDGE_CUDA(cudaStreamSynchronize(s), "upload mesh");
+  ctx->meshSet = true;
+  return EDGE_B200_OK;
+}
+
+int edge_b200_upload_element_data(edge_b200_ctx *ctx, const double *star_e, const double *fs_e,
+                                  const double *star_a, const double *src_a, const double *fs_a,
+                                  const double *omega) {
+  if (!ctx || !star_e || !fs_e) return EDGE_B200_EINVAL;
+  const int rm = ctx->cfg.n_rms;
+  if (rm && (!star_a || !src_a || !fs_a || !omega)) return EDGE_B200_EINVAL;
+  cudaStream_t s = ctx->stream;
+  const size_t n = ctx->nEl;
+  EDGE_CUDA(upload(ctx->starE, star_e, n * 72 * sizeof(double), s), "upload starE");
+  EDGE_CUDA(upload(ctx->fsE, fs_e, n * 2 * 4 * 81 * sizeof(double), s), "upload fsE");
+  if (rm) {
+    EDGE_CUDA(upload(ctx->starA, star_a, n * 27 * sizeof(double), s), "upload starA");
+    EDGE_CUDA(upload(ctx->srcA, src_a, n * rm * 12 * sizeof(double), s), "upload srcA");
+    EDGE_CUDA(upload(ctx->fsA, fs_a, n * 2 * 4 * 54 * sizeof(double), s), "upload fsA");
+    for (int m = 0; m < rm; m++) ctx->omega[m] = omega[m];
+  }
+  EDGE_CUDA(cudaStreamSynchronize(s), "upload element data");
+  ctx->dataSet = true;
+  return EDGE_B200_OK;
+}
+
+int edge_b200_upload_dofs(edge_b200_ctx *ctx, const void *dofs_e, const void *dofs_a) {
+  if (!ctx || !dofs_e || (ctx->cfg.n_rms && !dofs_a)) return EDGE_B200_EINVAL;
+  EDGE_CUDA(cudaMemcpyAsync(ctx->dofsE, dofs_e, ctx->dofsCount() * ctx->realSize, cudaMemcpyHostToDevice,
+                            ctx->stream), "upload dofsE");
+  if (ctx->cfg.n_rms)
+    EDGE_CUDA(cudaMemcpyAsync(ctx->dofsA, dofs_a, ctx->dofsACount() * ctx->realSize, cudaMemcpyHostToDevice,
+                              ctx->stream), "upload dofsA");
+  return EDGE_B200_OK;
+}
+
+int edge_b200_download_dofs(edge_b200_ctx *ctx, void *dofs_e, void *dofs_a) {
+  if (!ctx || !dofs_e) return EDGE_B200_EINVAL;
+  EDGE_CUDA(cudaMemcpyAsync(dofs_e, ctx->dofsE, ctx->dofsCount() * ctx->realSize, cudaMemcpyDeviceToHost,
+                            ctx->stream), "download dofsE");
+  if (ctx->cfg.n_rms && dofs_a)
+    EDGE_CUDA(cudaMemcpyAsync(dofs_a, ctx->dofsA, ctx->dofsACount() * ctx->realSize, cudaMemcpyDeviceToHost,
+                              ctx->stream), "download dofsA");
+  EDGE_CUDA(cudaStreamSynchronize(ctx->stream), "download dofs");
+  return EDGE_B200_OK;
+}
+
+int edge_b200_download_tdofs(edge_b200_ctx *ctx, void *tdofs) {
+  if (!ctx || !tdofs) return EDGE_B200_EINVAL;
+  EDGE_CUDA(cudaMemcpyAsync(tdofs, ctx->tDofs, ctx->dofsCount() * ctx->realSize, cudaMemcpyDeviceToHost,
+                            ctx->stream), "download tDofs");
+  EDGE_CUDA(cudaStreamSynchronize(ctx->stream), "download tDofs");
+  return EDGE_B200_OK;
+}
+
+int edge_b200_set_sources(edge_b200_ctx *ctx, int n, const int64_t *el, const int32_t *run,
+                          const double *scal, const double *b_eval, const double *t0,
+                          const double *dt, const int64_t *ts_off, const int64_t *n_pts,
+                          int64_t n_ts, const double *ts) {
+  if (!ctx || n < 0) return EDGE_B200_EINVAL;
+  for (auto &p : ctx->srcMem) dfree(p);
+  ctx->src = SrcArgs{};
+  if (n == 0) return EDGE_B200_OK;
+  if (!el || !run || !scal || !b_eval || !t0 || !dt || !ts_off || !n_pts || !ts) return EDGE_B200_EINVAL;
+  std::vector<int32_t> off{0};
+  for (int i = 0; i < n; i++) {
+    if (el[i] < 0 || el[i] >= ctx->nEl || run[i] < 0 || run[i] >= ctx->cfg.n_runs || n_pts[i] < 1 ||
+        ts_off[i] < 0 || ts_off[i] + n_pts[i] > n_ts || !(dt[i] > 0))
+      return EDGE_B200_EINVAL;
+    if (i > 0 && (el[i] < el[i - 1] || (el[i] == el[i - 1] && run[i] < run[i - 1]))) return EDGE_B200_EINVAL;
+    if (i > 0 && (el[i] != el[i - 1] || run[i] != run[i - 1])) off.push_back(i);
+  }
+  off.push_back(n);
+  cudaStream_t s = ctx->stream;
+  const int B = ctx->B;
+  int32_t *dOff = nullptr;
+  int64_t *dEl = nullptr, *dTsOff = nullptr, *dNPts = nullptr;
+  int32_t *dRun = nullptr;
+  double *dScal = nullptr, *dBEval = nullptr, *dT0 = nullptr, *dDt = nullptr, *dTs = nullptr;
+  EDGE_CUDA(upload(dOff, off.data(), off.size() * sizeof(int32_t), s), "sources");
+  EDGE_CUDA(upload(dEl, el, n * sizeof(int64_t), s), "sources");
+  EDGE_CUDA(upload(dRun, run, n * sizeof(int32_t), s), "sources");
+  EDGE_CUDA(upload(dScal, scal, n * 9 * sizeof(double), s), "sources");
+  EDGE_CUDA(upload(dBEval, b_eval, (size_t)n * B * sizeof(double), s), "sources");
+  EDGE_CUDA(upload(dT0, t0, n * sizeof(double), s), "sources");
+  EDGE_CUDA(upload(dDt, dt, n * sizeof(double), s), "sources");
+  EDGE_CUDA(upload(dTsOff, ts_off, n * sizeof(int64_t), s), "sources");
+  EDGE_CUDA(upload(dNPts, n_pts, n * sizeof(int64_t), s), "sources");
+  EDGE_CUDA(upload(dTs, ts, n_ts * sizeof(double), s), "sources");
+  void *mem[] = {dOff, dEl, dRun, dScal, dBEval, dT0, dDt, dTsOff, dNPts, dTs};
+  for (int i = 0; i < 10; i++) ctx->srcMem[i] = mem[i];
+  ctx->src.nGrp = (int)off.size() - 1;
+  ctx->src.grpOff = dOff;
+  ctx->src.el = dEl;
+  ctx->src.run = dRun;
+  ctx->src.scal = dScal;
+  ctx->src.bEval = dBEval;
+  ctx->src.t0 = dT0;
+  ctx->src.dts = dDt;
+  ctx->src.tsOff = dTsOff;
+  ctx->src.nPts = dNPts;
+  ctx->src.ts = dTs;
+  ctx->src.tol = kTolTime;
+  EDGE_CUDA(cudaStreamSynchronize(s), "sources");
+  return EDGE_B200_OK;
+}
+
+int edge_b200_set_receivers(edge_b200_ctx *ctx, int n, const int64_t *el, const double *basis,
+                            double t_first, double period, int max_buf) {
+  if (!ctx || n < 0) return EDGE_B200_EINVAL;
+  dfree(ctx->dGrpEl); dfree(ctx->dGrpOff); dfree(ctx->dBasis); dfree(ctx->dBuf);
+  ctx->nRecv = ctx->nRecvGrp = 0;
+  if (n == 0) return EDGE_B200_OK;
+  if (!el || !basis || !(period > 0) || max_buf < 1) return EDGE_B200_EINVAL;
+  std::vector<int64_t> gEl;
+  std::vector<int32_t> gOff;
+  for (int i = 0; i < n; i++) {
+    if (el[i] < 0 || el[i] >= ctx->nEl || (i > 0 && el[i] < el[i - 1])) return EDGE_B200_EINVAL;
+    if (i == 0 || el[i] != el[i - 1]) {
+      gEl.push_back(el[i]);
+      gOff.push_back(i);
+    }
+  }
+  gOff.push_back(n);
+  cudaStream_t s = ctx->stream;
+  EDGE_CUDA(upload(ctx->dGrpEl, gEl.data(), gEl.size() * sizeof(int64_t), s), "receivers");
+  EDGE_CUDA(upload(ctx->dGrpOff, gOff.data(), gOff.size() * sizeof(int32_t), s), "receivers");
+  EDGE_CUDA(upload(ctx->dBasis, basis, (size_t)n * ctx->B * sizeof(double), s), "receivers");
+  const size_t bufCount = (size_t)n * max_buf * 9 * ctx->cfg.n_runs;
+  EDGE_CUDA(cudaMalloc(&ctx->dBuf, bufCount * sizeof(double)), "receivers");
+  EDGE_CUDA(cudaMemsetAsync(ctx->dBuf, 0, bufCount * sizeof(double), s), "receivers");
+  EDGE_CUDA(cudaStreamSynchronize(s), "receivers");
+  ctx->nRecv = n;
+  ctx->nRecvGrp = (int)gEl.size();
+  ctx->maxBuf = max_buf;
+  ctx->recvTime = t_first;
+  ctx->period = period;
+  ctx->recvCount = 0;
+  ctx->hBufTime.assign(max_buf, 0.0);
+  return EDGE_B200_OK;
+}
+
+int edge_b200_step(edge_b200_ctx *ctx, double t, double dt, int n_steps) {
+  if (!ctx || !(dt > 0) || n_steps < 0) return EDGE_B200_EINVAL;
+  if (!ctx->meshSet || !ctx->dataSet) return EDGE_B200_EINVAL;
+  cudaStream_t s = ctx->stream;
+  // receiver samples of every step (Receivers::getRecvTimeRel, io/Receivers.cpp:235-248)
+  std::vector<int> stepFirst(n_steps + 1, 0);
+  std::vector<double> tau;
+  std::vector<int32_t> slot;
+  {
+    double ts = t;
+    for (int st = 0; st < n_steps; st++) {
+      stepFirst[st] = (int)tau.size();
+      if (ctx->nRecv) {
+        while (ctx->recvTime > ts - kTolTime && ctx->recvTime < ts + dt - kTolTime) {
+          if (ctx->recvCount >= ctx->maxBuf) return EDGE_B200_EOVERFLOW;
+          tau.push_back(std::abs(ctx->recvTime - ts));
+          slot.push_back(ctx->recvCount);
+          ctx->hBufTime[ctx->recvCount] = ctx->recvTime;
+          ctx->recvCount++;
+          ctx->recvTime += ctx->period;
+        }
+      }
+      ts += dt;
+    }
+    stepFirst[n_steps] = (int)tau.size();
+  }
+  if (!tau.empty()) {
+    if (tau.size() > ctx->tauCap) {
+      dfree(ctx->dTau);
+      dfree(ctx->dSlot);
+      ctx->tauCap = std::max(tau.size(), (size_t)1024);
+      EDGE_CUDA(cudaMalloc(&ctx->dTau, ctx->tauCap * sizeof(double)), "receiver schedule");
+      EDGE_CUDA(cudaMalloc(&ctx->dSlot, ctx->tauCap * sizeof(int32_t)), "receiver schedule");
+    }
+    EDGE_CUDA(cudaMemcpyAsync(ctx->dTau, tau.data(), tau.size() * sizeof(double), cudaMemcpyHostToDevice, s),
+              "receiver schedule");
+    EDGE_CUDA(cudaMemcpyAsync(ctx->dSlot, slot.data(), slot.size() * sizeof(int32_t), cudaMemcpyHostToDevice, s),
+              "receiver schedule");
+  }
+  ctx->launches = 0;
+  StepArgsRaw a = ctx->args(dt);
+  double ts = t;
+  for (int st = 0; st < n_steps; st++) {
+    const int ns = stepFirst[st + 1] - stepFirst[st];
+    if (ns > 0 && ctx->nRecvGrp > 0) {
+      RecvArgs r;
+      r.grpEl = ctx->dGrpEl;
+      r.grpOff = ctx->dGrpOff;
+      r.basis = ctx->dBasis;
+      r.tau = ctx->dTau + stepFirst[st];
+      r.slot = ctx->dSlot + stepFirst[st];
+      r.nSamples = ns;
+      r.nGrp = ctx->nRecvGrp;
+      r.maxBuf = ctx->maxBuf;
+      r.buf = ctx->dBuf;
+      EDGE_CUDA(ctx->ks->recv(a, r, s), "receiver kernel");
+      ctx->launches++;
+    }
+    EDGE_CUDA(ctx->ks->local(a, s), "local kernel");
+    ctx->launches++;
+    if (ctx->src.nGrp > 0) {
+      SrcArgs sa = ctx->src;
+      sa.t = ts;
+      sa.dt = dt;
+      EDGE_CUDA(ctx->ks->sources(ctx->dofsE, sa, s), "source kernel");
+      ctx->launches++;
+    }
+    EDGE_CUDA(ctx->ks->neigh(a, s), "neighbour kernel");
+    ctx->launches++;
+    ts += dt;
+  }
+  return EDGE_B200_OK;
+}
+
+int edge_b200_read_receivers(edge_b200_ctx *ctx, double *buf, double *buf_time, int32_t *counts) {
+  if (!ctx) return EDGE_B200_EINVAL;
+  if (ctx->nRecv == 0) return EDGE_B200_OK;
+  const size_t bufCount = (size_t)ctx->nRecv * ctx->maxBuf * 9 * ctx->cfg.n_runs;
+  if (buf)
+    EDGE_CUDA(cudaMemcpyAsync(buf, ctx->dBuf, bufCount * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream),
+              "read receivers");
+  EDGE_CUDA(cudaStreamSynchronize(ctx->stream), "read receivers");
+  for (int i = 0; i < ctx->nRecv; i++) {
+    if (counts) counts[i] = ctx->recvCount;
+    if (buf_time)
+      for (int j = 0; j < ctx->maxBuf; j++) buf_time[(size_t)i * ctx->maxBuf + j] = j < ctx->recvCount ? ctx->hBufTime[j] : 0.0;
+  }
+  return EDGE_B200_OK;
+}
+
+int edge_b200_sync(edge_b200_ctx *ctx) {
+  if (!ctx) return EDGE_B200_EINVAL;
+  EDGE_CUDA(cudaStreamSynchronize(ctx->stream), "sync");
+  return EDGE_B200_OK;
+}
+
+int edge_b200_device_dofs(edge_b200_ctx *ctx, void **dofs_e, void **dofs_a, void **tdofs) {
+  if (!ctx) return EDGE_B200_EINVAL;
+  if (dofs_e) *dofs_e = ctx->dofsE;
+  if (dofs_a) *dofs_a = ctx->dofsA;
+  if (tdofs) *tdofs = ctx->tDofs;
+  return EDGE_B200_OK;
+}
+
+int64_t edge_b200_last_launches(const edge_b200_ctx *ctx) { return ctx ? ctx->launches : -1; }
+
+const char *edge_b200_last_error(const edge_b200_ctx *ctx) { return ctx ? ctx->err.c_str() : "null context"; }
+
+}  // extern "C"

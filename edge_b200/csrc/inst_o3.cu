@@ -1,0 +1,9 @@
+// Compiled configurations of order 3 (precision, fused runs, relaxation mechanisms).
+#include "kernel_impl.cuh"
+
+namespace edge_b200 {
+KernelSet *makeKernelSet_o3(int precision, int order, int runs, int rms) {
+#include "inst_o3.inc"
+  return nullptr;
+}
+}  // namespace edge_b200

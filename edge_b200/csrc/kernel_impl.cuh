@@ -1,0 +1,90 @@
+// KernelSet implementation for one configuration; included by the inst_*.cu translation units.
+#pragma once
+#include "kernel_set.h"
+#include "kernels.cuh"
+
+namespace edge_b200 {
+
+template <typename T, int O, int R, int RM>
+class KernelSetImpl final : public KernelSet {
+  using G = Geo<T, O, R, RM>;
+  int numSms_ = 0, occLocal_ = 1, occNeigh_ = 1, occRecv_ = 1;
+
+  static StepArgs<T> cast(const StepArgsRaw &a) {
+    StepArgs<T> b;
+    b.dofsE = static_cast<T *>(a.dofsE);
+    b.dofsA = static_cast<T *>(a.dofsA);
+    b.tDofs = static_cast<T *>(a.tDofs);
+    b.face = static_cast<T *>(a.face);
+    b.starE = a.starE;
+    b.starA = a.starA;
+    b.srcA = a.srcA;
+    b.fsE = a.fsE;
+    b.fsA = a.fsA;
+    b.elFaEl = a.elFaEl;
+    b.fId = a.fId;
+    b.vId = a.vId;
+    b.faType = a.faType;
+    b.nEl = a.nEl;
+    b.dt = a.dt;
+    for (int i = 0; i < 3; i++) b.omega[i] = a.omega[i];
+    return b;
+  }
+  static constexpr size_t smemLocal() { return G::smemBytes; }
+  static constexpr size_t smemNeigh() { return G::smemS0 * sizeof(T); }
+  static constexpr size_t smemRecv() { return (G::smemX + G::smemXA) * sizeof(T); }
+
+ public:
+  cudaError_t init(int device) override {
+    cudaError_t e;
+    if ((e = cudaDeviceGetAttribute(&numSms_, cudaDevAttrMultiProcessorCount, device))) return e;
+    if ((e = cudaFuncSetAttribute(kLocal<T, O, R, RM>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smemLocal())))
+      return e;
+    if ((e = cudaFuncSetAttribute(kNeigh<T, O, R, RM>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smemNeigh())))
+      return e;
+    if ((e = cudaFuncSetAttribute(kRecv<T, O, R, RM>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smemRecv())))
+      return e;
+    if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occLocal_, kLocal<T, O, R, RM>, G::NT, smemLocal())))
+      return e;
+    if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occNeigh_, kNeigh<T, O, R, RM>, G::NT, smemNeigh())))
+      return e;
+    occLocal_ = occLocal_ < 1 ? 1 : occLocal_;
+    occNeigh_ = occNeigh_ < 1 ? 1 : occNeigh_;
+    return cudaSuccess;
+  }
+  int elementsPerCta() const override { return G::E; }
+  int ctasLocal() const override { return numSms_ * occLocal_; }
+  int ctasNeigh() const override { return numSms_ * occNeigh_; }
+
+  static int grid(int64_t nEl, int cap) {
+    int64_t groups = (nEl + G::E - 1) / G::E;
+    return (int)(groups < cap ? (groups < 1 ? 1 : groups) : cap);
+  }
+
+  cudaError_t local(const StepArgsRaw &a, cudaStream_t s) override {
+    kLocal<T, O, R, RM><<<grid(a.nEl, ctasLocal()), G::NT, smemLocal(), s>>>(cast(a));
+    return cudaGetLastError();
+  }
+  cudaError_t neigh(const StepArgsRaw &a, cudaStream_t s) override {
+    kNeigh<T, O, R, RM><<<grid(a.nEl, ctasNeigh()), G::NT, smemNeigh(), s>>>(cast(a));
+    return cudaGetLastError();
+  }
+  cudaError_t recv(const StepArgsRaw &a, const RecvArgs &r, cudaStream_t s) override {
+    const int g = (r.nGrp + G::E - 1) / G::E;
+    if (g == 0) return cudaSuccess;
+    kRecv<T, O, R, RM><<<g, G::NT, smemRecv(), s>>>(cast(a), r);
+    return cudaGetLastError();
+  }
+  cudaError_t sources(void *dofsE, const SrcArgs &sa, cudaStream_t s) override {
+    if (sa.nGrp == 0) return cudaSuccess;
+    kSources<T, O, R><<<sa.nGrp, 128, 0, s>>>(static_cast<T *>(dofsE), sa);
+    return cudaGetLastError();
+  }
+};
+
+}  // namespace edge_b200
+
+// registry of one translation unit: a function returning the matching configuration
+#define EDGE_B200_CFG(T, O, R, RM, prec)                                    \
+  if (precision == prec && order == O && runs == R && rms == RM)           \
+    return new edge_b200::KernelSetImpl<T, O, R, RM>();

@@ -1,0 +1,317 @@
+"""Python mirror of the host setup API (mesh, material, element data, sources, receivers).
+
+Each function wraps the C ABI of ``libedge_b200.so`` (include/edge_b200.h); the semantics are
+EDGE's setup (src/impl/seismic/setup.inc) restated in C++ in ``csrc/host.cpp``.
+"""
+import ctypes as C
+from dataclasses import dataclass, field
+from typing import Optional
+
+import numpy as np
+
+from ._lib import check, lib, ptr
+
+FACE_INNER, FACE_FREE_SURFACE, FACE_OUTFLOW = 0, 1, 2
+
+
+def n_modes(order):
+    return order * (order + 1) * (order + 2) // 6
+
+
+def n_face_modes(order):
+    return order * (order + 1) // 2
+
+
+class Mesh:
+    """Tet mesh with EDGE-V's conventions (see edge_mesh_box in include/edge_b200.h)."""
+
+    def __init__(self, handle):
+        self._h = handle
+        nve, nfa, nel = C.c_int64(), C.c_int64(), C.c_int64()
+        check(lib().edge_mesh_sizes(handle, C.byref(nve), C.byref(nfa), C.byref(nel)), "edge_mesh_sizes")
+        self.n_ve, self.n_fa, self.n_el = nve.value, nfa.value, nel.value
+        ne, nf = self.n_el, self.n_fa
+        self.ve = np.zeros((self.n_ve, 3))
+        self.el_ve = np.zeros((ne, 4), np.int64)
+        self.el_fa = np.zeros((ne, 4), np.int64)
+        self.fa_el = np.zeros((nf, 2), np.int64)
+        self.fa_normal = np.zeros((nf, 3))
+        self.fa_tangent = np.zeros((nf, 2, 3))
+        self.fa_area = np.zeros(nf)
+        self.fa_type = np.zeros(nf, np.uint8)
+        self.el_vol = np.zeros(ne)
+        self.el_india = np.zeros(ne)
+        self.el_fa_el = np.zeros((ne, 4), np.int32)
+        self.fid = np.zeros((ne, 4), np.uint8)
+        self.vid = np.zeros((ne, 4), np.uint8)
+        self.el_fa_type = np.zeros((ne, 4), np.uint8)
+        check(lib().edge_mesh_arrays(handle, *[ptr(a) for a in (
+            self.ve, self.el_ve, self.el_fa, self.fa_el, self.fa_normal, self.fa_tangent,
+            self.fa_area, self.fa_type, self.el_vol, self.el_india, self.el_fa_el, self.fid,
+            self.vid, self.el_fa_type)]), "edge_mesh_arrays")
+
+    @classmethod
+    def box(cls, n, ext=(1e4, 1e4, 1e4), jitter=0.0, seed=0, bc_top=FACE_FREE_SURFACE,
+            bc_sides=FACE_OUTFLOW):
+        nx, ny, nz = (n, n, n) if np.isscalar(n) else n
+        h = C.c_void_p()
+        e = np.asarray(ext, dtype=np.float64)
+        check(lib().edge_mesh_box(nx, ny, nz, ptr(e), float(jitter), int(seed), bc_top, bc_sides,
+                                  C.byref(h)), "edge_mesh_box")
+        m = cls(h)
+        m.ext = tuple(float(x) for x in ext)
+        m.n_cubes = (nx, ny, nz)
+        return m
+
+    def __del__(self):
+        if getattr(self, "_h", None):
+            lib().edge_mesh_free(self._h)
+            self._h = None
+
+    def el_ve_crds(self):
+        return self.ve[self.el_ve]  # [nEl][4][3]
+
+    def centroids(self):
+        return self.el_ve_crds().mean(axis=1)
+
+
+def star(mesh, rho, lam, mu):
+    out = np.zeros((mesh.n_el, 3, 24))
+    a = [np.ascontiguousarray(x, np.float64) for x in (rho, lam, mu)]
+    check(lib().edge_setup_star(mesh._h, *[ptr(x) for x in a], ptr(out)), "edge_setup_star")
+    return out
+
+
+def star_anelastic(mesh):
+    out = np.zeros((mesh.n_el, 3, 9))
+    check(lib().edge_setup_star_anelastic(mesh._h, ptr(out)), "edge_setup_star_anelastic")
+    return out
+
+
+def flux_solvers(mesh, rho, lam, mu, n_rms=0):
+    fsE = np.zeros((2, mesh.n_el, 4, 81))
+    fsA = np.zeros((2, mesh.n_el, 4, 54)) if n_rms else None
+    a = [np.ascontiguousarray(x, np.float64) for x in (rho, lam, mu)]
+    check(lib().edge_setup_flux_solvers(mesh._h, n_rms, *[ptr(x) for x in a], ptr(fsE), ptr(fsA)),
+          "edge_setup_flux_solvers")
+    return fsE, fsA
+
+
+def frequencies(n_rms, freq_cen, freq_rat):
+    out = np.zeros(2 * n_rms - 1)
+    check(lib().edge_setup_frequencies(n_rms, freq_cen, freq_rat, ptr(out)), "edge_setup_frequencies")
+    return out
+
+
+def anelastic_coeffs(n_rms, quality, freqs):
+    out = np.zeros(n_rms)
+    f = np.ascontiguousarray(freqs, np.float64)
+    check(lib().edge_setup_anelastic_coeffs(n_rms, quality, ptr(f), ptr(out)), "anelastic_coeffs")
+    return out
+
+
+def elastic_lame(n_rms, freq_ref, freqs, ck, cm, lam_phase, mu_phase):
+    le, me = C.c_double(), C.c_double()
+    a = [np.ascontiguousarray(x, np.float64) for x in (freqs, ck, cm)]
+    check(lib().edge_setup_elastic_lame(n_rms, freq_ref, *[ptr(x) for x in a], lam_phase, mu_phase,
+                                        C.byref(le), C.byref(me)), "elastic_lame")
+    return le.value, me.value
+
+
+def attenuation(n_rms, freq_cen, freq_rat, qp, qs, lam, mu):
+    """Returns (srcA[nEl][rm][12], omega[rm], lam_unrelaxed, mu_unrelaxed)."""
+    lam = np.array(lam, np.float64)
+    mu = np.array(mu, np.float64)
+    n = len(lam)
+    src = np.zeros((n, n_rms, 12))
+    om = np.zeros(n_rms)
+    qp = np.ascontiguousarray(qp, np.float64)
+    qs = np.ascontiguousarray(qs, np.float64)
+    check(lib().edge_setup_attenuation(n_rms, freq_cen, freq_rat, n, ptr(qp), ptr(qs), ptr(lam),
+                                       ptr(mu), ptr(src), ptr(om)), "edge_setup_attenuation")
+    return src, om, lam, mu
+
+
+def dt_cfl(mesh, order, rho, lam, mu):
+    out = C.c_double()
+    a = [np.ascontiguousarray(x, np.float64) for x in (rho, lam, mu)]
+    check(lib().edge_setup_dt_cfl(mesh._h, order, *[ptr(x) for x in a], C.byref(out)), "dt_cfl")
+    return out.value
+
+
+def locate(mesh, order, xyz, source=False):
+    xyz = np.ascontiguousarray(np.atleast_2d(xyz), np.float64)
+    n = xyz.shape[0]
+    el = np.zeros(n, np.int64)
+    ref = np.zeros((n, 3))
+    basis = np.zeros((n, n_modes(order)))
+    check(lib().edge_setup_locate(mesh._h, order, n, ptr(xyz), ptr(el), ptr(ref), ptr(basis),
+                                  1 if source else 0), "edge_setup_locate")
+    return el, ref, basis
+
+
+def eval_basis(order, ref):
+    out = np.zeros(n_modes(order))
+    r = np.ascontiguousarray(ref, np.float64)
+    check(lib().edge_setup_eval_basis(order, ptr(r), ptr(out)), "eval_basis")
+    return out
+
+
+def trafo(n, s, t):
+    T, Ti = np.zeros((9, 9)), np.zeros((9, 9))
+    a = [np.ascontiguousarray(x, np.float64) for x in (n, s, t)]
+    check(lib().edge_setup_trafo(*[ptr(x) for x in a], ptr(T), ptr(Ti)), "trafo")
+    return T, Ti
+
+
+def fs_pair(rho_l, rho_r, lam_l, lam_r, mu_l, mu_r, n, s, t, free_surface=False):
+    el, er, al, ar = np.zeros((9, 9)), np.zeros((9, 9)), np.zeros((6, 9)), np.zeros((6, 9))
+    a = [np.ascontiguousarray(x, np.float64) for x in (n, s, t)]
+    check(lib().edge_setup_fs_pair(rho_l, rho_r, lam_l, lam_r, mu_l, mu_r, *[ptr(x) for x in a],
+                                   1 if free_surface else 0, ptr(el), ptr(er), ptr(al), ptr(ar)),
+          "fs_pair")
+    return el, er, al, ar
+
+
+def ricker(t, f0, t0):
+    a = (np.pi * f0 * (t - t0)) ** 2
+    return (1.0 - 2.0 * a) * np.exp(-a)
+
+
+@dataclass
+class Problem:
+    """A complete setup of the element update: mesh, element data, sources, receivers, DOFs."""
+    order: int
+    runs: int
+    rm: int
+    mesh: Mesh
+    rho: np.ndarray
+    lam: np.ndarray
+    mu: np.ndarray
+    starE: np.ndarray
+    fsE: np.ndarray
+    dt: float
+    starA: Optional[np.ndarray] = None
+    srcA: Optional[np.ndarray] = None
+    fsA: Optional[np.ndarray] = None
+    omega: Optional[np.ndarray] = None
+    sources: dict = field(default_factory=dict)
+    receivers: dict = field(default_factory=dict)
+    name: str = ""
+
+    @property
+    def n_el(self):
+        return self.mesh.n_el
+
+    @property
+    def B(self):
+        return n_modes(self.order)
+
+    def zero_dofs(self, dtype=np.float64):
+        e = np.zeros((self.n_el, 9, self.B, self.runs), dtype)
+        a = np.zeros((self.n_el, self.rm, 6, self.B, self.runs), dtype) if self.rm else None
+        return e, a
+
+    def oracle_dict(self):
+        """Element data in the oracle's layout (tests only)."""
+        from . import dgmat
+        m = dgmat.matrices(self.order)
+        d = dict(order=self.order, runs=self.runs, rm=self.rm, nEl=self.n_el,
+                 stiffT=m["stiffT"], stiffV=m["stiffV"], fluxL=m["fluxL"], fluxN=m["fluxN"],
+                 fluxT=m["fluxT"], starE=self.starE, fsE=self.fsE, starA=self.starA,
+                 srcA=self.srcA, fsA=self.fsA, omega=self.omega,
+                 elFaEl=np.ascontiguousarray(self.mesh.el_fa_el),
+                 fIdElFaEl=np.ascontiguousarray(self.mesh.fid),
+                 vIdElFaEl=np.ascontiguousarray(self.mesh.vid),
+                 faType=np.ascontiguousarray(self.mesh.el_fa_type))
+        return {k: (np.ascontiguousarray(v) if isinstance(v, np.ndarray) else v) for k, v in d.items()}
+
+
+def make_sources(mesh, order, runs, positions, scalings, f0, t_onset, dt_series, n_series):
+    """Point sources: run r gets the point positions[r] with Voigt moment tensor scalings[r][9]
+    and a Ricker moment-rate series of peak frequency f0 delayed by t_onset, sampled every
+    dt_series (PointSources.hpp:525-768 reads the same quantities from HDF5)."""
+    positions = np.atleast_2d(positions)
+    el, ref, bEval = locate(mesh, order, positions, source=True)
+    ts_t = np.arange(n_series) * dt_series
+    series = ricker(ts_t, f0, t_onset)
+    recs = sorted(range(len(positions)), key=lambda s: (el[s], s % runs))
+    src = dict(n=len(positions), el=np.array([el[s] for s in recs], np.int64),
+               run=np.array([s % runs for s in recs], np.int32),
+               scal=np.ascontiguousarray([scalings[s] for s in recs], np.float64),
+               bEval=np.ascontiguousarray([bEval[s] for s in recs], np.float64),
+               t0=np.zeros(len(positions)), dt=np.full(len(positions), dt_series),
+               tsOff=np.arange(len(positions), dtype=np.int64) * n_series,
+               nPts=np.full(len(positions), n_series, np.int64),
+               ts=np.ascontiguousarray(np.tile(series, len(positions))))
+    return src
+
+
+def make_receivers(mesh, order, positions, period, t_end, t_first=0.0):
+    el, ref, basis = locate(mesh, order, positions, source=False)
+    order_idx = np.argsort(el, kind="stable")
+    maxbuf = int(np.ceil((t_end - t_first) / period)) + 2
+    return dict(n=len(positions), el=np.ascontiguousarray(el[order_idx]),
+                basis=np.ascontiguousarray(basis[order_idx]), period=float(period),
+                t_first=float(t_first), maxbuf=maxbuf, perm=order_idx,
+                positions=np.asarray(positions)[order_idx])
+
+
+def build_problem(n_cubes, order, runs, rm=0, ext=1e4, jitter=0.0, seed=3343, vp=6000.0,
+                  vs=3464.0, rho=2670.0, layers=None, lognormal_sigma=0.0, q_range=None,
+                  freq_cen=1.0, freq_rat=100.0, n_receivers=8, source="explosive", f0=2.0,
+                  n_steps=200, period=None, cfl=1.0, bc_top=FACE_FREE_SURFACE,
+                  bc_sides=FACE_OUTFLOW, name=""):
+    """Synthetic setups of the element update (box meshes, homogeneous or layered materials)."""
+    rng = np.random.default_rng(seed)
+    mesh = Mesh.box(n_cubes, (ext, ext, ext), jitter=jitter, seed=seed, bc_top=bc_top, bc_sides=bc_sides)
+    ne = mesh.n_el
+    if layers is None:
+        vpe = np.full(ne, vp)
+    else:
+        z = mesh.centroids()[:, 2]
+        bounds = np.linspace(0, ext, len(layers) + 1)
+        idx = np.clip(np.searchsorted(bounds, z, side="right") - 1, 0, len(layers) - 1)
+        # layers are listed top (free surface, z = ext) to bottom
+        vpe = np.asarray(layers, np.float64)[::-1][idx]
+    if lognormal_sigma > 0:
+        vpe = vpe * rng.lognormal(0.0, lognormal_sigma, ne)
+    vse = vpe / np.sqrt(3.0) if layers is not None else np.full(ne, vs) * (vpe / vp)
+    rhoe = np.full(ne, rho)
+    mu = rhoe * vse ** 2
+    lam = rhoe * vpe ** 2 - 2 * mu
+    srcA = omega = starA = fsA = None
+    if rm:
+        lo, hi = q_range if q_range else (50.0, 200.0)
+        qp = rng.uniform(lo, hi, ne)
+        qs = rng.uniform(lo, hi, ne)
+        srcA, omega, lam, mu = attenuation(rm, freq_cen, freq_rat, qp, qs, lam, mu)
+        starA = star_anelastic(mesh)
+    starE = star(mesh, rhoe, lam, mu)
+    fsE, fsA = flux_solvers(mesh, rhoe, lam, mu, rm)
+    dt = dt_cfl(mesh, order, rhoe, lam, mu) * cfl
+    t_end = n_steps * dt
+    # sources
+    if source == "explosive":
+        M0 = 1e15
+        pos = np.array([[ext / 2, ext / 2, ext / 2]] * runs)
+        scal = np.array([[M0, M0, M0, 0, 0, 0, 0, 0, 0]] * runs, np.float64)
+    elif source == "random":
+        pos = rng.uniform(0.1 * ext, 0.9 * ext, (runs, 3))
+        mt = rng.normal(0.0, 1.0, (runs, 6)) * 1e15
+        scal = np.concatenate([mt, np.zeros((runs, 3))], axis=1)
+    else:
+        pos, scal = None, None
+    src = {}
+    if pos is not None:
+        dts = dt / 10.0
+        n_series = int(np.ceil(t_end / dts)) + 4
+        src = make_sources(mesh, order, runs, pos, scal, f0, 1.2 / f0, dts, n_series)
+    rec = {}
+    if n_receivers:
+        rpos = rng.uniform(0.1 * ext, 0.9 * ext, (n_receivers, 3))
+        per = period if period else dt * 0.37
+        rec = make_receivers(mesh, order, rpos, per, t_end)
+    return Problem(order=order, runs=runs, rm=rm, mesh=mesh, rho=rhoe, lam=lam, mu=mu, starE=starE,
+                   fsE=fsE, dt=dt, starA=starA, srcA=srcA, fsA=fsA, omega=omega, sources=src,
+                   receivers=rec, name=name)

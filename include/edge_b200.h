@@ -1,0 +1,175 @@
+/*
+ * edge_b200: B200-native (sm_100a) tet4 ADER-DG elastic / viscoelastic element update behind a
+ * plain C ABI, plus the host-side setup that keeps EDGE's semantics.
+ *
+ * All functions return 0 on success or a negative edge_b200_status. Arrays are row-major, runs are
+ * the fastest dimension of every DOF array: dofsE[nEl][9][B][R], dofsA[nEl][rm][6][B][R], with
+ * B = O(O+1)(O+2)/6 element modes and F = O(O+1)/2 face modes for order O.
+ * Stress order is xx, yy, zz, xy, yz, xz, followed by the velocities u, v, w.
+ *
+ * The reference has no FFI for this path: its element update is the C++ template class
+ * AderDg<real, nRms, TET4, O, O, nCfr, sparse> (src/impl/seismic/solvers/AderDg.hpp), constructed in
+ * src/impl/seismic/setup.inc:265-290 and driven by src/impl/seismic/steps.inc:24-77. Each entry
+ * point below names the reference interface it replaces.
+ */
+#ifndef EDGE_B200_H
+#define EDGE_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum {
+  EDGE_B200_OK = 0,
+  EDGE_B200_EINVAL = -1,     /* invalid argument */
+  EDGE_B200_ENOMEM = -2,     /* allocation failed (host or device) */
+  EDGE_B200_EDEVICE = -3,    /* CUDA error */
+  EDGE_B200_ETIMEOUT = -4,   /* a bounded device wait gave up */
+  EDGE_B200_ENOTSUP = -5,    /* configuration not compiled in (order / runs / mechanisms) */
+  EDGE_B200_EMESH = -6,      /* inconsistent or degenerate mesh */
+  EDGE_B200_ENOTFOUND = -7,  /* point not inside the mesh */
+  EDGE_B200_EOVERFLOW = -8   /* receiver buffer full */
+} edge_b200_status;
+
+/* per element-face boundary types (t_spTypeElastic, src/impl/seismic/const.inc:143-149) */
+enum { EDGE_FACE_INNER = 0, EDGE_FACE_FREE_SURFACE = 1, EDGE_FACE_OUTFLOW = 2 };
+
+/* ============================== host setup (EDGE semantics) ================================== */
+
+typedef struct edge_mesh edge_mesh;
+
+/* Box [0,ext]^3 of nx*ny*nz cubes, each split into 6 congruent tets along its main diagonal;
+ * interior vertices jittered by seeded uniform +-jitter*h per coordinate (tets with detJ <= 0 are
+ * redrawn). The top face (z = ext[2]) gets bc_top, all other boundary faces bc_sides
+ * (EDGE_FACE_FREE_SURFACE or EDGE_FACE_OUTFLOW). Vertex / face / neighbour conventions follow
+ * EDGE-V: tools/edge_v/src/mesh/Mesh.cpp:288-375 (sorting), geom/Tet4.cpp:80-112 (orientation),
+ * geom/Tet4.cpp:114-229 and geom/Generic.cpp:92-116 (neighbour vertex / face ids),
+ * mesh/Mesh.cpp:763-841 with geom/Tria3.cpp:48-120 (normals, tangents). */
+int edge_mesh_box(int nx, int ny, int nz, const double ext[3], double jitter, uint64_t seed,
+                  int bc_top, int bc_sides, edge_mesh **out);
+int edge_mesh_sizes(const edge_mesh *m, int64_t *n_ve, int64_t *n_fa, int64_t *n_el);
+/* Any output pointer may be NULL. Shapes: ve[nVe][3], el_ve[nEl][4], el_fa[nEl][4],
+ * fa_el[nFa][2] (-1 = none), fa_normal[nFa][3], fa_tangent[nFa][2][3], fa_area[nFa],
+ * fa_type[nFa], el_vol[nEl], el_india[nEl], el_fa_el[nEl][4] (-1 = none),
+ * fid_el_fa_el / vid_el_fa_el / el_fa_type [nEl][4]. Replaces mesh::EdgeV getters
+ * (src/mesh/EdgeV.h:166-395). */
+int edge_mesh_arrays(const edge_mesh *m, double *ve, int64_t *el_ve, int64_t *el_fa,
+                     int64_t *fa_el, double *fa_normal, double *fa_tangent, double *fa_area,
+                     uint8_t *fa_type, double *el_vol, double *el_india, int32_t *el_fa_el,
+                     uint8_t *fid_el_fa_el, uint8_t *vid_el_fa_el, uint8_t *el_fa_type);
+void edge_mesh_free(edge_mesh *m);
+
+/* Elastic star matrices starE[nEl][3][24] (AderDgInit::initStar, AderDgInit.hpp:129-174 with
+ * Elasticity::star, Elasticity.cpp:167-301). lam/mu must already be the unrelaxed values when
+ * attenuation is on (AderDgInit::initSrcA, AderDgInit.hpp:91-117). */
+int edge_setup_star(const edge_mesh *m, const double *rho, const double *lam, const double *mu,
+                    double *star_e);
+/* Anelastic star matrices starA[nEl][3][9] (ViscoElasticity::star, ViscoElasticity.cpp:233-316). */
+int edge_setup_star_anelastic(const edge_mesh *m, double *star_a);
+/* Flux solvers fsE[2][nEl][4][81] and, if n_rms > 0, fsA[2][nEl][4][54]
+ * (AderDgInit::initFs / setUpFs, AderDgInit.hpp:288-665). */
+int edge_setup_flux_solvers(const edge_mesh *m, int n_rms, const double *rho, const double *lam,
+                            const double *mu, double *fs_e, double *fs_a);
+/* Relaxation frequencies, 2n-1 values (ViscoElasticity::frequencies, ViscoElasticity.h:168-183). */
+int edge_setup_frequencies(int n_rms, double freq_cen, double freq_rat, double *freqs);
+/* Per element: anelastic source matrices srcA[nEl][rm][12]; lam/mu are overwritten by the
+ * unrelaxed Lame parameters (AderDgInit::initSrcA, ViscoElasticity::src,
+ * ViscoElasticity.h:379-508 and ViscoElasticity.cpp:30-176). omega[rm] = freqs[2m]
+ * (AderDg.hpp:248-258). */
+int edge_setup_attenuation(int n_rms, double freq_cen, double freq_rat, int64_t n_el,
+                           const double *qp, const double *qs, double *lam, double *mu,
+                           double *src_a, double *omega);
+/* Least-squares anelastic coefficients of one wave type (ViscoElasticity::anelasticCoeffPs). */
+int edge_setup_anelastic_coeffs(int n_rms, double quality, const double *freqs, double *coeffs);
+/* Unrelaxed Lame parameters (ViscoElasticity::elasticLame). */
+int edge_setup_elastic_lame(int n_rms, double freq_ref, const double *freqs,
+                            const double *coeffs_kappa, const double *coeffs_mu, double lam_phase,
+                            double mu_phase, double *lam_el, double *mu_el);
+/* CFL time step: min over elements of 0.5 * inDia / vp / (2O-1) (common.hpp:84-133). */
+int edge_setup_dt_cfl(const edge_mesh *m, int order, const double *rho, const double *lam,
+                      const double *mu, double *dt_min);
+/* Locates n points; per point the element, reference coordinates and basis values
+ * basis[n][B]. scale_mass_jac != 0 multiplies by M^-1 and divides by detJ as point sources do
+ * (PointSources::initBasisEvals, PointSources.hpp:388-509); 0 gives plain basis values as
+ * receivers use (io/Receivers.cpp:33-180). */
+int edge_setup_locate(const edge_mesh *m, int order, int n, const double *xyz, int64_t *el,
+                      double *ref, double *basis, int scale_mass_jac);
+/* Basis of the given order evaluated at reference coordinates (dg::Basis::evalBasis). */
+int edge_setup_eval_basis(int order, const double ref[3], double *vals);
+/* Face-aligned <-> xyz transforms of the 9 quantities (common::setupTrafo3d / setupTrafoInv3d,
+ * src/impl/seismic/common.hpp:314-343) and the Godunov middle states (Elasticity::fs 3D,
+ * Elasticity.cpp:372-441; ViscoElasticity::fs 3D). Exposed for parity tests. */
+int edge_setup_trafo(const double n[3], const double s[3], const double t[3], double *t_mat,
+                     double *t_inv);
+int edge_setup_fs_pair(double rho_l, double rho_r, double lam_l, double lam_r, double mu_l,
+                       double mu_r, const double n[3], const double s[3], const double t[3],
+                       int free_surface, double *fs_el, double *fs_er, double *fs_al,
+                       double *fs_ar);
+
+/* ================================ device element update ======================================= */
+
+typedef struct edge_b200_ctx edge_b200_ctx;
+
+typedef struct {
+  int order;     /* O: 2..6 */
+  int n_runs;    /* R fused forward runs: 1, 2, 4, 8, 16 */
+  int n_rms;     /* relaxation mechanisms: 0..3 */
+  int precision; /* 64: plain FP64 path; 32: FP32 fused-run path (element data kept in FP64 on host) */
+  void *stream;  /* cudaStream_t; NULL = the legacy default stream */
+  int device;    /* CUDA device ordinal */
+} edge_b200_cfg;
+
+/* Creates the device context for n_el elements (replaces the AderDg constructor,
+ * AderDg.hpp:225-312, and the DOF allocations of data::Internal::initDense, Internal.hpp:559-568). */
+int edge_b200_create(const edge_b200_cfg *cfg, int64_t n_el, edge_b200_ctx **out);
+int edge_b200_destroy(edge_b200_ctx *ctx);
+/* Connectivity per element face (the elFaEl / fIdElFaEl / vIdElFaEl / faChars arguments of
+ * AderDg::neigh, AderDg.hpp:553-567). el_fa_el = -1 where there is no neighbour. */
+int edge_b200_upload_mesh(edge_b200_ctx *ctx, const int32_t *el_fa_el, const uint8_t *fid_el_fa_el,
+                          const uint8_t *vid_el_fa_el, const uint8_t *el_fa_type);
+/* FP64 element data: starE[nEl][3][24], fsE[2][nEl][4][81]; with mechanisms also
+ * starA[nEl][3][9], srcA[nEl][rm][12], fsA[2][nEl][4][54], omega[rm] (the m_starE / m_fsE /
+ * m_starA / m_srcA / m_fsA members the AderDg constructor builds). */
+int edge_b200_upload_element_data(edge_b200_ctx *ctx, const double *star_e, const double *fs_e,
+                                  const double *star_a, const double *src_a, const double *fs_a,
+                                  const double *omega);
+/* DOFs in the context precision (double for 64, float for 32); dofs_a may be NULL without
+ * mechanisms. */
+int edge_b200_upload_dofs(edge_b200_ctx *ctx, const void *dofs_e, const void *dofs_a);
+int edge_b200_download_dofs(edge_b200_ctx *ctx, void *dofs_e, void *dofs_a);
+/* Time-integrated DOFs tDofs[nEl][9][B][R] of the last local step (the tDofs[0] of steps.inc). */
+int edge_b200_download_tdofs(edge_b200_ctx *ctx, void *tdofs);
+/* Point sources sorted by (element, run); source s adds
+ *   int_t^{t+dt} series_s * scal[s][q] * b_eval[s][md]  to run run[s] of element el[s]
+ * (PointSources::apply, PointSources.hpp:887-931, with Series<1>::integrate, Series.hpp:59-134).
+ * Series s: n_pts[s] samples at ts[ts_off[s]...], start t0[s], spacing dt[s]. */
+int edge_b200_set_sources(edge_b200_ctx *ctx, int n, const int64_t *el, const int32_t *run,
+                          const double *scal, const double *b_eval, const double *t0,
+                          const double *dt, const int64_t *ts_off, const int64_t *n_pts,
+                          int64_t n_ts, const double *ts);
+/* Receivers grouped by element (el ascending; equal elements adjacent), basis[n][B] plain basis
+ * values, first output time t_first and sampling period (Receivers::init / getRecvTimeRel /
+ * writeRecvAll, io/Receivers.cpp:33-290). Up to max_buf samples are buffered per receiver. */
+int edge_b200_set_receivers(edge_b200_ctx *ctx, int n, const int64_t *el, const double *basis,
+                            double t_first, double period, int max_buf);
+/* n_steps GTS steps from time t with step dt: local -> sources -> neighbour
+ * (TimeGroupStatic::computeStep, src/time/TimeGroupStatic.cpp:113-127, steps.inc:24-77). */
+int edge_b200_step(edge_b200_ctx *ctx, double t, double dt, int n_steps);
+/* Receiver samples buf[n][max_buf][9][R] (FP64), their times buf_time[n][max_buf], counts[n]. */
+int edge_b200_read_receivers(edge_b200_ctx *ctx, double *buf, double *buf_time, int32_t *counts);
+/* Waits for all work of the context's stream. */
+int edge_b200_sync(edge_b200_ctx *ctx);
+/* Device pointers of the resident DOF arrays (for callers that keep data on the device). */
+int edge_b200_device_dofs(edge_b200_ctx *ctx, void **dofs_e, void **dofs_a, void **tdofs);
+/* Kernel launches issued by the last edge_b200_step call. */
+int64_t edge_b200_last_launches(const edge_b200_ctx *ctx);
+/* Last CUDA error string of the context (static storage). */
+const char *edge_b200_last_error(const edge_b200_ctx *ctx);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,59 @@
+"""ctypes bindings of the reference's own kernels compiled into oracle/_ref (test infrastructure).
+
+``load(order, runs, rm)`` returns the library for one configuration, building it from the reference
+checkout with ``oracle/ref.mk`` when it is missing and the checkout is present; ``None`` otherwise.
+"""
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+REF = os.environ.get("EDGE_REFERENCE", "/root/reference")
+_cache = {}
+
+
+def path(order, runs, rm):
+    return os.path.join(HERE, "_ref", f"libedgeref_O{order}_R{runs}_M{rm}.so")
+
+
+def load(order=4, runs=1, rm=0):
+    key = (order, runs, rm)
+    if key in _cache:
+        return _cache[key]
+    p = path(*key)
+    if not os.path.exists(p) and os.path.isdir(os.path.join(REF, "src")):
+        subprocess.run(["make", "-s", "-C", HERE, "-f", "ref.mk", f"CFGS={order}_{runs}_{rm}"],
+                       check=False, capture_output=True)
+    if not os.path.exists(p):
+        _cache[key] = None
+        return None
+    L = C.CDLL(p)
+    vp = C.c_void_p
+    L.ref_step_phase.argtypes = [C.c_int, C.c_long, C.c_double] + [vp] * 13
+    L.ref_series_int.restype = C.c_double
+    L.ref_series_int.argtypes = [C.c_double, C.c_double, C.c_long, vp, C.c_double, C.c_double]
+    L.ref_star.argtypes = [C.c_double] * 3 + [vp, vp]
+    L.ref_trafo.argtypes = [vp] * 5
+    L.ref_fs.argtypes = [C.c_double] * 6 + [vp] * 3 + [C.c_int, vp, vp]
+    L.ref_frequencies.argtypes = [C.c_int, C.c_double, C.c_double, vp]
+    _cache[key] = L
+    return L
+
+
+def _p(a):
+    return None if a is None else C.c_void_p(a.ctypes.data)
+
+
+def step(L, prob, state, t, dt, src_apply=None):
+    """One GTS step with the reference kernels: local, then src_apply(state) (sources), then neigh."""
+    args = [prob["starE"], prob.get("starA"), prob.get("srcA"), prob.get("omega"), prob["fsE"],
+            prob.get("fsA"), prob["elFaEl"], prob["fIdElFaEl"], prob["vIdElFaEl"], prob["faType"],
+            state["dofsE"], state.get("dofsA"), state["tDofs"]]
+    rc = L.ref_step_phase(0, prob["nEl"], dt, *[_p(a) for a in args])
+    assert rc == 0
+    if src_apply is not None:
+        src_apply(state)
+    rc = L.ref_step_phase(1, prob["nEl"], dt, *[_p(a) for a in args])
+    assert rc == 0
