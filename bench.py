@@ -1,0 +1,384 @@
+"""Benchmark of the tet4 ADER-DG element update on B200.
+
+One step = one GTS time step (local -> sources -> neighbour, with receiver sampling) over the whole
+mesh and all fused runs. Default workload (the headline configuration): a 10 km box of 48^3 cubes
+x 6 tets (663,552 tets), ORDER 5 (35 modes), 16 fused runs in FP32, homogeneous material
+(vp 6000, vs 3464, rho 2670), one seeded random point source per run (moment tensor N(0,1) x 1e15,
+1.5 Hz Ricker), 8 receivers, free surface on top and outflow elsewhere. Inputs are synthetic.
+
+Prints one JSON line (rank 0). ``--impl reference`` times the reference's own CPU kernels
+(compiled from its sources into oracle/_ref; the oracle port if that build is absent) on the host.
+Multi-GPU: replicas only (every rank runs the full workload; no data-path collective).
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "elastic element-updates/s: batched FP32 vs plain FP64 at rel-L2 1e-4; p50/p99"
+UNIT = "element-updates/s"
+
+WORKLOADS = {
+    # name: (cubes per axis, order, runs, mechanisms, precision, source, f0)
+    "box48_o5_r16_fp32": (48, 5, 16, 0, 32, "random", 1.5),
+    "box12_o4_r1_fp64": (12, 4, 1, 0, 64, "explosive", 2.0),
+    "box60j_o4_r8_m3_fp32": (60, 4, 8, 3, 32, "random", 2.0),
+}
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="edge", choices=["edge", "reference"])
+    ap.add_argument("--workload", default="box48_o5_r16_fp32", choices=sorted(WORKLOADS))
+    ap.add_argument("--e2e-steps", type=int, default=3)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-fp64", action="store_true")
+    return ap.parse_args()
+
+
+def dist_init(n_gpus):
+    import torch
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if ws > 1:
+        import datetime
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600),
+                                device_id=torch.device("cuda", local))
+    return ws, rank, local
+
+
+def barrier(ws):
+    if ws > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def max_over_ranks(x, ws):
+    if ws == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+class Clocks:
+    """Samples nvidia-smi while the timed region runs."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.th = threading.Thread(target=self._read, daemon=True)
+            self.th.start()
+        except (OSError, FileNotFoundError):
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            p = [x.strip() for x in ln.split(",")]
+            if len(p) < 9:
+                continue
+            try:
+                sm.append(float(p[1]))
+                mx = float(p[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, p[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def build_problem(name):
+    from edge_b200 import host
+    n, order, runs, rm, prec, source, f0 = WORKLOADS[name]
+    kw = {}
+    if rm:
+        kw = dict(jitter=0.2, layers=[4000.0, 5500.0, 6500.0], lognormal_sigma=0.1, q_range=(50.0, 200.0),
+                  freq_cen=1.0, freq_rat=100.0)
+    prob = host.build_problem(n, order, runs, rm=rm, ext=1e4, seed=3343, source=source, f0=f0,
+                              n_receivers=8, n_steps=500, name=name, **kw)
+    return prob, prec
+
+
+def algorithmic(prob, prec):
+    """Per-element algorithmic bytes and flops of one step (dense-in-modes counts as in the
+    roofline model of the path) for each kernel."""
+    from edge_b200.host import n_face_modes, n_modes
+    O, R, rm = prob.order, prob.runs, prob.rm
+    B, F, p = n_modes(O), n_face_modes(O), (8 if prec == 64 else 4)
+    Bm = lambda o: n_modes(o) if o > 0 else 0
+    ck = sum(3 * (2 * 9 * Bm(O - d) * Bm(O - d + 1) + 2 * 24 * Bm(O - d)) + 2 * 9 * Bm(O - d) for d in range(1, O))
+    vol = 3 * (2 * 9 * B * Bm(O - 1) + 2 * 24 * B)
+    surf = 4 * (2 * 9 * F * B + 2 * 81 * F + 2 * 9 * B * F)
+    dofs = (9 + 6 * rm) * B * R * p
+    face = 4 * 9 * F * R * p
+    local_bytes = 2 * dofs + face + 3 * 24 * 8 + 4 * 81 * 8 + (rm * 12 * 8 + 27 * 8 + 4 * 54 * 8 if rm else 0)
+    neigh_bytes = 2 * dofs + face + 4 * 81 * 8 + 4 * (4 + 1 + 1 + 1) + (4 * 54 * 8 if rm else 0)
+    return dict(local_bytes=local_bytes, neigh_bytes=neigh_bytes,
+                local_flops=(ck + vol + surf) * R, neigh_flops=surf * R)
+
+
+def measured_peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(path) as f:
+            d = json.load(f)
+        return d["hbm_gbs"], "of measured"
+    except (OSError, KeyError, ValueError):
+        return 6650.0, "of fallback"
+
+
+def traffic_from_profiles(workload):
+    """Per-launch DRAM bytes of the dominant kernel from the committed ncu summary, if present."""
+    path = os.path.join(ROOT, "profiles", f"kLocal_{workload}.txt")
+    try:
+        for line in open(path):
+            if line.startswith("dram_bytes_per_full_launch:"):
+                return float(line.split(":")[1])
+    except OSError:
+        pass
+    return None
+
+
+def cpu_sample_rate(order, runs, rm, n_cubes=12, steps=2):
+    """Reference CPU kernels (oracle/_ref, OpenMP over all host threads) on a bounded sample;
+    falls back to the C oracle port. Returns (element-updates/s, kind, cores, sample text)."""
+    import numpy as np
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    import oracle as orc
+    import ref as refmod
+    from edge_b200 import host
+    prob = host.build_problem(n_cubes, order, runs, rm=rm, ext=1e4, seed=3343, source=None, n_receivers=0,
+                              n_steps=steps)
+    d = prob.oracle_dict()
+    rng = np.random.default_rng(0)
+    st = dict(dofsE=rng.normal(size=(prob.n_el, 9, prob.B, runs)),
+              dofsA=rng.normal(size=(prob.n_el, rm, 6, prob.B, runs)) if rm else None,
+              tDofs=np.zeros((prob.n_el, 9, prob.B, runs)))
+    L = refmod.load(order, runs, rm)
+    cores = os.cpu_count() or 1
+    if L is not None:
+        kind = "reference"
+        t0 = time.perf_counter()
+        for _ in range(steps):
+            refmod.step(L, d, st, 0.0, prob.dt)
+        el = time.perf_counter() - t0
+    else:
+        kind, cores = "port", 1
+        t0 = time.perf_counter()
+        for _ in range(steps):
+            orc.step(d, st, 0.0, prob.dt)
+        el = time.perf_counter() - t0
+    sample = (f"{n_cubes}^3 cubes x 6 = {prob.n_el} tets, order {order}, {runs} runs, {rm} mechanisms, "
+              f"{steps} steps (local + neighbour), FP64")
+    return prob.n_el * runs * steps / el, kind, cores, sample
+
+
+def run_reference(a, ws, rank):
+    if rank != 0:
+        return
+    n, order, runs, rm, prec, source, f0 = WORKLOADS[a.workload]
+    vals = []
+    for i in range(a.warmup + a.steps):
+        v, kind, cores, sample = cpu_sample_rate(order, runs, rm, n_cubes=8, steps=1)
+        if i >= a.warmup:
+            vals.append(v)
+    value = statistics.median(vals)
+    out = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": a.gpus,
+           "steps": a.steps, "warmup": a.warmup, "higher_is_better": True, "scaling": "weak",
+           "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+           "config": {"workload": a.workload, "reference_sample": sample},
+           "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": kind, "sample": sample},
+           "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(out), flush=True)
+
+
+def main():
+    a = parse()
+    ws, rank, local = dist_init(a.gpus)
+    if a.impl == "reference":
+        run_reference(a, ws, rank)
+        barrier(ws)
+        return
+    import numpy as np
+    import torch
+    from edge_b200 import _lib
+    from edge_b200.solver import Solver
+
+    torch.cuda.set_device(local)
+    prob, prec = build_problem(a.workload)
+    stream = torch.cuda.Stream()
+    sv = Solver(prob, precision=prec, stream=stream.cuda_stream, device=local)
+    e0, a0 = prob.zero_dofs(np.float32 if prec == 32 else np.float64)
+    sv.upload_dofs(e0, a0)
+    units_per_step = prob.n_el * prob.runs
+
+    # warm-up, then K timed steps (inputs > L2: DOFs alone are several hundred MB)
+    sv.step(a.warmup)
+    sv.sync()
+    clocks = Clocks(local)
+    clocks.start()
+    barrier(ws)
+    torch.cuda.synchronize()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ev0.record(stream)
+    sv.step(a.steps)
+    launches = sv.launches()
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    barrier(ws)
+    clk = clocks.stop()
+    ms = ev0.elapsed_time(ev1)
+    ms_max = max_over_ranks(ms, ws)
+    value = units_per_step * a.steps * ws / (ms_max / 1e3)
+
+    # per-step latency and per-kernel times (a second pass with events around every launch)
+    step_ms = []
+    for _ in range(a.steps):
+        e_a, e_b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e_a.record(stream)
+        sv.step(1)
+        e_b.record(stream)
+        step_ms.append((e_a, e_b))
+    torch.cuda.synchronize()
+    step_ms = sorted(x.elapsed_time(y) for x, y in step_ms)
+    L = _lib.lib()
+    import ctypes as C
+    L.edge_b200_set_timing(sv._h, 1)
+    sv.step(a.steps)
+    kms = np.zeros(4)
+    kn = np.zeros(4, np.int64)
+    L.edge_b200_kernel_times(sv._h, _lib.ptr(kms), _lib.ptr(kn))
+    L.edge_b200_set_timing(sv._h, 0)
+    names = ["local", "neighbour", "sources", "receivers"]
+    shares = {names[i]: float(kms[i] / kms.sum()) for i in range(4) if kn[i]}
+    alg = algorithmic(prob, prec)
+    top = int(np.argmax(kms[:2]))
+    avg_ms = kms[top] / max(kn[top], 1)
+    bytes_launch = (alg["local_bytes"] if top == 0 else alg["neigh_bytes"]) * prob.n_el
+    flops_launch = (alg["local_flops"] if top == 0 else alg["neigh_flops"]) * prob.n_el
+    peak, peak_src = measured_peaks()
+    achieved = bytes_launch / (avg_ms / 1e3) / 1e9
+    traffic = traffic_from_profiles(a.workload)
+    roofline = {"bound": "hbm", "kernel": names[top], "achieved": achieved, "peak": peak, "unit": "GB/s",
+                "frac": achieved / peak, "peak_source": peak_src, "traffic": traffic,
+                "algorithmic_bytes_per_launch": bytes_launch,
+                "achieved_tflops": flops_launch / (avg_ms / 1e3) / 1e12,
+                "kernel_avg_ms": {names[i]: float(kms[i] / kn[i]) for i in range(4) if kn[i]},
+                "kernel_share": shares}
+
+    # end to end through the C ABI with host buffers: pinned H2D of the DOFs, one step, D2H of the DOFs
+    pin_e = torch.from_numpy(e0).pin_memory()
+    pin_a = torch.from_numpy(a0).pin_memory() if a0 is not None else None
+    out_e = torch.empty_like(pin_e).pin_memory()
+    out_a = torch.empty_like(pin_a).pin_memory() if pin_a is not None else None
+    ke = a.e2e_steps
+    barrier(ws)
+    torch.cuda.synchronize()
+    x0, x1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    x0.record(stream)
+    for _ in range(ke):
+        L.edge_b200_upload_dofs(sv._h, C.c_void_p(pin_e.data_ptr()),
+                                C.c_void_p(pin_a.data_ptr()) if pin_a is not None else None)
+        sv.step(1)
+        L.edge_b200_download_dofs(sv._h, C.c_void_p(out_e.data_ptr()),
+                                  C.c_void_p(out_a.data_ptr()) if out_a is not None else None)
+    x1.record(stream)
+    torch.cuda.synchronize()
+    e2e_ms = max_over_ranks(x0.elapsed_time(x1), ws)
+    dof_bytes = pin_e.numel() * pin_e.element_size() + (pin_a.numel() * pin_a.element_size() if pin_a is not None else 0)
+    e2e = {"value": units_per_step * ke * ws / (e2e_ms / 1e3), "unit": UNIT, "h2d_bytes_per_step": dof_bytes,
+           "d2h_bytes_per_step": dof_bytes,
+           "note": "per step: pinned host->device DOFs, one GTS step, device->host DOFs (the drop-in for host-resident DOFs)"}
+
+    # plain FP64 path on the same mesh (one run) for the batched-FP32 vs plain-FP64 ratio
+    fp64 = None
+    if not a.no_fp64 and prec == 32 and prob.rm == 0:
+        from edge_b200 import host
+        p64 = host.Problem(order=prob.order, runs=1, rm=0, mesh=prob.mesh, rho=prob.rho, lam=prob.lam,
+                           mu=prob.mu, starE=prob.starE, fsE=prob.fsE, dt=prob.dt, name="fp64")
+        s64 = Solver(p64, precision=64, stream=stream.cuda_stream, device=local)
+        z, _ = p64.zero_dofs()
+        s64.upload_dofs(z)
+        s64.step(2)
+        s64.sync()
+        k64 = max(2, a.steps // 4)
+        y0, y1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        y0.record(stream)
+        s64.step(k64)
+        y1.record(stream)
+        torch.cuda.synchronize()
+        v64 = prob.n_el * k64 / (y0.elapsed_time(y1) / 1e3)
+        fp64 = {"value": v64 * ws, "unit": UNIT, "ms_per_step": y0.elapsed_time(y1) / k64,
+                "config": {"order": prob.order, "runs": 1, "precision": "fp64"},
+                "batched_fp32_over_plain_fp64": value / (v64 * ws)}
+        s64.close()
+
+    cpu = None
+    if rank == 0 and not a.no_cpu_baseline:
+        v, kind, cores, sample = cpu_sample_rate(prob.order, prob.runs, prob.rm, n_cubes=8, steps=1)
+        cpu = {"value": v, "unit": UNIT, "cores": cores, "kind": kind, "sample": sample}
+
+    if rank == 0:
+        out = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": a.steps,
+               "warmup": a.warmup, "ms_per_step": ms_max / a.steps, "higher_is_better": True,
+               "scaling": "weak", "vs_baseline": None, "dtype": "f32" if prec == 32 else "f64",
+               "data": "synthetic",
+               "config": {"workload": a.workload, "tets": prob.n_el, "order": prob.order, "runs": prob.runs,
+                          "mechanisms": prob.rm, "precision": f"fp{prec}", "parallelism": f"replicas{ws}",
+                          "l2": "inputs larger than L2 (DOFs %.0f MB)" % (dof_bytes / 1e6),
+                          "dt": prob.dt},
+               "step_ms_p50": step_ms[len(step_ms) // 2], "step_ms_p99": step_ms[min(len(step_ms) - 1,
+                                                                                      int(0.99 * len(step_ms)))],
+               "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": int(launches),
+               "clocks": clk, "fp64_plain": fp64}
+        print(json.dumps(out), flush=True)
+    sv.close()
+    barrier(ws)
+    if ws > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

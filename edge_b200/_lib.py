@@ -48,6 +48,8 @@ _SIGS = {
     "edge_b200_device_dofs": (C.c_int, [vp, vp, vp, vp]),
     "edge_b200_last_launches": (i64, [vp]),
     "edge_b200_last_error": (C.c_char_p, [vp]),
+    "edge_b200_set_timing": (C.c_int, [vp, C.c_int]),
+    "edge_b200_kernel_times": (C.c_int, [vp, vp, vp]),
 }
 
 # every symbol include/edge_b200.h declares

@@ -73,6 +73,47 @@ struct edge_b200_ctx {
   size_t tauCap = 0;
   int64_t launches = 0;
   std::string err;
+  // optional per-kernel event timing: pairs of events per launch, resolved lazily
+  bool timing = false;
+  struct Timed { int kind; cudaEvent_t a, b; };
+  std::vector<Timed> timed;
+  std::vector<cudaEvent_t> eventPool;
+  double kernMs[4] = {0, 0, 0, 0};
+  int64_t kernN[4] = {0, 0, 0, 0};
+
+  cudaEvent_t takeEvent() {
+    if (!eventPool.empty()) {
+      cudaEvent_t e = eventPool.back();
+      eventPool.pop_back();
+      return e;
+    }
+    cudaEvent_t e = nullptr;
+    cudaEventCreate(&e);
+    return e;
+  }
+  void resolveTimes() {
+    for (auto &t : timed) {
+      float ms = 0;
+      cudaEventSynchronize(t.b);
+      cudaEventElapsedTime(&ms, t.a, t.b);
+      kernMs[t.kind] += ms;
+      kernN[t.kind]++;
+      eventPool.push_back(t.a);
+      eventPool.push_back(t.b);
+    }
+    timed.clear();
+  }
+  template <typename F>
+  cudaError_t launch(int kind, F &&f) {
+    if (!timing) return f();
+    cudaEvent_t a = takeEvent(), b = takeEvent();
+    cudaEventRecord(a, stream);
+    cudaError_t e = f();
+    cudaEventRecord(b, stream);
+    timed.push_back({kind, a, b});
+    if (timed.size() > 4096) resolveTimes();
+    return e;
+  }
 
   size_t dofsCount() const { return (size_t)nEl * 9 * B * cfg.n_runs; }
   size_t dofsACount() const { return (size_t)nEl * cfg.n_rms * 6 * B * cfg.n_runs; }
@@ -108,6 +149,11 @@ struct edge_b200_ctx {
     dfree(elFaEl); dfree(fId); dfree(vId); dfree(faType);
     for (auto &p : srcMem) dfree(p);
     dfree(dGrpEl); dfree(dGrpOff); dfree(dBasis); dfree(dBuf); dfree(dTau); dfree(dSlot);
+    for (auto &t : timed) {
+      cudaEventDestroy(t.a);
+      cudaEventDestroy(t.b);
+    }
+    for (auto e : eventPool) cudaEventDestroy(e);
     delete ks;
   }
 };
@@ -386,19 +432,19 @@ int edge_b200_step(edge_b200_ctx *ctx, double t, double dt, int n_steps) {
       r.nGrp = ctx->nRecvGrp;
       r.maxBuf = ctx->maxBuf;
       r.buf = ctx->dBuf;
-      EDGE_CUDA(ctx->ks->recv(a, r, s), "receiver kernel");
+      EDGE_CUDA(ctx->launch(3, [&] { return ctx->ks->recv(a, r, s); }), "receiver kernel");
       ctx->launches++;
     }
-    EDGE_CUDA(ctx->ks->local(a, s), "local kernel");
+    EDGE_CUDA(ctx->launch(0, [&] { return ctx->ks->local(a, s); }), "local kernel");
     ctx->launches++;
     if (ctx->src.nGrp > 0) {
       SrcArgs sa = ctx->src;
       sa.t = ts;
       sa.dt = dt;
-      EDGE_CUDA(ctx->ks->sources(ctx->dofsE, sa, s), "source kernel");
+      EDGE_CUDA(ctx->launch(2, [&] { return ctx->ks->sources(ctx->dofsE, sa, s); }), "source kernel");
       ctx->launches++;
     }
-    EDGE_CUDA(ctx->ks->neigh(a, s), "neighbour kernel");
+    EDGE_CUDA(ctx->launch(1, [&] { return ctx->ks->neigh(a, s); }), "neighbour kernel");
     ctx->launches++;
     ts += dt;
   }
@@ -436,6 +482,27 @@ int edge_b200_device_dofs(edge_b200_ctx *ctx, void **dofs_e, void **dofs_a, void
 }
 
 int64_t edge_b200_last_launches(const edge_b200_ctx *ctx) { return ctx ? ctx->launches : -1; }
+
+int edge_b200_set_timing(edge_b200_ctx *ctx, int enable) {
+  if (!ctx) return EDGE_B200_EINVAL;
+  ctx->resolveTimes();
+  ctx->timing = enable != 0;
+  for (int i = 0; i < 4; i++) {
+    ctx->kernMs[i] = 0;
+    ctx->kernN[i] = 0;
+  }
+  return EDGE_B200_OK;
+}
+
+int edge_b200_kernel_times(edge_b200_ctx *ctx, double *ms, int64_t *launches) {
+  if (!ctx) return EDGE_B200_EINVAL;
+  ctx->resolveTimes();
+  for (int i = 0; i < 4; i++) {
+    if (ms) ms[i] = ctx->kernMs[i];
+    if (launches) launches[i] = ctx->kernN[i];
+  }
+  return EDGE_B200_OK;
+}
 
 const char *edge_b200_last_error(const edge_b200_ctx *ctx) { return ctx ? ctx->err.c_str() : "null context"; }
 

@@ -166,6 +166,12 @@ int edge_b200_sync(edge_b200_ctx *ctx);
 int edge_b200_device_dofs(edge_b200_ctx *ctx, void **dofs_e, void **dofs_a, void **tdofs);
 /* Kernel launches issued by the last edge_b200_step call. */
 int64_t edge_b200_last_launches(const edge_b200_ctx *ctx);
+/* Per-kernel timing with CUDA events recorded on the context's stream around every launch
+ * (0 = off, the default). edge_b200_kernel_times returns, for kernels 0 = local, 1 = neighbour,
+ * 2 = sources, 3 = receivers, the summed milliseconds and launch counts since timing was enabled
+ * (synchronises the stream). */
+int edge_b200_set_timing(edge_b200_ctx *ctx, int enable);
+int edge_b200_kernel_times(edge_b200_ctx *ctx, double *ms, int64_t *launches);
 /* Last CUDA error string of the context (static storage). */
 const char *edge_b200_last_error(const edge_b200_ctx *ctx);
 

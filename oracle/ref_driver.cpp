@@ -14,6 +14,7 @@
 // provided from this repository's generator, which reproduces the reference pre-processor's values.
 #include <cstddef>
 #include <cstring>
+#include <iostream>
 #include <vector>
 
 #include "impl/seismic/kernels/TimePredVanilla.hpp"
@@ -71,9 +72,14 @@ struct Kernels {
   explicit Kernels(const double *omega) {
     double w[RM > 0 ? RM : 1] = {0};
     for (int i = 0; i < RM; i++) w[i] = omega[i];
+    // without easylogging the reference's verbose logs go to std::cout (io/logging.h:66-78);
+    // silence them while the kernels are generated
+    std::streambuf *saved = std::cout.rdbuf(nullptr);
     tp = new TP(RM ? w : nullptr, mem);
     vi = new VI(RM ? w : nullptr, mem);
     si = new SI(RM ? w : nullptr, mem);
+    std::cout.rdbuf(saved);
+    std::cout.clear();
   }
   ~Kernels() { delete tp; delete vi; delete si; }
 };

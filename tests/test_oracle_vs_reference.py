@@ -1,0 +1,31 @@
+"""The oracle's GTS step against the reference's own vanilla kernels (oracle/_ref).
+
+The reference build drives TimePredVanilla / VolIntVanilla / SurfIntVanilla unchanged; both sides
+get identical inputs (mesh, element data, DOFs) from the host setup. Skipped where the reference
+checkout was never available to compile oracle/_ref.
+"""
+import numpy as np
+import pytest
+
+import ref as refmod
+from helpers import OracleRun, random_dofs, rel_l2, small_problem
+
+
+@pytest.mark.parametrize("order,runs,rm", [(3, 1, 0), (4, 1, 0), (5, 1, 0), (4, 1, 3), (4, 8, 3)])
+def test_oracle_step_matches_reference_kernels(order, runs, rm):
+    L = refmod.load(order, runs, rm)
+    if L is None:
+        pytest.skip("reference build (oracle/_ref) unavailable")
+    prob = small_problem(n=2, order=order, runs=runs, rm=rm, jitter=0.15, source=None, n_receivers=0)
+    e0, a0 = random_dofs(prob, seed=order + 10 * rm)
+    orc = OracleRun(prob, e0, a0)
+    d = prob.oracle_dict()
+    st = dict(dofsE=e0.copy(), dofsA=None if a0 is None else a0.copy(),
+              tDofs=np.zeros_like(e0))
+    for _ in range(3):
+        orc.step()
+        refmod.step(L, d, st, 0.0, prob.dt)
+    assert rel_l2(orc.state["dofsE"], st["dofsE"]) < 1e-13
+    assert rel_l2(orc.state["tDofs"], st["tDofs"]) < 1e-13
+    if rm:
+        assert rel_l2(orc.state["dofsA"], st["dofsA"]) < 1e-13
