@@ -30,6 +30,8 @@ WORKLOADS = {
     "box48_o5_r16_fp32": (48, 5, 16, 0, 32, "random", 1.5),
     "box12_o4_r1_fp64": (12, 4, 1, 0, 64, "explosive", 2.0),
     "box60j_o4_r8_m3_fp32": (60, 4, 8, 3, 32, "random", 2.0),
+    # small case of the headline kernels for ncu captures (24,576 tets; DOFs 0.5 GB > L2)
+    "box16_o5_r16_fp32": (16, 5, 16, 0, 32, "random", 1.5),
 }
 
 
