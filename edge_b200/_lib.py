@@ -50,6 +50,7 @@ _SIGS = {
     "edge_b200_last_error": (C.c_char_p, [vp]),
     "edge_b200_set_timing": (C.c_int, [vp, C.c_int]),
     "edge_b200_kernel_times": (C.c_int, [vp, vp, vp]),
+    "edge_b200_step_noalloc": (C.c_int, [vp, i64, dbl, C.c_int] + [vp] * 12),
 }
 
 # every symbol include/edge_b200.h declares

@@ -6,4 +6,16 @@ KernelSet *makeKernelSet_o5(int precision, int order, int runs, int rms) {
 #include "inst_o5.inc"
   return nullptr;
 }
+
+// process-wide instances for callers that must not allocate (edge_b200_step_noalloc)
+KernelSet *staticKernelSet_o5(int precision, int order, int runs, int rms) {
+#undef EDGE_B200_CFG
+#define EDGE_B200_CFG(T, O, R, RM, prec)                          \
+  if (precision == prec && order == O && runs == R && rms == RM) { \
+    static KernelSetImpl<T, O, R, RM> inst;                       \
+    return &inst;                                                 \
+  }
+#include "inst_o5.inc"
+  return nullptr;
+}
 }  // namespace edge_b200

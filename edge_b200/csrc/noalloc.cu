@@ -1,0 +1,105 @@
+// edge_b200_step_noalloc: the GTS step over caller-owned device arrays with its scratch (the face
+// projections the local kernel writes and the neighbour kernel reads) in a static device array,
+// for callers that cannot allocate device memory while they run.
+#include <cuda_runtime.h>
+
+#include <mutex>
+
+#include "../../include/edge_b200.h"
+#include "kernel_set.h"
+#include "kernels.cuh"
+
+namespace edge_b200 {
+KernelSet *staticKernelSet_o2(int, int, int, int);
+KernelSet *staticKernelSet_o3(int, int, int, int);
+KernelSet *staticKernelSet_o4(int, int, int, int);
+KernelSet *staticKernelSet_o5(int, int, int, int);
+KernelSet *staticKernelSet_o6(int, int, int, int);
+}  // namespace edge_b200
+
+using namespace edge_b200;
+
+namespace {
+
+constexpr size_t kScratchBytes = EDGE_B200_NOALLOC_SCRATCH_BYTES;
+constexpr int kMaxDevices = 64;
+
+// Held by every GPU that loads the library, until the process exits.
+__device__ __align__(256) unsigned char g_faceScratch[kScratchBytes];
+
+// per device: the array's device address (host code only sees a stand-in symbol) and whether
+// the kernel set's launch attributes were set on that device
+std::mutex g_setupMutex;
+void *g_scratchPtr[kMaxDevices] = {};
+
+KernelSet *staticKernelSet(int precision, int order, int runs, int rms) {
+  switch (order) {
+    case 2: return staticKernelSet_o2(precision, order, runs, rms);
+    case 3: return staticKernelSet_o3(precision, order, runs, rms);
+    case 4: return staticKernelSet_o4(precision, order, runs, rms);
+    case 5: return staticKernelSet_o5(precision, order, runs, rms);
+    case 6: return staticKernelSet_o6(precision, order, runs, rms);
+    default: return nullptr;
+  }
+}
+
+}  // namespace
+
+extern "C" int edge_b200_step_noalloc(const edge_b200_cfg *cfg, int64_t n_el, double dt, int n_steps,
+                                      void *dofs_e, void *dofs_a, const double *star_e, const double *fs_e,
+                                      const double *star_a, const double *src_a, const double *fs_a,
+                                      const double *omega, const int32_t *el_fa_el,
+                                      const uint8_t *fid_el_fa_el, const uint8_t *vid_el_fa_el,
+                                      const uint8_t *el_fa_type) {
+  if (!cfg || n_el < 1 || !(dt > 0) || n_steps < 0) return EDGE_B200_EINVAL;
+  if (cfg->precision != 32 && cfg->precision != 64) return EDGE_B200_EINVAL;
+  if (cfg->n_rms < 0 || cfg->n_rms > 3 || cfg->n_runs < 1 || 32 % cfg->n_runs) return EDGE_B200_EINVAL;
+  if (cfg->device < 0 || cfg->device >= kMaxDevices) return EDGE_B200_EINVAL;
+  if (!dofs_e || !star_e || !fs_e || !el_fa_el || !fid_el_fa_el || !vid_el_fa_el || !el_fa_type)
+    return EDGE_B200_EINVAL;
+  if (cfg->n_rms && (!dofs_a || !star_a || !src_a || !fs_a || !omega)) return EDGE_B200_EINVAL;
+  const size_t realSize = cfg->precision == 64 ? 8 : 4;
+  const size_t faceBytes = (size_t)n_el * 4 * 9 * nFaceModes(cfg->order) * cfg->n_runs * realSize;
+  if (faceBytes > kScratchBytes) return EDGE_B200_ESCRATCH;
+  KernelSet *ks = staticKernelSet(cfg->precision, cfg->order, cfg->n_runs, cfg->n_rms);
+  if (!ks) return EDGE_B200_ENOTSUP;
+
+  if (cudaSetDevice(cfg->device) != cudaSuccess) return EDGE_B200_EDEVICE;
+  void *scratch = nullptr;
+  {
+    // set-up once per device, with that device current
+    std::lock_guard<std::mutex> lock(g_setupMutex);
+    if (!g_scratchPtr[cfg->device]) {
+      void *p = nullptr;
+      if (cudaGetSymbolAddress(&p, g_faceScratch) != cudaSuccess || !p) return EDGE_B200_EDEVICE;
+      g_scratchPtr[cfg->device] = p;
+    }
+    scratch = g_scratchPtr[cfg->device];
+    // sets the kernels' dynamic shared-memory limits and sizes the persistent grids (no allocation)
+    if (ks->init(cfg->device) != cudaSuccess) return EDGE_B200_EDEVICE;
+  }
+
+  StepArgsRaw a;
+  a.dofsE = dofs_e;
+  a.dofsA = cfg->n_rms ? dofs_a : nullptr;
+  a.tDofs = nullptr;
+  a.face = scratch;
+  a.starE = star_e;
+  a.starA = cfg->n_rms ? star_a : nullptr;
+  a.srcA = cfg->n_rms ? src_a : nullptr;
+  a.fsE = fs_e;
+  a.fsA = cfg->n_rms ? fs_a : nullptr;
+  a.elFaEl = el_fa_el;
+  a.fId = fid_el_fa_el;
+  a.vId = vid_el_fa_el;
+  a.faType = el_fa_type;
+  a.nEl = n_el;
+  a.dt = dt;
+  for (int m = 0; m < 3; m++) a.omega[m] = (cfg->n_rms && m < cfg->n_rms) ? omega[m] : 0.0;
+  cudaStream_t s = (cudaStream_t)cfg->stream;
+  for (int st = 0; st < n_steps; st++) {
+    if (ks->local(a, s) != cudaSuccess) return EDGE_B200_EDEVICE;
+    if (ks->neigh(a, s) != cudaSuccess) return EDGE_B200_EDEVICE;
+  }
+  return EDGE_B200_OK;
+}

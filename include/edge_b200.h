@@ -31,7 +31,8 @@ typedef enum {
   EDGE_B200_ENOTSUP = -5,    /* configuration not compiled in (order / runs / mechanisms) */
   EDGE_B200_EMESH = -6,      /* inconsistent or degenerate mesh */
   EDGE_B200_ENOTFOUND = -7,  /* point not inside the mesh */
-  EDGE_B200_EOVERFLOW = -8   /* receiver buffer full */
+  EDGE_B200_EOVERFLOW = -8,  /* receiver buffer full */
+  EDGE_B200_ESCRATCH = -9    /* problem too large for the static scratch of edge_b200_step_noalloc */
 } edge_b200_status;
 
 /* per element-face boundary types (t_spTypeElastic, src/impl/seismic/const.inc:143-149) */
@@ -172,6 +173,32 @@ int64_t edge_b200_last_launches(const edge_b200_ctx *ctx);
  * (synchronises the stream). */
 int edge_b200_set_timing(edge_b200_ctx *ctx, int enable);
 int edge_b200_kernel_times(edge_b200_ctx *ctx, double *ms, int64_t *launches);
+
+/* No counterpart in the reference. n_steps GTS steps (local kernel, then neighbour kernel; no
+ * sources, no receivers) over caller-owned DEVICE arrays, without allocating anything: no
+ * context, no cudaMalloc / cudaFree, no allocating library call. It is meant for callers that
+ * cannot allocate device memory while they run, e.g. a host that has handed every byte of the GPU
+ * to a fixed memory budget or pool, or one that must not hit the device-wide synchronisation
+ * cudaMalloc and cudaFree imply in the middle of its time loop.
+ * The face projections the two kernels exchange live in one file-scope device array of
+ * EDGE_B200_NOALLOC_SCRATCH_BYTES (32 MiB) that every GPU loading the library holds until exit; a
+ * problem needing more (n_el * 4 * 9 * F * R * sizeof(real) bytes) is rejected with
+ * EDGE_B200_ESCRATCH. The first call on a device looks up that array's device address (and sets
+ * the kernels' shared-memory limits) with the device current; make that first call before any
+ * stream capture. Every call shares the array: calls that overlap on the GPU (other streams,
+ * other host threads) race and must be serialised by the caller. Nothing in it needs to start at
+ * zero: each step writes every face projection before reading it.
+ * Arguments: cfg as for edge_b200_create (order, n_runs, n_rms, precision, stream, device);
+ * dofs_e / dofs_a in the cfg precision, element data in FP64 with the layouts of
+ * edge_b200_upload_element_data, connectivity as in edge_b200_upload_mesh, all on cfg->device;
+ * only omega (n_rms relaxation frequencies) is a host array. */
+#define EDGE_B200_NOALLOC_SCRATCH_BYTES (32u << 20)
+int edge_b200_step_noalloc(const edge_b200_cfg *cfg, int64_t n_el, double dt, int n_steps,
+                           void *dofs_e, void *dofs_a, const double *star_e, const double *fs_e,
+                           const double *star_a, const double *src_a, const double *fs_a,
+                           const double *omega, const int32_t *el_fa_el,
+                           const uint8_t *fid_el_fa_el, const uint8_t *vid_el_fa_el,
+                           const uint8_t *el_fa_type);
 /* Last CUDA error string of the context (static storage). */
 const char *edge_b200_last_error(const edge_b200_ctx *ctx);
 
