@@ -56,7 +56,7 @@ struct edge_b200_ctx {
   int32_t *elFaEl = nullptr;
   uint8_t *fId = nullptr, *vId = nullptr, *faType = nullptr;
   double omega[3] = {0, 0, 0};
-  bool meshSet = false, dataSet = false;
+  bool meshSet = false, dataSet = false, keepTDofs = false;
   // sources
   SrcArgs src{};
   void *srcMem[10] = {};
@@ -127,7 +127,7 @@ struct edge_b200_ctx {
     StepArgsRaw a;
     a.dofsE = dofsE;
     a.dofsA = dofsA;
-    a.tDofs = tDofs;
+    a.tDofs = keepTDofs ? tDofs : nullptr;
     a.face = face;
     a.starE = starE;
     a.starA = starA;
@@ -200,7 +200,6 @@ int edge_b200_create(const edge_b200_cfg *cfg, int64_t n_el, edge_b200_ctx **out
   size_t rs = ctx->realSize;
   if ((e = cudaMalloc(&ctx->dofsE, ctx->dofsCount() * rs)) ||
       (cfg->n_rms && (e = cudaMalloc(&ctx->dofsA, ctx->dofsACount() * rs))) ||
-      (e = cudaMalloc(&ctx->tDofs, ctx->dofsCount() * rs)) ||
       (e = cudaMalloc(&ctx->face, ctx->faceCount() * rs))) {
     delete ctx;
     return e == cudaErrorMemoryAllocation ? EDGE_B200_ENOMEM : EDGE_B200_EDEVICE;
@@ -282,8 +281,19 @@ int edge_b200_download_dofs(edge_b200_ctx *ctx, void *dofs_e, void *dofs_a) {
   return EDGE_B200_OK;
 }
 
+int edge_b200_keep_tdofs(edge_b200_ctx *ctx, int enable) {
+  if (!ctx) return EDGE_B200_EINVAL;
+  if (enable && !ctx->tDofs) {
+    cudaError_t e = cudaMalloc(&ctx->tDofs, ctx->dofsCount() * ctx->realSize);
+    if (e != cudaSuccess) return e == cudaErrorMemoryAllocation ? EDGE_B200_ENOMEM : ctx->fail(e, "keep tDofs");
+    EDGE_CUDA(cudaMemsetAsync(ctx->tDofs, 0, ctx->dofsCount() * ctx->realSize, ctx->stream), "keep tDofs");
+  }
+  ctx->keepTDofs = enable != 0;
+  return EDGE_B200_OK;
+}
+
 int edge_b200_download_tdofs(edge_b200_ctx *ctx, void *tdofs) {
-  if (!ctx || !tdofs) return EDGE_B200_EINVAL;
+  if (!ctx || !tdofs || !ctx->tDofs) return EDGE_B200_EINVAL;
   EDGE_CUDA(cudaMemcpyAsync(tdofs, ctx->tDofs, ctx->dofsCount() * ctx->realSize, cudaMemcpyDeviceToHost,
                             ctx->stream), "download tDofs");
   EDGE_CUDA(cudaStreamSynchronize(ctx->stream), "download tDofs");

@@ -30,9 +30,9 @@ class KernelSetImpl final : public KernelSet {
     for (int i = 0; i < 3; i++) b.omega[i] = a.omega[i];
     return b;
   }
-  static constexpr size_t smemLocal() { return G::smemBytes; }
-  static constexpr size_t smemNeigh() { return G::smemS0 * sizeof(T); }
-  static constexpr size_t smemRecv() { return (G::smemX + G::smemXA) * sizeof(T); }
+  static constexpr size_t smemLocal() { return G::smemLocal; }
+  static constexpr size_t smemNeigh() { return G::smemNeigh; }
+  static constexpr size_t smemRecv() { return G::smemLocal; }
 
  public:
   cudaError_t init(int device) override {

@@ -60,129 +60,32 @@ __device__ __forceinline__ T ldd(const double *p, int i) {
 }
 
 // ------------------------------------------------------------------------------------------------
-// compile-time loops over derivatives / dimensions / faces
+// geometry of a CTA and its shared memory
 // ------------------------------------------------------------------------------------------------
-template <int O, int D, int DIM, typename T>
-__device__ __forceinline__ void ckMul(const T *z, T *acc) { CkMul<O, D, DIM>::template run<T>(z, acc); }
-
 template <typename T, int O, int R, int RM>
 struct Geo {
   static constexpr int B = nModes(O), F = nFaceModes(O), E = 32 / R;
   static constexpr int NW = 9 + (RM ? 6 : 0);
   static constexpr int NT = NW * 32;
-  // shared memory: X [9][B][32], XA [RM][6][B][32], S0 [9][F][32]
-  static constexpr size_t smemX = size_t(9) * B * 32;
-  static constexpr size_t smemXA = size_t(RM) * 6 * B * 32;
-  static constexpr size_t smemS0 = size_t(9) * F * 32;
-  static constexpr size_t smemBytes = (smemX + smemXA + smemS0) * sizeof(T);
+  // D [9][B][32]   derivatives during the CK recursion, then the face tiles S0 [9][F][32]
+  // TI [9][B][32]  time-integrated DOFs
+  // XA [RM][6][B][32], TIA [RM][6][B][32]  anelastic derivatives and time integrals
+  static constexpr size_t nD = size_t(9) * B * 32;
+  static constexpr size_t nTI = size_t(9) * B * 32;
+  static constexpr size_t nXA = size_t(RM) * 6 * B * 32;
+  static constexpr size_t smemLocal = (nD + nTI + 2 * nXA) * sizeof(T);
+  static constexpr size_t smemNeigh = size_t(9) * F * 32 * sizeof(T);
+  // resident CTAs per SM the register allocation targets (65,536 registers per SM): FP32 keeps
+  // two 288-thread CTAs of each kernel (<= 113 registers); FP64 rows need twice the registers
+  // and keep one
+  static constexpr int minCtasLocal = (sizeof(T) == 4 && RM == 0 && smemLocal <= 110 * 1024) ? 2 : 1;
+  static constexpr int minCtasNeigh = sizeof(T) == 4 ? 2 : 1;
 };
 
-// z[k] = sum_i c[i] * X[col_i][k][l] for k < nK
-template <typename T, int B, int NK, int NS>
-__device__ __forceinline__ void mix(const T *X, int l, const int (&col)[NS], const T (&c)[NS], T *z) {
-#pragma unroll
-  for (int k = 0; k < NK; k++) {
-    T v = T(0);
-#pragma unroll
-    for (int i = 0; i < NS; i++) v = fmaT(c[i], X[(col[i] * B + k) * 32 + l], v);
-    z[k] = v;
-  }
+template <typename T>
+__device__ __forceinline__ T sm(const T *p, int row, int k, int B, int l) {
+  return p[(row * B + k) * 32 + l];
 }
-
-// ---------------------------------------- CK recursion -----------------------------------------
-template <typename T, int O, int R, int RM, int D>
-struct CkStep {
-  static constexpr int B = nModes(O);
-  // elastic derivative D (no anelasticity): in B(O-D+1) modes, out B(O-D) modes
-  static constexpr int NK = RM ? B : nModes(O - D + 1);
-  static constexpr int NN = RM ? nModes(O - 1) : nModes(O - D);
-  static constexpr int DK = RM ? 1 : D;  // which truncation of the stiffness product applies
-
-  __device__ __forceinline__ static void run(T *X, T *XA, int q, int l, const T (&cs)[3][3],
-                                             const int (&cols)[3], const T (&ca)[3][2],
-                                             const int (&colsA)[2], const T (&csrc)[3][3],
-                                             const int (&colsSrc)[3], const double *omega,
-                                             T sca, T *tI, T (*tIA)[B]) {
-    T acc[B];
-    T z[B];
-#pragma unroll
-    for (int n = 0; n < B; n++) acc[n] = T(0);
-    if (q < 9) {
-      const T c0[3] = {cs[0][0], cs[0][1], cs[0][2]}, c1[3] = {cs[1][0], cs[1][1], cs[1][2]},
-              c2[3] = {cs[2][0], cs[2][1], cs[2][2]};
-      mix<T, B, NK, 3>(X, l, cols, c0, z);
-      ckMul<O, DK, 0, T>(z, acc);
-      mix<T, B, NK, 3>(X, l, cols, c1, z);
-      ckMul<O, DK, 1, T>(z, acc);
-      mix<T, B, NK, 3>(X, l, cols, c2, z);
-      ckMul<O, DK, 2, T>(z, acc);
-      if (RM && q < 6) {
-        // der[d] += srcA_m * derA_m[d-1] (all B modes)
-#pragma unroll
-        for (int m = 0; m < RM; m++)
-#pragma unroll
-          for (int n = 0; n < B; n++) {
-            T v = acc[n];
-#pragma unroll
-            for (int i = 0; i < 3; i++) v = fmaT(csrc[m][i], XA[((m * 6 + colsSrc[i]) * B + n) * 32 + l], v);
-            acc[n] = v;
-          }
-      }
-    } else {
-      // anelastic strain-rate part Psi = sum_dim (starA_dim * der[d-1][u,v,w]) * (-K^T_dim)
-      int cv[2] = {6 + colsA[0], 6 + colsA[1]};
-      const T a0[2] = {ca[0][0], ca[0][1]}, a1[2] = {ca[1][0], ca[1][1]}, a2[2] = {ca[2][0], ca[2][1]};
-      mix<T, B, NK, 2>(X, l, cv, a0, z);
-      ckMul<O, DK, 0, T>(z, acc);
-      mix<T, B, NK, 2>(X, l, cv, a1, z);
-      ckMul<O, DK, 1, T>(z, acc);
-      mix<T, B, NK, 2>(X, l, cv, a2, z);
-      ckMul<O, DK, 2, T>(z, acc);
-    }
-    __syncthreads();
-    if (q < 9) {
-      constexpr int NW = RM ? B : NN;  // rows beyond NN are zero without anelasticity
-#pragma unroll
-      for (int n = 0; n < NW; n++) {
-        X[(q * B + n) * 32 + l] = acc[n];
-        tI[n] = fmaT(sca, acc[n], tI[n]);
-      }
-    } else if (RM) {
-      const int s = q - 9;
-#pragma unroll
-      for (int m = 0; m < RM; m++) {
-        const T om = T(omega[m]);
-#pragma unroll
-        for (int n = 0; n < B; n++) {
-          T *p = &XA[((m * 6 + s) * B + n) * 32 + l];
-          T v = om * (acc[n] + *p);
-          *p = v;
-          tIA[m][n] = fmaT(sca, v, tIA[m][n]);
-        }
-      }
-    }
-    __syncthreads();
-  }
-};
-
-template <typename T, int O, int R, int RM, int D>
-__device__ __forceinline__ void ckAll(T *X, T *XA, int q, int l, const T (&cs)[3][3], const int (&cols)[3],
-                                      const T (&ca)[3][2], const int (&colsA)[2], const T (&csrc)[3][3],
-                                      const int (&colsSrc)[3], const double *omega, T dt, T sca, T *tI,
-                                      T (*tIA)[nModes(O)]) {
-  if constexpr (D < O) {
-    sca = sca * dt / T(D + 1);
-    CkStep<T, O, R, RM, D>::run(X, XA, q, l, cs, cols, ca, colsA, csrc, colsSrc, omega, sca, tI, tIA);
-    ckAll<T, O, R, RM, D + 1>(X, XA, q, l, cs, cols, ca, colsA, csrc, colsSrc, omega, dt, sca, tI, tIA);
-  }
-}
-
-template <int O, int DIM, typename T>
-__device__ __forceinline__ void volMul(const T *z, T *acc) { VolMul<O, DIM>::template run<T>(z, acc); }
-template <int O, int FA, typename T>
-__device__ __forceinline__ void fluxLMul(const T *x, T *s) { FluxLMul<O, FA>::template run<T>(x, s); }
-template <int O, int FA, typename T>
-__device__ __forceinline__ void fluxTMul(const T *s, T *acc) { FluxTMul<O, FA>::template run<T>(s, acc); }
 
 // per-thread element coefficients
 template <typename T, int RM>
@@ -238,19 +141,125 @@ struct ElemCoef {
   }
 };
 
+// star mix of one reference direction: z(k) = sum_i c[i] * X[col_i][k][l]
+template <typename T, int B>
+struct StarMix {
+  const T *X;
+  int l;
+  int c0, c1, c2;
+  T a0, a1, a2;
+  __device__ __forceinline__ T operator()(int k) const {
+    T v = a0 * X[(c0 * B + k) * 32 + l];
+    v = fmaT(a1, X[(c1 * B + k) * 32 + l], v);
+    return fmaT(a2, X[(c2 * B + k) * 32 + l], v);
+  }
+};
+template <typename T, int B>
+struct StarMixA {  // anelastic star: two velocity columns
+  const T *X;
+  int l;
+  int c0, c1;
+  T a0, a1;
+  __device__ __forceinline__ T operator()(int k) const {
+    T v = a0 * X[((6 + c0) * B + k) * 32 + l];
+    return fmaT(a1, X[((6 + c1) * B + k) * 32 + l], v);
+  }
+};
+template <typename T, int B>
+struct RowRead {  // z(k) = X[row][k][l]
+  const T *X;
+  int row, l;
+  __device__ __forceinline__ T operator()(int k) const { return X[(row * B + k) * 32 + l]; }
+};
+
+// dofs rows 0..5 += sum_m srcA_m * Y_m (anelastic source matrices, all B modes)
+template <typename T, int B, int RM>
+__device__ __forceinline__ void addSrc(const ElemCoef<T, RM> &c, const T *Y, int l, T *acc) {
+#pragma unroll
+  for (int m = 0; m < RM; m++)
+#pragma unroll
+    for (int n = 0; n < B; n++) {
+      T v = acc[n];
+#pragma unroll
+      for (int i = 0; i < 3; i++) v = fmaT(c.csrc[m][i], Y[((m * 6 + c.colsSrc[i]) * B + n) * 32 + l], v);
+      acc[n] = v;
+    }
+}
+
+// ---------------------------------------- CK recursion -----------------------------------------
+// derivative D of TimePredVanilla::ck (TimePredVanilla.hpp:229-303) with the star matrix applied
+// before the stiffness product; der[D] replaces der[D-1] in X, TI += sca * der[D] (rows owned by
+// their warp), the anelastic warps update XA and TIA.
+template <typename T, int O, int R, int RM, int D>
+struct CkStep {
+  static constexpr int B = nModes(O);
+  static constexpr int NN = RM ? nModes(O - 1) : nModes(O - D);  // output modes of the product
+  static constexpr int DK = RM ? 1 : D;                           // truncation of the product
+
+  __device__ __forceinline__ static void run(T *X, T *TI, T *XA, T *TIA, int q, int l, const ElemCoef<T, RM> &c,
+                                             const double *omega, T sca) {
+    T acc[B];
+#pragma unroll
+    for (int n = 0; n < B; n++) acc[n] = T(0);
+    if (q < 9) {
+#pragma unroll
+      for (int dim = 0; dim < 3; dim++) {
+        StarMix<T, B> z{X, l, c.cols[0], c.cols[1], c.cols[2], c.cs[dim][0], c.cs[dim][1], c.cs[dim][2]};
+        if (dim == 0) CkMul<O, DK, 0>::template run<T>(z, acc);
+        if (dim == 1) CkMul<O, DK, 1>::template run<T>(z, acc);
+        if (dim == 2) CkMul<O, DK, 2>::template run<T>(z, acc);
+      }
+      if constexpr (RM > 0)
+        if (q < 6) addSrc<T, B, RM>(c, XA, l, acc);
+    } else if constexpr (RM > 0) {
+#pragma unroll
+      for (int dim = 0; dim < 3; dim++) {
+        StarMixA<T, B> z{X, l, c.colsA[0], c.colsA[1], c.ca[dim][0], c.ca[dim][1]};
+        if (dim == 0) CkMul<O, DK, 0>::template run<T>(z, acc);
+        if (dim == 1) CkMul<O, DK, 1>::template run<T>(z, acc);
+        if (dim == 2) CkMul<O, DK, 2>::template run<T>(z, acc);
+      }
+    }
+    __syncthreads();
+    if (q < 9) {
+      constexpr int NW = RM ? B : NN;  // modes beyond NN stay zero without anelasticity
+#pragma unroll
+      for (int n = 0; n < NW; n++) {
+        X[(q * B + n) * 32 + l] = acc[n];
+        T *t = &TI[(q * B + n) * 32 + l];
+        *t = fmaT(sca, acc[n], *t);
+      }
+    } else if constexpr (RM > 0) {
+      const int s = q - 9;
+#pragma unroll
+      for (int m = 0; m < RM; m++) {
+        const T om = T(omega[m]);
+#pragma unroll
+        for (int n = 0; n < B; n++) {
+          const int i = ((m * 6 + s) * B + n) * 32 + l;
+          const T v = om * (acc[n] + XA[i]);
+          XA[i] = v;
+          TIA[i] = fmaT(sca, v, TIA[i]);
+        }
+      }
+    }
+    __syncthreads();
+  }
+};
+
 // ------------------------------------------------------------------------------------------------
 // local step: CK, volume, local surface, face projections (AderDg::local, AderDg.hpp:338-534)
 // ------------------------------------------------------------------------------------------------
 template <typename T, int O, int R, int RM, int FA>
-__device__ __forceinline__ void localFace(const StepArgs<T> &a, T *X, T *S0, int q, int l, int64_t e,
-                                          int r, bool valid, const T *tI, T *acc, T *upA) {
+__device__ __forceinline__ void localFace(const StepArgs<T> &a, const T *TI, T *S0, int q, int l, int64_t e,
+                                          int r, bool valid, T *acc, T *upA) {
   using G = Geo<T, O, R, RM>;
   constexpr int B = G::B, F = G::F;
   T s[F];
   if (q < 9) {
 #pragma unroll
     for (int j = 0; j < F; j++) s[j] = T(0);
-    fluxLMul<O, FA, T>(tI, s);
+    FluxLMul<O, FA>::template run<T>(RowRead<T, B>{TI, q, l}, s);
 #pragma unroll
     for (int j = 0; j < F; j++) S0[(q * F + j) * 32 + l] = s[j];
     if (valid) {
@@ -259,40 +268,53 @@ __device__ __forceinline__ void localFace(const StepArgs<T> &a, T *X, T *S0, int
       for (int j = 0; j < F; j++) fb[j * R] = s[j];
     }
   }
-  __syncthreads();
-  // s1[j] = sum_q' fs[q][q'] * S0[q'][j]
+  // flux-solver row of this thread (elastic 9x9 or anelastic 6x9), loaded before the barrier
   T fr[9];
   if (q < 9) {
     const double *fp = a.fsE + ((e * 4 + FA) * 81 + q * 9);
 #pragma unroll
     for (int i = 0; i < 9; i++) fr[i] = valid ? T(__ldg(fp + i)) : T(0);
-  } else {
+  } else if constexpr (RM > 0) {
     const double *fp = a.fsA + ((e * 4 + FA) * 54 + (q - 9) * 9);
 #pragma unroll
     for (int i = 0; i < 9; i++) fr[i] = valid ? T(__ldg(fp + i)) : T(0);
   }
+  __syncthreads();
+  // s1[j] = sum_q' fs[q][q'] * S0[q'][j]
 #pragma unroll
   for (int j = 0; j < F; j++) {
-    T v = T(0);
+    T v = fr[0] * S0[j * 32 + l];
 #pragma unroll
-    for (int i = 0; i < 9; i++) v = fmaT(fr[i], S0[(i * F + j) * 32 + l], v);
+    for (int i = 1; i < 9; i++) v = fmaT(fr[i], S0[(i * F + j) * 32 + l], v);
     s[j] = v;
   }
   if (q < 9)
-    fluxTMul<O, FA, T>(s, acc);
+    FluxTMul<O, FA>::template run<T>(s, acc);
   else if constexpr (RM > 0)
-    fluxTMul<O, FA, T>(s, upA);
+    FluxTMul<O, FA>::template run<T>(s, upA);
   __syncthreads();
 }
 
+template <typename T, int O, int R, int RM, int D>
+__device__ __forceinline__ void ckAll(T *X, T *TI, T *XA, T *TIA, int q, int l, const ElemCoef<T, RM> &c,
+                                      const double *omega, T dt, T sca) {
+  if constexpr (D < O) {
+    sca = sca * dt / T(D + 1);
+    CkStep<T, O, R, RM, D>::run(X, TI, XA, TIA, q, l, c, omega, sca);
+    ckAll<T, O, R, RM, D + 1>(X, TI, XA, TIA, q, l, c, omega, dt, sca);
+  }
+}
+
 template <typename T, int O, int R, int RM>
-__global__ void __launch_bounds__(Geo<T, O, R, RM>::NT) kLocal(StepArgs<T> a) {
+__global__ void __launch_bounds__(Geo<T, O, R, RM>::NT, Geo<T, O, R, RM>::minCtasLocal) kLocal(StepArgs<T> a) {
   using G = Geo<T, O, R, RM>;
   constexpr int B = G::B, E = G::E;
   extern __shared__ __align__(16) unsigned char smem[];
   T *X = reinterpret_cast<T *>(smem);
-  T *XA = X + G::smemX;
-  T *S0 = XA + G::smemXA;
+  T *TI = X + G::nD;
+  T *XA = TI + G::nTI;
+  T *TIA = XA + G::nXA;
+  T *S0 = X;  // the face tiles reuse the derivative buffer once the recursion is done
   const int q = threadIdx.x >> 5, l = threadIdx.x & 31;
   const int eo = l / R, r = l % R;
   const int64_t nGroups = (a.nEl + E - 1) / E;
@@ -301,27 +323,26 @@ __global__ void __launch_bounds__(Geo<T, O, R, RM>::NT) kLocal(StepArgs<T> a) {
     const int64_t e = g * E + eo;
     const bool valid = e < a.nEl;
     const int64_t ev = valid ? e : 0;
-    T tI[B];
-    T tIA[RM ? RM : 1][B];
-    // load DOFs
+    // DOFs -> X, dt * DOFs -> TI (and the anelastic counterparts)
     if (q < 9) {
       const T *src = a.dofsE + ((ev * 9 + q) * B) * R + r;
 #pragma unroll
       for (int n = 0; n < B; n++) {
-        T v = valid ? src[n * R] : T(0);
+        const T v = valid ? src[n * R] : T(0);
         X[(q * B + n) * 32 + l] = v;
-        tI[n] = dt * v;
+        TI[(q * B + n) * 32 + l] = dt * v;
       }
-    } else if (RM) {
+    } else if constexpr (RM > 0) {
       const int s = q - 9;
 #pragma unroll
       for (int m = 0; m < RM; m++) {
         const T *src = a.dofsA + (((ev * RM + m) * 6 + s) * B) * R + r;
 #pragma unroll
         for (int n = 0; n < B; n++) {
-          T v = valid ? src[n * R] : T(0);
-          XA[((m * 6 + s) * B + n) * 32 + l] = v;
-          tIA[m][n] = dt * v;
+          const T v = valid ? src[n * R] : T(0);
+          const int i = ((m * 6 + s) * B + n) * 32 + l;
+          XA[i] = v;
+          TIA[i] = dt * v;
         }
       }
     }
@@ -329,80 +350,53 @@ __global__ void __launch_bounds__(Geo<T, O, R, RM>::NT) kLocal(StepArgs<T> a) {
     c.load(a, ev, valid, q);
     __syncthreads();
     // Cauchy-Kowalevski (TimePredVanilla::ck, TimePredVanilla.hpp:200-306)
-    ckAll<T, O, R, RM, 1>(X, XA, q, l, c.cs, c.cols, c.ca, c.colsA, c.csrc, c.colsSrc, a.omega, dt, dt,
-                          tI, tIA);
-    // time-integrated DOFs to shared memory (and global for callers that keep them)
-    if (q < 9) {
+    ckAll<T, O, R, RM, 1>(X, TI, XA, TIA, q, l, c, a.omega, dt, dt);
+    if (a.tDofs && valid && q < 9) {
+      T *dst = a.tDofs + ((e * 9 + q) * B) * R + r;
 #pragma unroll
-      for (int n = 0; n < B; n++) X[(q * B + n) * 32 + l] = tI[n];
-      if (a.tDofs && valid) {
-        T *dst = a.tDofs + ((e * 9 + q) * B) * R + r;
-#pragma unroll
-        for (int n = 0; n < B; n++) dst[n * R] = tI[n];
-      }
-    } else if (RM) {
-      const int s = q - 9;
-#pragma unroll
-      for (int m = 0; m < RM; m++)
-#pragma unroll
-        for (int n = 0; n < B; n++) XA[((m * 6 + s) * B + n) * 32 + l] = tIA[m][n];
+      for (int n = 0; n < B; n++) dst[n * R] = TI[(q * B + n) * 32 + l];
     }
-    __syncthreads();
     // volume integral (VolIntVanilla::apply, VolIntVanilla.hpp:189-241)
     T acc[B];
     T upA[RM ? B : 1];
-    {
-      constexpr int NK = nModes(O - 1);
-      T z[NK > 0 ? NK : 1];
-      if (q < 9) {
-        const T *src = a.dofsE + ((ev * 9 + q) * B) * R + r;
+    if (q < 9) {
+      const T *src = a.dofsE + ((ev * 9 + q) * B) * R + r;
 #pragma unroll
-        for (int n = 0; n < B; n++) acc[n] = valid ? src[n * R] : T(0);
-        const T c0[3] = {c.cs[0][0], c.cs[0][1], c.cs[0][2]}, c1[3] = {c.cs[1][0], c.cs[1][1], c.cs[1][2]},
-                c2[3] = {c.cs[2][0], c.cs[2][1], c.cs[2][2]};
-        mix<T, B, NK, 3>(X, l, c.cols, c0, z);
-        volMul<O, 0, T>(z, acc);
-        mix<T, B, NK, 3>(X, l, c.cols, c1, z);
-        volMul<O, 1, T>(z, acc);
-        mix<T, B, NK, 3>(X, l, c.cols, c2, z);
-        volMul<O, 2, T>(z, acc);
-        if (RM && q < 6) {
+      for (int n = 0; n < B; n++) acc[n] = valid ? src[n * R] : T(0);
 #pragma unroll
-          for (int m = 0; m < RM; m++)
+      for (int dim = 0; dim < 3; dim++) {
+        StarMix<T, B> z{TI, l, c.cols[0], c.cols[1], c.cols[2], c.cs[dim][0], c.cs[dim][1], c.cs[dim][2]};
+        if (dim == 0) VolMul<O, 0>::template run<T>(z, acc);
+        if (dim == 1) VolMul<O, 1>::template run<T>(z, acc);
+        if (dim == 2) VolMul<O, 2>::template run<T>(z, acc);
+      }
+      if constexpr (RM > 0)
+        if (q < 6) addSrc<T, B, RM>(c, TIA, l, acc);
+    } else if constexpr (RM > 0) {
 #pragma unroll
-            for (int n = 0; n < B; n++) {
-              T v = acc[n];
+      for (int n = 0; n < B; n++) {
+        acc[n] = T(0);
+        upA[n] = T(0);
+      }
 #pragma unroll
-              for (int i = 0; i < 3; i++) v = fmaT(c.csrc[m][i], XA[((m * 6 + c.colsSrc[i]) * B + n) * 32 + l], v);
-              acc[n] = v;
-            }
-        }
-      } else if constexpr (RM > 0) {
-#pragma unroll
-        for (int n = 0; n < B; n++) acc[n] = T(0);
-        int cv[2] = {6 + c.colsA[0], 6 + c.colsA[1]};
-        const T a0[2] = {c.ca[0][0], c.ca[0][1]}, a1[2] = {c.ca[1][0], c.ca[1][1]}, a2[2] = {c.ca[2][0], c.ca[2][1]};
-        mix<T, B, NK, 2>(X, l, cv, a0, z);
-        volMul<O, 0, T>(z, acc);
-        mix<T, B, NK, 2>(X, l, cv, a1, z);
-        volMul<O, 1, T>(z, acc);
-        mix<T, B, NK, 2>(X, l, cv, a2, z);
-        volMul<O, 2, T>(z, acc);
-#pragma unroll
-        for (int n = 0; n < B; n++) upA[n] = T(0);
+      for (int dim = 0; dim < 3; dim++) {
+        StarMixA<T, B> z{TI, l, c.colsA[0], c.colsA[1], c.ca[dim][0], c.ca[dim][1]};
+        if (dim == 0) VolMul<O, 0>::template run<T>(z, acc);
+        if (dim == 1) VolMul<O, 1>::template run<T>(z, acc);
+        if (dim == 2) VolMul<O, 2>::template run<T>(z, acc);
       }
     }
     // local surface integral (SurfIntVanilla::local, SurfIntVanilla.hpp:212-262) + face projections
-    localFace<T, O, R, RM, 0>(a, X, S0, q, l, ev, r, valid, tI, acc, upA);
-    localFace<T, O, R, RM, 1>(a, X, S0, q, l, ev, r, valid, tI, acc, upA);
-    localFace<T, O, R, RM, 2>(a, X, S0, q, l, ev, r, valid, tI, acc, upA);
-    localFace<T, O, R, RM, 3>(a, X, S0, q, l, ev, r, valid, tI, acc, upA);
+    localFace<T, O, R, RM, 0>(a, TI, S0, q, l, ev, r, valid, acc, upA);
+    localFace<T, O, R, RM, 1>(a, TI, S0, q, l, ev, r, valid, acc, upA);
+    localFace<T, O, R, RM, 2>(a, TI, S0, q, l, ev, r, valid, acc, upA);
+    localFace<T, O, R, RM, 3>(a, TI, S0, q, l, ev, r, valid, acc, upA);
     if (valid) {
       if (q < 9) {
         T *dst = a.dofsE + ((e * 9 + q) * B) * R + r;
 #pragma unroll
         for (int n = 0; n < B; n++) dst[n * R] = acc[n];
-      } else if (RM) {
+      } else if constexpr (RM > 0) {
         // dofsA_m += omega_m * (Psi_vol - tIntA_m) + omega_m * upA_surf
         const int s = q - 9;
 #pragma unroll
@@ -412,85 +406,95 @@ __global__ void __launch_bounds__(Geo<T, O, R, RM>::NT) kLocal(StepArgs<T> a) {
 #pragma unroll
           for (int n = 0; n < B; n++) {
             T v = dst[n * R];
-            v = fmaT(om, acc[n] - tIA[m][n], v);
+            v = fmaT(om, acc[n] - TIA[((m * 6 + s) * B + n) * 32 + l], v);
             v = fmaT(om, upA[n], v);
             dst[n * R] = v;
           }
         }
       }
     }
-    __syncthreads();
   }
 }
 
 // ------------------------------------------------------------------------------------------------
 // neighbour step (AderDg::neigh, AderDg.hpp:553-722)
 // ------------------------------------------------------------------------------------------------
-template <int O, int V, typename T>
-__device__ __forceinline__ void oriMul(const T *x, T *s) { OriMul<O, V>::template run<T>(x, s); }
+template <typename T, int O>
+struct FaceIn {  // one face's inputs for one thread, loaded ahead of its use
+  T x[nFaceModes(O)];
+  T fr[9];
+  int ty, v;
+};
 
 template <typename T, int O, int R, int RM, int FA>
-__device__ __forceinline__ void neighFace(const StepArgs<T> &a, T *S0, int q, int l, int64_t e, int r,
-                                          bool valid, T *acc, T *upA) {
-  using G = Geo<T, O, R, RM>;
-  constexpr int F = G::F;
-  const int ty = valid ? a.faType[e * 4 + FA] : FT_OUTFLOW;
+__device__ __forceinline__ void neighLoad(const StepArgs<T> &a, int q, int64_t e, int r, bool valid,
+                                          FaceIn<T, O> &in) {
+  constexpr int F = nFaceModes(O);
+  in.ty = valid ? a.faType[e * 4 + FA] : FT_OUTFLOW;
+  in.v = 0;
   if (q < 9) {
-    T s[F];
+    const T *fb = nullptr;
+    if (in.ty == FT_FREE) {
+      // own face projection with the local flux matrix; the mirror is in fsE[1]
+      fb = a.face + ((((e * 4 + FA) * 9 + q) * F) * R) + r;
+    } else if (in.ty == FT_INNER) {
+      const int64_t ne = a.elFaEl[e * 4 + FA];
+      const int fo = a.fId[e * 4 + FA];
+      in.v = a.vId[e * 4 + FA];
+      fb = a.face + ((((ne * 4 + fo) * 9 + q) * F) * R) + r;
+    }
+#pragma unroll
+    for (int j = 0; j < F; j++) in.x[j] = fb ? fb[j * R] : T(0);
+    const double *fp = a.fsE + ((a.nEl + e) * 4 + FA) * 81 + q * 9;
+#pragma unroll
+    for (int i = 0; i < 9; i++) in.fr[i] = in.ty != FT_OUTFLOW ? T(__ldg(fp + i)) : T(0);
+  } else if constexpr (RM > 0) {
+    const double *fp = a.fsA + ((a.nEl + e) * 4 + FA) * 54 + (q - 9) * 9;
+#pragma unroll
+    for (int i = 0; i < 9; i++) in.fr[i] = in.ty != FT_OUTFLOW ? T(__ldg(fp + i)) : T(0);
+  }
+}
+
+template <typename T, int O, int R, int RM, int FA>
+__device__ __forceinline__ void neighFace(T *S0, int q, int l, const FaceIn<T, O> &in, T *acc, T *upA) {
+  constexpr int F = nFaceModes(O);
+  T s[F];
+  if (q < 9) {
 #pragma unroll
     for (int j = 0; j < F; j++) s[j] = T(0);
-    if (ty == FT_FREE) {
-      // own face projection with the local flux matrix; the mirror is in fsE[1]
-      const T *fb = a.face + ((((e * 4 + FA) * 9 + q) * F) * R) + r;
+    if (in.ty == FT_FREE) {
 #pragma unroll
-      for (int j = 0; j < F; j++) s[j] = fb[j * R];
-    } else if (ty == FT_INNER) {
-      const int64_t ne = a.elFaEl[e * 4 + FA];
-      const int fo = a.fId[e * 4 + FA], v = a.vId[e * 4 + FA];
-      const T *fb = a.face + ((((ne * 4 + fo) * 9 + q) * F) * R) + r;
-      T x[F];
-#pragma unroll
-      for (int j = 0; j < F; j++) x[j] = fb[j * R];
-      if (v == 0)
-        oriMul<O, 0, T>(x, s);
-      else if (v == 1)
-        oriMul<O, 1, T>(x, s);
+      for (int j = 0; j < F; j++) s[j] = in.x[j];
+    } else if (in.ty == FT_INNER) {
+      if (in.v == 0)
+        OriMul<O, 0>::template run<T>(in.x, s);
+      else if (in.v == 1)
+        OriMul<O, 1>::template run<T>(in.x, s);
       else
-        oriMul<O, 2, T>(x, s);
+        OriMul<O, 2>::template run<T>(in.x, s);
     }
 #pragma unroll
     for (int j = 0; j < F; j++) S0[(q * F + j) * 32 + l] = s[j];
   }
   __syncthreads();
-  if (ty != FT_OUTFLOW) {
-    T fr[9];
-    if (q < 9) {
-      const double *fp = a.fsE + ((a.nEl + e) * 4 + FA) * 81 + q * 9;
-#pragma unroll
-      for (int i = 0; i < 9; i++) fr[i] = T(__ldg(fp + i));
-    } else {
-      const double *fp = a.fsA + ((a.nEl + e) * 4 + FA) * 54 + (q - 9) * 9;
-#pragma unroll
-      for (int i = 0; i < 9; i++) fr[i] = T(__ldg(fp + i));
-    }
-    T s[F];
+  if (in.ty != FT_OUTFLOW) {
 #pragma unroll
     for (int j = 0; j < F; j++) {
-      T v = T(0);
+      T v = in.fr[0] * S0[j * 32 + l];
 #pragma unroll
-      for (int i = 0; i < 9; i++) v = fmaT(fr[i], S0[(i * F + j) * 32 + l], v);
+      for (int i = 1; i < 9; i++) v = fmaT(in.fr[i], S0[(i * F + j) * 32 + l], v);
       s[j] = v;
     }
     if (q < 9)
-      fluxTMul<O, FA, T>(s, acc);
+      FluxTMul<O, FA>::template run<T>(s, acc);
     else if constexpr (RM > 0)
-      fluxTMul<O, FA, T>(s, upA);
+      FluxTMul<O, FA>::template run<T>(s, upA);
   }
   __syncthreads();
 }
 
 template <typename T, int O, int R, int RM>
-__global__ void __launch_bounds__(Geo<T, O, R, RM>::NT) kNeigh(StepArgs<T> a) {
+__global__ void __launch_bounds__(Geo<T, O, R, RM>::NT, Geo<T, O, R, RM>::minCtasNeigh) kNeigh(StepArgs<T> a) {
   using G = Geo<T, O, R, RM>;
   constexpr int B = G::B, E = G::E;
   extern __shared__ __align__(16) unsigned char smem[];
@@ -502,6 +506,8 @@ __global__ void __launch_bounds__(Geo<T, O, R, RM>::NT) kNeigh(StepArgs<T> a) {
     const int64_t e = g * E + eo;
     const bool valid = e < a.nEl;
     const int64_t ev = valid ? e : 0;
+    FaceIn<T, O> in0, in1;
+    neighLoad<T, O, R, RM, 0>(a, q, ev, r, valid, in0);
     T acc[B];
     T upA[RM ? B : 1];
     if (q < 9) {
@@ -512,16 +518,20 @@ __global__ void __launch_bounds__(Geo<T, O, R, RM>::NT) kNeigh(StepArgs<T> a) {
 #pragma unroll
       for (int n = 0; n < B; n++) upA[n] = T(0);
     }
-    neighFace<T, O, R, RM, 0>(a, S0, q, l, ev, r, valid, acc, upA);
-    neighFace<T, O, R, RM, 1>(a, S0, q, l, ev, r, valid, acc, upA);
-    neighFace<T, O, R, RM, 2>(a, S0, q, l, ev, r, valid, acc, upA);
-    neighFace<T, O, R, RM, 3>(a, S0, q, l, ev, r, valid, acc, upA);
+    // faces in pairs of buffers: the next face's inputs load while this face computes
+    neighLoad<T, O, R, RM, 1>(a, q, ev, r, valid, in1);
+    neighFace<T, O, R, RM, 0>(S0, q, l, in0, acc, upA);
+    neighLoad<T, O, R, RM, 2>(a, q, ev, r, valid, in0);
+    neighFace<T, O, R, RM, 1>(S0, q, l, in1, acc, upA);
+    neighLoad<T, O, R, RM, 3>(a, q, ev, r, valid, in1);
+    neighFace<T, O, R, RM, 2>(S0, q, l, in0, acc, upA);
+    neighFace<T, O, R, RM, 3>(S0, q, l, in1, acc, upA);
     if (valid) {
       if (q < 9) {
         T *dst = a.dofsE + ((e * 9 + q) * B) * R + r;
 #pragma unroll
         for (int n = 0; n < B; n++) dst[n * R] = acc[n];
-      } else if (RM) {
+      } else if constexpr (RM > 0) {
         // scatterUpdateA (SurfInt.hpp:139-156)
         const int s = q - 9;
 #pragma unroll
@@ -552,73 +562,73 @@ struct RecvArgs {
   double *buf;             // [nRecv][maxBuf][9][R]
 };
 
+template <typename T, int O, int R, int RM, int D>
+__device__ __forceinline__ void recvAll(T *X, T *TI, T *XA, T *TIA, int q, int l, const ElemCoef<T, RM> &c,
+                                        const double *omega, T dt, T sca, const RecvArgs &rv, int i0, int i1,
+                                        bool valid, int r) {
+  constexpr int B = nModes(O);
+  // value[i][j][q][r] += tau_j^D / D! * sum_{n < B(O-D)} basis_i[n] der_D[q][n]  (CK modes only,
+  // even with anelasticity: TimePred.hpp:149)
+  if (q < 9 && valid) {
+    constexpr int NCK = nModes(O - D);
+    for (int i = i0; i < i1; i++) {
+      double dotv = 0;
+#pragma unroll
+      for (int n = 0; n < NCK; n++) dotv += rv.basis[i * B + n] * double(X[(q * B + n) * 32 + l]);
+      for (int j = 0; j < rv.nSamples; j++) {
+        double cf = 1.0;
+        for (int k = 1; k <= D; k++) cf *= rv.tau[j] / k;
+        double *o = rv.buf + ((int64_t(i) * rv.maxBuf + rv.slot[j]) * 9 + q) * R + r;
+        *o = (D == 0 ? 0.0 : *o) + cf * dotv;
+      }
+    }
+  }
+  if constexpr (D + 1 < O) {
+    sca = sca * dt / T(D + 2);
+    CkStep<T, O, R, RM, D + 1>::run(X, TI, XA, TIA, q, l, c, omega, sca);
+    recvAll<T, O, R, RM, D + 1>(X, TI, XA, TIA, q, l, c, omega, dt, sca, rv, i0, i1, valid, r);
+  }
+}
+
 template <typename T, int O, int R, int RM>
 __global__ void __launch_bounds__(Geo<T, O, R, RM>::NT) kRecv(StepArgs<T> a, RecvArgs rv) {
   using G = Geo<T, O, R, RM>;
   constexpr int B = G::B, E = G::E;
   extern __shared__ __align__(16) unsigned char smem[];
   T *X = reinterpret_cast<T *>(smem);
-  T *XA = X + G::smemX;
+  T *TI = X + G::nD;
+  T *XA = TI + G::nTI;
+  T *TIA = XA + G::nXA;
   const int q = threadIdx.x >> 5, l = threadIdx.x & 31;
   const int eo = l / R, r = l % R;
   const int64_t grp = int64_t(blockIdx.x) * E + eo;
   const bool valid = grp < rv.nGrp;
   const int64_t ev = valid ? rv.grpEl[grp] : 0;
   const T dt = T(a.dt);
-  T tI[B];
-  T tIA[RM ? RM : 1][B];
   if (q < 9) {
     const T *src = a.dofsE + ((ev * 9 + q) * B) * R + r;
 #pragma unroll
-    for (int n = 0; n < B; n++) X[(q * B + n) * 32 + l] = valid ? src[n * R] : T(0);
-  } else if (RM) {
+    for (int n = 0; n < B; n++) {
+      X[(q * B + n) * 32 + l] = valid ? src[n * R] : T(0);
+      TI[(q * B + n) * 32 + l] = T(0);
+    }
+  } else if constexpr (RM > 0) {
     const int s = q - 9;
 #pragma unroll
     for (int m = 0; m < RM; m++) {
       const T *src = a.dofsA + (((ev * RM + m) * 6 + s) * B) * R + r;
 #pragma unroll
-      for (int n = 0; n < B; n++) XA[((m * 6 + s) * B + n) * 32 + l] = valid ? src[n * R] : T(0);
+      for (int n = 0; n < B; n++) {
+        XA[((m * 6 + s) * B + n) * 32 + l] = valid ? src[n * R] : T(0);
+        TIA[((m * 6 + s) * B + n) * 32 + l] = T(0);
+      }
     }
   }
   ElemCoef<T, RM> c;
   c.load(a, ev, valid, q);
   __syncthreads();
-  // accumulate value[i][j][q][r] = sum_d tau_j^d / d! * sum_{n < B(O-d)} basis_i[n] der_d[q][n]
   const int i0 = valid ? rv.grpOff[grp] : 0, i1 = valid ? rv.grpOff[grp + 1] : 0;
-  auto addDerivative = [&](int d) {
-    if (q >= 9 || !valid) return;
-    const int nck = nModes(O - d);
-    for (int i = i0; i < i1; i++) {
-      double dotv = 0;
-      for (int n = 0; n < nck; n++) dotv += rv.basis[i * B + n] * double(X[(q * B + n) * 32 + l]);
-      for (int j = 0; j < rv.nSamples; j++) {
-        double cf = 1.0;
-        for (int k = 1; k <= d; k++) cf *= rv.tau[j] / k;
-        double *o = rv.buf + ((int64_t(i) * rv.maxBuf + rv.slot[j]) * 9 + q) * R + r;
-        *o = (d == 0 ? 0.0 : *o) + cf * dotv;
-      }
-    }
-  };
-  addDerivative(0);
-  T sca = dt;
-  // derivative by derivative; the CK step writes der[d] into X
-#define EDGE_RECV_STEP(D)                                                                              \
-  if constexpr (D < O) {                                                                              \
-    sca = sca * dt / T(D + 1);                                                                        \
-    CkStep<T, O, R, RM, D>::run(X, XA, q, l, c.cs, c.cols, c.ca, c.colsA, c.csrc, c.colsSrc, a.omega, \
-                                sca, tI, tIA);                                                        \
-    addDerivative(D);                                                                                 \
-    __syncthreads();                                                                                  \
-  }
-  for (int n = 0; n < B; n++) tI[n] = T(0);
-  for (int m = 0; m < (RM ? RM : 1); m++)
-    for (int n = 0; n < B; n++) tIA[m][n] = T(0);
-  EDGE_RECV_STEP(1)
-  EDGE_RECV_STEP(2)
-  EDGE_RECV_STEP(3)
-  EDGE_RECV_STEP(4)
-  EDGE_RECV_STEP(5)
-#undef EDGE_RECV_STEP
+  recvAll<T, O, R, RM, 0>(X, TI, XA, TIA, q, l, c, a.omega, dt, dt, rv, i0, i1, valid, r);
 }
 
 // ------------------------------------------------------------------------------------------------

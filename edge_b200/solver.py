@@ -62,6 +62,9 @@ class Solver:
         self._chk(lib().edge_b200_download_dofs(self._h, ptr(e), ptr(a)), "download_dofs")
         return e, a
 
+    def keep_tdofs(self, enable=True):
+        self._chk(lib().edge_b200_keep_tdofs(self._h, 1 if enable else 0), "keep_tdofs")
+
     def download_tdofs(self):
         p = self.prob
         t = np.zeros((p.n_el, 9, p.B, p.runs), self.dtype)

@@ -141,7 +141,10 @@ int edge_b200_upload_element_data(edge_b200_ctx *ctx, const double *star_e, cons
  * mechanisms. */
 int edge_b200_upload_dofs(edge_b200_ctx *ctx, const void *dofs_e, const void *dofs_a);
 int edge_b200_download_dofs(edge_b200_ctx *ctx, void *dofs_e, void *dofs_a);
-/* Time-integrated DOFs tDofs[nEl][9][B][R] of the last local step (the tDofs[0] of steps.inc). */
+/* Keep the time-integrated DOFs tDofs[nEl][9][B][R] of each local step (the tDofs[0] of
+ * steps.inc) in device memory (allocated on first enable; off by default, which saves their HBM
+ * writes), and copy the last step's to the host (EDGE_B200_EINVAL unless kept). */
+int edge_b200_keep_tdofs(edge_b200_ctx *ctx, int enable);
 int edge_b200_download_tdofs(edge_b200_ctx *ctx, void *tdofs);
 /* Point sources sorted by (element, run); source s adds
  *   int_t^{t+dt} series_s * scal[s][q] * b_eval[s][md]  to run run[s] of element el[s]

@@ -305,25 +305,32 @@ int oracle_step(int O, int R, int rm, long nEl, double t, double dt, const doubl
                 const double *srcTs, double tolTime) {
   const int B = nmodes(O);
   const size_t szE = (size_t)9 * B * R, szM = (size_t)6 * B * R;
+  int overflow = 0;
+  /* step 0: local (elements are independent; receivers of an element are found by bisection) */
+#pragma omp parallel reduction(| : overflow)
+  {
   double *der = malloc((size_t)O * szE * sizeof(double));
   double *tIntA = rm ? malloc((size_t)rm * szM * sizeof(double)) : NULL;
   double *pred = malloc(szE * sizeof(double));
-  double *upA = rm ? malloc(szM * sizeof(double)) : NULL;
-  int re = 0;
-  /* step 0: local */
+#pragma omp for schedule(dynamic, 16)
   for (long el = 0; el < nEl; el++) {
     double *dE = dofsE + el * szE, *dA = rm ? dofsA + el * rm * szM : NULL;
     double *tD = tDofs + el * szE;
     oracle_ck(O, R, rm, dt, stiffT, starE + el * 72, rm ? starA + el * 27 : NULL,
               rm ? srcA + el * 12 * rm : NULL, omega, dE, dA, der, tD, tIntA);
-    while (re < nRe && recvEl[re] < el) re++;
+    int lo = 0, hi = nRe;
+    while (lo < hi) {
+      int mid = (lo + hi) / 2;
+      if (recvEl[mid] < el) lo = mid + 1; else hi = mid;
+    }
+    const int re = lo;
     if (re < nRe && recvEl[re] == el) {
       for (;;) {
         double tr = recvTime[re];
         if (!(tr > t - tolTime && tr < t + dt - tolTime)) break;
         oracle_eval_pred(O, R, fabs(tr - t), der, pred);
         for (int r2 = re; r2 < nRe && recvEl[r2] == el; r2++) {
-          if (recvCount[r2] >= maxBuf) { free(der); free(tIntA); free(pred); free(upA); return -1; }
+          if (recvCount[r2] >= maxBuf) { overflow = 1; recvTime[re] = t + dt; break; }
           double *buf = recvBuf + ((size_t)r2 * maxBuf + recvCount[r2]) * 9 * R;
           for (int q = 0; q < 9; q++) {
             for (int r = 0; r < R; r++) buf[q * R + r] = 0;
@@ -342,6 +349,11 @@ int oracle_step(int O, int R, int rm, long nEl, double t, double dt, const doubl
     oracle_surf_local(O, R, rm, fluxL, fluxT, fsE + el * 4 * 81,
                       rm ? fsA + el * 4 * 54 : NULL, omega, tD, dE, dA);
   }
+  free(der);
+  free(tIntA);
+  free(pred);
+  }
+  if (overflow) return -1;
   /* step 1: point sources */
   for (int s = 0; s < nSrc; s++) {
     double in = oracle_series_int(srcDt[s], srcT0[s], srcNPts[s], srcTs + srcTsOff[s], t, t + dt,
@@ -356,6 +368,10 @@ int oracle_step(int O, int R, int rm, long nEl, double t, double dt, const doubl
   /* step 2: neighbour */
   const double *fsE1 = fsE + (size_t)nEl * 4 * 81;
   const double *fsA1 = rm ? fsA + (size_t)nEl * 4 * 54 : NULL;
+#pragma omp parallel
+  {
+  double *upA = rm ? malloc(szM * sizeof(double)) : NULL;
+#pragma omp for schedule(dynamic, 16)
   for (long el = 0; el < nEl; el++) {
     if (rm) memset(upA, 0, szM * sizeof(double));
     for (int f = 0; f < 4; f++) {
@@ -370,9 +386,7 @@ int oracle_step(int O, int R, int rm, long nEl, double t, double dt, const doubl
     }
     if (rm) scatter_upA(B, R, rm, omega, upA, dofsA + el * rm * szM);
   }
-  free(der);
-  free(tIntA);
-  free(pred);
   free(upA);
+  }
   return 0;
 }

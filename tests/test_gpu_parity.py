@@ -20,6 +20,7 @@ def _run_both(prob, precision, n_steps, dofs_seed=1, scale=1.0):
     e0, a0 = random_dofs(prob, seed=dofs_seed, scale=scale)
     orc = OracleRun(prob, e0, a0)
     s = Solver(prob, precision=precision)
+    s.keep_tdofs(True)
     s.upload_dofs(e0, a0)
     s.step(n_steps)
     orc.step(n_steps)
