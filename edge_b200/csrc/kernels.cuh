@@ -73,7 +73,14 @@ struct Geo {
   static constexpr size_t nD = size_t(9) * B * 32;
   static constexpr size_t nTI = size_t(9) * B * 32;
   static constexpr size_t nXA = size_t(RM) * 6 * B * 32;
-  static constexpr size_t smemLocal = (nD + nTI + 2 * nXA) * sizeof(T);
+  static constexpr size_t nS0 = size_t(9) * F * 32;
+  // the time integral lives in shared memory when that fits (227 KB per CTA); otherwise in
+  // registers during the recursion and in D afterwards, with the face tiles S0 behind D
+  // (the anelastic time integrals follow the same rule: registers, then the XA region)
+  static constexpr bool tiSmem = (nD + nTI + 2 * nXA) * sizeof(T) <= 227 * 1024;
+  static constexpr size_t nTIs = tiSmem ? nTI : nS0;
+  static constexpr size_t nTIA = tiSmem ? nXA : 0;
+  static constexpr size_t smemLocal = (nD + nTIs + nXA + nTIA) * sizeof(T);
   static constexpr size_t smemNeigh = size_t(9) * F * 32 * sizeof(T);
   // resident CTAs per SM the register allocation targets (65,536 registers per SM): FP32 keeps
   // two 288-thread CTAs of each kernel (<= 113 registers); FP64 rows need twice the registers
@@ -197,7 +204,7 @@ struct CkStep {
   static constexpr int DK = RM ? 1 : D;                           // truncation of the product
 
   __device__ __forceinline__ static void run(T *X, T *TI, T *XA, T *TIA, int q, int l, const ElemCoef<T, RM> &c,
-                                             const double *omega, T sca) {
+                                             const double *omega, T sca, T *tIr, T (*tIAr)[B]) {
     T acc[B];
 #pragma unroll
     for (int n = 0; n < B; n++) acc[n] = T(0);
@@ -226,8 +233,12 @@ struct CkStep {
 #pragma unroll
       for (int n = 0; n < NW; n++) {
         X[(q * B + n) * 32 + l] = acc[n];
-        T *t = &TI[(q * B + n) * 32 + l];
-        *t = fmaT(sca, acc[n], *t);
+        if constexpr (Geo<T, O, R, RM>::tiSmem) {
+          T *t = &TI[(q * B + n) * 32 + l];
+          *t = fmaT(sca, acc[n], *t);
+        } else {
+          tIr[n] = fmaT(sca, acc[n], tIr[n]);
+        }
       }
     } else if constexpr (RM > 0) {
       const int s = q - 9;
@@ -239,7 +250,10 @@ struct CkStep {
           const int i = ((m * 6 + s) * B + n) * 32 + l;
           const T v = om * (acc[n] + XA[i]);
           XA[i] = v;
-          TIA[i] = fmaT(sca, v, TIA[i]);
+          if constexpr (Geo<T, O, R, RM>::tiSmem)
+            TIA[i] = fmaT(sca, v, TIA[i]);
+          else
+            tIAr[m][n] = fmaT(sca, v, tIAr[m][n]);
         }
       }
     }
@@ -297,11 +311,11 @@ __device__ __forceinline__ void localFace(const StepArgs<T> &a, const T *TI, T *
 
 template <typename T, int O, int R, int RM, int D>
 __device__ __forceinline__ void ckAll(T *X, T *TI, T *XA, T *TIA, int q, int l, const ElemCoef<T, RM> &c,
-                                      const double *omega, T dt, T sca) {
+                                      const double *omega, T dt, T sca, T *tIr, T (*tIAr)[nModes(O)]) {
   if constexpr (D < O) {
     sca = sca * dt / T(D + 1);
-    CkStep<T, O, R, RM, D>::run(X, TI, XA, TIA, q, l, c, omega, sca);
-    ckAll<T, O, R, RM, D + 1>(X, TI, XA, TIA, q, l, c, omega, dt, sca);
+    CkStep<T, O, R, RM, D>::run(X, TI, XA, TIA, q, l, c, omega, sca, tIr, tIAr);
+    ckAll<T, O, R, RM, D + 1>(X, TI, XA, TIA, q, l, c, omega, dt, sca, tIr, tIAr);
   }
 }
 
@@ -311,10 +325,13 @@ __global__ void __launch_bounds__(Geo<T, O, R, RM>::NT, Geo<T, O, R, RM>::minCta
   constexpr int B = G::B, E = G::E;
   extern __shared__ __align__(16) unsigned char smem[];
   T *X = reinterpret_cast<T *>(smem);
-  T *TI = X + G::nD;
-  T *XA = TI + G::nTI;
-  T *TIA = XA + G::nXA;
-  T *S0 = X;  // the face tiles reuse the derivative buffer once the recursion is done
+  T *XA = X + G::nD + G::nTIs;
+  // shared-memory time integrals: TI behind D and TIA behind XA, face tiles reuse D after the
+  // recursion; register time integrals: copied into D and XA after the recursion, face tiles
+  // behind D
+  T *TI = G::tiSmem ? X + G::nD : X;
+  T *TIA = G::tiSmem ? XA + G::nXA : XA;
+  T *S0 = G::tiSmem ? X : X + G::nD;
   const int q = threadIdx.x >> 5, l = threadIdx.x & 31;
   const int eo = l / R, r = l % R;
   const int64_t nGroups = (a.nEl + E - 1) / E;
@@ -323,6 +340,8 @@ __global__ void __launch_bounds__(Geo<T, O, R, RM>::NT, Geo<T, O, R, RM>::minCta
     const int64_t e = g * E + eo;
     const bool valid = e < a.nEl;
     const int64_t ev = valid ? e : 0;
+    T tIr[G::tiSmem ? 1 : B];
+    T tIAr[(G::tiSmem || RM == 0) ? 1 : RM][B];
     // DOFs -> X, dt * DOFs -> TI (and the anelastic counterparts)
     if (q < 9) {
       const T *src = a.dofsE + ((ev * 9 + q) * B) * R + r;
@@ -330,7 +349,10 @@ __global__ void __launch_bounds__(Geo<T, O, R, RM>::NT, Geo<T, O, R, RM>::minCta
       for (int n = 0; n < B; n++) {
         const T v = valid ? src[n * R] : T(0);
         X[(q * B + n) * 32 + l] = v;
-        TI[(q * B + n) * 32 + l] = dt * v;
+        if constexpr (G::tiSmem)
+          TI[(q * B + n) * 32 + l] = dt * v;
+        else
+          tIr[n] = dt * v;
       }
     } else if constexpr (RM > 0) {
       const int s = q - 9;
@@ -342,7 +364,10 @@ __global__ void __launch_bounds__(Geo<T, O, R, RM>::NT, Geo<T, O, R, RM>::minCta
           const T v = valid ? src[n * R] : T(0);
           const int i = ((m * 6 + s) * B + n) * 32 + l;
           XA[i] = v;
-          TIA[i] = dt * v;
+          if constexpr (G::tiSmem)
+            TIA[i] = dt * v;
+          else
+            tIAr[m][n] = dt * v;
         }
       }
     }
@@ -350,7 +375,20 @@ __global__ void __launch_bounds__(Geo<T, O, R, RM>::NT, Geo<T, O, R, RM>::minCta
     c.load(a, ev, valid, q);
     __syncthreads();
     // Cauchy-Kowalevski (TimePredVanilla::ck, TimePredVanilla.hpp:200-306)
-    ckAll<T, O, R, RM, 1>(X, TI, XA, TIA, q, l, c, a.omega, dt, dt);
+    ckAll<T, O, R, RM, 1>(X, TI, XA, TIA, q, l, c, a.omega, dt, dt, tIr, tIAr);
+    if constexpr (!G::tiSmem) {
+      if (q < 9) {
+#pragma unroll
+        for (int n = 0; n < B; n++) X[(q * B + n) * 32 + l] = tIr[n];
+      } else if constexpr (RM > 0) {
+        const int s = q - 9;
+#pragma unroll
+        for (int m = 0; m < RM; m++)
+#pragma unroll
+          for (int n = 0; n < B; n++) XA[((m * 6 + s) * B + n) * 32 + l] = tIAr[m][n];
+      }
+      __syncthreads();
+    }
     if (a.tDofs && valid && q < 9) {
       T *dst = a.tDofs + ((e * 9 + q) * B) * R + r;
 #pragma unroll
@@ -565,7 +603,7 @@ struct RecvArgs {
 template <typename T, int O, int R, int RM, int D>
 __device__ __forceinline__ void recvAll(T *X, T *TI, T *XA, T *TIA, int q, int l, const ElemCoef<T, RM> &c,
                                         const double *omega, T dt, T sca, const RecvArgs &rv, int i0, int i1,
-                                        bool valid, int r) {
+                                        bool valid, int r, T *tIr, T (*tIAr)[nModes(O)]) {
   constexpr int B = nModes(O);
   // value[i][j][q][r] += tau_j^D / D! * sum_{n < B(O-D)} basis_i[n] der_D[q][n]  (CK modes only,
   // even with anelasticity: TimePred.hpp:149)
@@ -585,8 +623,8 @@ __device__ __forceinline__ void recvAll(T *X, T *TI, T *XA, T *TIA, int q, int l
   }
   if constexpr (D + 1 < O) {
     sca = sca * dt / T(D + 2);
-    CkStep<T, O, R, RM, D + 1>::run(X, TI, XA, TIA, q, l, c, omega, sca);
-    recvAll<T, O, R, RM, D + 1>(X, TI, XA, TIA, q, l, c, omega, dt, sca, rv, i0, i1, valid, r);
+    CkStep<T, O, R, RM, D + 1>::run(X, TI, XA, TIA, q, l, c, omega, sca, tIr, tIAr);
+    recvAll<T, O, R, RM, D + 1>(X, TI, XA, TIA, q, l, c, omega, dt, sca, rv, i0, i1, valid, r, tIr, tIAr);
   }
 }
 
@@ -596,21 +634,27 @@ __global__ void __launch_bounds__(Geo<T, O, R, RM>::NT) kRecv(StepArgs<T> a, Rec
   constexpr int B = G::B, E = G::E;
   extern __shared__ __align__(16) unsigned char smem[];
   T *X = reinterpret_cast<T *>(smem);
+  T *XA = X + G::nD + G::nTIs;
+  // time integrals are carried along but unused here (only the derivatives are sampled)
+  T *TIA = G::tiSmem ? XA + G::nXA : XA;
   T *TI = X + G::nD;
-  T *XA = TI + G::nTI;
-  T *TIA = XA + G::nXA;
   const int q = threadIdx.x >> 5, l = threadIdx.x & 31;
   const int eo = l / R, r = l % R;
   const int64_t grp = int64_t(blockIdx.x) * E + eo;
   const bool valid = grp < rv.nGrp;
   const int64_t ev = valid ? rv.grpEl[grp] : 0;
   const T dt = T(a.dt);
+  T tIr[G::tiSmem ? 1 : B];
+  T tIAr[(G::tiSmem || RM == 0) ? 1 : RM][B];
   if (q < 9) {
     const T *src = a.dofsE + ((ev * 9 + q) * B) * R + r;
 #pragma unroll
     for (int n = 0; n < B; n++) {
       X[(q * B + n) * 32 + l] = valid ? src[n * R] : T(0);
-      TI[(q * B + n) * 32 + l] = T(0);
+      if constexpr (G::tiSmem)
+        TI[(q * B + n) * 32 + l] = T(0);
+      else
+        tIr[n] = T(0);
     }
   } else if constexpr (RM > 0) {
     const int s = q - 9;
@@ -620,7 +664,10 @@ __global__ void __launch_bounds__(Geo<T, O, R, RM>::NT) kRecv(StepArgs<T> a, Rec
 #pragma unroll
       for (int n = 0; n < B; n++) {
         XA[((m * 6 + s) * B + n) * 32 + l] = valid ? src[n * R] : T(0);
-        TIA[((m * 6 + s) * B + n) * 32 + l] = T(0);
+        if constexpr (G::tiSmem)
+          TIA[((m * 6 + s) * B + n) * 32 + l] = T(0);
+        else
+          tIAr[m][n] = T(0);
       }
     }
   }
@@ -628,7 +675,7 @@ __global__ void __launch_bounds__(Geo<T, O, R, RM>::NT) kRecv(StepArgs<T> a, Rec
   c.load(a, ev, valid, q);
   __syncthreads();
   const int i0 = valid ? rv.grpOff[grp] : 0, i1 = valid ? rv.grpOff[grp + 1] : 0;
-  recvAll<T, O, R, RM, 0>(X, TI, XA, TIA, q, l, c, a.omega, dt, dt, rv, i0, i1, valid, r);
+  recvAll<T, O, R, RM, 0>(X, TI, XA, TIA, q, l, c, a.omega, dt, dt, rv, i0, i1, valid, r, tIr, tIAr);
 }
 
 // ------------------------------------------------------------------------------------------------
