@@ -60,39 +60,90 @@ __device__ __forceinline__ T ldd(const double *p, int i) {
 }
 
 // ------------------------------------------------------------------------------------------------
-// geometry of a CTA and its shared memory
+// shared-memory layout: one contiguous, padded row per (quantity, lane)
 // ------------------------------------------------------------------------------------------------
+// A tile [rows][32 lanes][S] keeps each lane's modes contiguous so a thread moves four modes with
+// one 128-bit access. S is padded so that the eight lanes of a 128-bit phase hit distinct bank
+// groups (S / (16 / sizeof(T)) odd) and rows can be read in groups of four past their end.
+template <typename T>
+__host__ __device__ constexpr int padRow(int n) {
+  const int w = 16 / int(sizeof(T));  // elements per 128-bit access
+  int m = (((n + 3) / 4) * 4 + w - 1) / w;
+  if (m % 2 == 0) m++;
+  return m * w;
+}
+
+template <typename T>
+__device__ __forceinline__ void ld4(const T *p, T (&v)[4]);
+template <>
+__device__ __forceinline__ void ld4<float>(const float *p, float (&v)[4]) {
+  const float4 t = *reinterpret_cast<const float4 *>(p);
+  v[0] = t.x; v[1] = t.y; v[2] = t.z; v[3] = t.w;
+}
+template <>
+__device__ __forceinline__ void ld4<double>(const double *p, double (&v)[4]) {
+  const double2 a = *reinterpret_cast<const double2 *>(p), b = *reinterpret_cast<const double2 *>(p + 2);
+  v[0] = a.x; v[1] = a.y; v[2] = b.x; v[3] = b.y;
+}
+template <typename T>
+__device__ __forceinline__ void st4(T *p, const T *v);
+template <>
+__device__ __forceinline__ void st4<float>(float *p, const float *v) {
+  *reinterpret_cast<float4 *>(p) = make_float4(v[0], v[1], v[2], v[3]);
+}
+template <>
+__device__ __forceinline__ void st4<double>(double *p, const double *v) {
+  *reinterpret_cast<double2 *>(p) = make_double2(v[0], v[1]);
+  *reinterpret_cast<double2 *>(p + 2) = make_double2(v[2], v[3]);
+}
+// v[0..N) -> row (128-bit stores, scalar tail)
+template <typename T, int N>
+__device__ __forceinline__ void stRow(T *p, const T *v) {
+#pragma unroll
+  for (int n = 0; n + 4 <= N; n += 4) st4<T>(p + n, v + n);
+#pragma unroll
+  for (int n = (N / 4) * 4; n < N; n++) p[n] = v[n];
+}
+template <typename T, int N>
+__device__ __forceinline__ void ldRow(const T *p, T *v) {
+#pragma unroll
+  for (int n = 0; n + 4 <= N; n += 4) {
+    T t[4];
+    ld4<T>(p + n, t);
+#pragma unroll
+    for (int i = 0; i < 4; i++) v[n + i] = t[i];
+  }
+#pragma unroll
+  for (int n = (N / 4) * 4; n < N; n++) v[n] = p[n];
+}
+
 template <typename T, int O, int R, int RM>
 struct Geo {
   static constexpr int B = nModes(O), F = nFaceModes(O), E = 32 / R;
   static constexpr int NW = 9 + (RM ? 6 : 0);
   static constexpr int NT = NW * 32;
-  // D [9][B][32]   derivatives during the CK recursion, then the face tiles S0 [9][F][32]
-  // TI [9][B][32]  time-integrated DOFs
-  // XA [RM][6][B][32], TIA [RM][6][B][32]  anelastic derivatives and time integrals
-  static constexpr size_t nD = size_t(9) * B * 32;
-  static constexpr size_t nTI = size_t(9) * B * 32;
-  static constexpr size_t nXA = size_t(RM) * 6 * B * 32;
-  static constexpr size_t nS0 = size_t(9) * F * 32;
-  // the time integral lives in shared memory when that fits (227 KB per CTA); otherwise in
-  // registers during the recursion and in D afterwards, with the face tiles S0 behind D
-  // (the anelastic time integrals follow the same rule: registers, then the XA region)
-  static constexpr bool tiSmem = (nD + nTI + 2 * nXA) * sizeof(T) <= 227 * 1024;
-  static constexpr size_t nTIs = tiSmem ? nTI : nS0;
+  static constexpr int SB = padRow<T>(B), SF = padRow<T>(F);
+  // X [9][32][SB]   derivatives during the CK recursion
+  // TI [9][32][SB]  time-integrated DOFs
+  // XA / TIA [RM][6][32][SB]  anelastic derivatives / time integrals
+  // S0 [9][32][SF]  face tiles
+  static constexpr size_t nX = size_t(9) * 32 * SB;
+  static constexpr size_t nXA = size_t(RM) * 6 * 32 * SB;
+  static constexpr size_t nS0 = size_t(9) * 32 * SF;
+  // The time integrals live in shared memory when that fits (227 KB per CTA); the face tiles
+  // then reuse X. Otherwise they stay in registers during the recursion and are copied into X /
+  // XA afterwards, with the face tiles behind X.
+  static constexpr bool tiSmem = (2 * nX + 2 * nXA) * sizeof(T) <= 227 * 1024;
+  static constexpr size_t nTI = tiSmem ? nX : nS0;
   static constexpr size_t nTIA = tiSmem ? nXA : 0;
-  static constexpr size_t smemLocal = (nD + nTIs + nXA + nTIA) * sizeof(T);
-  static constexpr size_t smemNeigh = size_t(9) * F * 32 * sizeof(T);
+  static constexpr size_t smemLocal = (nX + nTI + nXA + nTIA) * sizeof(T);
+  static constexpr size_t smemNeigh = nS0 * sizeof(T);
   // resident CTAs per SM the register allocation targets (65,536 registers per SM): FP32 keeps
   // two 288-thread CTAs of each kernel (<= 113 registers); FP64 rows need twice the registers
   // and keep one
   static constexpr int minCtasLocal = (sizeof(T) == 4 && RM == 0 && smemLocal <= 110 * 1024) ? 2 : 1;
-  static constexpr int minCtasNeigh = sizeof(T) == 4 ? 2 : 1;
+  static constexpr int minCtasNeigh = (sizeof(T) == 4 && RM == 0) ? 2 : 1;
 };
-
-template <typename T>
-__device__ __forceinline__ T sm(const T *p, int row, int k, int B, int l) {
-  return p[(row * B + k) * 32 + l];
-}
 
 // per-thread element coefficients
 template <typename T, int RM>
@@ -148,48 +199,68 @@ struct ElemCoef {
   }
 };
 
-// star mix of one reference direction: z(k) = sum_i c[i] * X[col_i][k][l]
-template <typename T, int B>
-struct StarMix {
-  const T *X;
-  int l;
-  int c0, c1, c2;
-  T a0, a1, a2;
-  __device__ __forceinline__ T operator()(int k) const {
-    T v = a0 * X[(c0 * B + k) * 32 + l];
-    v = fmaT(a1, X[(c1 * B + k) * 32 + l], v);
-    return fmaT(a2, X[(c2 * B + k) * 32 + l], v);
+// operand of the stiffness products: star mix of three source rows, shared by the three directions
+// zz[dim][i] = sum_s c[dim][s] * X[col_s][l][k0 + i]
+template <typename T, int S>
+struct Mix3 {
+  const T *r0, *r1, *r2;  // source rows of this lane
+  const T (*c)[3];
+  template <int K0>
+  __device__ __forceinline__ void load(T (&zz)[3][4]) const {
+    T v0[4], v1[4], v2[4];
+    ld4<T>(r0 + K0, v0);
+    ld4<T>(r1 + K0, v1);
+    ld4<T>(r2 + K0, v2);
+#pragma unroll
+    for (int d = 0; d < 3; d++)
+#pragma unroll
+      for (int i = 0; i < 4; i++) zz[d][i] = fmaT(c[d][2], v2[i], fmaT(c[d][1], v1[i], c[d][0] * v0[i]));
   }
 };
-template <typename T, int B>
-struct StarMixA {  // anelastic star: two velocity columns
-  const T *X;
-  int l;
-  int c0, c1;
-  T a0, a1;
-  __device__ __forceinline__ T operator()(int k) const {
-    T v = a0 * X[((6 + c0) * B + k) * 32 + l];
-    return fmaT(a1, X[((6 + c1) * B + k) * 32 + l], v);
+// anelastic star: two velocity rows
+template <typename T, int S>
+struct Mix2 {
+  const T *r0, *r1;
+  const T (*c)[2];
+  template <int K0>
+  __device__ __forceinline__ void load(T (&zz)[3][4]) const {
+    T v0[4], v1[4];
+    ld4<T>(r0 + K0, v0);
+    ld4<T>(r1 + K0, v1);
+#pragma unroll
+    for (int d = 0; d < 3; d++)
+#pragma unroll
+      for (int i = 0; i < 4; i++) zz[d][i] = fmaT(c[d][1], v1[i], c[d][0] * v0[i]);
   }
 };
-template <typename T, int B>
-struct RowRead {  // z(k) = X[row][k][l]
-  const T *X;
-  int row, l;
-  __device__ __forceinline__ T operator()(int k) const { return X[(row * B + k) * 32 + l]; }
+// the thread's own row
+template <typename T>
+struct OwnRow {
+  const T *r;
+  template <int K0>
+  __device__ __forceinline__ void load(T (&zz)[1][4]) const { ld4<T>(r + K0, zz[0]); }
 };
 
+template <typename T, int S>
+__device__ __forceinline__ const T *rowPtr(const T *base, int row, int l) {
+  return base + (row * 32 + l) * S;
+}
+template <typename T, int S>
+__device__ __forceinline__ T *rowPtr(T *base, int row, int l) {
+  return base + (row * 32 + l) * S;
+}
+
 // dofs rows 0..5 += sum_m srcA_m * Y_m (anelastic source matrices, all B modes)
-template <typename T, int B, int RM>
+template <typename T, int B, int S, int RM>
 __device__ __forceinline__ void addSrc(const ElemCoef<T, RM> &c, const T *Y, int l, T *acc) {
 #pragma unroll
   for (int m = 0; m < RM; m++)
 #pragma unroll
-    for (int n = 0; n < B; n++) {
-      T v = acc[n];
+    for (int i = 0; i < 3; i++) {
+      T y[B];
+      ldRow<T, B>(rowPtr<T, S>(Y, m * 6 + c.colsSrc[i], l), y);
 #pragma unroll
-      for (int i = 0; i < 3; i++) v = fmaT(c.csrc[m][i], Y[((m * 6 + c.colsSrc[i]) * B + n) * 32 + l], v);
-      acc[n] = v;
+      for (int n = 0; n < B; n++) acc[n] = fmaT(c.csrc[m][i], y[n], acc[n]);
     }
 }
 
@@ -199,7 +270,8 @@ __device__ __forceinline__ void addSrc(const ElemCoef<T, RM> &c, const T *Y, int
 // their warp), the anelastic warps update XA and TIA.
 template <typename T, int O, int R, int RM, int D>
 struct CkStep {
-  static constexpr int B = nModes(O);
+  using G = Geo<T, O, R, RM>;
+  static constexpr int B = G::B, S = G::SB;
   static constexpr int NN = RM ? nModes(O - 1) : nModes(O - D);  // output modes of the product
   static constexpr int DK = RM ? 1 : D;                           // truncation of the product
 
@@ -209,57 +281,89 @@ struct CkStep {
 #pragma unroll
     for (int n = 0; n < B; n++) acc[n] = T(0);
     if (q < 9) {
-#pragma unroll
-      for (int dim = 0; dim < 3; dim++) {
-        StarMix<T, B> z{X, l, c.cols[0], c.cols[1], c.cols[2], c.cs[dim][0], c.cs[dim][1], c.cs[dim][2]};
-        if (dim == 0) CkMul<O, DK, 0>::template run<T>(z, acc);
-        if (dim == 1) CkMul<O, DK, 1>::template run<T>(z, acc);
-        if (dim == 2) CkMul<O, DK, 2>::template run<T>(z, acc);
-      }
+      Mix3<T, S> z{rowPtr<T, S>(X, c.cols[0], l), rowPtr<T, S>(X, c.cols[1], l), rowPtr<T, S>(X, c.cols[2], l),
+                   c.cs};
+      CkMul<O, DK>::template run<T>(z, acc);
       if constexpr (RM > 0)
-        if (q < 6) addSrc<T, B, RM>(c, XA, l, acc);
+        if (q < 6) addSrc<T, B, S, RM>(c, XA, l, acc);
     } else if constexpr (RM > 0) {
-#pragma unroll
-      for (int dim = 0; dim < 3; dim++) {
-        StarMixA<T, B> z{X, l, c.colsA[0], c.colsA[1], c.ca[dim][0], c.ca[dim][1]};
-        if (dim == 0) CkMul<O, DK, 0>::template run<T>(z, acc);
-        if (dim == 1) CkMul<O, DK, 1>::template run<T>(z, acc);
-        if (dim == 2) CkMul<O, DK, 2>::template run<T>(z, acc);
-      }
+      Mix2<T, S> z{rowPtr<T, S>(X, 6 + c.colsA[0], l), rowPtr<T, S>(X, 6 + c.colsA[1], l), c.ca};
+      CkMul<O, DK>::template run<T>(z, acc);
     }
     __syncthreads();
     if (q < 9) {
       constexpr int NW = RM ? B : NN;  // modes beyond NN stay zero without anelasticity
+      stRow<T, NW>(rowPtr<T, S>(X, q, l), acc);
+      if constexpr (G::tiSmem) {
+        T t[NW];
+        T *p = rowPtr<T, S>(TI, q, l);
+        ldRow<T, NW>(p, t);
 #pragma unroll
-      for (int n = 0; n < NW; n++) {
-        X[(q * B + n) * 32 + l] = acc[n];
-        if constexpr (Geo<T, O, R, RM>::tiSmem) {
-          T *t = &TI[(q * B + n) * 32 + l];
-          *t = fmaT(sca, acc[n], *t);
-        } else {
-          tIr[n] = fmaT(sca, acc[n], tIr[n]);
-        }
+        for (int n = 0; n < NW; n++) t[n] = fmaT(sca, acc[n], t[n]);
+        stRow<T, NW>(p, t);
+      } else {
+#pragma unroll
+        for (int n = 0; n < NW; n++) tIr[n] = fmaT(sca, acc[n], tIr[n]);
       }
     } else if constexpr (RM > 0) {
       const int s = q - 9;
 #pragma unroll
       for (int m = 0; m < RM; m++) {
         const T om = T(omega[m]);
+        T *px = rowPtr<T, S>(XA, m * 6 + s, l);
+        T v[B];
+        ldRow<T, B>(px, v);
 #pragma unroll
-        for (int n = 0; n < B; n++) {
-          const int i = ((m * 6 + s) * B + n) * 32 + l;
-          const T v = om * (acc[n] + XA[i]);
-          XA[i] = v;
-          if constexpr (Geo<T, O, R, RM>::tiSmem)
-            TIA[i] = fmaT(sca, v, TIA[i]);
-          else
-            tIAr[m][n] = fmaT(sca, v, tIAr[m][n]);
+        for (int n = 0; n < B; n++) v[n] = om * (acc[n] + v[n]);
+        stRow<T, B>(px, v);
+        if constexpr (G::tiSmem) {
+          T *pt = rowPtr<T, S>(TIA, m * 6 + s, l);
+          T t[B];
+          ldRow<T, B>(pt, t);
+#pragma unroll
+          for (int n = 0; n < B; n++) t[n] = fmaT(sca, v[n], t[n]);
+          stRow<T, B>(pt, t);
+        } else {
+#pragma unroll
+          for (int n = 0; n < B; n++) tIAr[m][n] = fmaT(sca, v[n], tIAr[m][n]);
         }
       }
     }
     __syncthreads();
   }
 };
+
+template <typename T, int O, int R, int RM, int D>
+__device__ __forceinline__ void ckAll(T *X, T *TI, T *XA, T *TIA, int q, int l, const ElemCoef<T, RM> &c,
+                                      const double *omega, T dt, T sca, T *tIr, T (*tIAr)[nModes(O)]) {
+  if constexpr (D < O) {
+    sca = sca * dt / T(D + 1);
+    CkStep<T, O, R, RM, D>::run(X, TI, XA, TIA, q, l, c, omega, sca, tIr, tIAr);
+    ckAll<T, O, R, RM, D + 1>(X, TI, XA, TIA, q, l, c, omega, dt, sca, tIr, tIAr);
+  }
+}
+
+// s1[j] = sum_i fr[i] * S0[i][l][j] for j < F (128-bit loads over j)
+template <typename T, int F, int SF>
+__device__ __forceinline__ void faceMix(const T *S0, int l, const T (&fr)[9], T *s) {
+#pragma unroll
+  for (int j0 = 0; j0 < F; j0 += 4) {
+    T v[4];
+    ld4<T>(rowPtr<T, SF>(S0, 0, l) + j0, v);
+    T o[4];
+#pragma unroll
+    for (int u = 0; u < 4; u++) o[u] = fr[0] * v[u];
+#pragma unroll
+    for (int i = 1; i < 9; i++) {
+      ld4<T>(rowPtr<T, SF>(S0, i, l) + j0, v);
+#pragma unroll
+      for (int u = 0; u < 4; u++) o[u] = fmaT(fr[i], v[u], o[u]);
+    }
+#pragma unroll
+    for (int u = 0; u < 4; u++)
+      if (j0 + u < F) s[j0 + u] = o[u];
+  }
+}
 
 // ------------------------------------------------------------------------------------------------
 // local step: CK, volume, local surface, face projections (AderDg::local, AderDg.hpp:338-534)
@@ -268,14 +372,13 @@ template <typename T, int O, int R, int RM, int FA>
 __device__ __forceinline__ void localFace(const StepArgs<T> &a, const T *TI, T *S0, int q, int l, int64_t e,
                                           int r, bool valid, T *acc, T *upA) {
   using G = Geo<T, O, R, RM>;
-  constexpr int B = G::B, F = G::F;
+  constexpr int F = G::F, SF = G::SF, SB = G::SB;
   T s[F];
   if (q < 9) {
 #pragma unroll
     for (int j = 0; j < F; j++) s[j] = T(0);
-    FluxLMul<O, FA>::template run<T>(RowRead<T, B>{TI, q, l}, s);
-#pragma unroll
-    for (int j = 0; j < F; j++) S0[(q * F + j) * 32 + l] = s[j];
+    FluxLMul<O, FA>::template run<T>(OwnRow<T>{rowPtr<T, SB>(TI, q, l)}, s);
+    stRow<T, F>(rowPtr<T, SF>(S0, q, l), s);
     if (valid) {
       T *fb = a.face + ((((e * 4 + FA) * 9 + q) * F) * R) + r;
 #pragma unroll
@@ -294,14 +397,7 @@ __device__ __forceinline__ void localFace(const StepArgs<T> &a, const T *TI, T *
     for (int i = 0; i < 9; i++) fr[i] = valid ? T(__ldg(fp + i)) : T(0);
   }
   __syncthreads();
-  // s1[j] = sum_q' fs[q][q'] * S0[q'][j]
-#pragma unroll
-  for (int j = 0; j < F; j++) {
-    T v = fr[0] * S0[j * 32 + l];
-#pragma unroll
-    for (int i = 1; i < 9; i++) v = fmaT(fr[i], S0[(i * F + j) * 32 + l], v);
-    s[j] = v;
-  }
+  faceMix<T, F, SF>(S0, l, fr, s);
   if (q < 9)
     FluxTMul<O, FA>::template run<T>(s, acc);
   else if constexpr (RM > 0)
@@ -309,29 +405,18 @@ __device__ __forceinline__ void localFace(const StepArgs<T> &a, const T *TI, T *
   __syncthreads();
 }
 
-template <typename T, int O, int R, int RM, int D>
-__device__ __forceinline__ void ckAll(T *X, T *TI, T *XA, T *TIA, int q, int l, const ElemCoef<T, RM> &c,
-                                      const double *omega, T dt, T sca, T *tIr, T (*tIAr)[nModes(O)]) {
-  if constexpr (D < O) {
-    sca = sca * dt / T(D + 1);
-    CkStep<T, O, R, RM, D>::run(X, TI, XA, TIA, q, l, c, omega, sca, tIr, tIAr);
-    ckAll<T, O, R, RM, D + 1>(X, TI, XA, TIA, q, l, c, omega, dt, sca, tIr, tIAr);
-  }
-}
-
 template <typename T, int O, int R, int RM>
 __global__ void __launch_bounds__(Geo<T, O, R, RM>::NT, Geo<T, O, R, RM>::minCtasLocal) kLocal(StepArgs<T> a) {
   using G = Geo<T, O, R, RM>;
-  constexpr int B = G::B, E = G::E;
+  constexpr int B = G::B, E = G::E, SB = G::SB;
   extern __shared__ __align__(16) unsigned char smem[];
   T *X = reinterpret_cast<T *>(smem);
-  T *XA = X + G::nD + G::nTIs;
-  // shared-memory time integrals: TI behind D and TIA behind XA, face tiles reuse D after the
-  // recursion; register time integrals: copied into D and XA after the recursion, face tiles
-  // behind D
-  T *TI = G::tiSmem ? X + G::nD : X;
+  T *XA = X + G::nX + G::nTI;
+  // see Geo: time integrals in shared memory (TI behind X, TIA behind XA, face tiles reuse X) or
+  // in registers (copied into X / XA after the recursion, face tiles behind X)
+  T *TI = G::tiSmem ? X + G::nX : X;
   T *TIA = G::tiSmem ? XA + G::nXA : XA;
-  T *S0 = G::tiSmem ? X : X + G::nD;
+  T *S0 = G::tiSmem ? X : X + G::nX;
   const int q = threadIdx.x >> 5, l = threadIdx.x & 31;
   const int eo = l / R, r = l % R;
   const int64_t nGroups = (a.nEl + E - 1) / E;
@@ -345,29 +430,34 @@ __global__ void __launch_bounds__(Geo<T, O, R, RM>::NT, Geo<T, O, R, RM>::minCta
     // DOFs -> X, dt * DOFs -> TI (and the anelastic counterparts)
     if (q < 9) {
       const T *src = a.dofsE + ((ev * 9 + q) * B) * R + r;
+      T v[B];
 #pragma unroll
-      for (int n = 0; n < B; n++) {
-        const T v = valid ? src[n * R] : T(0);
-        X[(q * B + n) * 32 + l] = v;
-        if constexpr (G::tiSmem)
-          TI[(q * B + n) * 32 + l] = dt * v;
-        else
-          tIr[n] = dt * v;
+      for (int n = 0; n < B; n++) v[n] = valid ? src[n * R] : T(0);
+      stRow<T, B>(rowPtr<T, SB>(X, q, l), v);
+#pragma unroll
+      for (int n = 0; n < B; n++) v[n] = dt * v[n];
+      if constexpr (G::tiSmem)
+        stRow<T, B>(rowPtr<T, SB>(TI, q, l), v);
+      else {
+#pragma unroll
+        for (int n = 0; n < B; n++) tIr[n] = v[n];
       }
     } else if constexpr (RM > 0) {
       const int s = q - 9;
 #pragma unroll
       for (int m = 0; m < RM; m++) {
         const T *src = a.dofsA + (((ev * RM + m) * 6 + s) * B) * R + r;
+        T v[B];
 #pragma unroll
-        for (int n = 0; n < B; n++) {
-          const T v = valid ? src[n * R] : T(0);
-          const int i = ((m * 6 + s) * B + n) * 32 + l;
-          XA[i] = v;
-          if constexpr (G::tiSmem)
-            TIA[i] = dt * v;
-          else
-            tIAr[m][n] = dt * v;
+        for (int n = 0; n < B; n++) v[n] = valid ? src[n * R] : T(0);
+        stRow<T, B>(rowPtr<T, SB>(XA, m * 6 + s, l), v);
+#pragma unroll
+        for (int n = 0; n < B; n++) v[n] = dt * v[n];
+        if constexpr (G::tiSmem)
+          stRow<T, B>(rowPtr<T, SB>(TIA, m * 6 + s, l), v);
+        else {
+#pragma unroll
+          for (int n = 0; n < B; n++) tIAr[m][n] = v[n];
         }
       }
     }
@@ -378,21 +468,20 @@ __global__ void __launch_bounds__(Geo<T, O, R, RM>::NT, Geo<T, O, R, RM>::minCta
     ckAll<T, O, R, RM, 1>(X, TI, XA, TIA, q, l, c, a.omega, dt, dt, tIr, tIAr);
     if constexpr (!G::tiSmem) {
       if (q < 9) {
-#pragma unroll
-        for (int n = 0; n < B; n++) X[(q * B + n) * 32 + l] = tIr[n];
+        stRow<T, B>(rowPtr<T, SB>(X, q, l), tIr);
       } else if constexpr (RM > 0) {
         const int s = q - 9;
 #pragma unroll
-        for (int m = 0; m < RM; m++)
-#pragma unroll
-          for (int n = 0; n < B; n++) XA[((m * 6 + s) * B + n) * 32 + l] = tIAr[m][n];
+        for (int m = 0; m < RM; m++) stRow<T, B>(rowPtr<T, SB>(XA, m * 6 + s, l), tIAr[m]);
       }
       __syncthreads();
     }
     if (a.tDofs && valid && q < 9) {
+      T t[B];
+      ldRow<T, B>(rowPtr<T, SB>(TI, q, l), t);
       T *dst = a.tDofs + ((e * 9 + q) * B) * R + r;
 #pragma unroll
-      for (int n = 0; n < B; n++) dst[n * R] = TI[(q * B + n) * 32 + l];
+      for (int n = 0; n < B; n++) dst[n * R] = t[n];
     }
     // volume integral (VolIntVanilla::apply, VolIntVanilla.hpp:189-241)
     T acc[B];
@@ -401,28 +490,19 @@ __global__ void __launch_bounds__(Geo<T, O, R, RM>::NT, Geo<T, O, R, RM>::minCta
       const T *src = a.dofsE + ((ev * 9 + q) * B) * R + r;
 #pragma unroll
       for (int n = 0; n < B; n++) acc[n] = valid ? src[n * R] : T(0);
-#pragma unroll
-      for (int dim = 0; dim < 3; dim++) {
-        StarMix<T, B> z{TI, l, c.cols[0], c.cols[1], c.cols[2], c.cs[dim][0], c.cs[dim][1], c.cs[dim][2]};
-        if (dim == 0) VolMul<O, 0>::template run<T>(z, acc);
-        if (dim == 1) VolMul<O, 1>::template run<T>(z, acc);
-        if (dim == 2) VolMul<O, 2>::template run<T>(z, acc);
-      }
+      Mix3<T, SB> z{rowPtr<T, SB>(TI, c.cols[0], l), rowPtr<T, SB>(TI, c.cols[1], l),
+                    rowPtr<T, SB>(TI, c.cols[2], l), c.cs};
+      VolMul<O>::template run<T>(z, acc);
       if constexpr (RM > 0)
-        if (q < 6) addSrc<T, B, RM>(c, TIA, l, acc);
+        if (q < 6) addSrc<T, B, SB, RM>(c, TIA, l, acc);
     } else if constexpr (RM > 0) {
 #pragma unroll
       for (int n = 0; n < B; n++) {
         acc[n] = T(0);
         upA[n] = T(0);
       }
-#pragma unroll
-      for (int dim = 0; dim < 3; dim++) {
-        StarMixA<T, B> z{TI, l, c.colsA[0], c.colsA[1], c.ca[dim][0], c.ca[dim][1]};
-        if (dim == 0) VolMul<O, 0>::template run<T>(z, acc);
-        if (dim == 1) VolMul<O, 1>::template run<T>(z, acc);
-        if (dim == 2) VolMul<O, 2>::template run<T>(z, acc);
-      }
+      Mix2<T, SB> z{rowPtr<T, SB>(TI, 6 + c.colsA[0], l), rowPtr<T, SB>(TI, 6 + c.colsA[1], l), c.ca};
+      VolMul<O>::template run<T>(z, acc);
     }
     // local surface integral (SurfIntVanilla::local, SurfIntVanilla.hpp:212-262) + face projections
     localFace<T, O, R, RM, 0>(a, TI, S0, q, l, ev, r, valid, acc, upA);
@@ -440,11 +520,13 @@ __global__ void __launch_bounds__(Geo<T, O, R, RM>::NT, Geo<T, O, R, RM>::minCta
 #pragma unroll
         for (int m = 0; m < RM; m++) {
           const T om = T(a.omega[m]);
+          T ti[B];
+          ldRow<T, B>(rowPtr<T, SB>(TIA, m * 6 + s, l), ti);
           T *dst = a.dofsA + (((e * RM + m) * 6 + s) * B) * R + r;
 #pragma unroll
           for (int n = 0; n < B; n++) {
             T v = dst[n * R];
-            v = fmaT(om, acc[n] - TIA[((m * 6 + s) * B + n) * 32 + l], v);
+            v = fmaT(om, acc[n] - ti[n], v);
             v = fmaT(om, upA[n], v);
             dst[n * R] = v;
           }
@@ -457,72 +539,49 @@ __global__ void __launch_bounds__(Geo<T, O, R, RM>::NT, Geo<T, O, R, RM>::minCta
 // ------------------------------------------------------------------------------------------------
 // neighbour step (AderDg::neigh, AderDg.hpp:553-722)
 // ------------------------------------------------------------------------------------------------
-template <typename T, int O>
-struct FaceIn {  // one face's inputs for one thread, loaded ahead of its use
-  T x[nFaceModes(O)];
-  T fr[9];
-  int ty, v;
-};
-
 template <typename T, int O, int R, int RM, int FA>
-__device__ __forceinline__ void neighLoad(const StepArgs<T> &a, int q, int64_t e, int r, bool valid,
-                                          FaceIn<T, O> &in) {
-  constexpr int F = nFaceModes(O);
-  in.ty = valid ? a.faType[e * 4 + FA] : FT_OUTFLOW;
-  in.v = 0;
+__device__ __forceinline__ void neighFace(const StepArgs<T> &a, T *S0, int q, int l, int64_t e, int r,
+                                          bool valid, T *acc, T *upA) {
+  using G = Geo<T, O, R, RM>;
+  constexpr int F = G::F, SF = G::SF;
+  const int ty = valid ? a.faType[e * 4 + FA] : FT_OUTFLOW;
+  T fr[9];
   if (q < 9) {
-    const T *fb = nullptr;
-    if (in.ty == FT_FREE) {
-      // own face projection with the local flux matrix; the mirror is in fsE[1]
-      fb = a.face + ((((e * 4 + FA) * 9 + q) * F) * R) + r;
-    } else if (in.ty == FT_INNER) {
-      const int64_t ne = a.elFaEl[e * 4 + FA];
-      const int fo = a.fId[e * 4 + FA];
-      in.v = a.vId[e * 4 + FA];
-      fb = a.face + ((((ne * 4 + fo) * 9 + q) * F) * R) + r;
-    }
+    T s[F];
 #pragma unroll
-    for (int j = 0; j < F; j++) in.x[j] = fb ? fb[j * R] : T(0);
+    for (int j = 0; j < F; j++) s[j] = T(0);
+    if (ty == FT_FREE) {
+      // own face projection with the local flux matrix; the mirror is in fsE[1]
+      const T *fb = a.face + ((((e * 4 + FA) * 9 + q) * F) * R) + r;
+#pragma unroll
+      for (int j = 0; j < F; j++) s[j] = fb[j * R];
+    } else if (ty == FT_INNER) {
+      const int64_t ne = a.elFaEl[e * 4 + FA];
+      const int fo = a.fId[e * 4 + FA], v = a.vId[e * 4 + FA];
+      const T *fb = a.face + ((((ne * 4 + fo) * 9 + q) * F) * R) + r;
+      T x[F];
+#pragma unroll
+      for (int j = 0; j < F; j++) x[j] = fb[j * R];
+      if (v == 0)
+        OriMul<O, 0>::template run<T>(x, s);
+      else if (v == 1)
+        OriMul<O, 1>::template run<T>(x, s);
+      else
+        OriMul<O, 2>::template run<T>(x, s);
+    }
+    stRow<T, F>(rowPtr<T, SF>(S0, q, l), s);
     const double *fp = a.fsE + ((a.nEl + e) * 4 + FA) * 81 + q * 9;
 #pragma unroll
-    for (int i = 0; i < 9; i++) in.fr[i] = in.ty != FT_OUTFLOW ? T(__ldg(fp + i)) : T(0);
+    for (int i = 0; i < 9; i++) fr[i] = ty != FT_OUTFLOW ? T(__ldg(fp + i)) : T(0);
   } else if constexpr (RM > 0) {
     const double *fp = a.fsA + ((a.nEl + e) * 4 + FA) * 54 + (q - 9) * 9;
 #pragma unroll
-    for (int i = 0; i < 9; i++) in.fr[i] = in.ty != FT_OUTFLOW ? T(__ldg(fp + i)) : T(0);
-  }
-}
-
-template <typename T, int O, int R, int RM, int FA>
-__device__ __forceinline__ void neighFace(T *S0, int q, int l, const FaceIn<T, O> &in, T *acc, T *upA) {
-  constexpr int F = nFaceModes(O);
-  T s[F];
-  if (q < 9) {
-#pragma unroll
-    for (int j = 0; j < F; j++) s[j] = T(0);
-    if (in.ty == FT_FREE) {
-#pragma unroll
-      for (int j = 0; j < F; j++) s[j] = in.x[j];
-    } else if (in.ty == FT_INNER) {
-      if (in.v == 0)
-        OriMul<O, 0>::template run<T>(in.x, s);
-      else if (in.v == 1)
-        OriMul<O, 1>::template run<T>(in.x, s);
-      else
-        OriMul<O, 2>::template run<T>(in.x, s);
-    }
-#pragma unroll
-    for (int j = 0; j < F; j++) S0[(q * F + j) * 32 + l] = s[j];
+    for (int i = 0; i < 9; i++) fr[i] = ty != FT_OUTFLOW ? T(__ldg(fp + i)) : T(0);
   }
   __syncthreads();
-  if (in.ty != FT_OUTFLOW) {
-#pragma unroll
-    for (int j = 0; j < F; j++) {
-      T v = in.fr[0] * S0[j * 32 + l];
-#pragma unroll
-      for (int i = 1; i < 9; i++) v = fmaT(in.fr[i], S0[(i * F + j) * 32 + l], v);
-      s[j] = v;
-    }
+  if (ty != FT_OUTFLOW) {
+    T s[F];
+    faceMix<T, F, SF>(S0, l, fr, s);
     if (q < 9)
       FluxTMul<O, FA>::template run<T>(s, acc);
     else if constexpr (RM > 0)
@@ -544,8 +603,6 @@ __global__ void __launch_bounds__(Geo<T, O, R, RM>::NT, Geo<T, O, R, RM>::minCta
     const int64_t e = g * E + eo;
     const bool valid = e < a.nEl;
     const int64_t ev = valid ? e : 0;
-    FaceIn<T, O> in0, in1;
-    neighLoad<T, O, R, RM, 0>(a, q, ev, r, valid, in0);
     T acc[B];
     T upA[RM ? B : 1];
     if (q < 9) {
@@ -556,14 +613,10 @@ __global__ void __launch_bounds__(Geo<T, O, R, RM>::NT, Geo<T, O, R, RM>::minCta
 #pragma unroll
       for (int n = 0; n < B; n++) upA[n] = T(0);
     }
-    // faces in pairs of buffers: the next face's inputs load while this face computes
-    neighLoad<T, O, R, RM, 1>(a, q, ev, r, valid, in1);
-    neighFace<T, O, R, RM, 0>(S0, q, l, in0, acc, upA);
-    neighLoad<T, O, R, RM, 2>(a, q, ev, r, valid, in0);
-    neighFace<T, O, R, RM, 1>(S0, q, l, in1, acc, upA);
-    neighLoad<T, O, R, RM, 3>(a, q, ev, r, valid, in1);
-    neighFace<T, O, R, RM, 2>(S0, q, l, in0, acc, upA);
-    neighFace<T, O, R, RM, 3>(S0, q, l, in1, acc, upA);
+    neighFace<T, O, R, RM, 0>(a, S0, q, l, ev, r, valid, acc, upA);
+    neighFace<T, O, R, RM, 1>(a, S0, q, l, ev, r, valid, acc, upA);
+    neighFace<T, O, R, RM, 2>(a, S0, q, l, ev, r, valid, acc, upA);
+    neighFace<T, O, R, RM, 3>(a, S0, q, l, ev, r, valid, acc, upA);
     if (valid) {
       if (q < 9) {
         T *dst = a.dofsE + ((e * 9 + q) * B) * R + r;
@@ -604,15 +657,16 @@ template <typename T, int O, int R, int RM, int D>
 __device__ __forceinline__ void recvAll(T *X, T *TI, T *XA, T *TIA, int q, int l, const ElemCoef<T, RM> &c,
                                         const double *omega, T dt, T sca, const RecvArgs &rv, int i0, int i1,
                                         bool valid, int r, T *tIr, T (*tIAr)[nModes(O)]) {
-  constexpr int B = nModes(O);
+  constexpr int B = nModes(O), SB = Geo<T, O, R, RM>::SB;
   // value[i][j][q][r] += tau_j^D / D! * sum_{n < B(O-D)} basis_i[n] der_D[q][n]  (CK modes only,
   // even with anelasticity: TimePred.hpp:149)
   if (q < 9 && valid) {
     constexpr int NCK = nModes(O - D);
+    const T *xr = rowPtr<T, SB>(X, q, l);
     for (int i = i0; i < i1; i++) {
       double dotv = 0;
 #pragma unroll
-      for (int n = 0; n < NCK; n++) dotv += rv.basis[i * B + n] * double(X[(q * B + n) * 32 + l]);
+      for (int n = 0; n < NCK; n++) dotv += rv.basis[i * B + n] * double(xr[n]);
       for (int j = 0; j < rv.nSamples; j++) {
         double cf = 1.0;
         for (int k = 1; k <= D; k++) cf *= rv.tau[j] / k;
@@ -631,13 +685,13 @@ __device__ __forceinline__ void recvAll(T *X, T *TI, T *XA, T *TIA, int q, int l
 template <typename T, int O, int R, int RM>
 __global__ void __launch_bounds__(Geo<T, O, R, RM>::NT) kRecv(StepArgs<T> a, RecvArgs rv) {
   using G = Geo<T, O, R, RM>;
-  constexpr int B = G::B, E = G::E;
+  constexpr int B = G::B, E = G::E, SB = G::SB;
   extern __shared__ __align__(16) unsigned char smem[];
   T *X = reinterpret_cast<T *>(smem);
-  T *XA = X + G::nD + G::nTIs;
+  T *XA = X + G::nX + G::nTI;
   // time integrals are carried along but unused here (only the derivatives are sampled)
+  T *TI = X + G::nX;
   T *TIA = G::tiSmem ? XA + G::nXA : XA;
-  T *TI = X + G::nD;
   const int q = threadIdx.x >> 5, l = threadIdx.x & 31;
   const int eo = l / R, r = l % R;
   const int64_t grp = int64_t(blockIdx.x) * E + eo;
@@ -646,28 +700,35 @@ __global__ void __launch_bounds__(Geo<T, O, R, RM>::NT) kRecv(StepArgs<T> a, Rec
   const T dt = T(a.dt);
   T tIr[G::tiSmem ? 1 : B];
   T tIAr[(G::tiSmem || RM == 0) ? 1 : RM][B];
+  T zero[B];
+#pragma unroll
+  for (int n = 0; n < B; n++) zero[n] = T(0);
   if (q < 9) {
     const T *src = a.dofsE + ((ev * 9 + q) * B) * R + r;
+    T v[B];
 #pragma unroll
-    for (int n = 0; n < B; n++) {
-      X[(q * B + n) * 32 + l] = valid ? src[n * R] : T(0);
-      if constexpr (G::tiSmem)
-        TI[(q * B + n) * 32 + l] = T(0);
-      else
-        tIr[n] = T(0);
+    for (int n = 0; n < B; n++) v[n] = valid ? src[n * R] : T(0);
+    stRow<T, B>(rowPtr<T, SB>(X, q, l), v);
+    if constexpr (G::tiSmem)
+      stRow<T, B>(rowPtr<T, SB>(TI, q, l), zero);
+    else {
+#pragma unroll
+      for (int n = 0; n < B; n++) tIr[n] = T(0);
     }
   } else if constexpr (RM > 0) {
     const int s = q - 9;
 #pragma unroll
     for (int m = 0; m < RM; m++) {
       const T *src = a.dofsA + (((ev * RM + m) * 6 + s) * B) * R + r;
+      T v[B];
 #pragma unroll
-      for (int n = 0; n < B; n++) {
-        XA[((m * 6 + s) * B + n) * 32 + l] = valid ? src[n * R] : T(0);
-        if constexpr (G::tiSmem)
-          TIA[((m * 6 + s) * B + n) * 32 + l] = T(0);
-        else
-          tIAr[m][n] = T(0);
+      for (int n = 0; n < B; n++) v[n] = valid ? src[n * R] : T(0);
+      stRow<T, B>(rowPtr<T, SB>(XA, m * 6 + s, l), v);
+      if constexpr (G::tiSmem)
+        stRow<T, B>(rowPtr<T, SB>(TIA, m * 6 + s, l), zero);
+      else {
+#pragma unroll
+        for (int n = 0; n < B; n++) tIAr[m][n] = T(0);
       }
     }
   }
