@@ -82,6 +82,7 @@ struct edge_mesh {
   std::vector<int64_t> faVe;     // [nFa][3] ascending vertex ids
   std::vector<int64_t> faEl;     // [nFa][2] ascending, -1 = none (left is always present)
   std::vector<uint8_t> faType;   // [nFa] EDGE_FACE_*
+  std::vector<int64_t> faPartner; // [nFa] element across a periodic boundary face, -1 otherwise
   std::vector<double> faNormal;  // [nFa][3]
   std::vector<double> faTangent; // [nFa][2][3]
   std::vector<double> faArea;    // [nFa]
@@ -202,9 +203,11 @@ extern "C" {
 int edge_mesh_box(int nx, int ny, int nz, const double ext[3], double jitter, uint64_t seed,
                   int bc_top, int bc_sides, edge_mesh **out) {
   if (!out || nx < 1 || ny < 1 || nz < 1 || !ext || jitter < 0 || jitter >= 0.5) return EDGE_B200_EINVAL;
-  if ((bc_top != EDGE_FACE_FREE_SURFACE && bc_top != EDGE_FACE_OUTFLOW) ||
-      (bc_sides != EDGE_FACE_FREE_SURFACE && bc_sides != EDGE_FACE_OUTFLOW))
+  const bool periodic = bc_top == EDGE_FACE_PERIODIC && bc_sides == EDGE_FACE_PERIODIC;
+  if (!periodic && ((bc_top != EDGE_FACE_FREE_SURFACE && bc_top != EDGE_FACE_OUTFLOW) ||
+                    (bc_sides != EDGE_FACE_FREE_SURFACE && bc_sides != EDGE_FACE_OUTFLOW)))
     return EDGE_B200_EINVAL;
+  if (periodic && (nx < 2 || ny < 2 || nz < 2)) return EDGE_B200_EINVAL;
   edge_mesh *m = new (std::nothrow) edge_mesh();
   if (!m) return EDGE_B200_ENOMEM;
   const int64_t vx = nx + 1, vy = ny + 1, vz = nz + 1;
@@ -327,7 +330,7 @@ int edge_mesh_box(int nx, int ny, int nz, const double ext[3], double jitter, ui
     if (m->faEl[2 * fa + 1] != -1) continue;
     bool top = true;
     for (int i = 0; i < 3; i++) top = top && std::abs(m->ve[3 * m->faVe[3 * fa + i] + 2] - ext[2]) < 1e-9 * ext[2];
-    m->faType[fa] = (uint8_t)(top ? bc_top : bc_sides);
+    m->faType[fa] = (uint8_t)(periodic ? EDGE_FACE_INNER : (top ? bc_top : bc_sides));
   }
   // neighbours per element face
   m->elFaEl.assign(4 * nEl, -1);
@@ -339,6 +342,66 @@ int edge_mesh_box(int nx, int ny, int nz, const double ext[3], double jitter, ui
       m->elFaEl[4 * e + f] = (int32_t)(a == e ? b : a);
       m->elFaType[4 * e + f] = m->faType[fa];
     }
+  // periodic boxes: pair each boundary face with its translate on the opposite side (grid
+  // indices of boundary vertices are exact, jitter moves interior vertices only), as EDGE-V
+  // pairs periodic faces by matching coordinates (mesh/Mesh.cpp:190-286)
+  const int64_t nGrid[3] = {nx, ny, nz};
+  auto gridIdx = [&](int64_t v, int64_t g[3]) {
+    g[0] = v % vx;
+    g[1] = (v / vx) % vy;
+    g[2] = v / (vx * vy);
+  };
+  std::vector<int64_t> perNe(4 * nEl, -1);   // periodic neighbour element
+  std::vector<int> perFo(4 * nEl, -1), perDir(4 * nEl, -1);
+  m->faPartner.assign(nFa, -1);
+  if (periodic) {
+    std::map<std::array<int64_t, 7>, std::pair<int64_t, int>> open;  // key -> (element, local face)
+    for (int64_t e = 0; e < nEl; e++)
+      for (int f = 0; f < 4; f++) {
+        if (m->elFaEl[4 * e + f] != -1) continue;
+        int64_t fa = m->elFa[4 * e + f];
+        int64_t g[3][3];
+        for (int i = 0; i < 3; i++) gridIdx(m->faVe[3 * fa + i], g[i]);
+        int dir = -1;
+        for (int d = 0; d < 3; d++)
+          if (g[0][d] == g[1][d] && g[1][d] == g[2][d] && (g[0][d] == 0 || g[0][d] == nGrid[d])) dir = d;
+        if (dir < 0) {
+          delete m;
+          return EDGE_B200_EMESH;
+        }
+        std::array<int64_t, 7> key{};
+        key[0] = dir;
+        std::array<std::pair<int64_t, int64_t>, 3> other;
+        for (int i = 0; i < 3; i++) other[i] = {g[i][(dir + 1) % 3], g[i][(dir + 2) % 3]};
+        std::sort(other.begin(), other.end());
+        for (int i = 0; i < 3; i++) {
+          key[1 + 2 * i] = other[i].first;
+          key[2 + 2 * i] = other[i].second;
+        }
+        auto it = open.find(key);
+        if (it == open.end()) {
+          open.emplace(key, std::make_pair(e, f));
+        } else {
+          const int64_t e1 = it->second.first;
+          const int f1 = it->second.second;
+          perNe[4 * e + f] = e1;
+          perFo[4 * e + f] = f1;
+          perDir[4 * e + f] = dir;
+          perNe[4 * e1 + f1] = e;
+          perFo[4 * e1 + f1] = f;
+          perDir[4 * e1 + f1] = dir;
+          m->elFaEl[4 * e + f] = (int32_t)e1;
+          m->elFaEl[4 * e1 + f1] = (int32_t)e;
+          m->faPartner[m->elFa[4 * e + f]] = e1;
+          m->faPartner[m->elFa[4 * e1 + f1]] = e;
+          open.erase(it);
+        }
+      }
+    if (!open.empty()) {
+      delete m;
+      return EDGE_B200_EMESH;
+    }
+  }
   // neighbour face ids (geom/Generic.cpp:92-116) and vertex ids (geom/Tet4.cpp:114-229)
   m->fIdElFaEl.assign(4 * nEl, 255);
   m->vIdElFaEl.assign(4 * nEl, 255);
@@ -347,12 +410,24 @@ int edge_mesh_box(int nx, int ny, int nz, const double ext[3], double jitter, ui
       int64_t ne = m->elFaEl[4 * e + f];
       if (ne < 0) continue;
       int fAd = -1;
-      for (int g = 0; g < 4; g++)
-        if (m->elFaEl[4 * ne + g] == e) {
-          fAd = g;
-          break;
-        }
+      if (perNe[4 * e + f] >= 0) {
+        fAd = perFo[4 * e + f];
+      } else {
+        for (int g = 0; g < 4; g++)
+          if (m->elFaEl[4 * ne + g] == e && m->elFa[4 * ne + g] == m->elFa[4 * e + f]) {
+            fAd = g;
+            break;
+          }
+      }
       int64_t ve0 = f <= 2 ? m->elVe[4 * e + 0] : m->elVe[4 * e + 1];
+      if (perNe[4 * e + f] >= 0) {
+        // the matching vertex of the neighbour sits on the opposite side of the box
+        const int d = perDir[4 * e + f];
+        int64_t g[3];
+        gridIdx(ve0, g);
+        g[d] = g[d] == 0 ? nGrid[d] : 0;
+        ve0 = vid(g[0], g[1], g[2]);
+      }
       int veAd = -1;
       for (int g = 0; g < 4; g++)
         if (m->elVe[4 * ne + g] == ve0) veAd = g;
@@ -630,7 +705,8 @@ int edge_setup_flux_solvers(const edge_mesh *m, int n_rms, const double *rho, co
     }
     if (fIdL < 0 || (elR >= 0 && fIdR < 0)) return EDGE_B200_EMESH;
     const int ty = m->faType[fa];
-    const int64_t mR = elR >= 0 ? elR : elL;  // boundaries: right material = left
+    // boundaries: right material = left (AderDgInit.hpp:490-493); periodic faces: the partner's
+    const int64_t mR = elR >= 0 ? elR : (m->faPartner[fa] >= 0 ? m->faPartner[fa] : elL);
     const double *n = &m->faNormal[3 * fa], *s = &m->faTangent[6 * fa], *t = &m->faTangent[6 * fa + 3];
     double el[81], er[81], al[54], ar[54];
     int rc = edge_setup_fs_pair(rho[elL], rho[mR], lam[elL], lam[mR], mu[elL], mu[mR], n, s, t,

@@ -11,7 +11,7 @@ import numpy as np
 
 from ._lib import check, lib, ptr
 
-FACE_INNER, FACE_FREE_SURFACE, FACE_OUTFLOW = 0, 1, 2
+FACE_INNER, FACE_FREE_SURFACE, FACE_OUTFLOW, FACE_PERIODIC = 0, 1, 2, 3
 
 
 def n_modes(order):
@@ -315,3 +315,88 @@ def build_problem(n_cubes, order, runs, rm=0, ext=1e4, jitter=0.0, seed=3343, vp
     return Problem(order=order, runs=runs, rm=rm, mesh=mesh, rho=rhoe, lam=lam, mu=mu, starE=starE,
                    fsE=fsE, dt=dt, starA=starA, srcA=srcA, fsA=fsA, omega=omega, sources=src,
                    receivers=rec, name=name)
+
+
+# ------------------------------------------------------------------------------------------------
+# initial values and error norms (InitialDofs::dg / ::err, src/setups/InitialDofs.hpp:172-373)
+# ------------------------------------------------------------------------------------------------
+def tet_quadrature(n):
+    """Collapsed (Duffy) Gauss-Legendre rule on the unit tet: points [P][3], weights [P]."""
+    x, w = np.polynomial.legendre.leggauss(n)
+    x, w = (x + 1) / 2, w / 2
+    a, b, c = np.meshgrid(x, x, x, indexing="ij")
+    wa, wb, wc = np.meshgrid(w, w, w, indexing="ij")
+    xi3 = c
+    xi2 = b * (1 - c)
+    xi1 = a * (1 - b) * (1 - c)
+    wt = wa * wb * wc * (1 - b) * (1 - c) ** 2
+    return np.stack([xi1.ravel(), xi2.ravel(), xi3.ravel()], axis=1), wt.ravel()
+
+
+def basis_at(order, pts):
+    """Basis values V[P][B] at reference points (monomial form of the generated basis)."""
+    from . import dgmat
+    mons = dgmat.basis_monomials(order)
+    V = np.zeros((len(pts), len(mons)))
+    for b, terms in enumerate(mons):
+        for (ea, eb, ec), cf in terms:
+            V[:, b] += float(cf) * pts[:, 0] ** ea * pts[:, 1] ** eb * pts[:, 2] ** ec
+    return V
+
+
+def _phys_points(mesh, pts, chunk):
+    v = mesh.ve[mesh.el_ve[chunk]]                      # [E][4][3]
+    jac = v[:, 1:, :] - v[:, :1, :]                     # [E][3][3]
+    x = v[:, None, 0, :] + np.einsum("pa,ead->epd", pts, jac)
+    return x, np.abs(np.linalg.det(jac))
+
+
+def project(mesh, order, fn, runs=1, n_quad=None, chunk=20000):
+    """L2 projection of fn(x[..., 3]) -> q[..., 9] onto the DG basis: dofs[nEl][9][B][runs]."""
+    from . import dgmat
+    pts, wts = tet_quadrature(n_quad or order + 2)
+    V = basis_at(order, pts)
+    minv = dgmat.matrices(order)["massInv"]
+    B = n_modes(order)
+    out = np.zeros((mesh.n_el, 9, B, runs))
+    for s in range(0, mesh.n_el, chunk):
+        idx = np.arange(s, min(s + chunk, mesh.n_el))
+        x, _ = _phys_points(mesh, pts, idx)
+        q = fn(x)                                        # [E][P][9]
+        d = np.einsum("epq,p,pb->eqb", q, wts, V) * minv[None, None, :]
+        out[idx] = d[..., None]
+    return out
+
+
+def l2_error(mesh, order, dofs, fn, run=0, n_quad=None, chunk=20000):
+    """Per-quantity L2 norms over the mesh of (DG solution - fn) and of fn."""
+    pts, wts = tet_quadrature(n_quad or order + 3)
+    V = basis_at(order, pts)
+    err = np.zeros(9)
+    ref = np.zeros(9)
+    for s in range(0, mesh.n_el, chunk):
+        idx = np.arange(s, min(s + chunk, mesh.n_el))
+        x, det = _phys_points(mesh, pts, idx)
+        q = fn(x)
+        qh = np.einsum("eqb,pb->epq", np.asarray(dofs[idx, :, :, run], np.float64), V)
+        err += np.einsum("epq,p,e->q", (qh - q) ** 2, wts, det)
+        ref += np.einsum("epq,p,e->q", q ** 2, wts, det)
+    return np.sqrt(err), np.sqrt(ref)
+
+
+def plane_wave_p(rho, lam, mu, kvec, amp=1.0):
+    """P plane wave a = amp sin(k.x - w t): v = n a, sigma = -(lam I + 2 mu n n) a / cp."""
+    kvec = np.asarray(kvec, np.float64)
+    kn = np.linalg.norm(kvec)
+    n = kvec / kn
+    cp = np.sqrt((lam + 2 * mu) / rho)
+    om = cp * kn
+    # Voigt xx, yy, zz, xy, yz, xz
+    pairs = [(0, 0), (1, 1), (2, 2), (0, 1), (1, 2), (0, 2)]
+    sig = np.array([-(lam * (i == j) + 2 * mu * n[i] * n[j]) / cp for i, j in pairs])
+    vec = np.concatenate([sig, n])
+
+    def fn(x, t=0.0):
+        a = amp * np.sin(x @ kvec - om * t)
+        return a[..., None] * vec
+    return fn

@@ -35,8 +35,10 @@ typedef enum {
   EDGE_B200_ESCRATCH = -9    /* problem too large for the static scratch of edge_b200_step_noalloc */
 } edge_b200_status;
 
-/* per element-face boundary types (t_spTypeElastic, src/impl/seismic/const.inc:143-149) */
-enum { EDGE_FACE_INNER = 0, EDGE_FACE_FREE_SURFACE = 1, EDGE_FACE_OUTFLOW = 2 };
+/* per element-face boundary types (t_spTypeElastic, src/impl/seismic/const.inc:143-149);
+ * EDGE_FACE_PERIODIC is only a mesh-builder request: periodic faces become inner faces whose
+ * neighbour sits on the opposite side of the box (PERIODIC = 106 in the reference) */
+enum { EDGE_FACE_INNER = 0, EDGE_FACE_FREE_SURFACE = 1, EDGE_FACE_OUTFLOW = 2, EDGE_FACE_PERIODIC = 3 };
 
 /* ============================== host setup (EDGE semantics) ================================== */
 
@@ -45,7 +47,8 @@ typedef struct edge_mesh edge_mesh;
 /* Box [0,ext]^3 of nx*ny*nz cubes, each split into 6 congruent tets along its main diagonal;
  * interior vertices jittered by seeded uniform +-jitter*h per coordinate (tets with detJ <= 0 are
  * redrawn). The top face (z = ext[2]) gets bc_top, all other boundary faces bc_sides
- * (EDGE_FACE_FREE_SURFACE or EDGE_FACE_OUTFLOW). Vertex / face / neighbour conventions follow
+ * (EDGE_FACE_FREE_SURFACE or EDGE_FACE_OUTFLOW; both EDGE_FACE_PERIODIC for a periodic box with at
+ * least 2 cubes per direction). Vertex / face / neighbour conventions follow
  * EDGE-V: tools/edge_v/src/mesh/Mesh.cpp:288-375 (sorting), geom/Tet4.cpp:80-112 (orientation),
  * geom/Tet4.cpp:114-229 and geom/Generic.cpp:92-116 (neighbour vertex / face ids),
  * mesh/Mesh.cpp:763-841 with geom/Tria3.cpp:48-120 (normals, tangents). */

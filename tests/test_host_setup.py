@@ -151,6 +151,27 @@ def test_mesh_conventions(jitter):
         assert (c[mesh.fa_el[fa, 0]] - mesh.fa_normal[fa] * 0 - face_pt) is not None
 
 
+@pytest.mark.parametrize("order", [3, 4])
+def test_periodic_box_traces_match(order):
+    """Periodic boxes: faces on opposite sides are neighbours; a field whose values agree on
+    opposite sides (x(L-x) + y(L-y) + z(L-z)) has matching traces across them too."""
+    L = 2.0
+    mesh = host.Mesh.box(3, (L, L, L), jitter=0.1, seed=3, bc_top=host.FACE_PERIODIC,
+                         bc_sides=host.FACE_PERIODIC)
+    assert np.all(mesh.el_fa_el >= 0) and np.all(mesh.el_fa_type == host.FACE_INNER)
+    m = dgmat.matrices(order)
+    fn = lambda x: np.stack([(x[..., 0] * (L - x[..., 0]) + x[..., 1] * (L - x[..., 1])
+                              + x[..., 2] * (L - x[..., 2]))] * 9, axis=-1)
+    cs = host.project(mesh, order, fn)[:, 0, :, 0]
+    for e in range(mesh.n_el):
+        assert mesh.el_fa_el[mesh.el_fa_el[e, 0], mesh.fid[e, 0]] == e
+        for f in range(4):
+            ne = mesh.el_fa_el[e, f]
+            lhs = cs[e] @ m["fluxL"][f]
+            rhs = cs[ne] @ m["fluxN"][4 * mesh.vid[e, f] + mesh.fid[e, f]]
+            np.testing.assert_allclose(lhs, rhs, atol=1e-10 * np.abs(lhs).max())
+
+
 @pytest.mark.parametrize("order", [2, 3, 4])
 def test_neighbour_flux_matrices_match_traces(order):
     """A polynomial field projected elementwise must have matching face traces:
