@@ -11,6 +11,7 @@
 #include "../../include/edge_b200.h"
 #include "kernel_set.h"
 #include "kernels.cuh"
+#include "layout.cuh"
 
 namespace edge_b200 {
 KernelSet *makeKernelSet_o2(int, int, int, int);
@@ -115,9 +116,33 @@ struct edge_b200_ctx {
     return e;
   }
 
-  size_t dofsCount() const { return (size_t)nEl * 9 * B * cfg.n_runs; }
-  size_t dofsACount() const { return (size_t)nEl * cfg.n_rms * 6 * B * cfg.n_runs; }
-  size_t faceCount() const { return (size_t)nEl * 4 * 9 * F * cfg.n_runs; }
+  // device-resident row layout (padded rows of GB / GF elements) and the reference layout
+  int GB = 0, GF = 0;
+  void *stage = nullptr;  // reference-layout staging for uploads / downloads, allocated on first use
+  size_t dofsCount() const { return (size_t)nEl * 9 * cfg.n_runs * GB; }
+  size_t dofsACount() const { return (size_t)nEl * cfg.n_rms * 6 * cfg.n_runs * GB; }
+  size_t faceCount() const { return (size_t)nEl * 4 * 9 * cfg.n_runs * GF; }
+  size_t refCount(int rows) const { return (size_t)nEl * rows * B * cfg.n_runs; }
+  cudaError_t ensureStage() {
+    if (stage) return cudaSuccess;
+    const size_t n = std::max(refCount(9), refCount(6 * cfg.n_rms));
+    return cudaMalloc(&stage, n * realSize);
+  }
+  // host (reference layout) -> device rows
+  cudaError_t uploadRows(void *rows, const void *host, int rowsPerEl) {
+    cudaError_t e;
+    if ((e = ensureStage())) return e;
+    if ((e = cudaMemcpyAsync(stage, host, refCount(rowsPerEl) * realSize, cudaMemcpyHostToDevice, stream))) return e;
+    return convertLayout(true, cfg.precision, stage, rows, nEl * rowsPerEl, B, cfg.n_runs, GB, stream);
+  }
+  // device rows -> host (reference layout); synchronises the stream
+  cudaError_t downloadRows(void *host, const void *rows, int rowsPerEl) {
+    cudaError_t e;
+    if ((e = ensureStage())) return e;
+    if ((e = convertLayout(false, cfg.precision, rows, stage, nEl * rowsPerEl, B, cfg.n_runs, GB, stream))) return e;
+    if ((e = cudaMemcpyAsync(host, stage, refCount(rowsPerEl) * realSize, cudaMemcpyDeviceToHost, stream))) return e;
+    return cudaStreamSynchronize(stream);
+  }
 
   int fail(cudaError_t e, const char *what) {
     err = std::string(what) + ": " + cudaGetErrorString(e);
@@ -148,7 +173,7 @@ struct edge_b200_ctx {
     dfree(starE); dfree(starA); dfree(srcA); dfree(fsE); dfree(fsA);
     dfree(elFaEl); dfree(fId); dfree(vId); dfree(faType);
     for (auto &p : srcMem) dfree(p);
-    dfree(dGrpEl); dfree(dGrpOff); dfree(dBasis); dfree(dBuf); dfree(dTau); dfree(dSlot);
+    dfree(dGrpEl); dfree(dGrpOff); dfree(dBasis); dfree(dBuf); dfree(dTau); dfree(dSlot); dfree(stage);
     for (auto &t : timed) {
       cudaEventDestroy(t.a);
       cudaEventDestroy(t.b);
@@ -191,6 +216,8 @@ int edge_b200_create(const edge_b200_cfg *cfg, int64_t n_el, edge_b200_ctx **out
   ctx->B = nModes(cfg->order);
   ctx->F = nFaceModes(cfg->order);
   ctx->realSize = cfg->precision == 64 ? 8 : 4;
+  ctx->GB = rowPad(ctx->B, cfg->precision);
+  ctx->GF = rowPad(ctx->F, cfg->precision);
   ctx->stream = (cudaStream_t)cfg->stream;
   cudaError_t e;
   if ((e = cudaSetDevice(cfg->device)) != cudaSuccess || (e = ks->init(cfg->device)) != cudaSuccess) {
@@ -262,22 +289,15 @@ int edge_b200_upload_element_data(edge_b200_ctx *ctx, const double *star_e, cons
 
 int edge_b200_upload_dofs(edge_b200_ctx *ctx, const void *dofs_e, const void *dofs_a) {
   if (!ctx || !dofs_e || (ctx->cfg.n_rms && !dofs_a)) return EDGE_B200_EINVAL;
-  EDGE_CUDA(cudaMemcpyAsync(ctx->dofsE, dofs_e, ctx->dofsCount() * ctx->realSize, cudaMemcpyHostToDevice,
-                            ctx->stream), "upload dofsE");
-  if (ctx->cfg.n_rms)
-    EDGE_CUDA(cudaMemcpyAsync(ctx->dofsA, dofs_a, ctx->dofsACount() * ctx->realSize, cudaMemcpyHostToDevice,
-                              ctx->stream), "upload dofsA");
+  EDGE_CUDA(ctx->uploadRows(ctx->dofsE, dofs_e, 9), "upload dofsE");
+  if (ctx->cfg.n_rms) EDGE_CUDA(ctx->uploadRows(ctx->dofsA, dofs_a, 6 * ctx->cfg.n_rms), "upload dofsA");
   return EDGE_B200_OK;
 }
 
 int edge_b200_download_dofs(edge_b200_ctx *ctx, void *dofs_e, void *dofs_a) {
   if (!ctx || !dofs_e) return EDGE_B200_EINVAL;
-  EDGE_CUDA(cudaMemcpyAsync(dofs_e, ctx->dofsE, ctx->dofsCount() * ctx->realSize, cudaMemcpyDeviceToHost,
-                            ctx->stream), "download dofsE");
-  if (ctx->cfg.n_rms && dofs_a)
-    EDGE_CUDA(cudaMemcpyAsync(dofs_a, ctx->dofsA, ctx->dofsACount() * ctx->realSize, cudaMemcpyDeviceToHost,
-                              ctx->stream), "download dofsA");
-  EDGE_CUDA(cudaStreamSynchronize(ctx->stream), "download dofs");
+  EDGE_CUDA(ctx->downloadRows(dofs_e, ctx->dofsE, 9), "download dofsE");
+  if (ctx->cfg.n_rms && dofs_a) EDGE_CUDA(ctx->downloadRows(dofs_a, ctx->dofsA, 6 * ctx->cfg.n_rms), "download dofsA");
   return EDGE_B200_OK;
 }
 
@@ -294,9 +314,7 @@ int edge_b200_keep_tdofs(edge_b200_ctx *ctx, int enable) {
 
 int edge_b200_download_tdofs(edge_b200_ctx *ctx, void *tdofs) {
   if (!ctx || !tdofs || !ctx->tDofs) return EDGE_B200_EINVAL;
-  EDGE_CUDA(cudaMemcpyAsync(tdofs, ctx->tDofs, ctx->dofsCount() * ctx->realSize, cudaMemcpyDeviceToHost,
-                            ctx->stream), "download tDofs");
-  EDGE_CUDA(cudaStreamSynchronize(ctx->stream), "download tDofs");
+  EDGE_CUDA(ctx->downloadRows(tdofs, ctx->tDofs, 9), "download tDofs");
   return EDGE_B200_OK;
 }
 

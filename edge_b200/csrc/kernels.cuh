@@ -7,10 +7,11 @@
 // mode products (the global DG matrices) run in registers as compile-time sparse FMA sequences
 // (gen/dg_sparse.cuh). CTAs are persistent and loop over element groups.
 //
-// Data per element (runs fastest): dofsE [9][B][R], dofsA [RM][6][B][R], face buffer
-// [4][9][F][R] = tInt * fluxL_f (the time-integrated DOFs projected on each face, read by the
-// neighbours), star [3][24] / starA [3][9] / srcA [RM][12] / fsE [2][.][4][81] / fsA [2][.][4][54] in
-// FP64, converted to the kernel precision on load.
+// Data per element, device-resident layout (a contiguous row of modes per quantity and run, padded
+// to 16 bytes: GB = B, GF = F rounded up): dofsE [9][R][GB], dofsA [RM*6][R][GB], face buffer
+// [4][9][R][GF] = tInt * fluxL_f (the time-integrated DOFs projected on each face, read by the
+// neighbours); star [3][24] / starA [3][9] / srcA [RM][12] / fsE [2][.][4][81] / fsA [2][.][4][54]
+// in FP64, converted to the kernel precision on load.
 #pragma once
 #include <cstdint>
 
@@ -25,10 +26,10 @@ enum { FT_INNER = 0, FT_FREE = 1, FT_OUTFLOW = 2 };
 
 template <typename T>
 struct StepArgs {
-  T *dofsE;             // [nEl][9][B][R]
-  T *dofsA;             // [nEl][RM][6][B][R]
-  T *tDofs;             // [nEl][9][B][R] or null
-  T *face;              // [nEl][4][9][F][R]
+  T *dofsE;             // [nEl][9][R][GB]
+  T *dofsA;             // [nEl][RM*6][R][GB]
+  T *tDofs;             // [nEl][9][R][GB] or null
+  T *face;              // [nEl][4][9][R][GF]
   const double *starE;  // [nEl][3][24]
   const double *starA;  // [nEl][3][9]
   const double *srcA;   // [nEl][RM][12]
@@ -117,8 +118,81 @@ __device__ __forceinline__ void ldRow(const T *p, T *v) {
   for (int n = (N / 4) * 4; n < N; n++) v[n] = p[n];
 }
 
+// ------------------------------------------------------------------------------------------------
+// device-resident layout: one contiguous row of modes per (element, quantity, run)
+// ------------------------------------------------------------------------------------------------
+// dofsE [nEl][9][R][GB], dofsA [nEl][RM*6][R][GB], tDofs like dofsE, face [nEl][4][9][R][GF]:
+// rows padded to 16 bytes so a thread moves its row with 128-bit accesses. The reference layout
+// [nEl][9][B][R] exists only at the C ABI (uploads and downloads transpose on the device).
+template <typename T>
+__host__ __device__ constexpr int padGlobal(int n) {
+  const int w = 16 / int(sizeof(T));
+  return ((n + w - 1) / w) * w;
+}
+// row r of quantity row q of element e, with nRows quantity rows per element
+template <typename T, int R, int G>
+__device__ __forceinline__ T *gRow(T *base, int64_t e, int nRows, int q, int r) {
+  return base + ((e * nRows + q) * R + r) * int64_t(G);
+}
+template <typename T, int R, int G>
+__device__ __forceinline__ const T *gRow(const T *base, int64_t e, int nRows, int q, int r) {
+  return base + ((e * nRows + q) * R + r) * int64_t(G);
+}
+// v[0..N) <- global row (128-bit loads; the row is padded to a multiple of four elements)
+template <typename T, int N>
+__device__ __forceinline__ void ldRowG(const T *p, T *v, bool valid) {
+  constexpr int G = padGlobal<T>(N);
+  if (!valid) {
+#pragma unroll
+    for (int n = 0; n < N; n++) v[n] = T(0);
+    return;
+  }
+  if constexpr (sizeof(T) == 4) {
+#pragma unroll
+    for (int n = 0; n < G; n += 4) {
+      const float4 t = *reinterpret_cast<const float4 *>(p + n);
+      const T u[4] = {t.x, t.y, t.z, t.w};
+#pragma unroll
+      for (int i = 0; i < 4; i++)
+        if (n + i < N) v[n + i] = u[i];
+    }
+  } else {
+#pragma unroll
+    for (int n = 0; n < G; n += 2) {
+      const double2 t = *reinterpret_cast<const double2 *>(p + n);
+      v[n] = t.x;
+      if (n + 1 < N) v[n + 1] = t.y;
+    }
+  }
+}
+// global row <- v[0..N) (128-bit stores; padding is written as zero)
+template <typename T, int N>
+__device__ __forceinline__ void stRowG(T *p, const T *v) {
+  constexpr int G = padGlobal<T>(N);
+  if constexpr (sizeof(T) == 4) {
+#pragma unroll
+    for (int n = 0; n < G; n += 4) {
+      float4 t;
+      t.x = v[n];
+      t.y = n + 1 < N ? v[n + 1] : T(0);
+      t.z = n + 2 < N ? v[n + 2] : T(0);
+      t.w = n + 3 < N ? v[n + 3] : T(0);
+      *reinterpret_cast<float4 *>(p + n) = t;
+    }
+  } else {
+#pragma unroll
+    for (int n = 0; n < G; n += 2) {
+      double2 t;
+      t.x = v[n];
+      t.y = n + 1 < N ? v[n + 1] : T(0);
+      *reinterpret_cast<double2 *>(p + n) = t;
+    }
+  }
+}
+
 template <typename T, int O, int R, int RM>
 struct Geo {
+  static constexpr int GB = padGlobal<T>(nModes(O)), GF = padGlobal<T>(nFaceModes(O));
   static constexpr int B = nModes(O), F = nFaceModes(O), E = 32 / R;
   static constexpr int NW = 9 + (RM ? 6 : 0);
   static constexpr int NT = NW * 32;
@@ -379,11 +453,7 @@ __device__ __forceinline__ void localFace(const StepArgs<T> &a, const T *TI, T *
     for (int j = 0; j < F; j++) s[j] = T(0);
     FluxLMul<O, FA>::template run<T>(OwnRow<T>{rowPtr<T, SB>(TI, q, l)}, s);
     stRow<T, F>(rowPtr<T, SF>(S0, q, l), s);
-    if (valid) {
-      T *fb = a.face + ((((e * 4 + FA) * 9 + q) * F) * R) + r;
-#pragma unroll
-      for (int j = 0; j < F; j++) fb[j * R] = s[j];
-    }
+    if (valid) stRowG<T, F>(gRow<T, R, G::GF>(a.face, e * 4 + FA, 9, q, r), s);
   }
   // flux-solver row of this thread (elastic 9x9 or anelastic 6x9), loaded before the barrier
   T fr[9];
@@ -429,10 +499,8 @@ __global__ void __launch_bounds__(Geo<T, O, R, RM>::NT, Geo<T, O, R, RM>::minCta
     T tIAr[(G::tiSmem || RM == 0) ? 1 : RM][B];
     // DOFs -> X, dt * DOFs -> TI (and the anelastic counterparts)
     if (q < 9) {
-      const T *src = a.dofsE + ((ev * 9 + q) * B) * R + r;
       T v[B];
-#pragma unroll
-      for (int n = 0; n < B; n++) v[n] = valid ? src[n * R] : T(0);
+      ldRowG<T, B>(gRow<T, R, G::GB>(a.dofsE, ev, 9, q, r), v, valid);
       stRow<T, B>(rowPtr<T, SB>(X, q, l), v);
 #pragma unroll
       for (int n = 0; n < B; n++) v[n] = dt * v[n];
@@ -446,10 +514,8 @@ __global__ void __launch_bounds__(Geo<T, O, R, RM>::NT, Geo<T, O, R, RM>::minCta
       const int s = q - 9;
 #pragma unroll
       for (int m = 0; m < RM; m++) {
-        const T *src = a.dofsA + (((ev * RM + m) * 6 + s) * B) * R + r;
         T v[B];
-#pragma unroll
-        for (int n = 0; n < B; n++) v[n] = valid ? src[n * R] : T(0);
+        ldRowG<T, B>(gRow<T, R, G::GB>(a.dofsA, ev, RM * 6, m * 6 + s, r), v, valid);
         stRow<T, B>(rowPtr<T, SB>(XA, m * 6 + s, l), v);
 #pragma unroll
         for (int n = 0; n < B; n++) v[n] = dt * v[n];
@@ -479,17 +545,13 @@ __global__ void __launch_bounds__(Geo<T, O, R, RM>::NT, Geo<T, O, R, RM>::minCta
     if (a.tDofs && valid && q < 9) {
       T t[B];
       ldRow<T, B>(rowPtr<T, SB>(TI, q, l), t);
-      T *dst = a.tDofs + ((e * 9 + q) * B) * R + r;
-#pragma unroll
-      for (int n = 0; n < B; n++) dst[n * R] = t[n];
+      stRowG<T, B>(gRow<T, R, G::GB>(a.tDofs, e, 9, q, r), t);
     }
     // volume integral (VolIntVanilla::apply, VolIntVanilla.hpp:189-241)
     T acc[B];
     T upA[RM ? B : 1];
     if (q < 9) {
-      const T *src = a.dofsE + ((ev * 9 + q) * B) * R + r;
-#pragma unroll
-      for (int n = 0; n < B; n++) acc[n] = valid ? src[n * R] : T(0);
+      ldRowG<T, B>(gRow<T, R, G::GB>(a.dofsE, ev, 9, q, r), acc, valid);
       Mix3<T, SB> z{rowPtr<T, SB>(TI, c.cols[0], l), rowPtr<T, SB>(TI, c.cols[1], l),
                     rowPtr<T, SB>(TI, c.cols[2], l), c.cs};
       VolMul<O>::template run<T>(z, acc);
@@ -511,9 +573,7 @@ __global__ void __launch_bounds__(Geo<T, O, R, RM>::NT, Geo<T, O, R, RM>::minCta
     localFace<T, O, R, RM, 3>(a, TI, S0, q, l, ev, r, valid, acc, upA);
     if (valid) {
       if (q < 9) {
-        T *dst = a.dofsE + ((e * 9 + q) * B) * R + r;
-#pragma unroll
-        for (int n = 0; n < B; n++) dst[n * R] = acc[n];
+        stRowG<T, B>(gRow<T, R, G::GB>(a.dofsE, e, 9, q, r), acc);
       } else if constexpr (RM > 0) {
         // dofsA_m += omega_m * (Psi_vol - tIntA_m) + omega_m * upA_surf
         const int s = q - 9;
@@ -522,14 +582,15 @@ __global__ void __launch_bounds__(Geo<T, O, R, RM>::NT, Geo<T, O, R, RM>::minCta
           const T om = T(a.omega[m]);
           T ti[B];
           ldRow<T, B>(rowPtr<T, SB>(TIA, m * 6 + s, l), ti);
-          T *dst = a.dofsA + (((e * RM + m) * 6 + s) * B) * R + r;
+          T *dst = gRow<T, R, G::GB>(a.dofsA, e, RM * 6, m * 6 + s, r);
+          T v[B];
+          ldRowG<T, B>(dst, v, true);
 #pragma unroll
           for (int n = 0; n < B; n++) {
-            T v = dst[n * R];
-            v = fmaT(om, acc[n] - ti[n], v);
-            v = fmaT(om, upA[n], v);
-            dst[n * R] = v;
+            v[n] = fmaT(om, acc[n] - ti[n], v[n]);
+            v[n] = fmaT(om, upA[n], v[n]);
           }
+          stRowG<T, B>(dst, v);
         }
       }
     }
@@ -552,16 +613,12 @@ __device__ __forceinline__ void neighFace(const StepArgs<T> &a, T *S0, int q, in
     for (int j = 0; j < F; j++) s[j] = T(0);
     if (ty == FT_FREE) {
       // own face projection with the local flux matrix; the mirror is in fsE[1]
-      const T *fb = a.face + ((((e * 4 + FA) * 9 + q) * F) * R) + r;
-#pragma unroll
-      for (int j = 0; j < F; j++) s[j] = fb[j * R];
+      ldRowG<T, F>(gRow<T, R, G::GF>(a.face, e * 4 + FA, 9, q, r), s, true);
     } else if (ty == FT_INNER) {
       const int64_t ne = a.elFaEl[e * 4 + FA];
       const int fo = a.fId[e * 4 + FA], v = a.vId[e * 4 + FA];
-      const T *fb = a.face + ((((ne * 4 + fo) * 9 + q) * F) * R) + r;
       T x[F];
-#pragma unroll
-      for (int j = 0; j < F; j++) x[j] = fb[j * R];
+      ldRowG<T, F>(gRow<T, R, G::GF>(a.face, ne * 4 + fo, 9, q, r), x, true);
       if (v == 0)
         OriMul<O, 0>::template run<T>(x, s);
       else if (v == 1)
@@ -606,9 +663,7 @@ __global__ void __launch_bounds__(Geo<T, O, R, RM>::NT, Geo<T, O, R, RM>::minCta
     T acc[B];
     T upA[RM ? B : 1];
     if (q < 9) {
-      const T *src = a.dofsE + ((ev * 9 + q) * B) * R + r;
-#pragma unroll
-      for (int n = 0; n < B; n++) acc[n] = valid ? src[n * R] : T(0);
+      ldRowG<T, B>(gRow<T, R, G::GB>(a.dofsE, ev, 9, q, r), acc, valid);
     } else if constexpr (RM > 0) {
 #pragma unroll
       for (int n = 0; n < B; n++) upA[n] = T(0);
@@ -619,18 +674,19 @@ __global__ void __launch_bounds__(Geo<T, O, R, RM>::NT, Geo<T, O, R, RM>::minCta
     neighFace<T, O, R, RM, 3>(a, S0, q, l, ev, r, valid, acc, upA);
     if (valid) {
       if (q < 9) {
-        T *dst = a.dofsE + ((e * 9 + q) * B) * R + r;
-#pragma unroll
-        for (int n = 0; n < B; n++) dst[n * R] = acc[n];
+        stRowG<T, B>(gRow<T, R, G::GB>(a.dofsE, e, 9, q, r), acc);
       } else if constexpr (RM > 0) {
         // scatterUpdateA (SurfInt.hpp:139-156)
         const int s = q - 9;
 #pragma unroll
         for (int m = 0; m < RM; m++) {
           const T om = T(a.omega[m]);
-          T *dst = a.dofsA + (((e * RM + m) * 6 + s) * B) * R + r;
+          T *dst = gRow<T, R, G::GB>(a.dofsA, e, RM * 6, m * 6 + s, r);
+          T v[B];
+          ldRowG<T, B>(dst, v, true);
 #pragma unroll
-          for (int n = 0; n < B; n++) dst[n * R] = fmaT(om, upA[n], dst[n * R]);
+          for (int n = 0; n < B; n++) v[n] = fmaT(om, upA[n], v[n]);
+          stRowG<T, B>(dst, v);
         }
       }
     }
@@ -704,10 +760,8 @@ __global__ void __launch_bounds__(Geo<T, O, R, RM>::NT) kRecv(StepArgs<T> a, Rec
 #pragma unroll
   for (int n = 0; n < B; n++) zero[n] = T(0);
   if (q < 9) {
-    const T *src = a.dofsE + ((ev * 9 + q) * B) * R + r;
     T v[B];
-#pragma unroll
-    for (int n = 0; n < B; n++) v[n] = valid ? src[n * R] : T(0);
+    ldRowG<T, B>(gRow<T, R, G::GB>(a.dofsE, ev, 9, q, r), v, valid);
     stRow<T, B>(rowPtr<T, SB>(X, q, l), v);
     if constexpr (G::tiSmem)
       stRow<T, B>(rowPtr<T, SB>(TI, q, l), zero);
@@ -719,10 +773,8 @@ __global__ void __launch_bounds__(Geo<T, O, R, RM>::NT) kRecv(StepArgs<T> a, Rec
     const int s = q - 9;
 #pragma unroll
     for (int m = 0; m < RM; m++) {
-      const T *src = a.dofsA + (((ev * RM + m) * 6 + s) * B) * R + r;
       T v[B];
-#pragma unroll
-      for (int n = 0; n < B; n++) v[n] = valid ? src[n * R] : T(0);
+      ldRowG<T, B>(gRow<T, R, G::GB>(a.dofsA, ev, RM * 6, m * 6 + s, r), v, valid);
       stRow<T, B>(rowPtr<T, SB>(XA, m * 6 + s, l), v);
       if constexpr (G::tiSmem)
         stRow<T, B>(rowPtr<T, SB>(TIA, m * 6 + s, l), zero);
@@ -793,7 +845,7 @@ __global__ void kSources(T *dofsE, SrcArgs s) {
     for (int i = s.grpOff[g]; i < s.grpOff[g + 1]; i++) {
       const double in = seriesIntegral(s.dts[i], s.t0[i], s.nPts[i], s.ts + s.tsOff[i], s.t, s.t + s.dt, s.tol);
       const double sc = in * s.scal[i * 9 + q];
-      T *p = dofsE + ((s.el[i] * 9 + q) * B + md) * R + s.run[i];
+      T *p = dofsE + ((s.el[i] * 9 + q) * R + s.run[i]) * int64_t(padGlobal<T>(B)) + md;
       *p = T(double(*p) + sc * s.bEval[i * B + md]);
     }
   }

@@ -1,6 +1,7 @@
 // edge_b200_step_noalloc: the GTS step over caller-owned device arrays with its scratch (the face
-// projections the local kernel writes and the neighbour kernel reads) in a static device array,
-// for callers that cannot allocate device memory while they run.
+// projections the local kernel writes and the neighbour kernel reads, and the DOFs converted to the
+// kernels' row layout) in a static device array, for callers that cannot allocate device memory
+// while they run.
 #include <cuda_runtime.h>
 
 #include <mutex>
@@ -8,6 +9,7 @@
 #include "../../include/edge_b200.h"
 #include "kernel_set.h"
 #include "kernels.cuh"
+#include "layout.cuh"
 
 namespace edge_b200 {
 KernelSet *staticKernelSet_o2(int, int, int, int);
@@ -59,8 +61,14 @@ extern "C" int edge_b200_step_noalloc(const edge_b200_cfg *cfg, int64_t n_el, do
     return EDGE_B200_EINVAL;
   if (cfg->n_rms && (!dofs_a || !star_a || !src_a || !fs_a || !omega)) return EDGE_B200_EINVAL;
   const size_t realSize = cfg->precision == 64 ? 8 : 4;
-  const size_t faceBytes = (size_t)n_el * 4 * 9 * nFaceModes(cfg->order) * cfg->n_runs * realSize;
-  if (faceBytes > kScratchBytes) return EDGE_B200_ESCRATCH;
+  // scratch: face projections, then the DOFs in the device-resident row layout (256-byte aligned)
+  const int B = nModes(cfg->order), GB = rowPad(B, cfg->precision);
+  const int GF = rowPad(nFaceModes(cfg->order), cfg->precision);
+  auto align = [](size_t x) { return (x + 255) / 256 * 256; };
+  const size_t faceBytes = align((size_t)n_el * 4 * 9 * cfg->n_runs * GF * realSize);
+  const size_t dofsBytes = align((size_t)n_el * 9 * cfg->n_runs * GB * realSize);
+  const size_t dofsABytes = align((size_t)n_el * 6 * cfg->n_rms * cfg->n_runs * GB * realSize);
+  if (faceBytes + dofsBytes + dofsABytes > kScratchBytes) return EDGE_B200_ESCRATCH;
   KernelSet *ks = staticKernelSet(cfg->precision, cfg->order, cfg->n_runs, cfg->n_rms);
   if (!ks) return EDGE_B200_ENOTSUP;
 
@@ -80,10 +88,11 @@ extern "C" int edge_b200_step_noalloc(const edge_b200_cfg *cfg, int64_t n_el, do
   }
 
   StepArgsRaw a;
-  a.dofsE = dofs_e;
-  a.dofsA = cfg->n_rms ? dofs_a : nullptr;
+  unsigned char *sc = static_cast<unsigned char *>(scratch);
+  a.dofsE = sc + faceBytes;
+  a.dofsA = cfg->n_rms ? sc + faceBytes + dofsBytes : nullptr;
   a.tDofs = nullptr;
-  a.face = scratch;
+  a.face = sc;
   a.starE = star_e;
   a.starA = cfg->n_rms ? star_a : nullptr;
   a.srcA = cfg->n_rms ? src_a : nullptr;
@@ -97,9 +106,17 @@ extern "C" int edge_b200_step_noalloc(const edge_b200_cfg *cfg, int64_t n_el, do
   a.dt = dt;
   for (int m = 0; m < 3; m++) a.omega[m] = (cfg->n_rms && m < cfg->n_rms) ? omega[m] : 0.0;
   cudaStream_t s = (cudaStream_t)cfg->stream;
+  // the caller's DOFs (reference layout) into the scratch rows, the steps, and back
+  const int R = cfg->n_runs, P = cfg->precision;
+  if (convertLayout(true, P, dofs_e, a.dofsE, n_el * 9, B, R, GB, s) != cudaSuccess) return EDGE_B200_EDEVICE;
+  if (cfg->n_rms && convertLayout(true, P, dofs_a, a.dofsA, n_el * 6 * cfg->n_rms, B, R, GB, s) != cudaSuccess)
+    return EDGE_B200_EDEVICE;
   for (int st = 0; st < n_steps; st++) {
     if (ks->local(a, s) != cudaSuccess) return EDGE_B200_EDEVICE;
     if (ks->neigh(a, s) != cudaSuccess) return EDGE_B200_EDEVICE;
   }
+  if (convertLayout(false, P, a.dofsE, dofs_e, n_el * 9, B, R, GB, s) != cudaSuccess) return EDGE_B200_EDEVICE;
+  if (cfg->n_rms && convertLayout(false, P, a.dofsA, dofs_a, n_el * 6 * cfg->n_rms, B, R, GB, s) != cudaSuccess)
+    return EDGE_B200_EDEVICE;
   return EDGE_B200_OK;
 }

@@ -169,7 +169,9 @@ int edge_b200_step(edge_b200_ctx *ctx, double t, double dt, int n_steps);
 int edge_b200_read_receivers(edge_b200_ctx *ctx, double *buf, double *buf_time, int32_t *counts);
 /* Waits for all work of the context's stream. */
 int edge_b200_sync(edge_b200_ctx *ctx);
-/* Device pointers of the resident DOF arrays (for callers that keep data on the device). */
+/* Device pointers of the resident DOF arrays (for callers that keep data on the device). They use
+ * the kernels' row layout, not the reference layout: dofsE [nEl][9][R][GB], dofsA [nEl][rm*6][R][GB],
+ * tdofs like dofsE, with GB = B rounded up to 16 bytes (a multiple of 4 floats / 2 doubles). */
 int edge_b200_device_dofs(edge_b200_ctx *ctx, void **dofs_e, void **dofs_a, void **tdofs);
 /* Kernel launches issued by the last edge_b200_step call. */
 int64_t edge_b200_last_launches(const edge_b200_ctx *ctx);
@@ -186,10 +188,11 @@ int edge_b200_kernel_times(edge_b200_ctx *ctx, double *ms, int64_t *launches);
  * cannot allocate device memory while they run, e.g. a host that has handed every byte of the GPU
  * to a fixed memory budget or pool, or one that must not hit the device-wide synchronisation
  * cudaMalloc and cudaFree imply in the middle of its time loop.
- * The face projections the two kernels exchange live in one file-scope device array of
- * EDGE_B200_NOALLOC_SCRATCH_BYTES (32 MiB) that every GPU loading the library holds until exit; a
- * problem needing more (n_el * 4 * 9 * F * R * sizeof(real) bytes) is rejected with
- * EDGE_B200_ESCRATCH. The first call on a device looks up that array's device address (and sets
+ * Its scratch -- the face projections the two kernels exchange and a copy of the DOFs in the
+ * kernels' row layout (rows of B and F padded to 16 bytes) -- lives in one file-scope device array
+ * of EDGE_B200_NOALLOC_SCRATCH_BYTES (32 MiB) that every GPU loading the library holds until exit;
+ * a problem needing more (about n_el * R * (4 * 9 * F + (9 + 6 * n_rms) * B) * sizeof(real)
+ * bytes) is rejected with EDGE_B200_ESCRATCH. The first call on a device looks up that array's device address (and sets
  * the kernels' shared-memory limits) with the device current; make that first call before any
  * stream capture. Every call shares the array: calls that overlap on the GPU (other streams,
  * other host threads) race and must be serialised by the caller. Nothing in it needs to start at
