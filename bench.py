@@ -45,6 +45,9 @@ def parse():
     ap.add_argument("--e2e-steps", type=int, default=3)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-fp64", action="store_true")
+    ap.add_argument("--serve-requests", type=int, default=160,
+                    help="requests of the serving run (Poisson arrivals); 0 skips it")
+    ap.add_argument("--serve-rate", type=float, default=40.0, help="mean arrivals per second")
     return ap.parse_args()
 
 
@@ -216,6 +219,54 @@ def cpu_sample_rate(order, runs, rm, n_cubes=12, steps=2):
     return prob.n_el * runs * steps / el, kind, cores, sample
 
 
+def run_serve(n_req, rate, device, seed=3343):
+    """The serving form: Poisson arrivals of simulation requests (own point source, 5-16
+    receivers, 100-300 steps) on two meshes (16^3 and 12^3 cubes x 6 tets) at orders 4 and 5,
+    continuously batched into 16-run FP32 pools; reports latency percentiles and the delivered
+    element updates per second against running the same requests one after another as plain
+    FP64 single runs (timed on the same pools' meshes)."""
+    import numpy as np
+    import torch
+    from edge_b200 import host, serve
+    from edge_b200.solver import Solver
+    specs = {"box16": serve.MeshSpec(16), "box12": serve.MeshSpec(12, ext=7.5e3)}
+    keys = [(m, o) for m in specs for o in (4, 5)]
+    reqs = serve.make_stream(n_req, rate, specs, orders=(4, 5), steps=(100, 300), seed=seed)
+    srv = serve.Server(specs, runs=16, precision=32, chunk=20, device=device)
+    srv.warm(keys)
+    done = srv.run(reqs, clock="wall")
+    wall = srv.wall
+    n_el = {m: srv.meshes.get(m)[0].n_el for m in specs}
+    srv.close()
+    useful = sum(n_el[r.mesh] * r.n_steps for r in done)
+    # plain FP64, one run, same mesh and order: ms per step
+    ms64 = {}
+    for m, o in keys:
+        mesh, rho, lam, mu, star, fsE = srv.meshes.get(m)
+        dt = host.dt_cfl(mesh, o, rho, lam, mu)
+        p = host.Problem(order=o, runs=1, rm=0, mesh=mesh, rho=rho, lam=lam, mu=mu, starE=star, fsE=fsE, dt=dt)
+        st = torch.cuda.Stream(device=device)
+        sv = Solver(p, precision=64, stream=st.cuda_stream, device=device)
+        sv.upload_dofs(p.zero_dofs()[0])
+        sv.step(3)
+        sv.sync()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(st)
+        sv.step(20)
+        e1.record(st)
+        torch.cuda.synchronize()
+        ms64[(m, o)] = e0.elapsed_time(e1) / 20
+        sv.close()
+    serial_s = sum(ms64[(r.mesh, r.order)] * r.n_steps for r in done) / 1e3
+    lat = serve.latency_stats(done)
+    return {"requests": len(done), "arrival_rate_per_s": rate, "wall_s": wall,
+            "latency_s_p50": lat["p50"], "latency_s_p99": lat["p99"],
+            "delivered_element_updates_per_s": useful / wall,
+            "serial_plain_fp64_s": serial_s, "speedup_vs_serial_plain_fp64": serial_s / wall,
+            "pools": len(keys), "slots_per_pool": 16, "chunk_steps": 20,
+            "note": "wall-clock from the first arrival; latency = arrival -> last receiver sample on the host"}
+
+
 def run_reference(a, ws, rank):
     if rank != 0:
         return
@@ -361,6 +412,11 @@ def main():
         v, kind, cores, sample = cpu_sample_rate(prob.order, prob.runs, prob.rm, n_cubes=8, steps=1)
         cpu = {"value": v, "unit": UNIT, "cores": cores, "kind": kind, "sample": sample}
 
+    sv.close()
+    serving = None
+    if a.serve_requests > 0:
+        serving = run_serve(a.serve_requests, a.serve_rate, local)
+
     if rank == 0:
         out = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": a.steps,
                "warmup": a.warmup, "ms_per_step": ms_max / a.steps, "higher_is_better": True,
@@ -373,9 +429,8 @@ def main():
                "step_ms_p50": step_ms[len(step_ms) // 2], "step_ms_p99": step_ms[min(len(step_ms) - 1,
                                                                                       int(0.99 * len(step_ms)))],
                "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": int(launches),
-               "clocks": clk, "fp64_plain": fp64}
+               "clocks": clk, "fp64_plain": fp64, "serving": serving}
         print(json.dumps(out), flush=True)
-    sv.close()
     barrier(ws)
     if ws > 1:
         import torch.distributed as dist

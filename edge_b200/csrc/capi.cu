@@ -42,6 +42,39 @@ void dfree(P *&p) {
   if (p) cudaFree((void *)p);
   p = nullptr;
 }
+
+// A device array that keeps its allocation while later contents fit (cudaFree synchronises the
+// device, which would stall the other contexts' streams on every re-set of sources or receivers).
+struct DevBuf {
+  void *p = nullptr;
+  size_t cap = 0;
+  cudaError_t fit(size_t bytes) {
+    if (bytes <= cap) return cudaSuccess;
+    dfree(p);
+    cap = 0;
+    cudaError_t e = cudaMalloc(&p, bytes);
+    if (e == cudaSuccess) cap = bytes;
+    return e;
+  }
+  cudaError_t put(const void *src, size_t bytes, cudaStream_t s) {
+    cudaError_t e = fit(bytes ? bytes : 1);
+    if (e == cudaSuccess && bytes) e = cudaMemcpyAsync(p, src, bytes, cudaMemcpyHostToDevice, s);
+    return e;
+  }
+  template <typename T>
+  T *as() const { return static_cast<T *>(p); }
+  ~DevBuf() { dfree(p); }
+};
+
+// rows [nRows][R][G] <- src [nRows][B] for one run (zeros when src is null)
+template <typename T>
+__global__ void kSetRun(T *rows, const T *src, int64_t nRows, int B, int R, int G, int run) {
+  const int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (i >= nRows * G) return;
+  const int64_t row = i / G;
+  const int n = int(i % G);
+  rows[(row * R + run) * G + n] = (src && n < B) ? src[row * B + n] : T(0);
+}
 }  // namespace
 
 struct edge_b200_ctx {
@@ -60,14 +93,12 @@ struct edge_b200_ctx {
   bool meshSet = false, dataSet = false, keepTDofs = false;
   // sources
   SrcArgs src{};
-  void *srcMem[10] = {};
+  DevBuf srcMem[10];
   // receivers
   int nRecv = 0, nRecvGrp = 0, maxBuf = 0;
   double recvTime = 0, period = 0;
   int32_t recvCount = 0;
-  int64_t *dGrpEl = nullptr;
-  int32_t *dGrpOff = nullptr;
-  double *dBasis = nullptr, *dBuf = nullptr, *dBufTime = nullptr;
+  DevBuf grpEl, grpOff, basis, recvBuf;
   std::vector<double> hBufTime;
   double *dTau = nullptr;
   int32_t *dSlot = nullptr;
@@ -172,8 +203,7 @@ struct edge_b200_ctx {
     dfree(dofsE); dfree(dofsA); dfree(tDofs); dfree(face);
     dfree(starE); dfree(starA); dfree(srcA); dfree(fsE); dfree(fsA);
     dfree(elFaEl); dfree(fId); dfree(vId); dfree(faType);
-    for (auto &p : srcMem) dfree(p);
-    dfree(dGrpEl); dfree(dGrpOff); dfree(dBasis); dfree(dBuf); dfree(dTau); dfree(dSlot); dfree(stage);
+    dfree(dTau); dfree(dSlot); dfree(stage);
     for (auto &t : timed) {
       cudaEventDestroy(t.a);
       cudaEventDestroy(t.b);
@@ -301,6 +331,30 @@ int edge_b200_download_dofs(edge_b200_ctx *ctx, void *dofs_e, void *dofs_a) {
   return EDGE_B200_OK;
 }
 
+int edge_b200_set_run_dofs(edge_b200_ctx *ctx, int run, const void *dofs_e, const void *dofs_a) {
+  if (!ctx || run < 0 || run >= ctx->cfg.n_runs) return EDGE_B200_EINVAL;
+  EDGE_CUDA(ctx->ensureStage(), "set run dofs");
+  const int rm = ctx->cfg.n_rms;
+  for (int part = 0; part < (rm ? 2 : 1); part++) {
+    const void *src = part == 0 ? dofs_e : dofs_a;
+    void *rows = part == 0 ? ctx->dofsE : ctx->dofsA;
+    const int64_t nRows = ctx->nEl * (part == 0 ? 9 : 6 * rm);
+    if (src)
+      EDGE_CUDA(cudaMemcpyAsync(ctx->stage, src, nRows * ctx->B * ctx->realSize, cudaMemcpyHostToDevice,
+                                ctx->stream), "set run dofs");
+    const int64_t n = nRows * ctx->GB;
+    const int grid = (int)((n + 255) / 256);
+    if (ctx->cfg.precision == 64)
+      kSetRun<double><<<grid, 256, 0, ctx->stream>>>((double *)rows, src ? (const double *)ctx->stage : nullptr,
+                                                     nRows, ctx->B, ctx->cfg.n_runs, ctx->GB, run);
+    else
+      kSetRun<float><<<grid, 256, 0, ctx->stream>>>((float *)rows, src ? (const float *)ctx->stage : nullptr,
+                                                    nRows, ctx->B, ctx->cfg.n_runs, ctx->GB, run);
+    EDGE_CUDA(cudaGetLastError(), "set run dofs");
+  }
+  return EDGE_B200_OK;
+}
+
 int edge_b200_keep_tdofs(edge_b200_ctx *ctx, int enable) {
   if (!ctx) return EDGE_B200_EINVAL;
   if (enable && !ctx->tDofs) {
@@ -323,7 +377,6 @@ int edge_b200_set_sources(edge_b200_ctx *ctx, int n, const int64_t *el, const in
                           const double *dt, const int64_t *ts_off, const int64_t *n_pts,
                           int64_t n_ts, const double *ts) {
   if (!ctx || n < 0) return EDGE_B200_EINVAL;
-  for (auto &p : ctx->srcMem) dfree(p);
   ctx->src = SrcArgs{};
   if (n == 0) return EDGE_B200_OK;
   if (!el || !run || !scal || !b_eval || !t0 || !dt || !ts_off || !n_pts || !ts) return EDGE_B200_EINVAL;
@@ -338,33 +391,28 @@ int edge_b200_set_sources(edge_b200_ctx *ctx, int n, const int64_t *el, const in
   off.push_back(n);
   cudaStream_t s = ctx->stream;
   const int B = ctx->B;
-  int32_t *dOff = nullptr;
-  int64_t *dEl = nullptr, *dTsOff = nullptr, *dNPts = nullptr;
-  int32_t *dRun = nullptr;
-  double *dScal = nullptr, *dBEval = nullptr, *dT0 = nullptr, *dDt = nullptr, *dTs = nullptr;
-  EDGE_CUDA(upload(dOff, off.data(), off.size() * sizeof(int32_t), s), "sources");
-  EDGE_CUDA(upload(dEl, el, n * sizeof(int64_t), s), "sources");
-  EDGE_CUDA(upload(dRun, run, n * sizeof(int32_t), s), "sources");
-  EDGE_CUDA(upload(dScal, scal, n * 9 * sizeof(double), s), "sources");
-  EDGE_CUDA(upload(dBEval, b_eval, (size_t)n * B * sizeof(double), s), "sources");
-  EDGE_CUDA(upload(dT0, t0, n * sizeof(double), s), "sources");
-  EDGE_CUDA(upload(dDt, dt, n * sizeof(double), s), "sources");
-  EDGE_CUDA(upload(dTsOff, ts_off, n * sizeof(int64_t), s), "sources");
-  EDGE_CUDA(upload(dNPts, n_pts, n * sizeof(int64_t), s), "sources");
-  EDGE_CUDA(upload(dTs, ts, n_ts * sizeof(double), s), "sources");
-  void *mem[] = {dOff, dEl, dRun, dScal, dBEval, dT0, dDt, dTsOff, dNPts, dTs};
-  for (int i = 0; i < 10; i++) ctx->srcMem[i] = mem[i];
+  DevBuf *m = ctx->srcMem;
+  EDGE_CUDA(m[0].put(off.data(), off.size() * sizeof(int32_t), s), "sources");
+  EDGE_CUDA(m[1].put(el, n * sizeof(int64_t), s), "sources");
+  EDGE_CUDA(m[2].put(run, n * sizeof(int32_t), s), "sources");
+  EDGE_CUDA(m[3].put(scal, n * 9 * sizeof(double), s), "sources");
+  EDGE_CUDA(m[4].put(b_eval, (size_t)n * B * sizeof(double), s), "sources");
+  EDGE_CUDA(m[5].put(t0, n * sizeof(double), s), "sources");
+  EDGE_CUDA(m[6].put(dt, n * sizeof(double), s), "sources");
+  EDGE_CUDA(m[7].put(ts_off, n * sizeof(int64_t), s), "sources");
+  EDGE_CUDA(m[8].put(n_pts, n * sizeof(int64_t), s), "sources");
+  EDGE_CUDA(m[9].put(ts, n_ts * sizeof(double), s), "sources");
   ctx->src.nGrp = (int)off.size() - 1;
-  ctx->src.grpOff = dOff;
-  ctx->src.el = dEl;
-  ctx->src.run = dRun;
-  ctx->src.scal = dScal;
-  ctx->src.bEval = dBEval;
-  ctx->src.t0 = dT0;
-  ctx->src.dts = dDt;
-  ctx->src.tsOff = dTsOff;
-  ctx->src.nPts = dNPts;
-  ctx->src.ts = dTs;
+  ctx->src.grpOff = m[0].as<int32_t>();
+  ctx->src.el = m[1].as<int64_t>();
+  ctx->src.run = m[2].as<int32_t>();
+  ctx->src.scal = m[3].as<double>();
+  ctx->src.bEval = m[4].as<double>();
+  ctx->src.t0 = m[5].as<double>();
+  ctx->src.dts = m[6].as<double>();
+  ctx->src.tsOff = m[7].as<int64_t>();
+  ctx->src.nPts = m[8].as<int64_t>();
+  ctx->src.ts = m[9].as<double>();
   ctx->src.tol = kTolTime;
   EDGE_CUDA(cudaStreamSynchronize(s), "sources");
   return EDGE_B200_OK;
@@ -373,7 +421,6 @@ int edge_b200_set_sources(edge_b200_ctx *ctx, int n, const int64_t *el, const in
 int edge_b200_set_receivers(edge_b200_ctx *ctx, int n, const int64_t *el, const double *basis,
                             double t_first, double period, int max_buf) {
   if (!ctx || n < 0) return EDGE_B200_EINVAL;
-  dfree(ctx->dGrpEl); dfree(ctx->dGrpOff); dfree(ctx->dBasis); dfree(ctx->dBuf);
   ctx->nRecv = ctx->nRecvGrp = 0;
   if (n == 0) return EDGE_B200_OK;
   if (!el || !basis || !(period > 0) || max_buf < 1) return EDGE_B200_EINVAL;
@@ -388,12 +435,12 @@ int edge_b200_set_receivers(edge_b200_ctx *ctx, int n, const int64_t *el, const 
   }
   gOff.push_back(n);
   cudaStream_t s = ctx->stream;
-  EDGE_CUDA(upload(ctx->dGrpEl, gEl.data(), gEl.size() * sizeof(int64_t), s), "receivers");
-  EDGE_CUDA(upload(ctx->dGrpOff, gOff.data(), gOff.size() * sizeof(int32_t), s), "receivers");
-  EDGE_CUDA(upload(ctx->dBasis, basis, (size_t)n * ctx->B * sizeof(double), s), "receivers");
+  EDGE_CUDA(ctx->grpEl.put(gEl.data(), gEl.size() * sizeof(int64_t), s), "receivers");
+  EDGE_CUDA(ctx->grpOff.put(gOff.data(), gOff.size() * sizeof(int32_t), s), "receivers");
+  EDGE_CUDA(ctx->basis.put(basis, (size_t)n * ctx->B * sizeof(double), s), "receivers");
   const size_t bufCount = (size_t)n * max_buf * 9 * ctx->cfg.n_runs;
-  EDGE_CUDA(cudaMalloc(&ctx->dBuf, bufCount * sizeof(double)), "receivers");
-  EDGE_CUDA(cudaMemsetAsync(ctx->dBuf, 0, bufCount * sizeof(double), s), "receivers");
+  EDGE_CUDA(ctx->recvBuf.fit(bufCount * sizeof(double)), "receivers");
+  EDGE_CUDA(cudaMemsetAsync(ctx->recvBuf.p, 0, bufCount * sizeof(double), s), "receivers");
   EDGE_CUDA(cudaStreamSynchronize(s), "receivers");
   ctx->nRecv = n;
   ctx->nRecvGrp = (int)gEl.size();
@@ -402,6 +449,14 @@ int edge_b200_set_receivers(edge_b200_ctx *ctx, int n, const int64_t *el, const 
   ctx->period = period;
   ctx->recvCount = 0;
   ctx->hBufTime.assign(max_buf, 0.0);
+  return EDGE_B200_OK;
+}
+
+int edge_b200_rewind_receivers(edge_b200_ctx *ctx, double t_first) {
+  if (!ctx) return EDGE_B200_EINVAL;
+  ctx->recvTime = t_first;
+  ctx->recvCount = 0;
+  std::fill(ctx->hBufTime.begin(), ctx->hBufTime.end(), 0.0);
   return EDGE_B200_OK;
 }
 
@@ -451,15 +506,15 @@ int edge_b200_step(edge_b200_ctx *ctx, double t, double dt, int n_steps) {
     const int ns = stepFirst[st + 1] - stepFirst[st];
     if (ns > 0 && ctx->nRecvGrp > 0) {
       RecvArgs r;
-      r.grpEl = ctx->dGrpEl;
-      r.grpOff = ctx->dGrpOff;
-      r.basis = ctx->dBasis;
+      r.grpEl = ctx->grpEl.as<int64_t>();
+      r.grpOff = ctx->grpOff.as<int32_t>();
+      r.basis = ctx->basis.as<double>();
       r.tau = ctx->dTau + stepFirst[st];
       r.slot = ctx->dSlot + stepFirst[st];
       r.nSamples = ns;
       r.nGrp = ctx->nRecvGrp;
       r.maxBuf = ctx->maxBuf;
-      r.buf = ctx->dBuf;
+      r.buf = ctx->recvBuf.as<double>();
       EDGE_CUDA(ctx->launch(3, [&] { return ctx->ks->recv(a, r, s); }), "receiver kernel");
       ctx->launches++;
     }
@@ -484,7 +539,7 @@ int edge_b200_read_receivers(edge_b200_ctx *ctx, double *buf, double *buf_time, 
   if (ctx->nRecv == 0) return EDGE_B200_OK;
   const size_t bufCount = (size_t)ctx->nRecv * ctx->maxBuf * 9 * ctx->cfg.n_runs;
   if (buf)
-    EDGE_CUDA(cudaMemcpyAsync(buf, ctx->dBuf, bufCount * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream),
+    EDGE_CUDA(cudaMemcpyAsync(buf, ctx->recvBuf.p, bufCount * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream),
               "read receivers");
   EDGE_CUDA(cudaStreamSynchronize(ctx->stream), "read receivers");
   for (int i = 0; i < ctx->nRecv; i++) {

@@ -144,6 +144,11 @@ int edge_b200_upload_element_data(edge_b200_ctx *ctx, const double *star_e, cons
  * mechanisms. */
 int edge_b200_upload_dofs(edge_b200_ctx *ctx, const void *dofs_e, const void *dofs_a);
 int edge_b200_download_dofs(edge_b200_ctx *ctx, void *dofs_e, void *dofs_a);
+/* Sets the DOFs of one fused run only (the other runs keep theirs): dofs_e [nEl][9][B] and, with
+ * mechanisms, dofs_a [nEl][rm][6][B] in the context precision; NULL sets that run to zero. Used
+ * when a run slot is handed to a new simulation while the others continue (no counterpart in the
+ * reference, whose fused runs start and end together). */
+int edge_b200_set_run_dofs(edge_b200_ctx *ctx, int run, const void *dofs_e, const void *dofs_a);
 /* Keep the time-integrated DOFs tDofs[nEl][9][B][R] of each local step (the tDofs[0] of
  * steps.inc) in device memory (allocated on first enable; off by default, which saves their HBM
  * writes), and copy the last step's to the host (EDGE_B200_EINVAL unless kept). */
@@ -162,6 +167,9 @@ int edge_b200_set_sources(edge_b200_ctx *ctx, int n, const int64_t *el, const in
  * writeRecvAll, io/Receivers.cpp:33-290). Up to max_buf samples are buffered per receiver. */
 int edge_b200_set_receivers(edge_b200_ctx *ctx, int n, const int64_t *el, const double *basis,
                             double t_first, double period, int max_buf);
+/* Restarts receiver sampling at t_first with an empty buffer, keeping receivers and buffer
+ * allocation (no device allocation, so other streams keep running). */
+int edge_b200_rewind_receivers(edge_b200_ctx *ctx, double t_first);
 /* n_steps GTS steps from time t with step dt: local -> sources -> neighbour
  * (TimeGroupStatic::computeStep, src/time/TimeGroupStatic.cpp:113-127, steps.inc:24-77). */
 int edge_b200_step(edge_b200_ctx *ctx, double t, double dt, int n_steps);
