@@ -18,6 +18,7 @@ class Cfg(C.Structure):
 
 _SIGS = {
     "edge_mesh_box": (C.c_int, [C.c_int, C.c_int, C.c_int, vp, dbl, u64, C.c_int, C.c_int, vp]),
+    "edge_mesh_from_arrays": (C.c_int, [i64, vp, i64, vp, i64, vp, vp, C.c_int, C.c_int, vp, vp]),
     "edge_mesh_sizes": (C.c_int, [vp, vp, vp, vp]),
     "edge_mesh_arrays": (C.c_int, [vp] * 15),
     "edge_mesh_free": (None, [vp]),

@@ -185,6 +185,175 @@ void buildLocateGrid(edge_mesh &m) {
         for (int k = box[e][2]; k <= box[e][5]; k++) m.cellEl[pos[((int64_t)k * m.ng[1] + j) * m.ng[0] + i]++] = e;
 }
 
+// EDGE-V normalisation: sort element vertices, then fix the orientation (mesh/Mesh.cpp:312-313,
+// geom/Tet4.cpp:80-112); faces of an element with ascending vertices a<b<c<d are {abc},{abd},
+// {acd},{bcd}, i.e. local face f omits local vertex 3-f. An element whose volume is below
+// TOL.MESH relative to its longest edge cubed is degenerate.
+int normalizeElements(edge_mesh &m) {
+  const int64_t nEl = m.nEl();
+  for (int64_t e = 0; e < nEl; e++) {
+    int64_t *ev = &m.elVe[4 * e];
+    std::sort(ev, ev + 4);
+    double v[4][3];
+    m.veCrds(e, v);
+    double lMax = 0;
+    for (int a = 0; a < 4; a++)
+      for (int b = a + 1; b < 4; b++) {
+        double d[3] = {v[b][0] - v[a][0], v[b][1] - v[a][1], v[b][2] - v[a][2]};
+        lMax = std::max(lMax, norm(d));
+      }
+    double j3[3][3];
+    m.jac(e, j3);
+    const double d = det3(j3);
+    if (!(std::abs(d) > kTolMesh * lMax * lMax * lMax)) return EDGE_B200_EMESH;
+    if (d < 0) std::swap(ev[2], ev[3]);
+  }
+  return EDGE_B200_OK;
+}
+
+// unique faces in order of first appearance (element order, local face order), faEl ascending
+// with "none" last (std::sort of faEl with none = max, Mesh.cpp:306); a face shared by more than
+// two elements is an error
+int buildFaces(edge_mesh &m) {
+  const int64_t nEl = m.nEl();
+  std::map<std::array<int64_t, 3>, int64_t> faceIds;
+  m.elFa.assign(4 * nEl, -1);
+  m.faVe.clear();
+  m.faEl.clear();
+  for (int64_t e = 0; e < nEl; e++) {
+    const int64_t *ev = &m.elVe[4 * e];
+    for (int f = 0; f < 4; f++) {
+      std::array<int64_t, 3> key = {ev[kFaVe[f][0]], ev[kFaVe[f][1]], ev[kFaVe[f][2]]};
+      std::sort(key.begin(), key.end());
+      auto it = faceIds.find(key);
+      int64_t fa;
+      if (it == faceIds.end()) {
+        fa = (int64_t)faceIds.size();
+        faceIds.emplace(key, fa);
+        m.faVe.insert(m.faVe.end(), key.begin(), key.end());
+        m.faEl.push_back(e);
+        m.faEl.push_back(-1);
+      } else {
+        fa = it->second;
+        if (m.faEl[2 * fa + 1] != -1) return EDGE_B200_EMESH;
+        m.faEl[2 * fa + 1] = e;
+      }
+      m.elFa[4 * e + f] = fa;
+    }
+  }
+  const int64_t nFa = m.nFa();
+  for (int64_t fa = 0; fa < nFa; fa++) {
+    int64_t a = m.faEl[2 * fa], b = m.faEl[2 * fa + 1];
+    if (b != -1 && b < a) std::swap(m.faEl[2 * fa], m.faEl[2 * fa + 1]);
+  }
+  m.faType.assign(nFa, EDGE_FACE_INNER);
+  m.faPartner.assign(nFa, -1);
+  return EDGE_B200_OK;
+}
+
+// neighbour and type per element face (from faEl and faType)
+void buildNeighbours(edge_mesh &m) {
+  const int64_t nEl = m.nEl();
+  m.elFaEl.assign(4 * nEl, -1);
+  m.elFaType.assign(4 * nEl, EDGE_FACE_INNER);
+  for (int64_t e = 0; e < nEl; e++)
+    for (int f = 0; f < 4; f++) {
+      int64_t fa = m.elFa[4 * e + f];
+      int64_t a = m.faEl[2 * fa], b = m.faEl[2 * fa + 1];
+      m.elFaEl[4 * e + f] = (int32_t)(a == e ? b : a);
+      m.elFaType[4 * e + f] = m.faType[fa];
+    }
+}
+
+// neighbour face ids (geom/Generic.cpp:92-116) and vertex ids (geom/Tet4.cpp:114-229). perFo
+// holds the neighbour's local face across a periodic face (-1 elsewhere); partnerVe maps this
+// element's vertex to the neighbour's matching vertex across such a face.
+template <typename PartnerVe>
+int buildFaceIds(edge_mesh &m, const std::vector<int> &perFo, PartnerVe partnerVe) {
+  const int64_t nEl = m.nEl();
+  m.fIdElFaEl.assign(4 * nEl, 255);
+  m.vIdElFaEl.assign(4 * nEl, 255);
+  for (int64_t e = 0; e < nEl; e++)
+    for (int f = 0; f < 4; f++) {
+      int64_t ne = m.elFaEl[4 * e + f];
+      if (ne < 0) continue;
+      const bool per = !perFo.empty() && perFo[4 * e + f] >= 0;
+      int fAd = -1;
+      if (per) {
+        fAd = perFo[4 * e + f];
+      } else {
+        for (int g = 0; g < 4; g++)
+          if (m.elFaEl[4 * ne + g] == e && m.elFa[4 * ne + g] == m.elFa[4 * e + f]) {
+            fAd = g;
+            break;
+          }
+      }
+      int64_t ve0 = f <= 2 ? m.elVe[4 * e + 0] : m.elVe[4 * e + 1];
+      if (per) ve0 = partnerVe(e, f, ve0);
+      int veAd = -1;
+      for (int g = 0; g < 4; g++)
+        if (m.elVe[4 * ne + g] == ve0) veAd = g;
+      int vId = -1;
+      if (fAd >= 0)
+        for (int i = 0; i < 3; i++)
+          if (kFaVe[fAd][i] == veAd) vId = i;
+      if (fAd < 0 || vId < 0) return EDGE_B200_EMESH;
+      m.fIdElFaEl[4 * e + f] = (uint8_t)fAd;
+      m.vIdElFaEl[4 * e + f] = (uint8_t)vId;
+    }
+  return EDGE_B200_OK;
+}
+
+// face normals (away from the left element's vertex opposite the face), tangents and areas;
+// element volumes and in-diameters 6V/S (geom/Tet4.cpp:30-78); the point-location grid
+void buildGeometry(edge_mesh &m) {
+  const int64_t nFa = m.nFa(), nEl = m.nEl();
+  m.faNormal.resize(3 * nFa);
+  m.faTangent.resize(6 * nFa);
+  m.faArea.resize(nFa);
+  for (int64_t fa = 0; fa < nFa; fa++) {
+    double v[3][3];
+    for (int i = 0; i < 3; i++)
+      for (int d = 0; d < 3; d++) v[i][d] = m.ve[3 * m.faVe[3 * fa + i] + d];
+    int64_t el = m.faEl[2 * fa];
+    int64_t np = -1;
+    for (int a = 0; a < 4; a++) {
+      int64_t x = m.elVe[4 * el + a];
+      if (x != m.faVe[3 * fa] && x != m.faVe[3 * fa + 1] && x != m.faVe[3 * fa + 2]) np = x;
+    }
+    triaFrame(v, &m.ve[3 * np], &m.faTangent[6 * fa], &m.faTangent[6 * fa + 3], &m.faNormal[3 * fa]);
+    double d0[3], d1[3], c[3];
+    for (int d = 0; d < 3; d++) {
+      d0[d] = v[1][d] - v[0][d];
+      d1[d] = v[2][d] - v[0][d];
+    }
+    cross(d0, d1, c);
+    m.faArea[fa] = norm(c) / 2;
+  }
+  m.elVol.resize(nEl);
+  m.elInDia.resize(nEl);
+  for (int64_t e = 0; e < nEl; e++) {
+    double j3[3][3];
+    m.jac(e, j3);
+    double vol = std::abs(det3(j3)) / 6;
+    double s = 0;
+    for (int f = 0; f < 4; f++) s += 2 * m.faArea[m.elFa[4 * e + f]];
+    m.elVol[e] = vol;
+    m.elInDia[e] = 12 * vol / s;
+  }
+  buildLocateGrid(m);
+}
+
+// Morton (Z-order) key of a point in the unit cube, 21 bits per axis
+uint64_t mortonKey(const double x[3]) {
+  uint64_t k = 0;
+  uint32_t c[3];
+  for (int d = 0; d < 3; d++) c[d] = (uint32_t)std::min(std::max(x[d], 0.0) * 2097151.0, 2097151.0);
+  for (int b = 20; b >= 0; b--)
+    for (int d = 0; d < 3; d++) k = (k << 1) | ((c[d] >> b) & 1u);
+  return k;
+}
+
 // reference coordinates of a physical point (linalg/Mappings.hpp phyToRef)
 void phyToRef(const edge_mesh &m, int64_t el, const double x[3], double xi[3]) {
   double j[3][3], ji[3][3], v[4][3];
@@ -272,76 +441,20 @@ int edge_mesh_box(int nx, int ny, int nz, const double ext[3], double jitter, ui
       }
     }
   }
-  // EDGE-V normalisation: sort element vertices, then fix the orientation
-  // (mesh/Mesh.cpp:312-313, geom/Tet4.cpp:80-112); faces of an element with ascending vertices
-  // a<b<c<d are {abc},{abd},{acd},{bcd}, i.e. local face f omits local vertex 3-f.
-  std::vector<uint8_t> swapped(nEl, 0);
-  for (int64_t e = 0; e < nEl; e++) {
-    int64_t *ev = &m->elVe[4 * e];
-    std::sort(ev, ev + 4);
-    double j3[3][3];
-    m->jac(e, j3);
-    double d = det3(j3);
-    if (std::abs(d) <= kTolMesh * h[0] * h[1] * h[2]) {
-      delete m;
-      return EDGE_B200_EMESH;
-    }
-    if (d < 0) {
-      std::swap(ev[2], ev[3]);
-      swapped[e] = 1;
-    }
-  }
-  // unique faces in order of first appearance (element order, local face order)
-  std::map<std::array<int64_t, 3>, int64_t> faceIds;
-  m->elFa.assign(4 * nEl, -1);
-  for (int64_t e = 0; e < nEl; e++) {
-    const int64_t *ev = &m->elVe[4 * e];
-    for (int f = 0; f < 4; f++) {
-      std::array<int64_t, 3> key = {ev[kFaVe[f][0]], ev[kFaVe[f][1]], ev[kFaVe[f][2]]};
-      std::sort(key.begin(), key.end());
-      auto it = faceIds.find(key);
-      int64_t fa;
-      if (it == faceIds.end()) {
-        fa = (int64_t)faceIds.size();
-        faceIds.emplace(key, fa);
-        m->faVe.insert(m->faVe.end(), key.begin(), key.end());
-        m->faEl.push_back(e);
-        m->faEl.push_back(-1);
-      } else {
-        fa = it->second;
-        if (m->faEl[2 * fa + 1] != -1) {
-          delete m;
-          return EDGE_B200_EMESH;
-        }
-        m->faEl[2 * fa + 1] = e;
-      }
-      m->elFa[4 * e + f] = fa;
-    }
+  int rc;
+  if ((rc = normalizeElements(*m)) || (rc = buildFaces(*m))) {
+    delete m;
+    return rc;
   }
   const int64_t nFa = m->nFa();
-  // faEl ascending with "none" last (std::sort of faEl with none = max, Mesh.cpp:306)
-  for (int64_t fa = 0; fa < nFa; fa++) {
-    int64_t a = m->faEl[2 * fa], b = m->faEl[2 * fa + 1];
-    if (b != -1 && b < a) std::swap(m->faEl[2 * fa], m->faEl[2 * fa + 1]);
-  }
   // boundary types
-  m->faType.assign(nFa, EDGE_FACE_INNER);
   for (int64_t fa = 0; fa < nFa; fa++) {
     if (m->faEl[2 * fa + 1] != -1) continue;
     bool top = true;
     for (int i = 0; i < 3; i++) top = top && std::abs(m->ve[3 * m->faVe[3 * fa + i] + 2] - ext[2]) < 1e-9 * ext[2];
     m->faType[fa] = (uint8_t)(periodic ? EDGE_FACE_INNER : (top ? bc_top : bc_sides));
   }
-  // neighbours per element face
-  m->elFaEl.assign(4 * nEl, -1);
-  m->elFaType.assign(4 * nEl, EDGE_FACE_INNER);
-  for (int64_t e = 0; e < nEl; e++)
-    for (int f = 0; f < 4; f++) {
-      int64_t fa = m->elFa[4 * e + f];
-      int64_t a = m->faEl[2 * fa], b = m->faEl[2 * fa + 1];
-      m->elFaEl[4 * e + f] = (int32_t)(a == e ? b : a);
-      m->elFaType[4 * e + f] = m->faType[fa];
-    }
+  buildNeighbours(*m);
   // periodic boxes: pair each boundary face with its translate on the opposite side (grid
   // indices of boundary vertices are exact, jitter moves interior vertices only), as EDGE-V
   // pairs periodic faces by matching coordinates (mesh/Mesh.cpp:190-286)
@@ -351,10 +464,10 @@ int edge_mesh_box(int nx, int ny, int nz, const double ext[3], double jitter, ui
     g[1] = (v / vx) % vy;
     g[2] = v / (vx * vy);
   };
-  std::vector<int64_t> perNe(4 * nEl, -1);   // periodic neighbour element
-  std::vector<int> perFo(4 * nEl, -1), perDir(4 * nEl, -1);
-  m->faPartner.assign(nFa, -1);
+  std::vector<int> perFo, perDir;
   if (periodic) {
+    perFo.assign(4 * nEl, -1);
+    perDir.assign(4 * nEl, -1);
     std::map<std::array<int64_t, 7>, std::pair<int64_t, int>> open;  // key -> (element, local face)
     for (int64_t e = 0; e < nEl; e++)
       for (int f = 0; f < 4; f++) {
@@ -384,10 +497,8 @@ int edge_mesh_box(int nx, int ny, int nz, const double ext[3], double jitter, ui
         } else {
           const int64_t e1 = it->second.first;
           const int f1 = it->second.second;
-          perNe[4 * e + f] = e1;
           perFo[4 * e + f] = f1;
           perDir[4 * e + f] = dir;
-          perNe[4 * e1 + f1] = e;
           perFo[4 * e1 + f1] = f;
           perDir[4 * e1 + f1] = dir;
           m->elFaEl[4 * e + f] = (int32_t)e1;
@@ -402,81 +513,101 @@ int edge_mesh_box(int nx, int ny, int nz, const double ext[3], double jitter, ui
       return EDGE_B200_EMESH;
     }
   }
-  // neighbour face ids (geom/Generic.cpp:92-116) and vertex ids (geom/Tet4.cpp:114-229)
-  m->fIdElFaEl.assign(4 * nEl, 255);
-  m->vIdElFaEl.assign(4 * nEl, 255);
-  for (int64_t e = 0; e < nEl; e++)
-    for (int f = 0; f < 4; f++) {
-      int64_t ne = m->elFaEl[4 * e + f];
-      if (ne < 0) continue;
-      int fAd = -1;
-      if (perNe[4 * e + f] >= 0) {
-        fAd = perFo[4 * e + f];
-      } else {
-        for (int g = 0; g < 4; g++)
-          if (m->elFaEl[4 * ne + g] == e && m->elFa[4 * ne + g] == m->elFa[4 * e + f]) {
-            fAd = g;
-            break;
-          }
+  // across a periodic face the matching vertex of the neighbour sits on the opposite side
+  auto partnerVe = [&](int64_t e, int f, int64_t ve0) {
+    const int d = perDir[4 * e + f];
+    int64_t g[3];
+    gridIdx(ve0, g);
+    g[d] = g[d] == 0 ? nGrid[d] : 0;
+    return vid(g[0], g[1], g[2]);
+  };
+  if ((rc = buildFaceIds(*m, perFo, partnerVe))) {
+    delete m;
+    return rc;
+  }
+  buildGeometry(*m);
+  *out = m;
+  return EDGE_B200_OK;
+}
+
+int edge_mesh_from_arrays(int64_t n_ve, const double *ve, int64_t n_el, const int64_t *el_ve, int64_t n_bf,
+                          const int64_t *bf_ve, const int32_t *bf_tag, int default_type, int reorder,
+                          int64_t *el_perm, edge_mesh **out) {
+  if (!out || n_ve < 4 || !ve || n_el < 1 || !el_ve || n_bf < 0 || (n_bf && (!bf_ve || !bf_tag)))
+    return EDGE_B200_EINVAL;
+  if (n_el > std::numeric_limits<int32_t>::max()) return EDGE_B200_EINVAL;
+  if (default_type != -1 && default_type != EDGE_FACE_FREE_SURFACE && default_type != EDGE_FACE_OUTFLOW)
+    return EDGE_B200_EINVAL;
+  for (int64_t i = 0; i < 4 * n_el; i++)
+    if (el_ve[i] < 0 || el_ve[i] >= n_ve) return EDGE_B200_EINVAL;
+  // boundary tags by sorted vertex triple: EDGE's physical groups 101 (free surface), 105 (outflow)
+  std::map<std::array<int64_t, 3>, uint8_t> tagged;
+  for (int64_t i = 0; i < n_bf; i++) {
+    std::array<int64_t, 3> key = {bf_ve[3 * i], bf_ve[3 * i + 1], bf_ve[3 * i + 2]};
+    for (int64_t k : key)
+      if (k < 0 || k >= n_ve) return EDGE_B200_EINVAL;
+    std::sort(key.begin(), key.end());
+    uint8_t ty;
+    if (bf_tag[i] == 101) ty = EDGE_FACE_FREE_SURFACE;
+    else if (bf_tag[i] == 105) ty = EDGE_FACE_OUTFLOW;
+    else return EDGE_B200_ENOTSUP;
+    tagged[key] = ty;
+  }
+  edge_mesh *m = new (std::nothrow) edge_mesh();
+  if (!m) return EDGE_B200_ENOMEM;
+  m->ve.assign(ve, ve + 3 * n_ve);
+  std::vector<int64_t> perm(n_el);
+  for (int64_t e = 0; e < n_el; e++) perm[e] = e;
+  if (reorder) {
+    // elements along a Z-order curve of their centroids, for neighbour locality in the device
+    // gathers (EDGE-V reorders elements for its partitions and time groups instead)
+    double lo[3] = {1e300, 1e300, 1e300}, hi[3] = {-1e300, -1e300, -1e300};
+    for (int64_t v = 0; v < n_ve; v++)
+      for (int d = 0; d < 3; d++) {
+        lo[d] = std::min(lo[d], ve[3 * v + d]);
+        hi[d] = std::max(hi[d], ve[3 * v + d]);
       }
-      int64_t ve0 = f <= 2 ? m->elVe[4 * e + 0] : m->elVe[4 * e + 1];
-      if (perNe[4 * e + f] >= 0) {
-        // the matching vertex of the neighbour sits on the opposite side of the box
-        const int d = perDir[4 * e + f];
-        int64_t g[3];
-        gridIdx(ve0, g);
-        g[d] = g[d] == 0 ? nGrid[d] : 0;
-        ve0 = vid(g[0], g[1], g[2]);
-      }
-      int veAd = -1;
-      for (int g = 0; g < 4; g++)
-        if (m->elVe[4 * ne + g] == ve0) veAd = g;
-      int vId = -1;
-      for (int i = 0; i < 3; i++)
-        if (kFaVe[fAd][i] == veAd) vId = i;
-      if (fAd < 0 || vId < 0) {
-        delete m;
-        return EDGE_B200_EMESH;
-      }
-      m->fIdElFaEl[4 * e + f] = (uint8_t)fAd;
-      m->vIdElFaEl[4 * e + f] = (uint8_t)vId;
+    double span = 0;
+    for (int d = 0; d < 3; d++) span = std::max(span, hi[d] - lo[d]);
+    std::vector<uint64_t> key(n_el);
+    for (int64_t e = 0; e < n_el; e++) {
+      double c[3] = {0, 0, 0};
+      for (int a = 0; a < 4; a++)
+        for (int d = 0; d < 3; d++) c[d] += ve[3 * el_ve[4 * e + a] + d] / 4;
+      for (int d = 0; d < 3; d++) c[d] = (c[d] - lo[d]) / (span > 0 ? span : 1.0);
+      key[e] = mortonKey(c);
     }
-  // face geometry: normals point away from the left element's vertex opposite the face
-  m->faNormal.resize(3 * nFa);
-  m->faTangent.resize(6 * nFa);
-  m->faArea.resize(nFa);
+    std::stable_sort(perm.begin(), perm.end(), [&](int64_t a, int64_t b) { return key[a] < key[b]; });
+  }
+  m->elVe.resize(4 * n_el);
+  for (int64_t e = 0; e < n_el; e++)
+    for (int a = 0; a < 4; a++) m->elVe[4 * e + a] = el_ve[4 * perm[e] + a];
+  int rc;
+  if ((rc = normalizeElements(*m)) || (rc = buildFaces(*m))) {
+    delete m;
+    return rc;
+  }
+  const int64_t nFa = m->nFa();
   for (int64_t fa = 0; fa < nFa; fa++) {
-    double v[3][3];
-    for (int i = 0; i < 3; i++)
-      for (int d = 0; d < 3; d++) v[i][d] = m->ve[3 * m->faVe[3 * fa + i] + d];
-    int64_t el = m->faEl[2 * fa];
-    int64_t np = -1;
-    for (int a = 0; a < 4; a++) {
-      int64_t x = m->elVe[4 * el + a];
-      if (x != m->faVe[3 * fa] && x != m->faVe[3 * fa + 1] && x != m->faVe[3 * fa + 2]) np = x;
+    if (m->faEl[2 * fa + 1] != -1) continue;
+    std::array<int64_t, 3> key = {m->faVe[3 * fa], m->faVe[3 * fa + 1], m->faVe[3 * fa + 2]};
+    auto it = tagged.find(key);
+    if (it != tagged.end()) {
+      m->faType[fa] = it->second;
+    } else if (default_type >= 0) {
+      m->faType[fa] = (uint8_t)default_type;
+    } else {
+      delete m;
+      return EDGE_B200_EMESH;
     }
-    triaFrame(v, &m->ve[3 * np], &m->faTangent[6 * fa], &m->faTangent[6 * fa + 3], &m->faNormal[3 * fa]);
-    double d0[3], d1[3], c[3];
-    for (int d = 0; d < 3; d++) {
-      d0[d] = v[1][d] - v[0][d];
-      d1[d] = v[2][d] - v[0][d];
-    }
-    cross(d0, d1, c);
-    m->faArea[fa] = norm(c) / 2;
   }
-  // element volume and in-diameter 6V/S (geom/Tet4.cpp:30-78)
-  m->elVol.resize(nEl);
-  m->elInDia.resize(nEl);
-  for (int64_t e = 0; e < nEl; e++) {
-    double j3[3][3];
-    m->jac(e, j3);
-    double vol = std::abs(det3(j3)) / 6;
-    double s = 0;
-    for (int f = 0; f < 4; f++) s += 2 * m->faArea[m->elFa[4 * e + f]];
-    m->elVol[e] = vol;
-    m->elInDia[e] = 12 * vol / s;
+  buildNeighbours(*m);
+  if ((rc = buildFaceIds(*m, std::vector<int>(), [](int64_t, int, int64_t v) { return v; }))) {
+    delete m;
+    return rc;
   }
-  buildLocateGrid(*m);
+  buildGeometry(*m);
+  if (el_perm) std::copy(perm.begin(), perm.end(), el_perm);
   *out = m;
   return EDGE_B200_OK;
 }

@@ -63,6 +63,45 @@ class Mesh:
         m.n_cubes = (nx, ny, nz)
         return m
 
+    @classmethod
+    def from_arrays(cls, ve, el_ve, bf_ve=None, bf_tag=None, default_type=-1, reorder=True):
+        """Mesh of arbitrary tets (edge_mesh_from_arrays): boundary faces bf_ve[n][3] tagged 101
+        (free surface) / 105 (outflow); untagged boundary faces get default_type (-1 rejects).
+        The input index of each mesh element is kept in ``el_perm``."""
+        ve = np.ascontiguousarray(ve, np.float64)
+        el_ve = np.ascontiguousarray(el_ve, np.int64)
+        bf_ve = np.ascontiguousarray(np.zeros((0, 3)) if bf_ve is None else bf_ve, np.int64)
+        bf_tag = np.ascontiguousarray(np.zeros(0) if bf_tag is None else bf_tag, np.int32)
+        perm = np.zeros(len(el_ve), np.int64)
+        h = C.c_void_p()
+        check(lib().edge_mesh_from_arrays(len(ve), ptr(ve), len(el_ve), ptr(el_ve), len(bf_ve), ptr(bf_ve),
+                                          ptr(bf_tag), int(default_type), 1 if reorder else 0, ptr(perm),
+                                          C.byref(h)), "edge_mesh_from_arrays")
+        m = cls(h)
+        m.el_perm = perm
+        return m
+
+    @classmethod
+    def from_gmsh(cls, path, default_type=-1, reorder=True):
+        """Mesh of a gmsh ASCII file (MSH 2.2 / 4.1, tets + tagged boundary triangles)."""
+        from .gmsh import read_msh
+        ve, el_ve, bf_ve, bf_tag = read_msh(path)
+        return cls.from_arrays(ve, el_ve, bf_ve, bf_tag, default_type, reorder)
+
+    def boundary_faces(self):
+        """(bf_ve [n][3], reference tag [n]) of the boundary faces (101 free surface, 105 outflow)."""
+        b = self.fa_el[:, 1] < 0
+        tag = np.where(self.fa_type[b] == FACE_FREE_SURFACE, 101, 105).astype(np.int32)
+        return np.ascontiguousarray(self.fa_ve()[b]), tag
+
+    def fa_ve(self):
+        """Vertices of each face (ascending), from the element faces."""
+        out = np.zeros((self.n_fa, 3), np.int64)
+        loc = np.array([[0, 1, 2], [0, 1, 3], [0, 2, 3], [1, 2, 3]])
+        for f in range(4):
+            out[self.el_fa[:, f]] = np.sort(self.el_ve[:, loc[f]], axis=1)
+        return out
+
     def __del__(self):
         if getattr(self, "_h", None):
             lib().edge_mesh_free(self._h)
@@ -261,10 +300,12 @@ def build_problem(n_cubes, order, runs, rm=0, ext=1e4, jitter=0.0, seed=3343, vp
                   vs=3464.0, rho=2670.0, layers=None, lognormal_sigma=0.0, q_range=None,
                   freq_cen=1.0, freq_rat=100.0, n_receivers=8, source="explosive", f0=2.0,
                   n_steps=200, period=None, cfl=1.0, bc_top=FACE_FREE_SURFACE,
-                  bc_sides=FACE_OUTFLOW, name=""):
-    """Synthetic setups of the element update (box meshes, homogeneous or layered materials)."""
+                  bc_sides=FACE_OUTFLOW, name="", mesh=None):
+    """Synthetic setups of the element update (box meshes, homogeneous or layered materials).
+    A given ``mesh`` (e.g. Mesh.from_gmsh of a box [0, ext]^3) replaces the generated box."""
     rng = np.random.default_rng(seed)
-    mesh = Mesh.box(n_cubes, (ext, ext, ext), jitter=jitter, seed=seed, bc_top=bc_top, bc_sides=bc_sides)
+    if mesh is None:
+        mesh = Mesh.box(n_cubes, (ext, ext, ext), jitter=jitter, seed=seed, bc_top=bc_top, bc_sides=bc_sides)
     ne = mesh.n_el
     if layers is None:
         vpe = np.full(ne, vp)

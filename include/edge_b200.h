@@ -54,6 +54,19 @@ typedef struct edge_mesh edge_mesh;
  * mesh/Mesh.cpp:763-841 with geom/Tria3.cpp:48-120 (normals, tangents). */
 int edge_mesh_box(int nx, int ny, int nz, const double ext[3], double jitter, uint64_t seed,
                   int bc_top, int bc_sides, edge_mesh **out);
+/* Tet4 mesh from vertices ve[n_ve][3] and elements el_ve[n_el][4] (any vertex order), e.g. as read
+ * from a gmsh file (EDGE-V io/Gmsh.cpp:120-251), with the same EDGE-V conventions as
+ * edge_mesh_box. Boundary faces bf_ve[n_bf][3] carry the reference's physical-group tags bf_tag
+ * (101 free surface, 105 outflow, src/impl/seismic/const.inc:144-146; any other tag, periodic 106
+ * included, gives EDGE_B200_ENOTSUP); boundary faces not listed get default_type
+ * (EDGE_FACE_FREE_SURFACE / EDGE_FACE_OUTFLOW, or -1 to reject the mesh with EDGE_B200_EMESH);
+ * tags on inner faces are ignored. reorder != 0 sorts the elements along a Z-order curve of their
+ * centroids (locality of the neighbour gathers); el_perm[n_el] (may be NULL) receives the input
+ * index of each mesh element. Faces shared by more than two elements or degenerate elements give
+ * EDGE_B200_EMESH. */
+int edge_mesh_from_arrays(int64_t n_ve, const double *ve, int64_t n_el, const int64_t *el_ve, int64_t n_bf,
+                          const int64_t *bf_ve, const int32_t *bf_tag, int default_type, int reorder,
+                          int64_t *el_perm, edge_mesh **out);
 int edge_mesh_sizes(const edge_mesh *m, int64_t *n_ve, int64_t *n_fa, int64_t *n_el);
 /* Any output pointer may be NULL. Shapes: ve[nVe][3], el_ve[nEl][4], el_fa[nEl][4],
  * fa_el[nFa][2] (-1 = none), fa_normal[nFa][3], fa_tangent[nFa][2][3], fa_area[nFa],
@@ -207,8 +220,9 @@ int edge_b200_kernel_times(edge_b200_ctx *ctx, double *ms, int64_t *launches);
  * zero: each step writes every face projection before reading it.
  * Arguments: cfg as for edge_b200_create (order, n_runs, n_rms, precision, stream, device);
  * dofs_e / dofs_a in the cfg precision, element data in FP64 with the layouts of
- * edge_b200_upload_element_data, connectivity as in edge_b200_upload_mesh, all on cfg->device;
- * only omega (n_rms relaxation frequencies) is a host array. */
+ * edge_b200_upload_element_data, connectivity as in edge_b200_upload_mesh, all on cfg->device
+ * (el_fa_el 16-byte aligned, the three byte arrays 4-byte aligned, as cudaMalloc returns them;
+ * EDGE_B200_EINVAL otherwise); only omega (n_rms relaxation frequencies) is a host array. */
 #define EDGE_B200_NOALLOC_SCRATCH_BYTES (32u << 20)
 int edge_b200_step_noalloc(const edge_b200_cfg *cfg, int64_t n_el, double dt, int n_steps,
                            void *dofs_e, void *dofs_a, const double *star_e, const double *fs_e,
