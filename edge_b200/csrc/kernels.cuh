@@ -211,12 +211,27 @@ struct Geo {
   static constexpr size_t nTI = tiSmem ? nX : nS0;
   static constexpr size_t nTIA = tiSmem ? nXA : 0;
   static constexpr size_t smemLocal = (nX + nTI + nXA + nTIA) * sizeof(T);
-  static constexpr size_t smemNeigh = nS0 * sizeof(T);
+  // neighbour kernel: a ring of NSN slots, each [9][32][SF] face rows and, for E <= 4, the E
+  // elements' flux-solver blocks (81 + 54 doubles); as many slots (2..4) as fit the shared memory
+  // of minCtasNeigh CTAs per SM (228 KB, 1 KB reserved per CTA)
+  static constexpr int minCtasNeigh = (sizeof(T) == 4 && RM == 0) ? 2 : 1;
+  static constexpr bool fsSmem = E <= 4;
+  static constexpr size_t slotNeigh =
+      (nS0 * sizeof(T) + 15) / 16 * 16 + (fsSmem ? size_t(E) * (81 + (RM ? 54 : 0)) * 8 : 0);
+  static constexpr size_t budgetNeigh = (228 * 1024) / minCtasNeigh - 1024;
+  // the next group's DOF rows [9][32][SB] are prefetched into a tile behind the slots when that
+  // leaves room for at least three slots
+  static constexpr size_t dofTileBytes = size_t(9) * 32 * SB * sizeof(T);
+  static constexpr bool dofTile = budgetNeigh >= dofTileBytes + 3 * slotNeigh;
+  static constexpr size_t slotRoom = budgetNeigh - (dofTile ? dofTileBytes : 0);
+  static constexpr int NSN = slotRoom / slotNeigh >= 4 ? 4 : int(slotRoom / slotNeigh);
+  static_assert(NSN >= 2, "neighbour kernel needs two slots");
+  static_assert(slotNeigh % 16 == 0, "slots start on 16-byte boundaries (cp.async targets)");
+  static constexpr size_t smemNeigh = NSN * slotNeigh + (dofTile ? dofTileBytes : 0);
   // resident CTAs per SM the register allocation targets (65,536 registers per SM): FP32 keeps
   // two 288-thread CTAs of each kernel (<= 113 registers); FP64 rows need twice the registers
   // and keep one
   static constexpr int minCtasLocal = (sizeof(T) == 4 && RM == 0 && smemLocal <= 110 * 1024) ? 2 : 1;
-  static constexpr int minCtasNeigh = (sizeof(T) == 4 && RM == 0) ? 2 : 1;
 };
 
 // per-thread element coefficients
@@ -600,78 +615,246 @@ __global__ void __launch_bounds__(Geo<T, O, R, RM>::NT, Geo<T, O, R, RM>::minCta
 // ------------------------------------------------------------------------------------------------
 // neighbour step (AderDg::neigh, AderDg.hpp:553-722)
 // ------------------------------------------------------------------------------------------------
+// The face rows a CTA reads (the neighbours' face projections, or its own for free-surface faces)
+// and the flux-solver blocks are gathered with asynchronous copies (cp.async, no registers held)
+// into a ring of NSN shared-memory slots, one slot per (element group, face) item, NSN - 1 items
+// ahead of the one being processed; the next group's DOF rows are prefetched the same way when
+// they fit. Per item: wait for its copies, rotate the neighbour's rows into this element's face
+// orientation in place, one CTA barrier, issue the copies of the item NSN - 1 ahead into the slot
+// the previous item released, then mix quantities and apply fluxT.
+
+__device__ __forceinline__ void cpAsync16(void *dst, const void *src) {
+  const unsigned d = static_cast<unsigned>(__cvta_generic_to_shared(dst));
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(d), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cpAsync8(void *dst, const void *src) {
+  const unsigned d = static_cast<unsigned>(__cvta_generic_to_shared(dst));
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(d), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cpAsyncCommit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cpAsyncWait() {
+  asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
+}
+
+// face connectivity of one element (all four faces), packed as loaded: neighbour ids, and one
+// byte per face for the neighbour's face id, the vertex id and the face type
+struct FaceMeta {
+  int32_t ne[4];
+  uint32_t fo, vi, ty;
+  __device__ __forceinline__ void load(const int32_t *elFaEl, const uint8_t *fId, const uint8_t *vId,
+                                       const uint8_t *faType, int64_t e, bool valid) {
+    if (valid) {
+      const int4 n = __ldg(reinterpret_cast<const int4 *>(elFaEl) + e);
+      ne[0] = n.x; ne[1] = n.y; ne[2] = n.z; ne[3] = n.w;
+      fo = __ldg(reinterpret_cast<const uint32_t *>(fId) + e);
+      vi = __ldg(reinterpret_cast<const uint32_t *>(vId) + e);
+      ty = __ldg(reinterpret_cast<const uint32_t *>(faType) + e);
+    } else {
+      ne[0] = ne[1] = ne[2] = ne[3] = 0;
+      fo = vi = 0;
+      ty = 0x02020202u;  // outflow on every face: nothing to gather or add
+    }
+  }
+  __device__ __forceinline__ int type(int f) const { return (ty >> (8 * f)) & 0xff; }
+  __device__ __forceinline__ int faceOf(int f) const { return (fo >> (8 * f)) & 0xff; }
+  __device__ __forceinline__ int vert(int f) const { return (vi >> (8 * f)) & 0xff; }
+};
+
+template <typename T, int O, int R, int RM>
+struct NeighSlots {
+  using G = Geo<T, O, R, RM>;
+  static constexpr int E = G::E, SF = G::SF, GF = G::GF, NT = G::NT;
+  static constexpr int W = 16 / int(sizeof(T));  // elements per 16-byte chunk
+  static constexpr int CPR = GF / W;             // 16-byte chunks per face row
+  static constexpr int CPRB = G::GB / W;         // 16-byte chunks per DOF row
+  static constexpr int NFS = 81 + (RM ? 54 : 0); // flux-solver doubles per element and face
+  static constexpr size_t rowsBytes = (G::nS0 * sizeof(T) + 15) / 16 * 16;
+  __device__ __forceinline__ static T *rows(unsigned char *base, int slot) {
+    return reinterpret_cast<T *>(base + slot * G::slotNeigh);
+  }
+  __device__ __forceinline__ static double *fs(unsigned char *base, int slot) {
+    return reinterpret_cast<double *>(base + slot * G::slotNeigh + rowsBytes);
+  }
+  __device__ __forceinline__ static T *dofTile(unsigned char *base) {
+    return reinterpret_cast<T *>(base + G::NSN * G::slotNeigh);
+  }
+
+  // the DOF rows of group g into the tile behind the slots (warp q copies quantity q's rows)
+  __device__ __forceinline__ static void issueDofs(const StepArgs<T> &a, unsigned char *base, int q, int l,
+                                                   int64_t g, bool groupValid) {
+    if constexpr (G::dofTile) {
+      const int eo = l / R, r = l % R;
+      const int64_t e = g * E + eo;
+      if (!groupValid || q >= 9 || e >= a.nEl) return;
+      const T *blk = a.dofsE + (e * 9 + q) * int64_t(R * G::GB);
+      T *dst = dofTile(base) + (q * 32 + eo * R) * G::SB;
+#pragma unroll
+      for (int it = 0; it < CPRB; it++) {
+        const int k = it * R + r;
+        const int row = k / CPRB, col = k % CPRB;
+        cpAsync16(dst + row * G::SB + col * W, blk + row * G::GB + col * W);
+      }
+    }
+  }
+
+  // copies of item (group g, face FA) into `slot`; m = connectivity of this lane's element
+  template <int FA>
+  __device__ __forceinline__ static void issue(const StepArgs<T> &a, unsigned char *base, int slot, int q, int l,
+                                               int64_t g, bool groupValid, const FaceMeta &m) {
+    if (groupValid) {
+      const int eo = l / R, r = l % R;
+      const int64_t e = g * E + eo;
+      const int ty = m.type(FA);
+      if (q < 9 && e < a.nEl && ty != FT_OUTFLOW) {
+        const int64_t srcFace = ty == FT_INNER ? int64_t(m.ne[FA]) * 4 + m.faceOf(FA) : e * 4 + FA;
+        const T *blk = a.face + (srcFace * 9 + q) * int64_t(R * GF);
+        T *dst = rows(base, slot) + (q * 32 + eo * R) * SF;
+#pragma unroll
+        for (int it = 0; it < CPR; it++) {
+          const int k = it * R + r;  // consecutive lanes move consecutive 16-byte chunks
+          const int row = k / CPR, col = k % CPR;
+          cpAsync16(dst + row * SF + col * W, blk + row * GF + col * W);
+        }
+      }
+      if constexpr (G::fsSmem) {
+        // flux-solver blocks fsE[1][e][FA] (and fsA[1][e][FA]) of the group's elements
+        double *fsDst = fs(base, slot);
+        for (int i = threadIdx.x; i < E * NFS; i += NT) {
+          const int eo2 = i / NFS, j = i % NFS;
+          const int64_t e2 = g * E + eo2;
+          if (e2 >= a.nEl) continue;
+          const double *src = j < 81 ? a.fsE + ((a.nEl + e2) * 4 + FA) * 81 + j
+                                     : a.fsA + ((a.nEl + e2) * 4 + FA) * 54 + (j - 81);
+          cpAsync8(fsDst + i, src);
+        }
+      }
+    }
+    cpAsyncCommit();
+  }
+};
+
+// the neighbour's rows of this item, rotated into this element's face orientation in place
 template <typename T, int O, int R, int RM, int FA>
-__device__ __forceinline__ void neighFace(const StepArgs<T> &a, T *S0, int q, int l, int64_t e, int r,
-                                          bool valid, T *acc, T *upA) {
+__device__ __forceinline__ void neighOrient(T *S, int q, int l, bool valid, const FaceMeta &m) {
   using G = Geo<T, O, R, RM>;
   constexpr int F = G::F, SF = G::SF;
-  const int ty = valid ? a.faType[e * 4 + FA] : FT_OUTFLOW;
-  T fr[9];
-  if (q < 9) {
-    T s[F];
+  if (q < 9 && valid && m.type(FA) == FT_INNER) {
+    T x[F], s[F];
+    ldRow<T, F>(rowPtr<T, SF>(S, q, l), x);
 #pragma unroll
     for (int j = 0; j < F; j++) s[j] = T(0);
-    if (ty == FT_FREE) {
-      // own face projection with the local flux matrix; the mirror is in fsE[1]
-      ldRowG<T, F>(gRow<T, R, G::GF>(a.face, e * 4 + FA, 9, q, r), s, true);
-    } else if (ty == FT_INNER) {
-      const int64_t ne = a.elFaEl[e * 4 + FA];
-      const int fo = a.fId[e * 4 + FA], v = a.vId[e * 4 + FA];
-      T x[F];
-      ldRowG<T, F>(gRow<T, R, G::GF>(a.face, ne * 4 + fo, 9, q, r), x, true);
-      if (v == 0)
-        OriMul<O, 0>::template run<T>(x, s);
-      else if (v == 1)
-        OriMul<O, 1>::template run<T>(x, s);
-      else
-        OriMul<O, 2>::template run<T>(x, s);
-    }
-    stRow<T, F>(rowPtr<T, SF>(S0, q, l), s);
-    const double *fp = a.fsE + ((a.nEl + e) * 4 + FA) * 81 + q * 9;
-#pragma unroll
-    for (int i = 0; i < 9; i++) fr[i] = ty != FT_OUTFLOW ? T(__ldg(fp + i)) : T(0);
-  } else if constexpr (RM > 0) {
-    const double *fp = a.fsA + ((a.nEl + e) * 4 + FA) * 54 + (q - 9) * 9;
-#pragma unroll
-    for (int i = 0; i < 9; i++) fr[i] = ty != FT_OUTFLOW ? T(__ldg(fp + i)) : T(0);
+    const int v = m.vert(FA);
+    if (v == 0)
+      OriMul<O, 0>::template run<T>(x, s);
+    else if (v == 1)
+      OriMul<O, 1>::template run<T>(x, s);
+    else
+      OriMul<O, 2>::template run<T>(x, s);
+    stRow<T, F>(rowPtr<T, SF>(S, q, l), s);
   }
-  __syncthreads();
-  if (ty != FT_OUTFLOW) {
-    T s[F];
-    faceMix<T, F, SF>(S0, l, fr, s);
-    if (q < 9)
-      FluxTMul<O, FA>::template run<T>(s, acc);
-    else if constexpr (RM > 0)
-      FluxTMul<O, FA>::template run<T>(s, upA);
+}
+
+template <typename T, int O, int R, int RM, int FA>
+__device__ __forceinline__ void neighApply(const StepArgs<T> &a, const T *S, const double *fs, int q, int l,
+                                           int64_t e, bool valid, const FaceMeta &m, T *acc, T *upA) {
+  using G = Geo<T, O, R, RM>;
+  using NS = NeighSlots<T, O, R, RM>;
+  constexpr int F = G::F, SF = G::SF;
+  if (!valid || m.type(FA) == FT_OUTFLOW) return;
+  T fr[9];
+  if constexpr (G::fsSmem) {
+    const int eo = l / R;
+    const double *fp = q < 9 ? fs + eo * NS::NFS + q * 9 : fs + eo * NS::NFS + 81 + (q - 9) * 9;
+#pragma unroll
+    for (int i = 0; i < 9; i++) fr[i] = T(fp[i]);
+  } else {
+    const double *fp = q < 9 ? a.fsE + ((a.nEl + e) * 4 + FA) * 81 + q * 9
+                             : a.fsA + ((a.nEl + e) * 4 + FA) * 54 + (q - 9) * 9;
+#pragma unroll
+    for (int i = 0; i < 9; i++) fr[i] = T(__ldg(fp + i));
   }
+  T s[F];
+  faceMix<T, F, SF>(S, l, fr, s);
+  if (q < 9)
+    FluxTMul<O, FA>::template run<T>(s, acc);
+  else if constexpr (RM > 0)
+    FluxTMul<O, FA>::template run<T>(s, upA);
+}
+
+// item (local group k, face FA): item index i = 4k + FA lives in slot i % NSN; after the barrier the
+// item i + NSN - 1 is issued into slot (i - 1) % NSN, which the barrier has released
+template <typename T, int O, int R, int RM, int FA>
+__device__ __forceinline__ void neighItem(const StepArgs<T> &a, unsigned char *base, int q, int l, int64_t e,
+                                          bool valid, const FaceMeta &cur, const FaceMeta &nxt, int64_t g,
+                                          bool nextValid, int64_t k, T *acc, T *upA) {
+  using NS = NeighSlots<T, O, R, RM>;
+  constexpr int NSN = Geo<T, O, R, RM>::NSN;
+  cpAsyncWait<NSN - 2>();
+  __syncwarp();
+  const int64_t item = k * 4 + FA;
+  const int slot = int(item % NSN);
+  T *S = NS::rows(base, slot);
+  neighOrient<T, O, R, RM, FA>(S, q, l, valid, cur);
   __syncthreads();
+  constexpr int AHEAD = FA + NSN - 1;
+  const int slotNext = int((item + NSN - 1) % NSN);
+  // the next group's DOF rows join the copies committed now (the barrier ordered this group's
+  // reads of the tile before them)
+  if constexpr (FA == 0) NS::issueDofs(a, base, q, l, g + gridDim.x, nextValid);
+  if constexpr (AHEAD < 4)
+    NS::template issue<AHEAD>(a, base, slotNext, q, l, g, true, cur);
+  else
+    NS::template issue<AHEAD - 4>(a, base, slotNext, q, l, g + gridDim.x, nextValid, nxt);
+  neighApply<T, O, R, RM, FA>(a, S, NS::fs(base, slot), q, l, e, valid, cur, acc, upA);
 }
 
 template <typename T, int O, int R, int RM>
 __global__ void __launch_bounds__(Geo<T, O, R, RM>::NT, Geo<T, O, R, RM>::minCtasNeigh) kNeigh(StepArgs<T> a) {
   using G = Geo<T, O, R, RM>;
-  constexpr int B = G::B, E = G::E;
+  using NS = NeighSlots<T, O, R, RM>;
+  constexpr int B = G::B, E = G::E, NSN = G::NSN;
   extern __shared__ __align__(16) unsigned char smem[];
-  T *S0 = reinterpret_cast<T *>(smem);
   const int q = threadIdx.x >> 5, l = threadIdx.x & 31;
   const int eo = l / R, r = l % R;
   const int64_t nGroups = (a.nEl + E - 1) / E;
-  for (int64_t g = blockIdx.x; g < nGroups; g += gridDim.x) {
+  int64_t g = blockIdx.x;
+  FaceMeta cur, nxt;
+  cur.load(a.elFaEl, a.fId, a.vId, a.faType, g * E + eo, g * E + eo < a.nEl);
+  // prologue: the first group's DOF rows and items 0 .. NSN-2 (its first faces)
+  NS::issueDofs(a, smem, q, l, g, g < nGroups);
+  NS::template issue<0>(a, smem, 0, q, l, g, g < nGroups, cur);
+  if constexpr (NSN > 2) NS::template issue<1>(a, smem, 1, q, l, g, g < nGroups, cur);
+  if constexpr (NSN > 3) NS::template issue<2>(a, smem, 2, q, l, g, g < nGroups, cur);
+  for (int64_t k = 0; g < nGroups; g += gridDim.x, k++) {
     const int64_t e = g * E + eo;
     const bool valid = e < a.nEl;
-    const int64_t ev = valid ? e : 0;
+    const int64_t gn = g + gridDim.x;
+    const bool nextValid = gn < nGroups;
+    nxt.load(a.elFaEl, a.fId, a.vId, a.faType, gn * E + eo, nextValid && gn * E + eo < a.nEl);
     T acc[B];
     T upA[RM ? B : 1];
     if (q < 9) {
-      ldRowG<T, B>(gRow<T, R, G::GB>(a.dofsE, ev, 9, q, r), acc, valid);
+      if constexpr (G::dofTile) {
+        // the group's DOF rows arrived with (or before) its first face item
+        cpAsyncWait<NSN - 2>();
+        __syncwarp();
+        if (valid)
+          ldRow<T, B>(rowPtr<T, G::SB>(NS::dofTile(smem), q, l), acc);
+        else
+#pragma unroll
+          for (int n = 0; n < B; n++) acc[n] = T(0);
+      } else {
+        ldRowG<T, B>(gRow<T, R, G::GB>(a.dofsE, valid ? e : 0, 9, q, r), acc, valid);
+      }
     } else if constexpr (RM > 0) {
 #pragma unroll
       for (int n = 0; n < B; n++) upA[n] = T(0);
     }
-    neighFace<T, O, R, RM, 0>(a, S0, q, l, ev, r, valid, acc, upA);
-    neighFace<T, O, R, RM, 1>(a, S0, q, l, ev, r, valid, acc, upA);
-    neighFace<T, O, R, RM, 2>(a, S0, q, l, ev, r, valid, acc, upA);
-    neighFace<T, O, R, RM, 3>(a, S0, q, l, ev, r, valid, acc, upA);
+    neighItem<T, O, R, RM, 0>(a, smem, q, l, e, valid, cur, nxt, g, nextValid, k, acc, upA);
+    neighItem<T, O, R, RM, 1>(a, smem, q, l, e, valid, cur, nxt, g, nextValid, k, acc, upA);
+    neighItem<T, O, R, RM, 2>(a, smem, q, l, e, valid, cur, nxt, g, nextValid, k, acc, upA);
+    neighItem<T, O, R, RM, 3>(a, smem, q, l, e, valid, cur, nxt, g, nextValid, k, acc, upA);
     if (valid) {
       if (q < 9) {
         stRowG<T, B>(gRow<T, R, G::GB>(a.dofsE, e, 9, q, r), acc);
@@ -690,7 +873,9 @@ __global__ void __launch_bounds__(Geo<T, O, R, RM>::NT, Geo<T, O, R, RM>::minCta
         }
       }
     }
+    cur = nxt;
   }
+  cpAsyncWait<0>();
 }
 
 // ------------------------------------------------------------------------------------------------

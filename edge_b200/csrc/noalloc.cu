@@ -4,6 +4,7 @@
 // while they run.
 #include <cuda_runtime.h>
 
+#include <cstdint>
 #include <mutex>
 
 #include "../../include/edge_b200.h"
@@ -60,6 +61,10 @@ extern "C" int edge_b200_step_noalloc(const edge_b200_cfg *cfg, int64_t n_el, do
   if (!dofs_e || !star_e || !fs_e || !el_fa_el || !fid_el_fa_el || !vid_el_fa_el || !el_fa_type)
     return EDGE_B200_EINVAL;
   if (cfg->n_rms && (!dofs_a || !star_a || !src_a || !fs_a || !omega)) return EDGE_B200_EINVAL;
+  // the neighbour kernel reads an element's four connectivity entries with one vector load
+  if (reinterpret_cast<uintptr_t>(el_fa_el) % 16 || reinterpret_cast<uintptr_t>(fid_el_fa_el) % 4 ||
+      reinterpret_cast<uintptr_t>(vid_el_fa_el) % 4 || reinterpret_cast<uintptr_t>(el_fa_type) % 4)
+    return EDGE_B200_EINVAL;
   const size_t realSize = cfg->precision == 64 ? 8 : 4;
   // scratch: face projections, then the DOFs in the device-resident row layout (256-byte aligned)
   const int B = nModes(cfg->order), GB = rowPad(B, cfg->precision);
