@@ -30,6 +30,8 @@ _SIGS = {
     "edge_setup_anelastic_coeffs": (C.c_int, [C.c_int, dbl, vp, vp]),
     "edge_setup_elastic_lame": (C.c_int, [C.c_int, dbl, vp, vp, vp, dbl, dbl, vp, vp]),
     "edge_setup_dt_cfl": (C.c_int, [vp, C.c_int, vp, vp, vp, vp]),
+    "edge_setup_dt_cfl_el": (C.c_int, [vp, C.c_int, vp, vp, vp, vp]),
+    "edge_setup_time_groups": (C.c_int, [vp, vp, C.c_int, dbl, vp, vp]),
     "edge_setup_locate": (C.c_int, [vp, C.c_int, C.c_int, vp, vp, vp, vp, C.c_int]),
     "edge_setup_eval_basis": (C.c_int, [C.c_int, vp, vp]),
     "edge_setup_trafo": (C.c_int, [vp] * 5),
@@ -47,6 +49,8 @@ _SIGS = {
     "edge_b200_set_sources": (C.c_int, [vp, C.c_int, vp, vp, vp, vp, vp, vp, vp, vp, i64, vp]),
     "edge_b200_set_receivers": (C.c_int, [vp, C.c_int, vp, vp, dbl, dbl, C.c_int]),
     "edge_b200_step": (C.c_int, [vp, dbl, dbl, C.c_int]),
+    "edge_b200_set_time_groups": (C.c_int, [vp, C.c_int, vp]),
+    "edge_b200_step_lts": (C.c_int, [vp, dbl, dbl, C.c_int]),
     "edge_b200_read_receivers": (C.c_int, [vp, vp, vp, vp]),
     "edge_b200_sync": (C.c_int, [vp]),
     "edge_b200_device_dofs": (C.c_int, [vp, vp, vp, vp]),

@@ -100,6 +100,25 @@ struct edge_b200_ctx {
   int32_t recvCount = 0;
   DevBuf grpEl, grpOff, basis, recvBuf;
   std::vector<double> hBufTime;
+  std::vector<int64_t> hRecvGrpEl;  // element of each receiver group (ascending)
+  std::vector<int32_t> hRecvOff;    // receivers of group g: hRecvOff[g] .. hRecvOff[g+1]
+  bool lastLts = false;             // the receivers were last advanced by edge_b200_step_lts
+  std::vector<int64_t> hSrcGrpEl;   // element of each source group (ascending)
+  // host copy of the connectivity (LTS relations are derived from it)
+  std::vector<int32_t> hElFaEl;
+  std::vector<uint8_t> hFId, hFaType;
+  // rate-2 LTS: time groups are element ranges [tgFirst[g], tgFirst[g+1]); per-group receiver
+  // clocks; compact face buffers of the elements at group interfaces
+  int nTg = 0;
+  std::vector<int64_t> tgFirst;
+  std::vector<double> tgRecvTime;
+  std::vector<int32_t> tgRecvCount;
+  DevBuf ltsFlags, ltsRel, sumIdx, halfIdx, faceSum, faceHalf1, faceHalf2;
+  int groupOf(int64_t el) const {
+    int g = 0;
+    while (g + 1 < nTg && el >= tgFirst[g + 1]) g++;
+    return g;
+  }
   double *dTau = nullptr;
   int32_t *dSlot = nullptr;
   size_t tauCap = 0;
@@ -195,6 +214,8 @@ struct edge_b200_ctx {
     a.vId = vId;
     a.faType = faType;
     a.nEl = nEl;
+    a.elFirst = 0;
+    a.elCount = nEl;
     a.dt = dt;
     for (int i = 0; i < 3; i++) a.omega[i] = omega[i];
     return a;
@@ -292,6 +313,9 @@ int edge_b200_upload_mesh(edge_b200_ctx *ctx, const int32_t *el_fa_el, const uin
   EDGE_CUDA(upload(ctx->vId, vid_el_fa_el, n, s), "upload vId");
   EDGE_CUDA(upload(ctx->faType, el_fa_type, n, s), "upload faType");
   EDGE_CUDA(cudaStreamSynchronize(s), "upload mesh");
+  ctx->hElFaEl.assign(el_fa_el, el_fa_el + n);
+  ctx->hFId.assign(fid_el_fa_el, fid_el_fa_el + n);
+  ctx->hFaType.assign(el_fa_type, el_fa_type + n);
   ctx->meshSet = true;
   return EDGE_B200_OK;
 }
@@ -378,6 +402,7 @@ int edge_b200_set_sources(edge_b200_ctx *ctx, int n, const int64_t *el, const in
                           int64_t n_ts, const double *ts) {
   if (!ctx || n < 0) return EDGE_B200_EINVAL;
   ctx->src = SrcArgs{};
+  ctx->hSrcGrpEl.clear();
   if (n == 0) return EDGE_B200_OK;
   if (!el || !run || !scal || !b_eval || !t0 || !dt || !ts_off || !n_pts || !ts) return EDGE_B200_EINVAL;
   std::vector<int32_t> off{0};
@@ -403,6 +428,7 @@ int edge_b200_set_sources(edge_b200_ctx *ctx, int n, const int64_t *el, const in
   EDGE_CUDA(m[8].put(n_pts, n * sizeof(int64_t), s), "sources");
   EDGE_CUDA(m[9].put(ts, n_ts * sizeof(double), s), "sources");
   ctx->src.nGrp = (int)off.size() - 1;
+  for (int g = 0; g + 1 < (int)off.size(); g++) ctx->hSrcGrpEl.push_back(el[off[g]]);
   ctx->src.grpOff = m[0].as<int32_t>();
   ctx->src.el = m[1].as<int64_t>();
   ctx->src.run = m[2].as<int32_t>();
@@ -449,6 +475,10 @@ int edge_b200_set_receivers(edge_b200_ctx *ctx, int n, const int64_t *el, const 
   ctx->period = period;
   ctx->recvCount = 0;
   ctx->hBufTime.assign(max_buf, 0.0);
+  ctx->hRecvGrpEl = gEl;
+  ctx->hRecvOff = gOff;
+  ctx->tgRecvTime.assign(ctx->nTg, t_first);
+  ctx->tgRecvCount.assign(ctx->nTg, 0);
   return EDGE_B200_OK;
 }
 
@@ -457,12 +487,15 @@ int edge_b200_rewind_receivers(edge_b200_ctx *ctx, double t_first) {
   ctx->recvTime = t_first;
   ctx->recvCount = 0;
   std::fill(ctx->hBufTime.begin(), ctx->hBufTime.end(), 0.0);
+  ctx->tgRecvTime.assign(ctx->nTg, t_first);
+  ctx->tgRecvCount.assign(ctx->nTg, 0);
   return EDGE_B200_OK;
 }
 
 int edge_b200_step(edge_b200_ctx *ctx, double t, double dt, int n_steps) {
   if (!ctx || !(dt > 0) || n_steps < 0) return EDGE_B200_EINVAL;
   if (!ctx->meshSet || !ctx->dataSet) return EDGE_B200_EINVAL;
+  ctx->lastLts = false;
   cudaStream_t s = ctx->stream;
   // receiver samples of every step (Receivers::getRecvTimeRel, io/Receivers.cpp:235-248)
   std::vector<int> stepFirst(n_steps + 1, 0);
@@ -534,6 +567,170 @@ int edge_b200_step(edge_b200_ctx *ctx, double t, double dt, int n_steps) {
   return EDGE_B200_OK;
 }
 
+int edge_b200_set_time_groups(edge_b200_ctx *ctx, int n_groups, const int64_t *group_first) {
+  if (!ctx || !ctx->meshSet || n_groups < 1 || n_groups > 16 || !group_first) return EDGE_B200_EINVAL;
+  if (group_first[0] != 0 || group_first[n_groups] != ctx->nEl) return EDGE_B200_EINVAL;
+  for (int g = 0; g < n_groups; g++)
+    if (group_first[g + 1] < group_first[g]) return EDGE_B200_EINVAL;
+  if (n_groups > 1 && !ctx->ks->ltsSupported()) return EDGE_B200_ENOTSUP;
+  const int64_t nEl = ctx->nEl;
+  std::vector<uint8_t> grp(nEl);
+  for (int g = 0; g < n_groups; g++)
+    for (int64_t e = group_first[g]; e < group_first[g + 1]; e++) grp[e] = (uint8_t)g;
+  // relation per inner face (rate 2: face neighbours differ by at most one group), element flags
+  std::vector<uint8_t> rel(4 * nEl, LTS_EQ), flags(nEl, 0);
+  for (int64_t e = 0; e < nEl; e++)
+    for (int f = 0; f < 4; f++) {
+      if (ctx->hFaType[4 * e + f] != EDGE_FACE_INNER) continue;
+      const int64_t ne = ctx->hElFaEl[4 * e + f];
+      const int d = int(grp[e]) - int(grp[ne]);
+      if (d > 1 || d < -1) return EDGE_B200_EINVAL;
+      rel[4 * e + f] = d > 0 ? LTS_GT : d < 0 ? LTS_LT : LTS_EQ;
+      if (d < 0) flags[e] |= LTS_HAS_LARGER;
+      if (d > 0) flags[e] |= LTS_HAS_SMALLER;
+    }
+  std::vector<int32_t> sIdx(nEl, -1), hIdx(nEl, -1);
+  int32_t nSum = 0, nHalf = 0;
+  for (int64_t e = 0; e < nEl; e++) {
+    if (flags[e] & LTS_HAS_LARGER) sIdx[e] = nSum++;
+    if (flags[e] & LTS_HAS_SMALLER) hIdx[e] = nHalf++;
+  }
+  cudaStream_t s = ctx->stream;
+  const size_t slotBytes = (size_t)4 * 9 * ctx->cfg.n_runs * ctx->GF * ctx->realSize;
+  EDGE_CUDA(ctx->ltsFlags.put(flags.data(), flags.size(), s), "time groups");
+  EDGE_CUDA(ctx->ltsRel.put(rel.data(), rel.size(), s), "time groups");
+  EDGE_CUDA(ctx->sumIdx.put(sIdx.data(), sIdx.size() * sizeof(int32_t), s), "time groups");
+  EDGE_CUDA(ctx->halfIdx.put(hIdx.data(), hIdx.size() * sizeof(int32_t), s), "time groups");
+  EDGE_CUDA(ctx->faceSum.fit(std::max<size_t>(nSum * slotBytes, 16)), "time groups");
+  EDGE_CUDA(ctx->faceHalf1.fit(std::max<size_t>(nHalf * slotBytes, 16)), "time groups");
+  EDGE_CUDA(ctx->faceHalf2.fit(std::max<size_t>(nHalf * slotBytes, 16)), "time groups");
+  EDGE_CUDA(cudaMemsetAsync(ctx->faceSum.p, 0, nSum * slotBytes, s), "time groups");
+  EDGE_CUDA(cudaMemsetAsync(ctx->faceHalf1.p, 0, nHalf * slotBytes, s), "time groups");
+  EDGE_CUDA(cudaMemsetAsync(ctx->faceHalf2.p, 0, nHalf * slotBytes, s), "time groups");
+  EDGE_CUDA(cudaStreamSynchronize(s), "time groups");
+  ctx->nTg = n_groups;
+  ctx->tgFirst.assign(group_first, group_first + n_groups + 1);
+  ctx->tgRecvTime.assign(n_groups, ctx->recvTime);
+  ctx->tgRecvCount.assign(n_groups, ctx->recvCount);
+  return EDGE_B200_OK;
+}
+
+int edge_b200_step_lts(edge_b200_ctx *ctx, double t, double dt_fun, int n_cycles) {
+  if (!ctx || !(dt_fun > 0) || n_cycles < 0 || ctx->nTg < 1) return EDGE_B200_EINVAL;
+  if (!ctx->meshSet || !ctx->dataSet) return EDGE_B200_EINVAL;
+  if (!ctx->ks->ltsSupported()) return EDGE_B200_ENOTSUP;
+  ctx->lastLts = true;
+  const int G = ctx->nTg;
+  const int64_t nFun = int64_t(1) << (G - 1);  // fundamental steps per cycle (largest group's step)
+  cudaStream_t s = ctx->stream;
+  // the work regions of the call, in the order of the rate-2 schedule: at fundamental step k the
+  // groups starting a step (k % 2^g == 0) run local + sources, then the groups ending one
+  // ((k+1) % 2^g == 0) run neigh (TimeGroupStatic / man_sched.inc dependencies, sequentialised)
+  struct Work { int kind, g, firstTs; double t, dt; int s0, s1; };
+  std::vector<Work> work;
+  std::vector<double> tau;
+  std::vector<int32_t> slot;
+  // receiver groups and source groups of each time group (both sorted by element)
+  std::vector<int> rB(G), rE(G), sB(G), sE(G);
+  for (int g = 0; g < G; g++) {
+    auto lo = ctx->tgFirst[g], hi = ctx->tgFirst[g + 1];
+    rB[g] = int(std::lower_bound(ctx->hRecvGrpEl.begin(), ctx->hRecvGrpEl.end(), lo) - ctx->hRecvGrpEl.begin());
+    rE[g] = int(std::lower_bound(ctx->hRecvGrpEl.begin(), ctx->hRecvGrpEl.end(), hi) - ctx->hRecvGrpEl.begin());
+    sB[g] = int(std::lower_bound(ctx->hSrcGrpEl.begin(), ctx->hSrcGrpEl.end(), lo) - ctx->hSrcGrpEl.begin());
+    sE[g] = int(std::lower_bound(ctx->hSrcGrpEl.begin(), ctx->hSrcGrpEl.end(), hi) - ctx->hSrcGrpEl.begin());
+  }
+  for (int64_t c = 0; c < n_cycles; c++)
+    for (int64_t k = 0; k < nFun; k++) {
+      const int64_t kk = c * nFun + k;  // fundamental step since t
+      for (int g = 0; g < G; g++) {
+        if (k % (int64_t(1) << g)) continue;
+        const double tg = t + double(kk) * dt_fun, dtg = dt_fun * double(int64_t(1) << g);
+        const int firstTs = ((kk >> g) & 1) == 0;
+        Work w{0, g, firstTs, tg, dtg, (int)tau.size(), 0};
+        if (ctx->nRecv && rE[g] > rB[g]) {
+          double &rt = ctx->tgRecvTime[g];
+          int32_t &rc = ctx->tgRecvCount[g];
+          while (rt > tg - kTolTime && rt < tg + dtg - kTolTime) {
+            if (rc >= ctx->maxBuf) return EDGE_B200_EOVERFLOW;
+            tau.push_back(std::abs(rt - tg));
+            slot.push_back(rc);
+            ctx->hBufTime[rc] = rt;
+            rc++;
+            rt += ctx->period;
+          }
+        }
+        w.s1 = (int)tau.size();
+        work.push_back(w);
+      }
+      for (int g = 0; g < G; g++) {
+        const int64_t span = int64_t(1) << g;
+        if ((k + 1) % span) continue;
+        const int64_t k0 = kk + 1 - span;  // the step that ends now started at k0
+        work.push_back(Work{1, g, ((k0 >> g) & 1) == 0, t + double(k0) * dt_fun, dt_fun * double(span), 0, 0});
+      }
+    }
+  if (!tau.empty()) {
+    if (tau.size() > ctx->tauCap) {
+      dfree(ctx->dTau);
+      dfree(ctx->dSlot);
+      ctx->tauCap = std::max(tau.size(), (size_t)1024);
+      EDGE_CUDA(cudaMalloc(&ctx->dTau, ctx->tauCap * sizeof(double)), "receiver schedule");
+      EDGE_CUDA(cudaMalloc(&ctx->dSlot, ctx->tauCap * sizeof(int32_t)), "receiver schedule");
+    }
+    EDGE_CUDA(cudaMemcpyAsync(ctx->dTau, tau.data(), tau.size() * sizeof(double), cudaMemcpyHostToDevice, s),
+              "receiver schedule");
+    EDGE_CUDA(cudaMemcpyAsync(ctx->dSlot, slot.data(), slot.size() * sizeof(int32_t), cudaMemcpyHostToDevice, s),
+              "receiver schedule");
+  }
+  ctx->launches = 0;
+  for (const Work &w : work) {
+    StepArgsRaw a = ctx->args(w.dt);
+    a.elFirst = ctx->tgFirst[w.g];
+    a.elCount = ctx->tgFirst[w.g + 1] - ctx->tgFirst[w.g];
+    a.faceSum = ctx->faceSum.p;
+    a.faceHalf1 = ctx->faceHalf1.p;
+    a.faceHalf2 = ctx->faceHalf2.p;
+    a.ltsFlags = ctx->ltsFlags.as<uint8_t>();
+    a.ltsRel = ctx->ltsRel.as<uint8_t>();
+    a.sumIdx = ctx->sumIdx.as<int32_t>();
+    a.halfIdx = ctx->halfIdx.as<int32_t>();
+    a.firstTs = w.firstTs;
+    if (a.elCount == 0) continue;
+    if (w.kind == 0) {
+      const int ns = w.s1 - w.s0;
+      if (ns > 0) {
+        RecvArgs r;
+        r.grpEl = ctx->grpEl.as<int64_t>() + rB[w.g];
+        r.grpOff = ctx->grpOff.as<int32_t>() + rB[w.g];
+        r.basis = ctx->basis.as<double>();
+        r.tau = ctx->dTau + w.s0;
+        r.slot = ctx->dSlot + w.s0;
+        r.nSamples = ns;
+        r.nGrp = rE[w.g] - rB[w.g];
+        r.maxBuf = ctx->maxBuf;
+        r.buf = ctx->recvBuf.as<double>();
+        EDGE_CUDA(ctx->launch(3, [&] { return ctx->ks->recv(a, r, s); }), "receiver kernel");
+        ctx->launches++;
+      }
+      EDGE_CUDA(ctx->launch(0, [&] { return ctx->ks->localLts(a, s); }), "local kernel");
+      ctx->launches++;
+      if (sE[w.g] > sB[w.g]) {
+        SrcArgs sa = ctx->src;
+        sa.grpOff += sB[w.g];
+        sa.nGrp = sE[w.g] - sB[w.g];
+        sa.t = w.t;
+        sa.dt = w.dt;
+        EDGE_CUDA(ctx->launch(2, [&] { return ctx->ks->sources(ctx->dofsE, sa, s); }), "source kernel");
+        ctx->launches++;
+      }
+    } else {
+      EDGE_CUDA(ctx->launch(1, [&] { return ctx->ks->neigh(a, s); }), "neighbour kernel");
+      ctx->launches++;
+    }
+  }
+  return EDGE_B200_OK;
+}
+
 int edge_b200_read_receivers(edge_b200_ctx *ctx, double *buf, double *buf_time, int32_t *counts) {
   if (!ctx) return EDGE_B200_EINVAL;
   if (ctx->nRecv == 0) return EDGE_B200_OK;
@@ -542,10 +739,15 @@ int edge_b200_read_receivers(edge_b200_ctx *ctx, double *buf, double *buf_time, 
     EDGE_CUDA(cudaMemcpyAsync(buf, ctx->recvBuf.p, bufCount * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream),
               "read receivers");
   EDGE_CUDA(cudaStreamSynchronize(ctx->stream), "read receivers");
-  for (int i = 0; i < ctx->nRecv; i++) {
-    if (counts) counts[i] = ctx->recvCount;
-    if (buf_time)
-      for (int j = 0; j < ctx->maxBuf; j++) buf_time[(size_t)i * ctx->maxBuf + j] = j < ctx->recvCount ? ctx->hBufTime[j] : 0.0;
+  for (int gi = 0; gi < ctx->nRecvGrp; gi++) {
+    const int64_t el = ctx->hRecvGrpEl[gi];
+    // receivers of one element share its group's clock (the GTS clock without time groups)
+    const int32_t cnt = ctx->lastLts ? ctx->tgRecvCount[ctx->groupOf(el)] : ctx->recvCount;
+    for (int i = ctx->hRecvOff[gi]; i < ctx->hRecvOff[gi + 1]; i++) {
+      if (counts) counts[i] = cnt;
+      if (buf_time)
+        for (int j = 0; j < ctx->maxBuf; j++) buf_time[(size_t)i * ctx->maxBuf + j] = j < cnt ? ctx->hBufTime[j] : 0.0;
+    }
   }
   return EDGE_B200_OK;
 }

@@ -1013,6 +1013,62 @@ int edge_setup_dt_cfl(const edge_mesh *m, int order, const double *rho, const do
   return EDGE_B200_OK;
 }
 
+int edge_setup_dt_cfl_el(const edge_mesh *m, int order, const double *rho, const double *lam,
+                         const double *mu, double *dt_el) {
+  if (!m || order < 1 || !rho || !lam || !mu || !dt_el) return EDGE_B200_EINVAL;
+  for (int64_t e = 0; e < m->nEl(); e++) {
+    double cp = std::sqrt((lam[e] + 2.0 * mu[e]) / rho[e]);
+    double dt = m->elInDia[e];
+    dt *= 0.5;  // SCALE_CFL (src/impl/seismic/const.inc:135-137)
+    dt /= cp;
+    dt /= 2.0 * order - 1;
+    dt_el[e] = dt;
+  }
+  return EDGE_B200_OK;
+}
+
+int edge_setup_time_groups(const edge_mesh *m, const double *dt_el, int n_groups, double fun_dt, uint8_t *el_tg,
+                           int64_t *n_norm) {
+  if (!m || !dt_el || !el_tg || n_groups < 1 || n_groups > 16 || !(fun_dt > 0) || fun_dt > 1)
+    return EDGE_B200_EINVAL;
+  const int64_t nEl = m->nEl();
+  double dtMin = std::numeric_limits<double>::max();
+  for (int64_t e = 0; e < nEl; e++) {
+    if (!(dt_el[e] > 0)) return EDGE_B200_EINVAL;
+    dtMin = std::min(dtMin, dt_el[e]);
+  }
+  // group boundaries fun_dt * 2^g of the relative steps (Groups::setElTg, time/Groups.cpp:84-100)
+  for (int64_t e = 0; e < nEl; e++) {
+    const double ts = dt_el[e] / dtMin;
+    int g = n_groups - 1;
+    double upper = fun_dt * 2;
+    for (int k = 0; k < n_groups - 1; k++, upper *= 2)
+      if (ts < upper) {
+        g = k;
+        break;
+      }
+    el_tg[e] = (uint8_t)g;
+  }
+  // face neighbours differ by at most one group (Groups::normalizeElTgs, time/Groups.cpp:47-82)
+  int64_t changes = 0;
+  for (;;) {
+    int64_t it = 0;
+    for (int64_t e = 0; e < nEl; e++)
+      for (int f = 0; f < 4; f++) {
+        const int64_t ad = m->elFaEl[4 * e + f];
+        if (ad < 0) continue;
+        if (el_tg[e] > el_tg[ad] + 1) {
+          el_tg[e] = (uint8_t)(el_tg[ad] + 1);
+          it++;
+        }
+      }
+    changes += it;
+    if (it == 0) break;
+  }
+  if (n_norm) *n_norm = changes;
+  return EDGE_B200_OK;
+}
+
 int edge_setup_eval_basis(int order, const double ref[3], double *vals) {
   edge_dg_tables t;
   if (!ref || !vals || edge_dg_get(order, &t)) return EDGE_B200_EINVAL;

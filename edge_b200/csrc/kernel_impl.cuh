@@ -8,7 +8,7 @@ namespace edge_b200 {
 template <typename T, int O, int R, int RM>
 class KernelSetImpl final : public KernelSet {
   using G = Geo<T, O, R, RM>;
-  int numSms_ = 0, occLocal_ = 1, occNeigh_ = 1, occRecv_ = 1;
+  int numSms_ = 0, occLocal_ = 1, occNeigh_ = 1, occRecv_ = 1, occLocalLts_ = 1;
 
   static StepArgs<T> cast(const StepArgsRaw &a) {
     StepArgs<T> b;
@@ -26,8 +26,18 @@ class KernelSetImpl final : public KernelSet {
     b.vId = a.vId;
     b.faType = a.faType;
     b.nEl = a.nEl;
+    b.elFirst = a.elFirst;
+    b.elCount = a.elCount;
     b.dt = a.dt;
     for (int i = 0; i < 3; i++) b.omega[i] = a.omega[i];
+    b.faceSum = static_cast<T *>(a.faceSum);
+    b.faceHalf1 = static_cast<T *>(a.faceHalf1);
+    b.faceHalf2 = static_cast<T *>(a.faceHalf2);
+    b.ltsFlags = a.ltsFlags;
+    b.ltsRel = a.ltsRel;
+    b.sumIdx = a.sumIdx;
+    b.halfIdx = a.halfIdx;
+    b.firstTs = a.firstTs;
     return b;
   }
   static constexpr size_t smemLocal() { return G::smemLocal; }
@@ -38,16 +48,25 @@ class KernelSetImpl final : public KernelSet {
   cudaError_t init(int device) override {
     cudaError_t e;
     if ((e = cudaDeviceGetAttribute(&numSms_, cudaDevAttrMultiProcessorCount, device))) return e;
-    if ((e = cudaFuncSetAttribute(kLocal<T, O, R, RM>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smemLocal())))
+    if ((e = cudaFuncSetAttribute(kLocal<T, O, R, RM, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smemLocal())))
       return e;
     if ((e = cudaFuncSetAttribute(kNeigh<T, O, R, RM>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smemNeigh())))
       return e;
     if ((e = cudaFuncSetAttribute(kRecv<T, O, R, RM>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smemRecv())))
       return e;
-    if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occLocal_, kLocal<T, O, R, RM>, G::NT, smemLocal())))
+    if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occLocal_, kLocal<T, O, R, RM, false>, G::NT, smemLocal())))
       return e;
     if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occNeigh_, kNeigh<T, O, R, RM>, G::NT, smemNeigh())))
       return e;
+    if constexpr (G::ltsOk) {
+      if ((e = cudaFuncSetAttribute(kLocal<T, O, R, RM, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    (int)G::smemLocalLts)))
+        return e;
+      if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occLocalLts_, kLocal<T, O, R, RM, true>, G::NT,
+                                                             G::smemLocalLts)))
+        return e;
+      occLocalLts_ = occLocalLts_ < 1 ? 1 : occLocalLts_;
+    }
     occLocal_ = occLocal_ < 1 ? 1 : occLocal_;
     occNeigh_ = occNeigh_ < 1 ? 1 : occNeigh_;
     return cudaSuccess;
@@ -62,11 +81,23 @@ class KernelSetImpl final : public KernelSet {
   }
 
   cudaError_t local(const StepArgsRaw &a, cudaStream_t s) override {
-    kLocal<T, O, R, RM><<<grid(a.nEl, ctasLocal()), G::NT, smemLocal(), s>>>(cast(a));
+    if (a.elCount < 1) return cudaSuccess;
+    kLocal<T, O, R, RM, false><<<grid(a.elCount, ctasLocal()), G::NT, smemLocal(), s>>>(cast(a));
     return cudaGetLastError();
   }
+  cudaError_t localLts(const StepArgsRaw &a, cudaStream_t s) override {
+    if constexpr (G::ltsOk) {
+      if (a.elCount < 1) return cudaSuccess;
+      kLocal<T, O, R, RM, true><<<grid(a.elCount, numSms_ * occLocalLts_), G::NT, G::smemLocalLts, s>>>(cast(a));
+      return cudaGetLastError();
+    } else {
+      return cudaErrorNotSupported;
+    }
+  }
+  bool ltsSupported() const override { return G::ltsOk; }
   cudaError_t neigh(const StepArgsRaw &a, cudaStream_t s) override {
-    kNeigh<T, O, R, RM><<<grid(a.nEl, ctasNeigh()), G::NT, smemNeigh(), s>>>(cast(a));
+    if (a.elCount < 1) return cudaSuccess;
+    kNeigh<T, O, R, RM><<<grid(a.elCount, ctasNeigh()), G::NT, smemNeigh(), s>>>(cast(a));
     return cudaGetLastError();
   }
   cudaError_t recv(const StepArgsRaw &a, const RecvArgs &r, cudaStream_t s) override {

@@ -11,13 +11,19 @@ struct SrcArgs;
 
 // StepArgs with the DOF pointers untyped; the concrete KernelSet casts to its precision.
 struct StepArgsRaw {
-  void *dofsE, *dofsA, *tDofs, *face;
-  const double *starE, *starA, *srcA, *fsE, *fsA;
-  const int32_t *elFaEl;
-  const uint8_t *fId, *vId, *faType;
-  int64_t nEl;
-  double dt;
-  double omega[3];
+  void *dofsE = nullptr, *dofsA = nullptr, *tDofs = nullptr, *face = nullptr;
+  const double *starE = nullptr, *starA = nullptr, *srcA = nullptr, *fsE = nullptr, *fsA = nullptr;
+  const int32_t *elFaEl = nullptr;
+  const uint8_t *fId = nullptr, *vId = nullptr, *faType = nullptr;
+  int64_t nEl = 0;
+  int64_t elFirst = 0, elCount = 0;  // element range of the launch (a time group, or all)
+  double dt = 0;
+  double omega[3] = {0, 0, 0};
+  // rate-2 LTS (all null for GTS): see StepArgs
+  void *faceSum = nullptr, *faceHalf1 = nullptr, *faceHalf2 = nullptr;
+  const uint8_t *ltsFlags = nullptr, *ltsRel = nullptr;
+  const int32_t *sumIdx = nullptr, *halfIdx = nullptr;
+  int firstTs = 0;
 };
 
 class KernelSet {
@@ -25,6 +31,9 @@ class KernelSet {
   virtual ~KernelSet() {}
   virtual cudaError_t init(int device) = 0;  // sets smem attributes, sizes the persistent grids
   virtual cudaError_t local(const StepArgsRaw &a, cudaStream_t s) = 0;
+  // local step with the LTS face buffers (the half-step time integral needs one more tile)
+  virtual cudaError_t localLts(const StepArgsRaw &a, cudaStream_t s) = 0;
+  virtual bool ltsSupported() const = 0;
   virtual cudaError_t neigh(const StepArgsRaw &a, cudaStream_t s) = 0;
   virtual cudaError_t recv(const StepArgsRaw &a, const RecvArgs &r, cudaStream_t s) = 0;
   virtual cudaError_t sources(void *dofsE, const SrcArgs &sa, cudaStream_t s) = 0;

@@ -38,9 +38,22 @@ struct StepArgs {
   const int32_t *elFaEl;
   const uint8_t *fId, *vId, *faType;
   int64_t nEl;
+  int64_t elFirst, elCount;  // the launch covers elements [elFirst, elFirst + elCount)
   double dt;
   double omega[3];
+  // rate-2 LTS (AderDg.hpp:384-417, 620-674), null for GTS. Elements with a larger neighbour keep
+  // the face projections of their time integrals summed over two steps (faceSum, compact slot
+  // sumIdx[el]); elements with a smaller neighbour those of the half-step integrals over [0, dt/2]
+  // and [dt/2, dt] (faceHalf1 / faceHalf2, slot halfIdx[el]). Each compact buffer is
+  // [slots][4][9][R][GF] like face.
+  T *faceSum, *faceHalf1, *faceHalf2;
+  const uint8_t *ltsFlags;  // [nEl] bit 0: a larger neighbour, bit 1: a smaller neighbour
+  const uint8_t *ltsRel;    // [nEl][4] 0 equal, 1 this element larger, 2 this element smaller
+  const int32_t *sumIdx, *halfIdx;
+  int firstTs;              // first step of a rate-2 pair of this group
 };
+enum { LTS_HAS_LARGER = 1, LTS_HAS_SMALLER = 2 };
+enum { LTS_EQ = 0, LTS_GT = 1, LTS_LT = 2 };
 
 // sparse patterns (row-major non-zeros): elastic star rows -> (index into the 24, column);
 // missing third entries use index -1 (coefficient 0) and a valid column.
@@ -211,6 +224,10 @@ struct Geo {
   static constexpr size_t nTI = tiSmem ? nX : nS0;
   static constexpr size_t nTIA = tiSmem ? nXA : 0;
   static constexpr size_t smemLocal = (nX + nTI + nXA + nTIA) * sizeof(T);
+  // LTS local step: one more [9][32][SB] tile for the half-step time integral (behind the rest);
+  // configurations whose time integrals do not fit shared memory have no LTS kernels
+  static constexpr size_t smemLocalLts = smemLocal + nX * sizeof(T);
+  static constexpr bool ltsOk = tiSmem && smemLocalLts <= 227 * 1024;
   // neighbour kernel: a ring of NSN slots, each [9][32][SF] face rows and, for E <= 4, the E
   // elements' flux-solver blocks (81 + 54 doubles); as many slots (2..4) as fit the shared memory
   // of minCtasNeigh CTAs per SM (228 KB, 1 KB reserved per CTA)
@@ -357,15 +374,17 @@ __device__ __forceinline__ void addSrc(const ElemCoef<T, RM> &c, const T *Y, int
 // derivative D of TimePredVanilla::ck (TimePredVanilla.hpp:229-303) with the star matrix applied
 // before the stiffness product; der[D] replaces der[D-1] in X, TI += sca * der[D] (rows owned by
 // their warp), the anelastic warps update XA and TIA.
-template <typename T, int O, int R, int RM, int D>
+template <typename T, int O, int R, int RM, int D, bool H = false>
 struct CkStep {
   using G = Geo<T, O, R, RM>;
   static constexpr int B = G::B, S = G::SB;
   static constexpr int NN = RM ? nModes(O - 1) : nModes(O - D);  // output modes of the product
   static constexpr int DK = RM ? 1 : D;                           // truncation of the product
 
+  // H: also TIh += scaH * der[D] (the time integral over the first half of the step, for LTS)
   __device__ __forceinline__ static void run(T *X, T *TI, T *XA, T *TIA, int q, int l, const ElemCoef<T, RM> &c,
-                                             const double *omega, T sca, T *tIr, T (*tIAr)[B]) {
+                                             const double *omega, T sca, T *tIr, T (*tIAr)[B], T *TIh = nullptr,
+                                             T scaH = T(0)) {
     T acc[B];
 #pragma unroll
     for (int n = 0; n < B; n++) acc[n] = T(0);
@@ -390,6 +409,13 @@ struct CkStep {
 #pragma unroll
         for (int n = 0; n < NW; n++) t[n] = fmaT(sca, acc[n], t[n]);
         stRow<T, NW>(p, t);
+        if constexpr (H) {
+          T *ph = rowPtr<T, S>(TIh, q, l);
+          ldRow<T, NW>(ph, t);
+#pragma unroll
+          for (int n = 0; n < NW; n++) t[n] = fmaT(scaH, acc[n], t[n]);
+          stRow<T, NW>(ph, t);
+        }
       } else {
 #pragma unroll
         for (int n = 0; n < NW; n++) tIr[n] = fmaT(sca, acc[n], tIr[n]);
@@ -422,13 +448,15 @@ struct CkStep {
   }
 };
 
-template <typename T, int O, int R, int RM, int D>
+template <typename T, int O, int R, int RM, int D, bool H = false>
 __device__ __forceinline__ void ckAll(T *X, T *TI, T *XA, T *TIA, int q, int l, const ElemCoef<T, RM> &c,
-                                      const double *omega, T dt, T sca, T *tIr, T (*tIAr)[nModes(O)]) {
+                                      const double *omega, T dt, T sca, T *tIr, T (*tIAr)[nModes(O)],
+                                      T *TIh = nullptr, T scaH = T(0)) {
   if constexpr (D < O) {
     sca = sca * dt / T(D + 1);
-    CkStep<T, O, R, RM, D>::run(X, TI, XA, TIA, q, l, c, omega, sca, tIr, tIAr);
-    ckAll<T, O, R, RM, D + 1>(X, TI, XA, TIA, q, l, c, omega, dt, sca, tIr, tIAr);
+    if constexpr (H) scaH = scaH * (dt * T(0.5)) / T(D + 1);
+    CkStep<T, O, R, RM, D, H>::run(X, TI, XA, TIA, q, l, c, omega, sca, tIr, tIAr, TIh, scaH);
+    ckAll<T, O, R, RM, D + 1, H>(X, TI, XA, TIA, q, l, c, omega, dt, sca, tIr, tIAr, TIh, scaH);
   }
 }
 
@@ -457,9 +485,9 @@ __device__ __forceinline__ void faceMix(const T *S0, int l, const T (&fr)[9], T 
 // ------------------------------------------------------------------------------------------------
 // local step: CK, volume, local surface, face projections (AderDg::local, AderDg.hpp:338-534)
 // ------------------------------------------------------------------------------------------------
-template <typename T, int O, int R, int RM, int FA>
+template <typename T, int O, int R, int RM, int FA, bool LTS = false>
 __device__ __forceinline__ void localFace(const StepArgs<T> &a, const T *TI, T *S0, int q, int l, int64_t e,
-                                          int r, bool valid, T *acc, T *upA) {
+                                          int r, bool valid, T *acc, T *upA, const T *TIh = nullptr) {
   using G = Geo<T, O, R, RM>;
   constexpr int F = G::F, SF = G::SF, SB = G::SB;
   T s[F];
@@ -469,6 +497,32 @@ __device__ __forceinline__ void localFace(const StepArgs<T> &a, const T *TI, T *
     FluxLMul<O, FA>::template run<T>(OwnRow<T>{rowPtr<T, SB>(TI, q, l)}, s);
     stRow<T, F>(rowPtr<T, SF>(S0, q, l), s);
     if (valid) stRowG<T, F>(gRow<T, R, G::GF>(a.face, e * 4 + FA, 9, q, r), s);
+    if constexpr (LTS) {
+      if (valid) {
+        const int fl = a.ltsFlags[e];
+        if (fl & LTS_HAS_LARGER) {
+          // face projection of the time integral summed over the two steps of a pair
+          T *p = gRow<T, R, G::GF>(a.faceSum, int64_t(a.sumIdx[e]) * 4 + FA, 9, q, r);
+          T v[F];
+          ldRowG<T, F>(p, v, !a.firstTs);
+#pragma unroll
+          for (int j = 0; j < F; j++) v[j] += s[j];
+          stRowG<T, F>(p, v);
+        }
+        if (fl & LTS_HAS_SMALLER) {
+          // face projections of the integrals over [0, dt/2] and [dt/2, dt]
+          T h[F];
+#pragma unroll
+          for (int j = 0; j < F; j++) h[j] = T(0);
+          FluxLMul<O, FA>::template run<T>(OwnRow<T>{rowPtr<T, SB>(TIh, q, l)}, h);
+          const int64_t slot = int64_t(a.halfIdx[e]) * 4 + FA;
+          stRowG<T, F>(gRow<T, R, G::GF>(a.faceHalf1, slot, 9, q, r), h);
+#pragma unroll
+          for (int j = 0; j < F; j++) h[j] = s[j] - h[j];
+          stRowG<T, F>(gRow<T, R, G::GF>(a.faceHalf2, slot, 9, q, r), h);
+        }
+      }
+    }
   }
   // flux-solver row of this thread (elastic 9x9 or anelastic 6x9), loaded before the barrier
   T fr[9];
@@ -490,25 +544,28 @@ __device__ __forceinline__ void localFace(const StepArgs<T> &a, const T *TI, T *
   __syncthreads();
 }
 
-template <typename T, int O, int R, int RM>
-__global__ void __launch_bounds__(Geo<T, O, R, RM>::NT, Geo<T, O, R, RM>::minCtasLocal) kLocal(StepArgs<T> a) {
+template <typename T, int O, int R, int RM, bool LTS>
+__global__ void __launch_bounds__(Geo<T, O, R, RM>::NT, LTS ? 1 : Geo<T, O, R, RM>::minCtasLocal)
+    kLocal(StepArgs<T> a) {
   using G = Geo<T, O, R, RM>;
   constexpr int B = G::B, E = G::E, SB = G::SB;
   extern __shared__ __align__(16) unsigned char smem[];
   T *X = reinterpret_cast<T *>(smem);
   T *XA = X + G::nX + G::nTI;
   // see Geo: time integrals in shared memory (TI behind X, TIA behind XA, face tiles reuse X) or
-  // in registers (copied into X / XA after the recursion, face tiles behind X)
+  // in registers (copied into X / XA after the recursion, face tiles behind X); with LTS the
+  // half-step integral TIh behind everything
   T *TI = G::tiSmem ? X + G::nX : X;
   T *TIA = G::tiSmem ? XA + G::nXA : XA;
   T *S0 = G::tiSmem ? X : X + G::nX;
+  T *TIh = LTS ? reinterpret_cast<T *>(smem + G::smemLocal) : nullptr;
   const int q = threadIdx.x >> 5, l = threadIdx.x & 31;
   const int eo = l / R, r = l % R;
-  const int64_t nGroups = (a.nEl + E - 1) / E;
+  const int64_t nGroups = (a.elCount + E - 1) / E;
   const T dt = T(a.dt);
   for (int64_t g = blockIdx.x; g < nGroups; g += gridDim.x) {
-    const int64_t e = g * E + eo;
-    const bool valid = e < a.nEl;
+    const int64_t e = a.elFirst + g * E + eo;
+    const bool valid = g * E + eo < a.elCount;
     const int64_t ev = valid ? e : 0;
     T tIr[G::tiSmem ? 1 : B];
     T tIAr[(G::tiSmem || RM == 0) ? 1 : RM][B];
@@ -517,6 +574,12 @@ __global__ void __launch_bounds__(Geo<T, O, R, RM>::NT, Geo<T, O, R, RM>::minCta
       T v[B];
       ldRowG<T, B>(gRow<T, R, G::GB>(a.dofsE, ev, 9, q, r), v, valid);
       stRow<T, B>(rowPtr<T, SB>(X, q, l), v);
+      if constexpr (LTS) {
+        T h[B];
+#pragma unroll
+        for (int n = 0; n < B; n++) h[n] = (dt * T(0.5)) * v[n];
+        stRow<T, B>(rowPtr<T, SB>(TIh, q, l), h);
+      }
 #pragma unroll
       for (int n = 0; n < B; n++) v[n] = dt * v[n];
       if constexpr (G::tiSmem)
@@ -546,7 +609,7 @@ __global__ void __launch_bounds__(Geo<T, O, R, RM>::NT, Geo<T, O, R, RM>::minCta
     c.load(a, ev, valid, q);
     __syncthreads();
     // Cauchy-Kowalevski (TimePredVanilla::ck, TimePredVanilla.hpp:200-306)
-    ckAll<T, O, R, RM, 1>(X, TI, XA, TIA, q, l, c, a.omega, dt, dt, tIr, tIAr);
+    ckAll<T, O, R, RM, 1, LTS>(X, TI, XA, TIA, q, l, c, a.omega, dt, dt, tIr, tIAr, TIh, dt * T(0.5));
     if constexpr (!G::tiSmem) {
       if (q < 9) {
         stRow<T, B>(rowPtr<T, SB>(X, q, l), tIr);
@@ -582,10 +645,10 @@ __global__ void __launch_bounds__(Geo<T, O, R, RM>::NT, Geo<T, O, R, RM>::minCta
       VolMul<O>::template run<T>(z, acc);
     }
     // local surface integral (SurfIntVanilla::local, SurfIntVanilla.hpp:212-262) + face projections
-    localFace<T, O, R, RM, 0>(a, TI, S0, q, l, ev, r, valid, acc, upA);
-    localFace<T, O, R, RM, 1>(a, TI, S0, q, l, ev, r, valid, acc, upA);
-    localFace<T, O, R, RM, 2>(a, TI, S0, q, l, ev, r, valid, acc, upA);
-    localFace<T, O, R, RM, 3>(a, TI, S0, q, l, ev, r, valid, acc, upA);
+    localFace<T, O, R, RM, 0, LTS>(a, TI, S0, q, l, ev, r, valid, acc, upA, TIh);
+    localFace<T, O, R, RM, 1, LTS>(a, TI, S0, q, l, ev, r, valid, acc, upA, TIh);
+    localFace<T, O, R, RM, 2, LTS>(a, TI, S0, q, l, ev, r, valid, acc, upA, TIh);
+    localFace<T, O, R, RM, 3, LTS>(a, TI, S0, q, l, ev, r, valid, acc, upA, TIh);
     if (valid) {
       if (q < 9) {
         stRowG<T, B>(gRow<T, R, G::GB>(a.dofsE, e, 9, q, r), acc);
@@ -637,27 +700,37 @@ __device__ __forceinline__ void cpAsyncWait() {
   asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
 }
 
-// face connectivity of one element (all four faces), packed as loaded: neighbour ids, and one
-// byte per face for the neighbour's face id, the vertex id and the face type
+// face connectivity of one element (all four faces): the face slot each face gathers from
+// (neighbour * 4 + its face id, or a compact LTS slot * 4 + face id), and one byte per face for the
+// buffer (LTS relation), the vertex id and the face type
 struct FaceMeta {
-  int32_t ne[4];
-  uint32_t fo, vi, ty;
-  __device__ __forceinline__ void load(const int32_t *elFaEl, const uint8_t *fId, const uint8_t *vId,
-                                       const uint8_t *faType, int64_t e, bool valid) {
+  int32_t src[4];
+  uint32_t rel, vi, ty;
+  template <typename T>
+  __device__ __forceinline__ void load(const StepArgs<T> &a, int64_t e, bool valid) {
     if (valid) {
-      const int4 n = __ldg(reinterpret_cast<const int4 *>(elFaEl) + e);
-      ne[0] = n.x; ne[1] = n.y; ne[2] = n.z; ne[3] = n.w;
-      fo = __ldg(reinterpret_cast<const uint32_t *>(fId) + e);
-      vi = __ldg(reinterpret_cast<const uint32_t *>(vId) + e);
-      ty = __ldg(reinterpret_cast<const uint32_t *>(faType) + e);
+      const int4 n = __ldg(reinterpret_cast<const int4 *>(a.elFaEl) + e);
+      const uint32_t fo = __ldg(reinterpret_cast<const uint32_t *>(a.fId) + e);
+      vi = __ldg(reinterpret_cast<const uint32_t *>(a.vId) + e);
+      ty = __ldg(reinterpret_cast<const uint32_t *>(a.faType) + e);
+      rel = a.ltsRel ? __ldg(reinterpret_cast<const uint32_t *>(a.ltsRel) + e) : 0u;
+      const int32_t ne[4] = {n.x, n.y, n.z, n.w};
+#pragma unroll
+      for (int f = 0; f < 4; f++) {
+        int32_t slotEl = ne[f];
+        const int rf = (rel >> (8 * f)) & 0xff;
+        if (((ty >> (8 * f)) & 0xff) == FT_INNER && rf != LTS_EQ)
+          slotEl = __ldg((rf == LTS_GT ? a.sumIdx : a.halfIdx) + ne[f]);
+        src[f] = slotEl * 4 + int32_t((fo >> (8 * f)) & 0xff);
+      }
     } else {
-      ne[0] = ne[1] = ne[2] = ne[3] = 0;
-      fo = vi = 0;
+      src[0] = src[1] = src[2] = src[3] = 0;
+      rel = vi = 0;
       ty = 0x02020202u;  // outflow on every face: nothing to gather or add
     }
   }
   __device__ __forceinline__ int type(int f) const { return (ty >> (8 * f)) & 0xff; }
-  __device__ __forceinline__ int faceOf(int f) const { return (fo >> (8 * f)) & 0xff; }
+  __device__ __forceinline__ int relation(int f) const { return (rel >> (8 * f)) & 0xff; }
   __device__ __forceinline__ int vert(int f) const { return (vi >> (8 * f)) & 0xff; }
 };
 
@@ -685,8 +758,8 @@ struct NeighSlots {
                                                    int64_t g, bool groupValid) {
     if constexpr (G::dofTile) {
       const int eo = l / R, r = l % R;
-      const int64_t e = g * E + eo;
-      if (!groupValid || q >= 9 || e >= a.nEl) return;
+      const int64_t e = a.elFirst + g * E + eo;
+      if (!groupValid || q >= 9 || g * E + eo >= a.elCount) return;
       const T *blk = a.dofsE + (e * 9 + q) * int64_t(R * G::GB);
       T *dst = dofTile(base) + (q * 32 + eo * R) * G::SB;
 #pragma unroll
@@ -704,11 +777,18 @@ struct NeighSlots {
                                                int64_t g, bool groupValid, const FaceMeta &m) {
     if (groupValid) {
       const int eo = l / R, r = l % R;
-      const int64_t e = g * E + eo;
+      const int64_t e = a.elFirst + g * E + eo;
       const int ty = m.type(FA);
-      if (q < 9 && e < a.nEl && ty != FT_OUTFLOW) {
-        const int64_t srcFace = ty == FT_INNER ? int64_t(m.ne[FA]) * 4 + m.faceOf(FA) : e * 4 + FA;
-        const T *blk = a.face + (srcFace * 9 + q) * int64_t(R * GF);
+      if (q < 9 && g * E + eo < a.elCount && ty != FT_OUTFLOW) {
+        // inner faces: the neighbour's projection over this element's step (its own face buffer,
+        // or with LTS its two-step sum / half-step buffer); free surface: this element's own
+        const T *buf = a.face;
+        if (ty == FT_INNER) {
+          const int rf = m.relation(FA);
+          buf = rf == LTS_EQ ? a.face : rf == LTS_GT ? a.faceSum : (a.firstTs ? a.faceHalf1 : a.faceHalf2);
+        }
+        const int64_t srcFace = ty == FT_INNER ? int64_t(m.src[FA]) : e * 4 + FA;
+        const T *blk = buf + (srcFace * 9 + q) * int64_t(R * GF);
         T *dst = rows(base, slot) + (q * 32 + eo * R) * SF;
 #pragma unroll
         for (int it = 0; it < CPR; it++) {
@@ -722,8 +802,8 @@ struct NeighSlots {
         double *fsDst = fs(base, slot);
         for (int i = threadIdx.x; i < E * NFS; i += NT) {
           const int eo2 = i / NFS, j = i % NFS;
-          const int64_t e2 = g * E + eo2;
-          if (e2 >= a.nEl) continue;
+          if (g * E + eo2 >= a.elCount) continue;
+          const int64_t e2 = a.elFirst + g * E + eo2;
           const double *src = j < 81 ? a.fsE + ((a.nEl + e2) * 4 + FA) * 81 + j
                                      : a.fsA + ((a.nEl + e2) * 4 + FA) * 54 + (j - 81);
           cpAsync8(fsDst + i, src);
@@ -817,21 +897,21 @@ __global__ void __launch_bounds__(Geo<T, O, R, RM>::NT, Geo<T, O, R, RM>::minCta
   extern __shared__ __align__(16) unsigned char smem[];
   const int q = threadIdx.x >> 5, l = threadIdx.x & 31;
   const int eo = l / R, r = l % R;
-  const int64_t nGroups = (a.nEl + E - 1) / E;
+  const int64_t nGroups = (a.elCount + E - 1) / E;
   int64_t g = blockIdx.x;
   FaceMeta cur, nxt;
-  cur.load(a.elFaEl, a.fId, a.vId, a.faType, g * E + eo, g * E + eo < a.nEl);
+  cur.load(a, a.elFirst + g * E + eo, g * E + eo < a.elCount);
   // prologue: the first group's DOF rows and items 0 .. NSN-2 (its first faces)
   NS::issueDofs(a, smem, q, l, g, g < nGroups);
   NS::template issue<0>(a, smem, 0, q, l, g, g < nGroups, cur);
   if constexpr (NSN > 2) NS::template issue<1>(a, smem, 1, q, l, g, g < nGroups, cur);
   if constexpr (NSN > 3) NS::template issue<2>(a, smem, 2, q, l, g, g < nGroups, cur);
   for (int64_t k = 0; g < nGroups; g += gridDim.x, k++) {
-    const int64_t e = g * E + eo;
-    const bool valid = e < a.nEl;
+    const int64_t e = a.elFirst + g * E + eo;
+    const bool valid = g * E + eo < a.elCount;
     const int64_t gn = g + gridDim.x;
     const bool nextValid = gn < nGroups;
-    nxt.load(a.elFaEl, a.fId, a.vId, a.faType, gn * E + eo, nextValid && gn * E + eo < a.nEl);
+    nxt.load(a, a.elFirst + gn * E + eo, nextValid && gn * E + eo < a.elCount);
     T acc[B];
     T upA[RM ? B : 1];
     if (q < 9) {

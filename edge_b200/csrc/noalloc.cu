@@ -108,6 +108,8 @@ extern "C" int edge_b200_step_noalloc(const edge_b200_cfg *cfg, int64_t n_el, do
   a.vId = vid_el_fa_el;
   a.faType = el_fa_type;
   a.nEl = n_el;
+  a.elFirst = 0;
+  a.elCount = n_el;
   a.dt = dt;
   for (int m = 0; m < 3; m++) a.omega[m] = (cfg->n_rms && m < cfg->n_rms) ? omega[m] : 0.0;
   cudaStream_t s = (cudaStream_t)cfg->stream;

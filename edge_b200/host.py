@@ -178,6 +178,48 @@ def dt_cfl(mesh, order, rho, lam, mu):
     return out.value
 
 
+def dt_cfl_el(mesh, order, rho, lam, mu):
+    """Per-element CFL time steps (edge_setup_dt_cfl_el)."""
+    out = np.zeros(mesh.n_el)
+    a = [np.ascontiguousarray(x, np.float64) for x in (rho, lam, mu)]
+    check(lib().edge_setup_dt_cfl_el(mesh._h, order, *[ptr(x) for x in a], ptr(out)), "dt_cfl_el")
+    return out
+
+
+def time_groups(mesh, dt_el, n_groups, fun_dt=1.0):
+    """Rate-2 LTS time group of every element (edge_setup_time_groups, EDGE-V's rules)."""
+    out = np.zeros(mesh.n_el, np.uint8)
+    check(lib().edge_setup_time_groups(mesh._h, ptr(np.ascontiguousarray(dt_el, np.float64)), int(n_groups),
+                                       float(fun_dt), ptr(out), None), "time_groups")
+    return out
+
+
+def lts_tables(mesh, el_tg):
+    """Element flags (1: a larger neighbour, 2: a smaller one) and per-face relations (0 equal,
+    1 this element larger, 2 smaller) of LTS time groups, as the device derives them."""
+    el_tg = np.asarray(el_tg, np.int64)
+    ne = mesh.el_fa_el.astype(np.int64)
+    inner = (mesh.el_fa_type == FACE_INNER) & (ne >= 0)
+    d = np.where(inner, el_tg[:, None] - el_tg[np.maximum(ne, 0)], 0)
+    if np.abs(d).max(initial=0) > 1:
+        raise ValueError("face neighbours differ by more than one time group")
+    rel = np.where(d > 0, 1, np.where(d < 0, 2, 0)).astype(np.uint8)
+    flags = (np.any(d < 0, axis=1) * 1 + np.any(d > 0, axis=1) * 2).astype(np.uint8)
+    return flags, np.ascontiguousarray(rel)
+
+
+def sort_by_groups(mesh, el_tg):
+    """The mesh with its elements ordered by time group (stable), the input index of each new
+    element, and group_first [G+1] (element ranges of the groups)."""
+    el_tg = np.asarray(el_tg)
+    perm = np.argsort(el_tg, kind="stable")
+    bf_ve, tag = mesh.boundary_faces()
+    m = Mesh.from_arrays(mesh.ve, mesh.el_ve[perm], bf_ve, tag, reorder=False)
+    n_groups = int(el_tg.max()) + 1
+    group_first = np.searchsorted(el_tg[perm], np.arange(n_groups + 1)).astype(np.int64)
+    return m, perm, group_first
+
+
 def locate(mesh, order, xyz, source=False):
     xyz = np.ascontiguousarray(np.atleast_2d(xyz), np.float64)
     n = xyz.shape[0]

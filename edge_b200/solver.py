@@ -80,6 +80,19 @@ class Solver:
             tt += dt
         self.t = tt
 
+    def set_time_groups(self, group_first):
+        """Rate-2 LTS time groups: group g = elements [group_first[g], group_first[g+1])."""
+        gf = np.ascontiguousarray(group_first, np.int64)
+        self.n_groups = len(gf) - 1
+        self._chk(lib().edge_b200_set_time_groups(self._h, self.n_groups, ptr(gf)), "set_time_groups")
+
+    def step_lts(self, n_cycles=1, dt_fun=None, t=None):
+        """n_cycles steps of the largest group (2^(G-1) fundamental steps of dt_fun each)."""
+        dt_fun = self.prob.dt if dt_fun is None else dt_fun
+        t0 = self.t if t is None else t
+        self._chk(lib().edge_b200_step_lts(self._h, t0, dt_fun, n_cycles), "step_lts")
+        self.t = t0 + float(n_cycles * (1 << (self.n_groups - 1))) * dt_fun
+
     def sync(self):
         self._chk(lib().edge_b200_sync(self._h), "sync")
 

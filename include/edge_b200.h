@@ -108,6 +108,16 @@ int edge_setup_elastic_lame(int n_rms, double freq_ref, const double *freqs,
 /* CFL time step: min over elements of 0.5 * inDia / vp / (2O-1) (common.hpp:84-133). */
 int edge_setup_dt_cfl(const edge_mesh *m, int order, const double *rho, const double *lam,
                       const double *mu, double *dt_min);
+/* Per-element CFL time steps dt_el[nEl] (the quantity edge_setup_dt_cfl minimises). */
+int edge_setup_dt_cfl_el(const edge_mesh *m, int order, const double *rho, const double *lam,
+                         const double *mu, double *dt_el);
+/* Rate-2 LTS time groups el_tg[nEl] of EDGE-V (time/Groups.cpp:84-100 setElTg, 47-82
+ * normalizeElTgs): with ts = dt_el / min(dt_el), an element joins the first group g with
+ * ts < fun_dt * 2^(g+1) (the last of n_groups takes the rest); groups are then lowered until face
+ * neighbours differ by at most one. Group g steps with fun_dt * min(dt_el) * 2^g. *n_norm
+ * (may be NULL) receives the number of lowerings. */
+int edge_setup_time_groups(const edge_mesh *m, const double *dt_el, int n_groups, double fun_dt, uint8_t *el_tg,
+                           int64_t *n_norm);
 /* Locates n points; per point the element, reference coordinates and basis values
  * basis[n][B]. scale_mass_jac != 0 multiplies by M^-1 and divides by detJ as point sources do
  * (PointSources::initBasisEvals, PointSources.hpp:388-509); 0 gives plain basis values as
@@ -186,6 +196,22 @@ int edge_b200_rewind_receivers(edge_b200_ctx *ctx, double t_first);
 /* n_steps GTS steps from time t with step dt: local -> sources -> neighbour
  * (TimeGroupStatic::computeStep, src/time/TimeGroupStatic.cpp:113-127, steps.inc:24-77). */
 int edge_b200_step(edge_b200_ctx *ctx, double t, double dt, int n_steps);
+/* Rate-2 local time stepping (EDGE's LTS: TimeGroupStatic, src/time/TimeGroupStatic.cpp:46-111,
+ * the work-region dependencies of src/impl/seismic/inc/time/man_sched.inc:37-206 and the LTS
+ * branches of AderDg::local / ::neigh, AderDg.hpp:384-417 and 620-674). The mesh elements must be
+ * ordered by time group: group g holds the elements [group_first[g], group_first[g+1]) and steps
+ * with dt_fun * 2^g; face neighbours differ by at most one group (edge_setup_time_groups gives
+ * such groups; sort the elements by group before building the context). Elements at group
+ * interfaces get device buffers for the face projections of their summed and half-step time
+ * integrals. EDGE_B200_ENOTSUP when n_groups > 1 and the configuration has no LTS kernels (the
+ * half-step integral needs shared memory the largest FP64 orders lack). */
+int edge_b200_set_time_groups(edge_b200_ctx *ctx, int n_groups, const int64_t *group_first);
+/* n_cycles steps of the largest group starting at t: per cycle 2^(n_groups-1) fundamental steps;
+ * at fundamental step k every group with k % 2^g == 0 samples its receivers and runs local +
+ * sources over [t_k, t_k + dt_fun 2^g), then every group whose step ends ((k+1) % 2^g == 0) runs
+ * neigh; t_k = t + k dt_fun counted from t. The first step of each rate-2 pair of a group starts the
+ * two-step sums. Receivers keep one clock per group (counts per receiver in read_receivers). */
+int edge_b200_step_lts(edge_b200_ctx *ctx, double t, double dt_fun, int n_cycles);
 /* Receiver samples buf[n][max_buf][9][R] (FP64), their times buf_time[n][max_buf], counts[n]. */
 int edge_b200_read_receivers(edge_b200_ctx *ctx, double *buf, double *buf_time, int32_t *counts);
 /* Waits for all work of the context's stream. */

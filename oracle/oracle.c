@@ -22,9 +22,12 @@
  *   oracle_surf_local  SurfIntVanilla::local          src/impl/seismic/kernels/SurfIntVanilla.hpp:212-262
  *   oracle_surf_neigh  SurfIntVanilla::neigh(+FluxInt) src/impl/seismic/kernels/SurfIntVanilla.hpp:274-357
  *   oracle_series_int  Series<1>::integrate           src/linalg/Series.hpp:59-134
+ *   oracle_integrate   TimePred::integrate            src/impl/seismic/kernels/TimePred.hpp:165-202
  *   oracle_step        steps 0/1/2 of one GTS step    src/impl/seismic/steps.inc:24-77 with
  *                      AderDg::local (AderDg.hpp:338-534), PointSources::apply (PointSources.hpp:887-931),
  *                      AderDg::neigh (AderDg.hpp:553-722), Receivers (io/Receivers.cpp:235-290)
+ *   oracle_lts_local / oracle_lts_neigh  the same work regions of one rate-2 LTS time group
+ *                      (AderDg.hpp:384-417 and 620-674, TimeGroupStatic.cpp:46-111)
  */
 #include <math.h>
 #include <stdlib.h>
@@ -273,51 +276,69 @@ double oracle_series_int(double dx, double xStart, long nPts, const double *vals
   return out;
 }
 
+/* TimePred::integrate (TimePred.hpp:165-202): tIntE = int_0^dt of the Taylor expansion of the
+ * elastic derivatives derE [O][9][B][R]; all modes with anelasticity, CK modes without */
+void oracle_integrate(int O, int R, int rm, double dt, const double *derE, double *tIntE) {
+  const int B = nmodes(O);
+  const size_t szE = (size_t)9 * B * R;
+  double sca = dt;
+  for (size_t i = 0; i < szE; i++) tIntE[i] = sca * derE[i];
+  for (int de = 1; de < O; de++) {
+    sca *= dt / (de + 1);
+    const int nCp = rm == 0 ? nmodes(O - de) : B;
+    for (int q = 0; q < 9; q++)
+      for (int md = 0; md < nCp; md++)
+        for (int r = 0; r < R; r++) {
+          size_t k = ((size_t)q * B + md) * R + r;
+          tIntE[k] += sca * derE[(size_t)de * szE + k];
+        }
+  }
+}
+
 /* face types of the per-element face table */
 enum { FT_INNER = 0, FT_FREE = 1, FT_OUTFLOW = 2 };
+/* rate-2 LTS: element flags (AderDg.hpp:384-417) and relation to the face neighbour (622-674) */
+enum { LTS_HAS_LARGER = 1, LTS_HAS_SMALLER = 2 };
+enum { LTS_EQ = 0, LTS_GT = 1, LTS_LT = 2 };
 
 /*
- * One GTS time step over the whole mesh: local (CK, receivers, volume, local surface) ->
- * point sources -> neighbour surface + anelastic scatter.
- *
+ * Local step (CK, receivers, volume, local surface) of the elements [first, first+n).
  * Receivers: nRe receivers grouped by element (recvEl ascending, equal elements adjacent); each
  * has basis values recvBasis[nRe][B] and its next output time recvTime[nRe] (updated). Output:
  * recvBuf[nRe][maxBuf][9][R], recvBufTime[nRe][maxBuf], recvCount[nRe] (updated). A group of
  * receivers in one element is evaluated at the first receiver's time (Receivers.cpp:250-290).
- *
- * Sources: nSrc point sources sorted by (element, run); source s adds
- * int_{t}^{t+dt} series * srcScal[s][q] * srcBEval[s][md] to run srcRun[s] of element srcEl[s].
- * Series s has srcNPts[s] samples at srcTsOff[s] in srcTs, start time srcT0[s], spacing srcDt[s].
+ * LTS (ltsFlags != NULL): elements with a larger neighbour add their time integral to tDofs1
+ * (reset when firstTs), elements with a smaller neighbour store the integral over [0, dt/2] in
+ * tDofs2 (AderDg.hpp:384-417).
  */
-int oracle_step(int O, int R, int rm, long nEl, double t, double dt, const double *stiffT,
-                const double *stiffV, const double *fluxL, const double *fluxN,
-                const double *fluxT, const double *starE, const double *starA,
-                const double *srcA, const double *omega, const double *fsE, const double *fsA,
-                const int *elFaEl, const unsigned char *fIdElFaEl,
-                const unsigned char *vIdElFaEl, const unsigned char *faType, double *dofsE,
-                double *dofsA, double *tDofs,
-                /* receivers */ int nRe, const long *recvEl, const double *recvBasis,
-                double *recvTime, double period, int maxBuf, double *recvBuf,
-                double *recvBufTime, int *recvCount,
-                /* sources */ int nSrc, const long *srcEl, const int *srcRun,
-                const double *srcScal, const double *srcBEval, const double *srcT0,
-                const double *srcDt, const long *srcTsOff, const long *srcNPts,
-                const double *srcTs, double tolTime) {
+static int local_range(int O, int R, int rm, long first, long n, double t, double dt,
+                       const double *stiffT, const double *stiffV, const double *fluxL,
+                       const double *fluxT, const double *starE, const double *starA,
+                       const double *srcA, const double *omega, const double *fsE, const double *fsA,
+                       double *dofsE, double *dofsA, double *tDofs, const unsigned char *ltsFlags,
+                       int firstTs, double *tDofs1, double *tDofs2, int nRe, const long *recvEl,
+                       const double *recvBasis, double *recvTime, double period, int maxBuf,
+                       double *recvBuf, double *recvBufTime, int *recvCount, double tolTime) {
   const int B = nmodes(O);
   const size_t szE = (size_t)9 * B * R, szM = (size_t)6 * B * R;
   int overflow = 0;
-  /* step 0: local (elements are independent; receivers of an element are found by bisection) */
 #pragma omp parallel reduction(| : overflow)
   {
   double *der = malloc((size_t)O * szE * sizeof(double));
   double *tIntA = rm ? malloc((size_t)rm * szM * sizeof(double)) : NULL;
   double *pred = malloc(szE * sizeof(double));
 #pragma omp for schedule(dynamic, 16)
-  for (long el = 0; el < nEl; el++) {
+  for (long el = first; el < first + n; el++) {
     double *dE = dofsE + el * szE, *dA = rm ? dofsA + el * rm * szM : NULL;
     double *tD = tDofs + el * szE;
     oracle_ck(O, R, rm, dt, stiffT, starE + el * 72, rm ? starA + el * 27 : NULL,
               rm ? srcA + el * 12 * rm : NULL, omega, dE, dA, der, tD, tIntA);
+    if (ltsFlags && (ltsFlags[el] & LTS_HAS_LARGER)) {
+      double *t1 = tDofs1 + el * szE;
+      if (firstTs) memset(t1, 0, szE * sizeof(double));
+      for (size_t i = 0; i < szE; i++) t1[i] += tD[i];
+    }
+    if (ltsFlags && (ltsFlags[el] & LTS_HAS_SMALLER)) oracle_integrate(O, R, rm, 0.5 * dt, der, tDofs2 + el * szE);
     int lo = 0, hi = nRe;
     while (lo < hi) {
       int mid = (lo + hi) / 2;
@@ -353,9 +374,22 @@ int oracle_step(int O, int R, int rm, long nEl, double t, double dt, const doubl
   free(tIntA);
   free(pred);
   }
-  if (overflow) return -1;
-  /* step 1: point sources */
+  return overflow ? -1 : 0;
+}
+
+/* Point sources of the elements [first, first+n) over [t, t+dt] (PointSources::apply,
+ * PointSources.hpp:887-931). Sources are sorted by (element, run); source s adds
+ * int_{t}^{t+dt} series * srcScal[s][q] * srcBEval[s][md] to run srcRun[s] of element srcEl[s].
+ * Series s has srcNPts[s] samples at srcTsOff[s] in srcTs, start time srcT0[s], spacing srcDt[s]. */
+static void sources_range(int O, int R, long first, long n, double t, double dt, double *dofsE,
+                          int nSrc, const long *srcEl, const int *srcRun, const double *srcScal,
+                          const double *srcBEval, const double *srcT0, const double *srcDt,
+                          const long *srcTsOff, const long *srcNPts, const double *srcTs,
+                          double tolTime) {
+  const int B = nmodes(O);
+  const size_t szE = (size_t)9 * B * R;
   for (int s = 0; s < nSrc; s++) {
+    if (srcEl[s] < first || srcEl[s] >= first + n) continue;
     double in = oracle_series_int(srcDt[s], srcT0[s], srcNPts[s], srcTs + srcTsOff[s], t, t + dt,
                                   0.0, tolTime);
     double *dE = dofsE + srcEl[s] * szE;
@@ -365,14 +399,28 @@ int oracle_step(int O, int R, int rm, long nEl, double t, double dt, const doubl
         dE[((size_t)q * B + md) * R + srcRun[s]] += sc * srcBEval[(size_t)s * B + md];
     }
   }
-  /* step 2: neighbour */
+}
+
+/* Neighbour step of the elements [first, first+n) (AderDg::neigh, AderDg.hpp:553-722). With LTS
+ * (ltsRel != NULL, [nEl][4]) the neighbour's time integral over this element's step is tDofs of
+ * an equal neighbour, tDofs1 of a smaller one (two steps summed) and, for a larger neighbour,
+ * tDofs2 (first half) on the first step of a pair, tDofs - tDofs2 (second half) otherwise. */
+static void neigh_range(int O, int R, int rm, long first, long n, long nEl, const double *fluxL,
+                        const double *fluxN, const double *fluxT, const double *fsE, const double *fsA,
+                        const double *omega, const int *elFaEl, const unsigned char *fIdElFaEl,
+                        const unsigned char *vIdElFaEl, const unsigned char *faType,
+                        const double *tDofs, const unsigned char *ltsRel, int firstTs,
+                        const double *tDofs1, const double *tDofs2, double *dofsE, double *dofsA) {
+  const int B = nmodes(O);
+  const size_t szE = (size_t)9 * B * R, szM = (size_t)6 * B * R;
   const double *fsE1 = fsE + (size_t)nEl * 4 * 81;
   const double *fsA1 = rm ? fsA + (size_t)nEl * 4 * 54 : NULL;
 #pragma omp parallel
   {
   double *upA = rm ? malloc(szM * sizeof(double)) : NULL;
+  double *diff = malloc(szE * sizeof(double));
 #pragma omp for schedule(dynamic, 16)
-  for (long el = 0; el < nEl; el++) {
+  for (long el = first; el < first + n; el++) {
     if (rm) memset(upA, 0, szM * sizeof(double));
     for (int f = 0; f < 4; f++) {
       int ty = faType[el * 4 + f];
@@ -380,13 +428,83 @@ int oracle_step(int O, int R, int rm, long nEl, double t, double dt, const doubl
       long ne = ty == FT_FREE ? el : elFaEl[el * 4 + f];
       int vId = ty == FT_FREE ? -1 : vIdElFaEl[el * 4 + f];
       int fId = ty == FT_FREE ? -1 : fIdElFaEl[el * 4 + f];
+      const double *tNe = tDofs + ne * szE;
+      const int rel = (ltsRel && ty == FT_INNER) ? ltsRel[el * 4 + f] : LTS_EQ;
+      if (rel == LTS_GT) {
+        tNe = tDofs1 + ne * szE;
+      } else if (rel == LTS_LT) {
+        if (firstTs) {
+          tNe = tDofs2 + ne * szE;
+        } else {
+          for (size_t i = 0; i < szE; i++) diff[i] = tDofs[ne * szE + i] - tDofs2[ne * szE + i];
+          tNe = diff;
+        }
+      }
       oracle_surf_neigh(O, R, rm, f, vId, fId, fluxL, fluxN, fluxT, fsE1 + (el * 4 + f) * 81,
-                        rm ? fsA1 + (el * 4 + f) * 54 : NULL, tDofs + ne * szE,
-                        dofsE + el * szE, upA);
+                        rm ? fsA1 + (el * 4 + f) * 54 : NULL, tNe, dofsE + el * szE, upA);
     }
     if (rm) scatter_upA(B, R, rm, omega, upA, dofsA + el * rm * szM);
   }
   free(upA);
+  free(diff);
   }
+}
+
+/* One GTS time step over the whole mesh: local -> point sources -> neighbour (steps 0/1/2 of
+ * src/impl/seismic/steps.inc:24-77). Returns -1 when a receiver buffer is full. */
+int oracle_step(int O, int R, int rm, long nEl, double t, double dt, const double *stiffT,
+                const double *stiffV, const double *fluxL, const double *fluxN,
+                const double *fluxT, const double *starE, const double *starA,
+                const double *srcA, const double *omega, const double *fsE, const double *fsA,
+                const int *elFaEl, const unsigned char *fIdElFaEl,
+                const unsigned char *vIdElFaEl, const unsigned char *faType, double *dofsE,
+                double *dofsA, double *tDofs,
+                /* receivers */ int nRe, const long *recvEl, const double *recvBasis,
+                double *recvTime, double period, int maxBuf, double *recvBuf,
+                double *recvBufTime, int *recvCount,
+                /* sources */ int nSrc, const long *srcEl, const int *srcRun,
+                const double *srcScal, const double *srcBEval, const double *srcT0,
+                const double *srcDt, const long *srcTsOff, const long *srcNPts,
+                const double *srcTs, double tolTime) {
+  if (local_range(O, R, rm, 0, nEl, t, dt, stiffT, stiffV, fluxL, fluxT, starE, starA, srcA, omega, fsE,
+                  fsA, dofsE, dofsA, tDofs, NULL, 0, NULL, NULL, nRe, recvEl, recvBasis, recvTime, period,
+                  maxBuf, recvBuf, recvBufTime, recvCount, tolTime))
+    return -1;
+  sources_range(O, R, 0, nEl, t, dt, dofsE, nSrc, srcEl, srcRun, srcScal, srcBEval, srcT0, srcDt, srcTsOff,
+                srcNPts, srcTs, tolTime);
+  neigh_range(O, R, rm, 0, nEl, nEl, fluxL, fluxN, fluxT, fsE, fsA, omega, elFaEl, fIdElFaEl, vIdElFaEl,
+              faType, tDofs, NULL, 0, NULL, NULL, dofsE, dofsA);
   return 0;
+}
+
+/* Rate-2 LTS work regions of one time group (the elements [first, first+n)): local with the
+ * tDofs1 / tDofs2 bookkeeping, then its sources, and later its neighbour step (TimeGroupStatic
+ * computeStep with steps.inc:24-77; the order across groups is the caller's). */
+int oracle_lts_local(int O, int R, int rm, long first, long n, int firstTs, double t, double dt,
+                     const double *stiffT, const double *stiffV, const double *fluxL, const double *fluxT,
+                     const double *starE, const double *starA, const double *srcA, const double *omega,
+                     const double *fsE, const double *fsA, const unsigned char *ltsFlags, double *dofsE,
+                     double *dofsA, double *tDofs, double *tDofs1, double *tDofs2, int nRe,
+                     const long *recvEl, const double *recvBasis, double *recvTime, double period,
+                     int maxBuf, double *recvBuf, double *recvBufTime, int *recvCount, int nSrc,
+                     const long *srcEl, const int *srcRun, const double *srcScal, const double *srcBEval,
+                     const double *srcT0, const double *srcDt, const long *srcTsOff, const long *srcNPts,
+                     const double *srcTs, double tolTime) {
+  if (local_range(O, R, rm, first, n, t, dt, stiffT, stiffV, fluxL, fluxT, starE, starA, srcA, omega, fsE,
+                  fsA, dofsE, dofsA, tDofs, ltsFlags, firstTs, tDofs1, tDofs2, nRe, recvEl, recvBasis,
+                  recvTime, period, maxBuf, recvBuf, recvBufTime, recvCount, tolTime))
+    return -1;
+  sources_range(O, R, first, n, t, dt, dofsE, nSrc, srcEl, srcRun, srcScal, srcBEval, srcT0, srcDt, srcTsOff,
+                srcNPts, srcTs, tolTime);
+  return 0;
+}
+
+void oracle_lts_neigh(int O, int R, int rm, long first, long n, long nEl, int firstTs, const double *fluxL,
+                      const double *fluxN, const double *fluxT, const double *fsE, const double *fsA,
+                      const double *omega, const int *elFaEl, const unsigned char *fIdElFaEl,
+                      const unsigned char *vIdElFaEl, const unsigned char *faType,
+                      const unsigned char *ltsRel, const double *tDofs, const double *tDofs1,
+                      const double *tDofs2, double *dofsE, double *dofsA) {
+  neigh_range(O, R, rm, first, n, nEl, fluxL, fluxN, fluxT, fsE, fsA, omega, elFaEl, fIdElFaEl, vIdElFaEl,
+              faType, tDofs, ltsRel, firstTs, tDofs1, tDofs2, dofsE, dofsA);
 }

@@ -36,6 +36,7 @@ def lib():
             subprocess.check_call(["make", "-s", "-C", _HERE, "liboracle.so"])
         _LIB = C.CDLL(path)
         _LIB.oracle_step.restype = C.c_int
+        _LIB.oracle_lts_local.restype = C.c_int
         _LIB.oracle_series_int.restype = C.c_double
         _LIB.oracle_series_int.argtypes = [C.c_double, C.c_double, C.c_long, C.c_void_p, C.c_double,
                                            C.c_double, C.c_double, C.c_double]
@@ -125,3 +126,74 @@ def step(prob, state, t, dt, recv=None, src=None, tol_time=1e-9):
         _ptr(src.get("nPts")), _ptr(src.get("ts")), C.c_double(tol_time))
     if rc != 0:
         raise RuntimeError("oracle_step failed (receiver buffer full?)")
+
+
+def _recv_args(recv):
+    if recv is None:
+        recv = dict(n=0, el=None, basis=None, time=None, period=1.0, maxbuf=0, buf=None, buftime=None,
+                    count=None)
+    return [C.c_int(recv["n"]), _ptr(recv["el"]), _ptr(recv["basis"]), _ptr(recv["time"]),
+            C.c_double(recv["period"]), C.c_int(recv["maxbuf"]), _ptr(recv["buf"]), _ptr(recv["buftime"]),
+            _ptr(recv["count"])]
+
+
+def _src_args(src):
+    src = src or dict(n=0)
+    return [C.c_int(src.get("n", 0)), _ptr(src.get("el")), _ptr(src.get("run")), _ptr(src.get("scal")),
+            _ptr(src.get("bEval")), _ptr(src.get("t0")), _ptr(src.get("dt")), _ptr(src.get("tsOff")),
+            _ptr(src.get("nPts")), _ptr(src.get("ts"))]
+
+
+def lts_local(prob, state, first, n, first_ts, t, dt, flags, recv=None, src=None, tol_time=1e-9):
+    """Local step + sources of the elements [first, first+n) of one LTS time group
+    (oracle_lts_local); state holds dofsE/dofsA/tDofs and the LTS buffers tDofs1/tDofs2."""
+    O, R, rm = prob["order"], prob["runs"], prob["rm"]
+    f64 = lambda k: _ptr(prob[k]) if prob.get(k) is not None else None
+    rc = lib().oracle_lts_local(
+        C.c_int(O), C.c_int(R), C.c_int(rm), C.c_long(first), C.c_long(n), C.c_int(1 if first_ts else 0),
+        C.c_double(t), C.c_double(dt), f64("stiffT"), f64("stiffV"), f64("fluxL"), f64("fluxT"), f64("starE"),
+        f64("starA"), f64("srcA"), f64("omega"), f64("fsE"), f64("fsA"), _ptr(flags), _ptr(state["dofsE"]),
+        _ptr(state.get("dofsA")), _ptr(state["tDofs"]), _ptr(state.get("tDofs1")), _ptr(state.get("tDofs2")),
+        *_recv_args(recv), *_src_args(src), C.c_double(tol_time))
+    if rc != 0:
+        raise RuntimeError("oracle_lts_local failed (receiver buffer full?)")
+
+
+def lts_neigh(prob, state, first, n, first_ts, rel):
+    """Neighbour step of the elements [first, first+n) of one LTS time group (oracle_lts_neigh)."""
+    O, R, rm = prob["order"], prob["runs"], prob["rm"]
+    f64 = lambda k: _ptr(prob[k]) if prob.get(k) is not None else None
+    lib().oracle_lts_neigh(
+        C.c_int(O), C.c_int(R), C.c_int(rm), C.c_long(first), C.c_long(n), C.c_long(prob["nEl"]),
+        C.c_int(1 if first_ts else 0), f64("fluxL"), f64("fluxN"), f64("fluxT"), f64("fsE"), f64("fsA"),
+        f64("omega"), _ptr(prob["elFaEl"]), _ptr(prob["fIdElFaEl"]), _ptr(prob["vIdElFaEl"]),
+        _ptr(prob["faType"]), _ptr(rel), _ptr(state["tDofs"]), _ptr(state.get("tDofs1")),
+        _ptr(state.get("tDofs2")), _ptr(state["dofsE"]), _ptr(state.get("dofsA")))
+
+
+def lts_cycles(prob, state, group_first, t, dt_fun, n_cycles, flags, rel, recv=None, src=None):
+    """n_cycles steps of the largest time group with the rate-2 schedule: at fundamental step k
+    (t_k = t + k dt_fun) every group g with k % 2^g == 0 runs local + sources over
+    [t_k, t_k + 2^g dt_fun), then every group whose step ends runs neigh; the first step of each
+    pair of a group (its step count even) resets the two-step sums (TimeGroupStatic.cpp:46-111,
+    man_sched.inc:37-206 sequentialised)."""
+    G = len(group_first) - 1
+    n_fun = 1 << (G - 1)
+    for c in range(n_cycles):
+        for k in range(n_fun):
+            kk = c * n_fun + k
+            for g in range(G):
+                if k % (1 << g):
+                    continue
+                lo, hi = int(group_first[g]), int(group_first[g + 1])
+                if hi > lo:
+                    lts_local(prob, state, lo, hi - lo, ((kk >> g) & 1) == 0, t + float(kk) * dt_fun,
+                              dt_fun * float(1 << g), flags, recv, src)
+            for g in range(G):
+                span = 1 << g
+                if (k + 1) % span:
+                    continue
+                lo, hi = int(group_first[g]), int(group_first[g + 1])
+                k0 = kk + 1 - span
+                if hi > lo:
+                    lts_neigh(prob, state, lo, hi - lo, ((k0 >> g) & 1) == 0, rel)
