@@ -23,7 +23,7 @@ def test_fp64_on_gmsh_mesh_matches_oracle(tmp_path, order):
     m = host.Mesh.from_gmsh(path)
     prob = host.build_problem(4, order, 1, seed=21, n_receivers=6, source="random", n_steps=20, mesh=m)
     e0, _ = random_dofs(prob, seed=3, scale=1e-3)
-    ref = OracleRun(prob, e0)
+    ref = OracleRun(prob, e0.copy())
     ref.step(20)
     s = Solver(prob, precision=64)
     try:
