@@ -66,6 +66,22 @@ struct DevBuf {
   ~DevBuf() { dfree(p); }
 };
 
+// halo exchange: blocks [9][R][GF] of face slots (element * 4 + face) to / from a packed buffer,
+// 16 bytes per thread; slots outside the face buffer are skipped
+__global__ void kFacePack(uint4 *face, uint4 *buf, const int32_t *slots, int n, int64_t blk16, int64_t nSlots,
+                          bool pack) {
+  const int64_t total = (int64_t)n * blk16;
+  for (int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < total; i += int64_t(gridDim.x) * blockDim.x) {
+    const int64_t k = i / blk16, w = i % blk16;
+    const int64_t sl = slots[k];
+    if (sl < 0 || sl >= nSlots) continue;
+    if (pack)
+      buf[i] = face[sl * blk16 + w];
+    else
+      face[sl * blk16 + w] = buf[i];
+  }
+}
+
 // rows [nRows][R][G] <- src [nRows][B] for one run (zeros when src is null)
 template <typename T>
 __global__ void kSetRun(T *rows, const T *src, int64_t nRows, int B, int R, int G, int run) {
@@ -80,6 +96,7 @@ __global__ void kSetRun(T *rows, const T *src, int64_t nRows, int B, int R, int 
 struct edge_b200_ctx {
   edge_b200_cfg cfg{};
   int64_t nEl = 0;
+  int64_t nOwned = 0;  // the kernels update elements [0, nOwned); the rest are halo ghosts
   int B = 0, F = 0;
   size_t realSize = 8;
   cudaStream_t stream = nullptr;
@@ -215,7 +232,7 @@ struct edge_b200_ctx {
     a.faType = faType;
     a.nEl = nEl;
     a.elFirst = 0;
-    a.elCount = nEl;
+    a.elCount = nOwned;
     a.dt = dt;
     for (int i = 0; i < 3; i++) a.omega[i] = omega[i];
     return a;
@@ -264,6 +281,7 @@ int edge_b200_create(const edge_b200_cfg *cfg, int64_t n_el, edge_b200_ctx **out
   ctx->cfg = *cfg;
   ctx->ks = ks;
   ctx->nEl = n_el;
+  ctx->nOwned = n_el;
   ctx->B = nModes(cfg->order);
   ctx->F = nFaceModes(cfg->order);
   ctx->realSize = cfg->precision == 64 ? 8 : 4;
@@ -492,7 +510,9 @@ int edge_b200_rewind_receivers(edge_b200_ctx *ctx, double t_first) {
   return EDGE_B200_OK;
 }
 
-int edge_b200_step(edge_b200_ctx *ctx, double t, double dt, int n_steps) {
+// n_steps GTS steps; phases selects the halves of each step (1: receivers, local, sources;
+// 2: neighbour; 3: both)
+static int runSteps(edge_b200_ctx *ctx, double t, double dt, int n_steps, int phases) {
   if (!ctx || !(dt > 0) || n_steps < 0) return EDGE_B200_EINVAL;
   if (!ctx->meshSet || !ctx->dataSet) return EDGE_B200_EINVAL;
   ctx->lastLts = false;
@@ -505,7 +525,7 @@ int edge_b200_step(edge_b200_ctx *ctx, double t, double dt, int n_steps) {
     double ts = t;
     for (int st = 0; st < n_steps; st++) {
       stepFirst[st] = (int)tau.size();
-      if (ctx->nRecv) {
+      if (ctx->nRecv && (phases & 1)) {
         while (ctx->recvTime > ts - kTolTime && ctx->recvTime < ts + dt - kTolTime) {
           if (ctx->recvCount >= ctx->maxBuf) return EDGE_B200_EOVERFLOW;
           tau.push_back(std::abs(ctx->recvTime - ts));
@@ -537,7 +557,7 @@ int edge_b200_step(edge_b200_ctx *ctx, double t, double dt, int n_steps) {
   double ts = t;
   for (int st = 0; st < n_steps; st++) {
     const int ns = stepFirst[st + 1] - stepFirst[st];
-    if (ns > 0 && ctx->nRecvGrp > 0) {
+    if ((phases & 1) && ns > 0 && ctx->nRecvGrp > 0) {
       RecvArgs r;
       r.grpEl = ctx->grpEl.as<int64_t>();
       r.grpOff = ctx->grpOff.as<int32_t>();
@@ -551,24 +571,68 @@ int edge_b200_step(edge_b200_ctx *ctx, double t, double dt, int n_steps) {
       EDGE_CUDA(ctx->launch(3, [&] { return ctx->ks->recv(a, r, s); }), "receiver kernel");
       ctx->launches++;
     }
-    EDGE_CUDA(ctx->launch(0, [&] { return ctx->ks->local(a, s); }), "local kernel");
-    ctx->launches++;
-    if (ctx->src.nGrp > 0) {
-      SrcArgs sa = ctx->src;
-      sa.t = ts;
-      sa.dt = dt;
-      EDGE_CUDA(ctx->launch(2, [&] { return ctx->ks->sources(ctx->dofsE, sa, s); }), "source kernel");
+    if (phases & 1) {
+      EDGE_CUDA(ctx->launch(0, [&] { return ctx->ks->local(a, s); }), "local kernel");
+      ctx->launches++;
+      if (ctx->src.nGrp > 0) {
+        SrcArgs sa = ctx->src;
+        sa.t = ts;
+        sa.dt = dt;
+        EDGE_CUDA(ctx->launch(2, [&] { return ctx->ks->sources(ctx->dofsE, sa, s); }), "source kernel");
+        ctx->launches++;
+      }
+    }
+    if (phases & 2) {
+      EDGE_CUDA(ctx->launch(1, [&] { return ctx->ks->neigh(a, s); }), "neighbour kernel");
       ctx->launches++;
     }
-    EDGE_CUDA(ctx->launch(1, [&] { return ctx->ks->neigh(a, s); }), "neighbour kernel");
-    ctx->launches++;
     ts += dt;
   }
   return EDGE_B200_OK;
 }
 
+int edge_b200_step(edge_b200_ctx *ctx, double t, double dt, int n_steps) {
+  return runSteps(ctx, t, dt, n_steps, 3);
+}
+
+int edge_b200_step_phase(edge_b200_ctx *ctx, double t, double dt, int phase) {
+  if (phase != 0 && phase != 1) return EDGE_B200_EINVAL;
+  return runSteps(ctx, t, dt, 1, phase == 0 ? 1 : 2);
+}
+
+int edge_b200_set_owned(edge_b200_ctx *ctx, int64_t n_owned) {
+  if (!ctx || n_owned < 0 || n_owned > ctx->nEl || ctx->nTg > 1) return EDGE_B200_EINVAL;
+  ctx->nOwned = n_owned;
+  return EDGE_B200_OK;
+}
+
+int64_t edge_b200_face_block_bytes(const edge_b200_ctx *ctx) {
+  return ctx ? (int64_t)9 * ctx->cfg.n_runs * ctx->GF * (int64_t)ctx->realSize : -1;
+}
+
+static int packFaces(edge_b200_ctx *ctx, int n, const int32_t *slots, void *buf, bool pack) {
+  if (!ctx || n < 0 || (n && (!slots || !buf))) return EDGE_B200_EINVAL;
+  if (n == 0) return EDGE_B200_OK;
+  const int64_t blk16 = edge_b200_face_block_bytes(ctx) / 16;
+  const int64_t total = (int64_t)n * blk16;
+  const int grid = (int)std::min<int64_t>((total + 255) / 256, 148 * 16);
+  kFacePack<<<grid, 256, 0, ctx->stream>>>(static_cast<uint4 *>(ctx->face), static_cast<uint4 *>(buf), slots,
+                                             n, blk16, ctx->nEl * 4, pack);
+  EDGE_CUDA(cudaGetLastError(), pack ? "pack faces" : "unpack faces");
+  return EDGE_B200_OK;
+}
+
+int edge_b200_pack_faces(edge_b200_ctx *ctx, int n, const int32_t *slots, void *out) {
+  return packFaces(ctx, n, slots, out, true);
+}
+
+int edge_b200_unpack_faces(edge_b200_ctx *ctx, int n, const int32_t *slots, const void *in) {
+  return packFaces(ctx, n, slots, const_cast<void *>(in), false);
+}
+
 int edge_b200_set_time_groups(edge_b200_ctx *ctx, int n_groups, const int64_t *group_first) {
   if (!ctx || !ctx->meshSet || n_groups < 1 || n_groups > 16 || !group_first) return EDGE_B200_EINVAL;
+  if (ctx->nOwned != ctx->nEl) return EDGE_B200_EINVAL;  // time groups cover the whole mesh
   if (group_first[0] != 0 || group_first[n_groups] != ctx->nEl) return EDGE_B200_EINVAL;
   for (int g = 0; g < n_groups; g++)
     if (group_first[g + 1] < group_first[g]) return EDGE_B200_EINVAL;

@@ -203,6 +203,37 @@ __device__ __forceinline__ void stRowG(T *p, const T *v) {
   }
 }
 
+// asynchronous global -> shared copies (cp.async: no registers held while in flight)
+__device__ __forceinline__ void cpAsync16(void *dst, const void *src) {
+  const unsigned d = static_cast<unsigned>(__cvta_generic_to_shared(dst));
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(d), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cpAsync8(void *dst, const void *src) {
+  const unsigned d = static_cast<unsigned>(__cvta_generic_to_shared(dst));
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(d), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cpAsyncCommit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cpAsyncWait() {
+  asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
+}
+
+// cooperative copy of the DOF rows [R][GB] of quantity q of an element into the tile rows
+// (q, eo * R + row) with stride S: warp q moves its quantity's rows, consecutive lanes consecutive
+// 16-byte chunks
+template <typename T, int R, int GB, int S>
+__device__ __forceinline__ void copyDofRows(T *tile, const T *dofsE, int64_t e, int q, int eo, int r) {
+  constexpr int W = 16 / int(sizeof(T)), CPRB = GB / W;
+  const T *blk = dofsE + (e * 9 + q) * int64_t(R * GB);
+  T *dst = tile + (q * 32 + eo * R) * S;
+#pragma unroll
+  for (int it = 0; it < CPRB; it++) {
+    const int k = it * R + r;
+    const int row = k / CPRB, col = k % CPRB;
+    cpAsync16(dst + row * S + col * W, blk + row * GB + col * W);
+  }
+}
+
 template <typename T, int O, int R, int RM>
 struct Geo {
   static constexpr int GB = padGlobal<T>(nModes(O)), GF = padGlobal<T>(nFaceModes(O));
@@ -223,7 +254,14 @@ struct Geo {
   static constexpr bool tiSmem = (2 * nX + 2 * nXA) * sizeof(T) <= 227 * 1024;
   static constexpr size_t nTI = tiSmem ? nX : nS0;
   static constexpr size_t nTIA = tiSmem ? nXA : 0;
-  static constexpr size_t smemLocal = (nX + nTI + nXA + nTIA) * sizeof(T);
+  // With room for the face tiles in a region of their own, X is free after the recursion: the
+  // local kernel then copies the DOF rows into X asynchronously (the current group's again after
+  // the recursion, for the volume integral, and the next group's during the face integrals)
+  static constexpr size_t baseLocal = (nX + nTI + nXA + nTIA) * sizeof(T);
+  static constexpr size_t localBudget =
+      (sizeof(T) == 4 && RM == 0 && baseLocal <= 110 * 1024) ? 110 * 1024 : 227 * 1024;
+  static constexpr bool asyncLocal = tiSmem && baseLocal + nS0 * sizeof(T) <= localBudget;
+  static constexpr size_t smemLocal = baseLocal + (asyncLocal ? nS0 * sizeof(T) : 0);
   // LTS local step: one more [9][32][SB] tile for the half-step time integral (behind the rest);
   // configurations whose time integrals do not fit shared memory have no LTS kernels
   static constexpr size_t smemLocalLts = smemLocal + nX * sizeof(T);
@@ -555,14 +593,22 @@ __global__ void __launch_bounds__(Geo<T, O, R, RM>::NT, LTS ? 1 : Geo<T, O, R, R
   // see Geo: time integrals in shared memory (TI behind X, TIA behind XA, face tiles reuse X) or
   // in registers (copied into X / XA after the recursion, face tiles behind X); with LTS the
   // half-step integral TIh behind everything
+  constexpr bool AS = G::asyncLocal;
   T *TI = G::tiSmem ? X + G::nX : X;
   T *TIA = G::tiSmem ? XA + G::nXA : XA;
-  T *S0 = G::tiSmem ? X : X + G::nX;
+  T *S0 = AS ? TIA + G::nTIA : (G::tiSmem ? X : X + G::nX);
   T *TIh = LTS ? reinterpret_cast<T *>(smem + G::smemLocal) : nullptr;
   const int q = threadIdx.x >> 5, l = threadIdx.x & 31;
   const int eo = l / R, r = l % R;
   const int64_t nGroups = (a.elCount + E - 1) / E;
   const T dt = T(a.dt);
+  if constexpr (AS) {
+    // the first group's DOF rows
+    const int64_t g0 = blockIdx.x;
+    if (q < 9 && g0 < nGroups && g0 * E + eo < a.elCount)
+      copyDofRows<T, R, G::GB, SB>(X, a.dofsE, a.elFirst + g0 * E + eo, q, eo, r);
+    cpAsyncCommit();
+  }
   for (int64_t g = blockIdx.x; g < nGroups; g += gridDim.x) {
     const int64_t e = a.elFirst + g * E + eo;
     const bool valid = g * E + eo < a.elCount;
@@ -572,8 +618,20 @@ __global__ void __launch_bounds__(Geo<T, O, R, RM>::NT, LTS ? 1 : Geo<T, O, R, R
     // DOFs -> X, dt * DOFs -> TI (and the anelastic counterparts)
     if (q < 9) {
       T v[B];
-      ldRowG<T, B>(gRow<T, R, G::GB>(a.dofsE, ev, 9, q, r), v, valid);
-      stRow<T, B>(rowPtr<T, SB>(X, q, l), v);
+      if constexpr (AS) {
+        cpAsyncWait<0>();
+        __syncwarp();
+        if (valid)
+          ldRow<T, B>(rowPtr<T, SB>(X, q, l), v);
+        else {
+#pragma unroll
+          for (int n = 0; n < B; n++) v[n] = T(0);
+          stRow<T, B>(rowPtr<T, SB>(X, q, l), v);
+        }
+      } else {
+        ldRowG<T, B>(gRow<T, R, G::GB>(a.dofsE, ev, 9, q, r), v, valid);
+        stRow<T, B>(rowPtr<T, SB>(X, q, l), v);
+      }
       if constexpr (LTS) {
         T h[B];
 #pragma unroll
@@ -629,7 +687,26 @@ __global__ void __launch_bounds__(Geo<T, O, R, RM>::NT, LTS ? 1 : Geo<T, O, R, R
     T acc[B];
     T upA[RM ? B : 1];
     if (q < 9) {
-      ldRowG<T, B>(gRow<T, R, G::GB>(a.dofsE, ev, 9, q, r), acc, valid);
+      if constexpr (AS) {
+        // the DOF rows again (X is free after the recursion; L2-resident since the group start)
+        if (valid) copyDofRows<T, R, G::GB, SB>(X, a.dofsE, e, q, eo, r);
+        cpAsyncCommit();
+        cpAsyncWait<0>();
+        __syncwarp();
+        if (valid)
+          ldRow<T, B>(rowPtr<T, SB>(X, q, l), acc);
+        else
+#pragma unroll
+          for (int n = 0; n < B; n++) acc[n] = T(0);
+        __syncwarp();
+        // the next group's DOF rows arrive during the volume and face integrals
+        const int64_t gn = g + gridDim.x;
+        if (gn < nGroups && gn * E + eo < a.elCount)
+          copyDofRows<T, R, G::GB, SB>(X, a.dofsE, a.elFirst + gn * E + eo, q, eo, r);
+        cpAsyncCommit();
+      } else {
+        ldRowG<T, B>(gRow<T, R, G::GB>(a.dofsE, ev, 9, q, r), acc, valid);
+      }
       Mix3<T, SB> z{rowPtr<T, SB>(TI, c.cols[0], l), rowPtr<T, SB>(TI, c.cols[1], l),
                     rowPtr<T, SB>(TI, c.cols[2], l), c.cs};
       VolMul<O>::template run<T>(z, acc);
@@ -673,6 +750,7 @@ __global__ void __launch_bounds__(Geo<T, O, R, RM>::NT, LTS ? 1 : Geo<T, O, R, R
       }
     }
   }
+  if constexpr (AS) cpAsyncWait<0>();
 }
 
 // ------------------------------------------------------------------------------------------------
@@ -685,20 +763,6 @@ __global__ void __launch_bounds__(Geo<T, O, R, RM>::NT, LTS ? 1 : Geo<T, O, R, R
 // they fit. Per item: wait for its copies, rotate the neighbour's rows into this element's face
 // orientation in place, one CTA barrier, issue the copies of the item NSN - 1 ahead into the slot
 // the previous item released, then mix quantities and apply fluxT.
-
-__device__ __forceinline__ void cpAsync16(void *dst, const void *src) {
-  const unsigned d = static_cast<unsigned>(__cvta_generic_to_shared(dst));
-  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(d), "l"(src) : "memory");
-}
-__device__ __forceinline__ void cpAsync8(void *dst, const void *src) {
-  const unsigned d = static_cast<unsigned>(__cvta_generic_to_shared(dst));
-  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(d), "l"(src) : "memory");
-}
-__device__ __forceinline__ void cpAsyncCommit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
-template <int N>
-__device__ __forceinline__ void cpAsyncWait() {
-  asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
-}
 
 // face connectivity of one element (all four faces): the face slot each face gathers from
 // (neighbour * 4 + its face id, or a compact LTS slot * 4 + face id), and one byte per face for the

@@ -93,3 +93,83 @@ def plan(mesh, n_parts):
                 part.recv[q] = np.stack([[g2l[int(x)] for x in ge], g[order]], 1).astype(np.int32)
         parts.append(part)
     return parts
+
+
+class PartSolver:
+    """One part of a partition on a device: its solver (owned elements + ghosts), the device index
+    lists of its send and receive faces, and packed face buffers per peer.
+
+    Per step: phase0 (receivers, local, sources of the owned elements), pack() -> {peer: buffer},
+    the transport moves each buffer to the peer (exchange_nccl between GPUs), unpack({peer: buffer})
+    into the ghosts' face slots, phase1 (neighbour)."""
+
+    def __init__(self, prob, part, precision=64, device=0, stream=None):
+        import types
+
+        import torch
+        from . import host
+        from ._lib import lib
+        from .solver import Solver
+        ids = part.global_ids()
+        mesh = types.SimpleNamespace(n_el=part.n_local, el_fa_el=part.el_fa_el, fid=part.fid, vid=part.vid,
+                                     el_fa_type=part.el_fa_type)
+        take = lambda a, ax=0: None if a is None else np.ascontiguousarray(np.take(a, ids, axis=ax))
+        local = host.Problem(order=prob.order, runs=prob.runs, rm=prob.rm, mesh=mesh, rho=take(prob.rho),
+                             lam=take(prob.lam), mu=take(prob.mu), starE=take(prob.starE), fsE=take(prob.fsE, 1),
+                             dt=prob.dt, starA=take(prob.starA), srcA=take(prob.srcA), fsA=take(prob.fsA, 1),
+                             omega=prob.omega, name=f"part{part.rank}")
+        self.part, self.prob = part, local
+        self.solver = Solver(local, precision=precision, stream=stream, device=device)
+        self.solver._chk(lib().edge_b200_set_owned(self.solver._h, part.n_owned), "set_owned")
+        self.block = lib().edge_b200_face_block_bytes(self.solver._h)
+        dev = torch.device("cuda", device)
+        slots = lambda lst: torch.from_numpy((lst[:, 0].astype(np.int64) * 4 + lst[:, 1]).astype(np.int32)).to(dev)
+        self.send_slots = {q: slots(v) for q, v in part.send.items()}
+        self.recv_slots = {q: slots(v) for q, v in part.recv.items()}
+        self.send_buf = {q: torch.empty(len(v) * self.block, dtype=torch.uint8, device=dev) for q, v in part.send.items()}
+        self.recv_buf = {q: torch.empty(len(v) * self.block, dtype=torch.uint8, device=dev) for q, v in part.recv.items()}
+
+    def upload_owned(self, dofs_e_global):
+        e = np.zeros((self.part.n_local,) + dofs_e_global.shape[1:], dofs_e_global.dtype)
+        e[:self.part.n_owned] = dofs_e_global[self.part.lo:self.part.hi]
+        self.solver.upload_dofs(e)
+
+    def download_owned(self):
+        e, a = self.solver.download_dofs()
+        return e[:self.part.n_owned], None if a is None else a[:self.part.n_owned]
+
+    def phase0(self, t, dt):
+        from ._lib import lib
+        self.solver._chk(lib().edge_b200_step_phase(self.solver._h, t, dt, 0), "step_phase 0")
+
+    def phase1(self, t, dt):
+        from ._lib import lib
+        self.solver._chk(lib().edge_b200_step_phase(self.solver._h, t, dt, 1), "step_phase 1")
+
+    def pack(self):
+        from ._lib import lib
+        for q, sl in self.send_slots.items():
+            self.solver._chk(lib().edge_b200_pack_faces(self.solver._h, len(sl), sl.data_ptr(),
+                                                        self.send_buf[q].data_ptr()), "pack_faces")
+        return self.send_buf
+
+    def unpack(self):
+        from ._lib import lib
+        for q, sl in self.recv_slots.items():
+            self.solver._chk(lib().edge_b200_unpack_faces(self.solver._h, len(sl), sl.data_ptr(),
+                                                          self.recv_buf[q].data_ptr()), "unpack_faces")
+
+    def close(self):
+        self.solver.close()
+
+
+def exchange_nccl(ps):
+    """Moves this rank's packed send buffers to their peers' receive buffers (torch.distributed
+    send / recv, NCCL between GPUs); every rank calls it once per step after pack(). The part's
+    solver must run on torch's current stream (stream=None), which NCCL orders its copies after."""
+    import torch.distributed as dist
+    ops = [dist.P2POp(dist.isend, b, q) for q, b in sorted(ps.send_buf.items())]
+    ops += [dist.P2POp(dist.irecv, b, q) for q, b in sorted(ps.recv_buf.items())]
+    if ops:
+        for r in dist.batch_isend_irecv(ops):
+            r.wait()

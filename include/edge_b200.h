@@ -196,6 +196,21 @@ int edge_b200_rewind_receivers(edge_b200_ctx *ctx, double t_first);
 /* n_steps GTS steps from time t with step dt: local -> sources -> neighbour
  * (TimeGroupStatic::computeStep, src/time/TimeGroupStatic.cpp:113-127, steps.inc:24-77). */
 int edge_b200_step(edge_b200_ctx *ctx, double t, double dt, int n_steps);
+/* Halo exchange between the halves of a step (EDGE's MPI path: the local step packs the
+ * face-projected time integrals of the send faces, AderDg.hpp:419-473, the neighbour step reads
+ * the received ones, 675-684). With edge_b200_set_owned the kernels update only the elements
+ * [0, n_owned); the elements behind are ghosts whose face projections arrive by
+ * edge_b200_unpack_faces. edge_b200_step_phase runs one step's first half (phase 0: receivers,
+ * local, sources) or second half (phase 1: neighbour). pack / unpack move the face blocks
+ * [9][R][GF] of n face slots (slots[i] = element * 4 + face, a device int32 array) to / from the
+ * device buffer out / in ([n] blocks of edge_b200_face_block_bytes each, GF = F rounded up to 16
+ * bytes), ordered on the context stream; slots outside the mesh are skipped. Time groups need the
+ * whole mesh owned. */
+int edge_b200_set_owned(edge_b200_ctx *ctx, int64_t n_owned);
+int edge_b200_step_phase(edge_b200_ctx *ctx, double t, double dt, int phase);
+int64_t edge_b200_face_block_bytes(const edge_b200_ctx *ctx);
+int edge_b200_pack_faces(edge_b200_ctx *ctx, int n, const int32_t *slots, void *out);
+int edge_b200_unpack_faces(edge_b200_ctx *ctx, int n, const int32_t *slots, const void *in);
 /* Rate-2 local time stepping (EDGE's LTS: TimeGroupStatic, src/time/TimeGroupStatic.cpp:46-111,
  * the work-region dependencies of src/impl/seismic/inc/time/man_sched.inc:37-206 and the LTS
  * branches of AderDg::local / ::neigh, AderDg.hpp:384-417 and 620-674). The mesh elements must be
