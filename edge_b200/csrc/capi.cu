@@ -82,6 +82,61 @@ __global__ void kFacePack(uint4 *face, uint4 *buf, const int32_t *slots, int n, 
   }
 }
 
+// Error norms against plane waves. Thread (q, r) of a CTA holds the DOF row of quantity q, run r
+// of an element, evaluates it at the quadrature points (basis values in shared memory) and the
+// reference sum of plane waves at the physical points; L1 / squared L2 accumulate with the
+// physical weights, Linf as a maximum; one atomic per thread and norm at the end.
+struct PlaneWave {
+  double k[3], omega, phase;
+  double amp[9];
+  int run;  // -1: every run
+};
+template <typename T>
+__global__ void kErrorNorms(const T *dofsE, const double *geom, int64_t nEl, int B, int R, int G, int nQp,
+                            const double *quad /* [nQp][3 + 1 + B]: xi, w, basis */, const PlaneWave *waves,
+                            int nWaves, double t, double *norms /* [3][9][R] */) {
+  extern __shared__ double sq[];
+  const int stride = 4 + B;
+  for (int i = threadIdx.x; i < nQp * stride; i += blockDim.x) sq[i] = quad[i];
+  __syncthreads();
+  const int q = threadIdx.x / R, r = threadIdx.x % R;
+  if (q >= 9) return;
+  double l1 = 0, l2 = 0, li = 0;
+  double row[64];
+  for (int64_t e = blockIdx.x; e < nEl; e += gridDim.x) {
+    const T *p = dofsE + ((e * 9 + q) * R + r) * int64_t(G);
+    for (int b = 0; b < B; b++) row[b] = double(p[b]);
+    const double *v = geom + e * 12;
+    double j[3][3];
+    for (int a = 0; a < 3; a++)
+      for (int d = 0; d < 3; d++) j[a][d] = v[3 * (a + 1) + d] - v[d];
+    const double det = fabs(j[0][0] * (j[1][1] * j[2][2] - j[1][2] * j[2][1]) -
+                            j[0][1] * (j[1][0] * j[2][2] - j[1][2] * j[2][0]) +
+                            j[0][2] * (j[1][0] * j[2][1] - j[1][1] * j[2][0]));
+    for (int k = 0; k < nQp; k++) {
+      const double *qp = sq + k * stride;
+      double uh = 0;
+      for (int b = 0; b < B; b++) uh += qp[4 + b] * row[b];
+      double x[3];
+      for (int d = 0; d < 3; d++) x[d] = v[d] + qp[0] * j[0][d] + qp[1] * j[1][d] + qp[2] * j[2][d];
+      double ur = 0;
+      for (int w = 0; w < nWaves; w++) {
+        const PlaneWave &pw = waves[w];
+        if (pw.run >= 0 && pw.run != r) continue;
+        ur += pw.amp[q] * sin(pw.k[0] * x[0] + pw.k[1] * x[1] + pw.k[2] * x[2] - pw.omega * t + pw.phase);
+      }
+      const double diff = fabs(uh - ur), wt = qp[3] * det;
+      l1 += diff * wt;
+      l2 += diff * diff * wt;
+      li = fmax(li, diff);
+    }
+  }
+  atomicAdd(norms + q * R + r, l1);
+  atomicAdd(norms + (9 + q) * R + r, l2);
+  // non-negative doubles order like their bit patterns
+  atomicMax(reinterpret_cast<unsigned long long *>(norms + (18 + q) * R + r), __double_as_longlong(li));
+}
+
 // rows [nRows][R][G] <- src [nRows][B] for one run (zeros when src is null)
 template <typename T>
 __global__ void kSetRun(T *rows, const T *src, int64_t nRows, int B, int R, int G, int run) {
@@ -131,6 +186,8 @@ struct edge_b200_ctx {
   std::vector<double> tgRecvTime;
   std::vector<int32_t> tgRecvCount;
   DevBuf ltsFlags, ltsRel, sumIdx, halfIdx, faceSum, faceHalf1, faceHalf2;
+  // element vertex coordinates [nEl][4][3] (error norms), plane waves and norm accumulators
+  DevBuf geom, waves, quad, norms;
   int groupOf(int64_t el) const {
     int g = 0;
     while (g + 1 < nTg && el >= tgFirst[g + 1]) g++;
@@ -812,6 +869,72 @@ int edge_b200_read_receivers(edge_b200_ctx *ctx, double *buf, double *buf_time, 
       if (buf_time)
         for (int j = 0; j < ctx->maxBuf; j++) buf_time[(size_t)i * ctx->maxBuf + j] = j < cnt ? ctx->hBufTime[j] : 0.0;
     }
+  }
+  return EDGE_B200_OK;
+}
+
+int edge_b200_upload_geometry(edge_b200_ctx *ctx, const double *el_ve_crds) {
+  if (!ctx || !el_ve_crds) return EDGE_B200_EINVAL;
+  EDGE_CUDA(ctx->geom.put(el_ve_crds, (size_t)ctx->nEl * 12 * sizeof(double), ctx->stream), "upload geometry");
+  EDGE_CUDA(cudaStreamSynchronize(ctx->stream), "upload geometry");
+  return EDGE_B200_OK;
+}
+
+int edge_b200_error_norms(edge_b200_ctx *ctx, double t, int n_waves, const double *waves, int n_qp,
+                          const double *qp_xi, const double *qp_w, const double *qp_basis, double *l1, double *l2,
+                          double *linf) {
+  if (!ctx || !ctx->geom.p || n_waves < 0 || n_waves > 64 || (n_waves && !waves) || n_qp < 1 || n_qp > 512 ||
+      !qp_xi || !qp_w || !qp_basis || ctx->B > 64)
+    return EDGE_B200_EINVAL;
+  const int B = ctx->B, R = ctx->cfg.n_runs;
+  std::vector<PlaneWave> pw(std::max(n_waves, 1));
+  for (int w = 0; w < n_waves; w++) {
+    const double *src = waves + 15 * w;  // k[3], omega, phase, amp[9], run
+    for (int d = 0; d < 3; d++) pw[w].k[d] = src[d];
+    pw[w].omega = src[3];
+    pw[w].phase = src[4];
+    for (int q = 0; q < 9; q++) pw[w].amp[q] = src[5 + q];
+    pw[w].run = (int)src[14];
+    if (pw[w].run >= R) return EDGE_B200_EINVAL;
+  }
+  std::vector<double> quad((size_t)n_qp * (4 + B));
+  for (int k = 0; k < n_qp; k++) {
+    double *d = &quad[(size_t)k * (4 + B)];
+    for (int i = 0; i < 3; i++) d[i] = qp_xi[3 * k + i];
+    d[3] = qp_w[k];
+    for (int b = 0; b < B; b++) d[4 + b] = qp_basis[(size_t)k * B + b];
+  }
+  cudaStream_t s = ctx->stream;
+  const size_t smem = quad.size() * sizeof(double);
+  if (smem > 200 * 1024) return EDGE_B200_EINVAL;
+  EDGE_CUDA(ctx->waves.put(pw.data(), pw.size() * sizeof(PlaneWave), s), "error norms");
+  EDGE_CUDA(ctx->quad.put(quad.data(), smem, s), "error norms");
+  EDGE_CUDA(ctx->norms.fit(27 * R * sizeof(double)), "error norms");
+  EDGE_CUDA(cudaMemsetAsync(ctx->norms.p, 0, 27 * R * sizeof(double), s), "error norms");
+  const int threads = ((9 * R + 31) / 32) * 32;
+  const int grid = (int)std::min<int64_t>(ctx->nEl, 148 * 8);
+  if (ctx->cfg.precision == 64) {
+    EDGE_CUDA(cudaFuncSetAttribute(kErrorNorms<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem),
+              "error norms");
+    kErrorNorms<double><<<grid, threads, smem, s>>>((const double *)ctx->dofsE, ctx->geom.as<double>(), ctx->nOwned,
+                                                    B, R, ctx->GB, n_qp, ctx->quad.as<double>(),
+                                                    ctx->waves.as<PlaneWave>(), n_waves, t, ctx->norms.as<double>());
+  } else {
+    EDGE_CUDA(cudaFuncSetAttribute(kErrorNorms<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem),
+              "error norms");
+    kErrorNorms<float><<<grid, threads, smem, s>>>((const float *)ctx->dofsE, ctx->geom.as<double>(), ctx->nOwned,
+                                                   B, R, ctx->GB, n_qp, ctx->quad.as<double>(),
+                                                   ctx->waves.as<PlaneWave>(), n_waves, t, ctx->norms.as<double>());
+  }
+  EDGE_CUDA(cudaGetLastError(), "error norms");
+  std::vector<double> h(27 * R);
+  EDGE_CUDA(cudaMemcpyAsync(h.data(), ctx->norms.p, h.size() * sizeof(double), cudaMemcpyDeviceToHost, s),
+            "error norms");
+  EDGE_CUDA(cudaStreamSynchronize(s), "error norms");
+  for (int i = 0; i < 9 * R; i++) {
+    if (l1) l1[i] = h[i];
+    if (l2) l2[i] = std::sqrt(h[9 * R + i]);
+    if (linf) linf[i] = h[18 * R + i];
   }
   return EDGE_B200_OK;
 }

@@ -467,6 +467,18 @@ def l2_error(mesh, order, dofs, fn, run=0, n_quad=None, chunk=20000):
     return np.sqrt(err), np.sqrt(ref)
 
 
+def plane_wave_rows(rho, lam, mu, kvec, amp=1.0, run=-1):
+    """The P plane wave of plane_wave_p as a row k[3], omega, phase, amp[9], run of the device
+    error norms (sin(k.x - omega t) times the eigenvector)."""
+    kvec = np.asarray(kvec, np.float64)
+    kn = np.linalg.norm(kvec)
+    n = kvec / kn
+    cp = np.sqrt((lam + 2 * mu) / rho)
+    pairs = [(0, 0), (1, 1), (2, 2), (0, 1), (1, 2), (0, 2)]
+    sig = np.array([-(lam * (i == j) + 2 * mu * n[i] * n[j]) / cp for i, j in pairs])
+    return np.concatenate([kvec, [cp * kn, 0.0], amp * np.concatenate([sig, n]), [run]])
+
+
 def plane_wave_p(rho, lam, mu, kvec, amp=1.0):
     """P plane wave a = amp sin(k.x - w t): v = n a, sigma = -(lam I + 2 mu n n) a / cp."""
     kvec = np.asarray(kvec, np.float64)

@@ -93,6 +93,25 @@ class Solver:
         self._chk(lib().edge_b200_step_lts(self._h, t0, dt_fun, n_cycles), "step_lts")
         self.t = t0 + float(n_cycles * (1 << (self.n_groups - 1))) * dt_fun
 
+    def upload_geometry(self):
+        crds = np.ascontiguousarray(self.prob.mesh.el_ve_crds(), np.float64)
+        self._chk(lib().edge_b200_upload_geometry(self._h, ptr(crds)), "upload_geometry")
+
+    def error_norms(self, waves, t=None, n_quad=None):
+        """L1 / L2 / Linf errors [9][R] against a sum of plane waves (rows k[3], omega, phase,
+        amp[9], run) on the device; the collapsed Gauss rule with order+1 points per direction."""
+        from . import host
+        t = self.t if t is None else t
+        pts, wts = host.tet_quadrature(n_quad or self.prob.order + 1)
+        V = host.basis_at(self.prob.order, pts)
+        w = np.ascontiguousarray(np.atleast_2d(waves), np.float64)
+        R = self.prob.runs
+        out = [np.zeros((9, R)) for _ in range(3)]
+        self._chk(lib().edge_b200_error_norms(self._h, t, len(w), ptr(w), len(pts), ptr(np.ascontiguousarray(pts)),
+                                              ptr(np.ascontiguousarray(wts)), ptr(np.ascontiguousarray(V)),
+                                              *[ptr(o) for o in out]), "error_norms")
+        return out
+
     def sync(self):
         self._chk(lib().edge_b200_sync(self._h), "sync")
 

@@ -196,6 +196,19 @@ int edge_b200_rewind_receivers(edge_b200_ctx *ctx, double t_first);
 /* n_steps GTS steps from time t with step dt: local -> sources -> neighbour
  * (TimeGroupStatic::computeStep, src/time/TimeGroupStatic.cpp:113-127, steps.inc:24-77). */
 int edge_b200_step(edge_b200_ctx *ctx, double t, double dt, int n_steps);
+/* Error norms of the device solution (InitialDofs::err, src/setups/InitialDofs.hpp:277-373, and
+ * the reduction of src/impl/seismic/fin.inc:23-64): per quantity and run, the L1, L2 and Linf norms
+ * of (DG solution - reference) over the owned elements at time t, with quadrature points
+ * qp_xi[n_qp][3] on the unit tet, weights qp_w[n_qp] and basis values qp_basis[n_qp][B] chosen by the
+ * caller (the reference uses its order+1 rule). The reference solution is a sum of plane waves
+ * (the family of EDGE's convergence setups; its exprtk expressions are not evaluated on the
+ * device): waves[n_waves][15] = k[3], omega, phase, amp[9], run (-1 = every run), adding
+ * amp[q] * sin(k . x - omega t + phase) to quantity q. Outputs l1 / l2 / linf [9][R] (host, any may
+ * be NULL). Needs edge_b200_upload_geometry (element vertex coordinates [nEl][4][3], FP64). */
+int edge_b200_upload_geometry(edge_b200_ctx *ctx, const double *el_ve_crds);
+int edge_b200_error_norms(edge_b200_ctx *ctx, double t, int n_waves, const double *waves, int n_qp,
+                          const double *qp_xi, const double *qp_w, const double *qp_basis, double *l1, double *l2,
+                          double *linf);
 /* Halo exchange between the halves of a step (EDGE's MPI path: the local step packs the
  * face-projected time integrals of the send faces, AderDg.hpp:419-473, the neighbour step reads
  * the received ones, 675-684). With edge_b200_set_owned the kernels update only the elements
