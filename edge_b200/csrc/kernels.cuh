@@ -234,6 +234,28 @@ __device__ __forceinline__ void copyDofRows(T *tile, const T *dofsE, int64_t e, 
   }
 }
 
+// the reverse for results: tile rows (q, eo * R + row), stride S -> the [R][G] rows of row block
+// blk in global memory, consecutive lanes storing consecutive 16-byte chunks (the caller orders the
+// tile rows before, e.g. with __syncwarp when warp q wrote them)
+template <typename T, int R, int G, int S>
+__device__ __forceinline__ void storeRowsCoalesced(const T *tile, T *blk, int q, int eo, int r) {
+  constexpr int W = 16 / int(sizeof(T)), CPR = G / W;
+  const T *src = tile + (q * 32 + eo * R) * S;
+#pragma unroll
+  for (int it = 0; it < CPR; it++) {
+    const int k = it * R + r;
+    const int row = k / CPR, col = k % CPR;
+    T v[4];
+    if constexpr (sizeof(T) == 4) {
+      ld4<T>(src + row * S + col * W, v);
+      *reinterpret_cast<float4 *>(blk + row * G + col * W) = make_float4(v[0], v[1], v[2], v[3]);
+    } else {
+      const double2 d = *reinterpret_cast<const double2 *>(src + row * S + col * W);
+      *reinterpret_cast<double2 *>(blk + row * G + col * W) = d;
+    }
+  }
+}
+
 template <typename T, int O, int R, int RM>
 struct Geo {
   static constexpr int GB = padGlobal<T>(nModes(O)), GF = padGlobal<T>(nFaceModes(O));
@@ -533,8 +555,17 @@ __device__ __forceinline__ void localFace(const StepArgs<T> &a, const T *TI, T *
 #pragma unroll
     for (int j = 0; j < F; j++) s[j] = T(0);
     FluxLMul<O, FA>::template run<T>(OwnRow<T>{rowPtr<T, SB>(TI, q, l)}, s);
-    stRow<T, F>(rowPtr<T, SF>(S0, q, l), s);
-    if (valid) stRowG<T, F>(gRow<T, R, G::GF>(a.face, e * 4 + FA, 9, q, r), s);
+    {
+      // the row padded to GF with zeros, then the warp's rows of each element as coalesced stores
+      T sp[G::GF];
+#pragma unroll
+      for (int j = 0; j < G::GF; j++) sp[j] = j < F ? s[j] : T(0);
+      stRow<T, G::GF>(rowPtr<T, SF>(S0, q, l), sp);
+    }
+    __syncwarp();
+    if (valid)
+      storeRowsCoalesced<T, R, G::GF, SF>(S0, a.face + ((e * 4 + FA) * 9 + q) * int64_t(R * G::GF), q, l / R,
+                                          l % R);
     if constexpr (LTS) {
       if (valid) {
         const int fl = a.ltsFlags[e];
@@ -726,9 +757,21 @@ __global__ void __launch_bounds__(Geo<T, O, R, RM>::NT, LTS ? 1 : Geo<T, O, R, R
     localFace<T, O, R, RM, 1, LTS>(a, TI, S0, q, l, ev, r, valid, acc, upA, TIh);
     localFace<T, O, R, RM, 2, LTS>(a, TI, S0, q, l, ev, r, valid, acc, upA, TIh);
     localFace<T, O, R, RM, 3, LTS>(a, TI, S0, q, l, ev, r, valid, acc, upA, TIh);
+    if constexpr (G::tiSmem) {
+      // the updated rows through the (now unused) time-integral tile, stored coalesced
+      if (q < 9) {
+        T ap[G::GB];
+#pragma unroll
+        for (int n = 0; n < G::GB; n++) ap[n] = n < B ? acc[n] : T(0);
+        stRow<T, G::GB>(rowPtr<T, SB>(TI, q, l), ap);
+        __syncwarp();
+        if (valid)
+          storeRowsCoalesced<T, R, G::GB, SB>(TI, a.dofsE + (e * 9 + q) * int64_t(R * G::GB), q, eo, r);
+      }
+    }
     if (valid) {
       if (q < 9) {
-        stRowG<T, B>(gRow<T, R, G::GB>(a.dofsE, e, 9, q, r), acc);
+        if constexpr (!G::tiSmem) stRowG<T, B>(gRow<T, R, G::GB>(a.dofsE, e, 9, q, r), acc);
       } else if constexpr (RM > 0) {
         // dofsA_m += omega_m * (Psi_vol - tIntA_m) + omega_m * upA_surf
         const int s = q - 9;
