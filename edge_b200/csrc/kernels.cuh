@@ -802,8 +802,8 @@ __global__ void __launch_bounds__(Geo<T, O, R, RM>::NT, LTS ? 1 : Geo<T, O, R, R
 // The face rows a CTA reads (the neighbours' face projections, or its own for free-surface faces)
 // and the flux-solver blocks are gathered with asynchronous copies (cp.async, no registers held)
 // into a ring of NSN shared-memory slots, one slot per (element group, face) item, NSN - 1 items
-// ahead of the one being processed; the next group's DOF rows are prefetched the same way when
-// they fit. Per item: wait for its copies, rotate the neighbour's rows into this element's face
+// ahead of the one being processed. Where a DOF tile fits, the updated DOF rows leave through it as
+// coalesced stores and the next group's DOF rows arrive in it asynchronously. Per item: wait for its copies, rotate the neighbour's rows into this element's face
 // orientation in place, one CTA barrier, issue the copies of the item NSN - 1 ahead into the slot
 // the previous item released, then mix quantities and apply fluxT.
 
@@ -988,7 +988,6 @@ __device__ __forceinline__ void neighItem(const StepArgs<T> &a, unsigned char *b
   const int slotNext = int((item + NSN - 1) % NSN);
   // the next group's DOF rows join the copies committed now (the barrier ordered this group's
   // reads of the tile before them)
-  if constexpr (FA == 0) NS::issueDofs(a, base, q, l, g + gridDim.x, nextValid);
   if constexpr (AHEAD < 4)
     NS::template issue<AHEAD>(a, base, slotNext, q, l, g, true, cur);
   else
@@ -1023,8 +1022,8 @@ __global__ void __launch_bounds__(Geo<T, O, R, RM>::NT, Geo<T, O, R, RM>::minCta
     T upA[RM ? B : 1];
     if (q < 9) {
       if constexpr (G::dofTile) {
-        // the group's DOF rows arrived with (or before) its first face item
-        cpAsyncWait<NSN - 2>();
+        // the group's DOF rows (committed last, at the end of the previous group)
+        cpAsyncWait<0>();
         __syncwarp();
         if (valid)
           ldRow<T, B>(rowPtr<T, G::SB>(NS::dofTile(smem), q, l), acc);
@@ -1042,9 +1041,26 @@ __global__ void __launch_bounds__(Geo<T, O, R, RM>::NT, Geo<T, O, R, RM>::minCta
     neighItem<T, O, R, RM, 1>(a, smem, q, l, e, valid, cur, nxt, g, nextValid, k, acc, upA);
     neighItem<T, O, R, RM, 2>(a, smem, q, l, e, valid, cur, nxt, g, nextValid, k, acc, upA);
     neighItem<T, O, R, RM, 3>(a, smem, q, l, e, valid, cur, nxt, g, nextValid, k, acc, upA);
+    if constexpr (G::dofTile) {
+      // the updated rows through the DOF tile (this warp's rows only), stored coalesced; then the
+      // next group's DOF rows into the tile
+      if (q < 9) {
+        T ap[G::GB];
+#pragma unroll
+        for (int n = 0; n < G::GB; n++) ap[n] = n < B ? acc[n] : T(0);
+        stRow<T, G::GB>(rowPtr<T, G::SB>(NS::dofTile(smem), q, l), ap);
+        __syncwarp();
+        if (valid)
+          storeRowsCoalesced<T, R, G::GB, G::SB>(NS::dofTile(smem), a.dofsE + (e * 9 + q) * int64_t(R * G::GB), q,
+                                                 eo, r);
+        __syncwarp();
+      }
+      NS::issueDofs(a, smem, q, l, g + gridDim.x, nextValid);
+      cpAsyncCommit();
+    }
     if (valid) {
       if (q < 9) {
-        stRowG<T, B>(gRow<T, R, G::GB>(a.dofsE, e, 9, q, r), acc);
+        if constexpr (!G::dofTile) stRowG<T, B>(gRow<T, R, G::GB>(a.dofsE, e, 9, q, r), acc);
       } else if constexpr (RM > 0) {
         // scatterUpdateA (SurfInt.hpp:139-156)
         const int s = q - 9;
