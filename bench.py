@@ -144,6 +144,10 @@ def build_problem(name):
     return prob, prec
 
 
+def host_n_modes(order):
+    return order * (order + 1) * (order + 2) // 6
+
+
 def algorithmic(prob, prec):
     """Per-element algorithmic bytes and flops of one step (dense-in-modes counts as in the
     roofline model of the path) for each kernel."""
@@ -220,29 +224,33 @@ def cpu_sample_rate(order, runs, rm, n_cubes=12, steps=2):
 
 
 def run_serve(n_req, rate, device, seed=3343):
-    """The serving form: Poisson arrivals of simulation requests (own point source, 5-16
-    receivers, 100-300 steps) on two meshes (16^3 and 12^3 cubes x 6 tets) at orders 4 and 5,
-    continuously batched into 16-run FP32 pools; reports latency percentiles and the delivered
-    element updates per second against running the same requests one after another as plain
-    FP64 single runs (timed on the same pools' meshes)."""
-    import numpy as np
+    """The serving form: simulation requests (own point source, 4-16 receivers, 100-300 steps) on
+    two meshes (16^3 and 12^3 cubes x 6 tets) at orders 4 and 5, continuously batched into 16-run
+    FP32 pools. Two passes over the same seeded requests: all arriving at once (capacity: delivered
+    element updates per second against running them one after another as plain FP64 single runs,
+    timed on the same meshes) and Poisson arrivals at `rate` per second (latency percentiles)."""
     import torch
     from edge_b200 import host, serve
     from edge_b200.solver import Solver
     specs = {"box16": serve.MeshSpec(16), "box12": serve.MeshSpec(12, ext=7.5e3)}
     keys = [(m, o) for m in specs for o in (4, 5)]
-    reqs = serve.make_stream(n_req, rate, specs, orders=(4, 5), steps=(100, 300), seed=seed)
-    srv = serve.Server(specs, runs=16, precision=32, chunk=20, device=device)
-    srv.warm(keys)
-    done = srv.run(reqs, clock="wall")
-    wall = srv.wall
-    n_el = {m: srv.meshes.get(m)[0].n_el for m in specs}
-    srv.close()
-    useful = sum(n_el[r.mesh] * r.n_steps for r in done)
+    out = {}
+    for name, r in (("burst", 1e6), ("poisson", rate)):
+        reqs = serve.make_stream(n_req, r, specs, orders=(4, 5), steps=(100, 300), seed=seed)
+        srv = serve.Server(specs, runs=16, precision=32, chunk=20, device=device)
+        srv.warm(keys)
+        done = srv.run(reqs, clock="wall")
+        n_el = {m: srv.meshes.get(m)[0].n_el for m in specs}
+        meshes = srv.meshes
+        srv.close()
+        lat = serve.latency_stats(done)
+        out[name] = dict(requests=len(done), arrival_rate_per_s=r, wall_s=srv.wall, latency_s_p50=lat["p50"],
+                         latency_s_p99=lat["p99"],
+                         delivered_element_updates_per_s=sum(n_el[x.mesh] * x.n_steps for x in done) / srv.wall)
     # plain FP64, one run, same mesh and order: ms per step
     ms64 = {}
     for m, o in keys:
-        mesh, rho, lam, mu, star, fsE = srv.meshes.get(m)
+        mesh, rho, lam, mu, star, fsE = meshes.get(m)
         dt = host.dt_cfl(mesh, o, rho, lam, mu)
         p = host.Problem(order=o, runs=1, rm=0, mesh=mesh, rho=rho, lam=lam, mu=mu, starE=star, fsE=fsE, dt=dt)
         st = torch.cuda.Stream(device=device)
@@ -257,14 +265,13 @@ def run_serve(n_req, rate, device, seed=3343):
         torch.cuda.synchronize()
         ms64[(m, o)] = e0.elapsed_time(e1) / 20
         sv.close()
-    serial_s = sum(ms64[(r.mesh, r.order)] * r.n_steps for r in done) / 1e3
-    lat = serve.latency_stats(done)
-    return {"requests": len(done), "arrival_rate_per_s": rate, "wall_s": wall,
-            "latency_s_p50": lat["p50"], "latency_s_p99": lat["p99"],
-            "delivered_element_updates_per_s": useful / wall,
-            "serial_plain_fp64_s": serial_s, "speedup_vs_serial_plain_fp64": serial_s / wall,
-            "pools": len(keys), "slots_per_pool": 16, "chunk_steps": 20,
-            "note": "wall-clock from the first arrival; latency = arrival -> last receiver sample on the host"}
+    reqs = serve.make_stream(n_req, rate, specs, orders=(4, 5), steps=(100, 300), seed=seed)
+    serial_s = sum(ms64[(x.mesh, x.order)] * x.n_steps for x in reqs) / 1e3
+    out["burst"]["serial_plain_fp64_s"] = serial_s
+    out["burst"]["speedup_vs_serial_plain_fp64"] = serial_s / out["burst"]["wall_s"]
+    out.update(pools=len(keys), slots_per_pool=16, chunk_steps=20,
+               note="wall clock from the first arrival; latency = arrival -> last receiver sample on the host")
+    return out
 
 
 def run_reference(a, ws, rank):
@@ -359,6 +366,19 @@ def main():
                 "achieved_tflops": flops_launch / (avg_ms / 1e3) / 1e12,
                 "kernel_avg_ms": {names[i]: float(kms[i] / kn[i]) for i in range(4) if kn[i]},
                 "kernel_share": shares}
+    # the neighbour-flux kernel (the HBM-bound one) on its own: bytes this design moves (face
+    # projections read, DOFs read + written, flux solvers, connectivity) and the reference algorithm's
+    # count (neighbours' time-integrated DOFs instead of face projections)
+    n_ms = kms[1] / max(kn[1], 1)
+    B_, F_, p_ = host_n_modes(prob.order), prob.order * (prob.order + 1) // 2, (8 if prec == 64 else 4)
+    ref_bytes = (3 * 9 * B_ * prob.runs * p_ + 4 * 81 * 8 + 4 * 6) * prob.n_el
+    roofline_neighbour = {"bound": "hbm", "kernel": "neighbour", "avg_ms": n_ms,
+                          "achieved": alg["neigh_bytes"] * prob.n_el / (n_ms / 1e3) / 1e9, "peak": peak,
+                          "unit": "GB/s", "peak_source": peak_src,
+                          "algorithmic_bytes_per_launch": alg["neigh_bytes"] * prob.n_el,
+                          "achieved_reference_count": ref_bytes / (n_ms / 1e3) / 1e9}
+    roofline_neighbour["frac"] = roofline_neighbour["achieved"] / peak
+    roofline_neighbour["frac_reference_count"] = roofline_neighbour["achieved_reference_count"] / peak
 
     # end to end through the C ABI with host buffers: pinned H2D of the DOFs, one step, D2H of the DOFs
     pin_e = torch.from_numpy(e0).pin_memory()
@@ -429,7 +449,7 @@ def main():
                "step_ms_p50": step_ms[len(step_ms) // 2], "step_ms_p99": step_ms[min(len(step_ms) - 1,
                                                                                       int(0.99 * len(step_ms)))],
                "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": int(launches),
-               "clocks": clk, "fp64_plain": fp64, "serving": serving}
+               "clocks": clk, "fp64_plain": fp64, "serving": serving, "roofline_neighbour": roofline_neighbour}
         print(json.dumps(out), flush=True)
     barrier(ws)
     if ws > 1:
