@@ -545,7 +545,9 @@ __device__ __forceinline__ void faceMix(const T *S0, int l, const T (&fr)[9], T 
 // ------------------------------------------------------------------------------------------------
 // local step: CK, volume, local surface, face projections (AderDg::local, AderDg.hpp:338-534)
 // ------------------------------------------------------------------------------------------------
-template <typename T, int O, int R, int RM, int FA, bool LTS = false>
+// TAIL: a barrier after the quantity mix, before the face tile is written again (not needed when
+// consecutive faces alternate between two tiles)
+template <typename T, int O, int R, int RM, int FA, bool LTS = false, bool TAIL = true>
 __device__ __forceinline__ void localFace(const StepArgs<T> &a, const T *TI, T *S0, int q, int l, int64_t e,
                                           int r, bool valid, T *acc, T *upA, const T *TIh = nullptr) {
   using G = Geo<T, O, R, RM>;
@@ -610,7 +612,7 @@ __device__ __forceinline__ void localFace(const StepArgs<T> &a, const T *TI, T *
     FluxTMul<O, FA>::template run<T>(s, acc);
   else if constexpr (RM > 0)
     FluxTMul<O, FA>::template run<T>(s, upA);
-  __syncthreads();
+  if constexpr (TAIL) __syncthreads();
 }
 
 template <typename T, int O, int R, int RM, bool LTS>
@@ -624,6 +626,10 @@ __global__ void __launch_bounds__(Geo<T, O, R, RM>::NT, LTS ? 1 : Geo<T, O, R, R
   // see Geo: time integrals in shared memory (TI behind X, TIA behind XA, face tiles reuse X) or
   // in registers (copied into X / XA after the recursion, face tiles behind X); with LTS the
   // half-step integral TIh behind everything
+  // AS (G::asyncLocal): the DOF rows arrive by cp.async (the next group's into this warp's TI rows
+  // at the end of a group, the current group's into X again after the recursion) and the faces
+  // alternate between a separate face tile (even faces) and X (odd faces): one barrier per face
+  // instead of two (the last face keeps both)
   constexpr bool AS = G::asyncLocal;
   T *TI = G::tiSmem ? X + G::nX : X;
   T *TIA = G::tiSmem ? XA + G::nXA : XA;
@@ -637,7 +643,7 @@ __global__ void __launch_bounds__(Geo<T, O, R, RM>::NT, LTS ? 1 : Geo<T, O, R, R
     // the first group's DOF rows
     const int64_t g0 = blockIdx.x;
     if (q < 9 && g0 < nGroups && g0 * E + eo < a.elCount)
-      copyDofRows<T, R, G::GB, SB>(X, a.dofsE, a.elFirst + g0 * E + eo, q, eo, r);
+      copyDofRows<T, R, G::GB, SB>(TI, a.dofsE, a.elFirst + g0 * E + eo, q, eo, r);
     cpAsyncCommit();
   }
   for (int64_t g = blockIdx.x; g < nGroups; g += gridDim.x) {
@@ -653,12 +659,11 @@ __global__ void __launch_bounds__(Geo<T, O, R, RM>::NT, LTS ? 1 : Geo<T, O, R, R
         cpAsyncWait<0>();
         __syncwarp();
         if (valid)
-          ldRow<T, B>(rowPtr<T, SB>(X, q, l), v);
-        else {
+          ldRow<T, B>(rowPtr<T, SB>(TI, q, l), v);
+        else
 #pragma unroll
           for (int n = 0; n < B; n++) v[n] = T(0);
-          stRow<T, B>(rowPtr<T, SB>(X, q, l), v);
-        }
+        stRow<T, B>(rowPtr<T, SB>(X, q, l), v);
       } else {
         ldRowG<T, B>(gRow<T, R, G::GB>(a.dofsE, ev, 9, q, r), v, valid);
         stRow<T, B>(rowPtr<T, SB>(X, q, l), v);
@@ -729,12 +734,6 @@ __global__ void __launch_bounds__(Geo<T, O, R, RM>::NT, LTS ? 1 : Geo<T, O, R, R
         else
 #pragma unroll
           for (int n = 0; n < B; n++) acc[n] = T(0);
-        __syncwarp();
-        // the next group's DOF rows arrive during the volume and face integrals
-        const int64_t gn = g + gridDim.x;
-        if (gn < nGroups && gn * E + eo < a.elCount)
-          copyDofRows<T, R, G::GB, SB>(X, a.dofsE, a.elFirst + gn * E + eo, q, eo, r);
-        cpAsyncCommit();
       } else {
         ldRowG<T, B>(gRow<T, R, G::GB>(a.dofsE, ev, 9, q, r), acc, valid);
       }
@@ -753,10 +752,18 @@ __global__ void __launch_bounds__(Geo<T, O, R, RM>::NT, LTS ? 1 : Geo<T, O, R, R
       VolMul<O>::template run<T>(z, acc);
     }
     // local surface integral (SurfIntVanilla::local, SurfIntVanilla.hpp:212-262) + face projections
-    localFace<T, O, R, RM, 0, LTS>(a, TI, S0, q, l, ev, r, valid, acc, upA, TIh);
-    localFace<T, O, R, RM, 1, LTS>(a, TI, S0, q, l, ev, r, valid, acc, upA, TIh);
-    localFace<T, O, R, RM, 2, LTS>(a, TI, S0, q, l, ev, r, valid, acc, upA, TIh);
-    localFace<T, O, R, RM, 3, LTS>(a, TI, S0, q, l, ev, r, valid, acc, upA, TIh);
+    if constexpr (AS) {
+      localFace<T, O, R, RM, 0, LTS, false>(a, TI, S0, q, l, ev, r, valid, acc, upA, TIh);
+      localFace<T, O, R, RM, 1, LTS, false>(a, TI, X, q, l, ev, r, valid, acc, upA, TIh);
+      localFace<T, O, R, RM, 2, LTS, false>(a, TI, S0, q, l, ev, r, valid, acc, upA, TIh);
+      // the barrier after the last face orders its readers of X before the next group writes X
+      localFace<T, O, R, RM, 3, LTS, true>(a, TI, X, q, l, ev, r, valid, acc, upA, TIh);
+    } else {
+      localFace<T, O, R, RM, 0, LTS>(a, TI, S0, q, l, ev, r, valid, acc, upA, TIh);
+      localFace<T, O, R, RM, 1, LTS>(a, TI, S0, q, l, ev, r, valid, acc, upA, TIh);
+      localFace<T, O, R, RM, 2, LTS>(a, TI, S0, q, l, ev, r, valid, acc, upA, TIh);
+      localFace<T, O, R, RM, 3, LTS>(a, TI, S0, q, l, ev, r, valid, acc, upA, TIh);
+    }
     if constexpr (G::tiSmem) {
       // the updated rows through the (now unused) time-integral tile, stored coalesced
       if (q < 9) {
@@ -767,7 +774,15 @@ __global__ void __launch_bounds__(Geo<T, O, R, RM>::NT, LTS ? 1 : Geo<T, O, R, R
         __syncwarp();
         if (valid)
           storeRowsCoalesced<T, R, G::GB, SB>(TI, a.dofsE + (e * 9 + q) * int64_t(R * G::GB), q, eo, r);
+        if constexpr (AS) {
+          // the next group's DOF rows into this warp's TI rows
+          __syncwarp();
+          const int64_t gn = g + gridDim.x;
+          if (gn < nGroups && gn * E + eo < a.elCount)
+            copyDofRows<T, R, G::GB, SB>(TI, a.dofsE, a.elFirst + gn * E + eo, q, eo, r);
+        }
       }
+      if constexpr (AS) cpAsyncCommit();
     }
     if (valid) {
       if (q < 9) {
