@@ -284,6 +284,8 @@ struct Geo {
       (sizeof(T) == 4 && RM == 0 && baseLocal <= 110 * 1024) ? 110 * 1024 : 227 * 1024;
   static constexpr bool asyncLocal = tiSmem && baseLocal + nS0 * sizeof(T) <= localBudget;
   static constexpr size_t smemLocal = baseLocal + (asyncLocal ? nS0 * sizeof(T) : 0);
+  // elastic CK with ping-pong derivatives between X and the separate face tile
+  static constexpr bool ckPingPong = asyncLocal && RM == 0 && nModes(O - 1) <= SF;
   // LTS local step: one more [9][32][SB] tile for the half-step time integral (behind the rest);
   // configurations whose time integrals do not fit shared memory have no LTS kernels
   static constexpr size_t smemLocalLts = smemLocal + nX * sizeof(T);
@@ -434,23 +436,31 @@ __device__ __forceinline__ void addSrc(const ElemCoef<T, RM> &c, const T *Y, int
 // derivative D of TimePredVanilla::ck (TimePredVanilla.hpp:229-303) with the star matrix applied
 // before the stiffness product; der[D] replaces der[D-1] in X, TI += sca * der[D] (rows owned by
 // their warp), the anelastic warps update XA and TIA.
-template <typename T, int O, int R, int RM, int D, bool H = false>
+// PP (ping-pong, elastic only): the derivatives alternate between X (even D, stride SB) and the
+// face tile XP (odd D, stride SF), so a level reads one buffer and writes the other and needs one
+// barrier instead of two (the truncated derivatives of levels >= 1 fit the face tile's rows)
+template <typename T, int O, int R, int RM, int D, bool H = false, bool PP = false>
 struct CkStep {
   using G = Geo<T, O, R, RM>;
   static constexpr int B = G::B, S = G::SB;
   static constexpr int NN = RM ? nModes(O - 1) : nModes(O - D);  // output modes of the product
   static constexpr int DK = RM ? 1 : D;                           // truncation of the product
+  static constexpr bool IN_P = PP && (D - 1) % 2 == 1, OUT_P = PP && D % 2 == 1;
+  static constexpr int SI = IN_P ? G::SF : S, SO = OUT_P ? G::SF : S;
+  static_assert(!PP || (RM == 0 && NN <= G::SF), "ping-pong derivatives must fit the face tile");
 
   // H: also TIh += scaH * der[D] (the time integral over the first half of the step, for LTS)
   __device__ __forceinline__ static void run(T *X, T *TI, T *XA, T *TIA, int q, int l, const ElemCoef<T, RM> &c,
                                              const double *omega, T sca, T *tIr, T (*tIAr)[B], T *TIh = nullptr,
-                                             T scaH = T(0)) {
+                                             T scaH = T(0), T *XP = nullptr) {
+    T *Xin = IN_P ? XP : X;
+    T *Xout = OUT_P ? XP : X;
     T acc[B];
 #pragma unroll
     for (int n = 0; n < B; n++) acc[n] = T(0);
     if (q < 9) {
-      Mix3<T, S> z{rowPtr<T, S>(X, c.cols[0], l), rowPtr<T, S>(X, c.cols[1], l), rowPtr<T, S>(X, c.cols[2], l),
-                   c.cs};
+      Mix3<T, SI> z{rowPtr<T, SI>(Xin, c.cols[0], l), rowPtr<T, SI>(Xin, c.cols[1], l),
+                    rowPtr<T, SI>(Xin, c.cols[2], l), c.cs};
       CkMul<O, DK>::template run<T>(z, acc);
       if constexpr (RM > 0)
         if (q < 6) addSrc<T, B, S, RM>(c, XA, l, acc);
@@ -458,10 +468,10 @@ struct CkStep {
       Mix2<T, S> z{rowPtr<T, S>(X, 6 + c.colsA[0], l), rowPtr<T, S>(X, 6 + c.colsA[1], l), c.ca};
       CkMul<O, DK>::template run<T>(z, acc);
     }
-    __syncthreads();
+    if constexpr (!PP) __syncthreads();
     if (q < 9) {
       constexpr int NW = RM ? B : NN;  // modes beyond NN stay zero without anelasticity
-      stRow<T, NW>(rowPtr<T, S>(X, q, l), acc);
+      stRow<T, NW>(rowPtr<T, SO>(Xout, q, l), acc);
       if constexpr (G::tiSmem) {
         T t[NW];
         T *p = rowPtr<T, S>(TI, q, l);
@@ -508,15 +518,15 @@ struct CkStep {
   }
 };
 
-template <typename T, int O, int R, int RM, int D, bool H = false>
+template <typename T, int O, int R, int RM, int D, bool H = false, bool PP = false>
 __device__ __forceinline__ void ckAll(T *X, T *TI, T *XA, T *TIA, int q, int l, const ElemCoef<T, RM> &c,
                                       const double *omega, T dt, T sca, T *tIr, T (*tIAr)[nModes(O)],
-                                      T *TIh = nullptr, T scaH = T(0)) {
+                                      T *TIh = nullptr, T scaH = T(0), T *XP = nullptr) {
   if constexpr (D < O) {
     sca = sca * dt / T(D + 1);
     if constexpr (H) scaH = scaH * (dt * T(0.5)) / T(D + 1);
-    CkStep<T, O, R, RM, D, H>::run(X, TI, XA, TIA, q, l, c, omega, sca, tIr, tIAr, TIh, scaH);
-    ckAll<T, O, R, RM, D + 1, H>(X, TI, XA, TIA, q, l, c, omega, dt, sca, tIr, tIAr, TIh, scaH);
+    CkStep<T, O, R, RM, D, H, PP>::run(X, TI, XA, TIA, q, l, c, omega, sca, tIr, tIAr, TIh, scaH, XP);
+    ckAll<T, O, R, RM, D + 1, H, PP>(X, TI, XA, TIA, q, l, c, omega, dt, sca, tIr, tIAr, TIh, scaH, XP);
   }
 }
 
@@ -703,7 +713,8 @@ __global__ void __launch_bounds__(Geo<T, O, R, RM>::NT, LTS ? 1 : Geo<T, O, R, R
     c.load(a, ev, valid, q);
     __syncthreads();
     // Cauchy-Kowalevski (TimePredVanilla::ck, TimePredVanilla.hpp:200-306)
-    ckAll<T, O, R, RM, 1, LTS>(X, TI, XA, TIA, q, l, c, a.omega, dt, dt, tIr, tIAr, TIh, dt * T(0.5));
+    ckAll<T, O, R, RM, 1, LTS, G::ckPingPong>(X, TI, XA, TIA, q, l, c, a.omega, dt, dt, tIr, tIAr, TIh,
+                                              dt * T(0.5), S0);
     if constexpr (!G::tiSmem) {
       if (q < 9) {
         stRow<T, B>(rowPtr<T, SB>(X, q, l), tIr);
