@@ -81,7 +81,9 @@ def test_fp64_all_boundary_types():
 
 
 @pytest.mark.parametrize("order,runs,rm", [(3, 16, 0), (4, 16, 0), (5, 16, 0), (6, 16, 0), (4, 8, 3),
-                                           (3, 1, 0), (4, 1, 0)])
+                                           (3, 1, 0), (4, 1, 0), (5, 1, 0),
+                                           (3, 4, 0), (4, 4, 0), (5, 4, 0), (6, 4, 0),
+                                           (3, 8, 0), (4, 8, 0), (5, 8, 0), (6, 8, 0), (3, 8, 3), (5, 8, 3)])
 def test_fp32_fused_runs_vs_fp64_oracle(order, runs, rm):
     prob = small_problem(n=2, order=order, runs=runs, rm=rm, jitter=0.15, n_steps=3, source="random")
     s, orc, e, a, t, (rb, rt, rc) = _run_both(prob, 32, 3)
