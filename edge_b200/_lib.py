@@ -50,6 +50,7 @@ _SIGS = {
     "edge_b200_set_receivers": (C.c_int, [vp, C.c_int, vp, vp, dbl, dbl, C.c_int]),
     "edge_b200_step": (C.c_int, [vp, dbl, dbl, C.c_int]),
     "edge_b200_upload_geometry": (C.c_int, [vp, vp]),
+    "edge_b200_wavefield": (C.c_int, [vp, vp]),
     "edge_b200_error_norms": (C.c_int, [vp, dbl, C.c_int, vp, C.c_int, vp, vp, vp, vp, vp, vp]),
     "edge_b200_set_owned": (C.c_int, [vp, i64]),
     "edge_b200_step_phase": (C.c_int, [vp, dbl, dbl, C.c_int]),

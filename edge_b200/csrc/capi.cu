@@ -137,6 +137,18 @@ __global__ void kErrorNorms(const T *dofsE, const double *geom, int64_t nEl, int
   atomicMax(reinterpret_cast<unsigned long long *>(norms + (18 + q) * R + r), __double_as_longlong(li));
 }
 
+// wave-field snapshot: the mode-0 coefficient (the element mean of the orthogonal basis) of every
+// quantity and run as FP32, out[run][q][el]
+template <typename T>
+__global__ void kWaveField(const T *dofsE, int64_t nEl, int R, int G, float *out) {
+  const int64_t total = nEl * 9 * R;
+  for (int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < total; i += int64_t(gridDim.x) * blockDim.x) {
+    const int64_t e = i % nEl, qr = i / nEl;
+    const int q = int(qr % 9), r = int(qr / 9);
+    out[i] = float(dofsE[((e * 9 + q) * R + r) * int64_t(G)]);
+  }
+}
+
 // rows [nRows][R][G] <- src [nRows][B] for one run (zeros when src is null)
 template <typename T>
 __global__ void kSetRun(T *rows, const T *src, int64_t nRows, int B, int R, int G, int run) {
@@ -936,6 +948,24 @@ int edge_b200_error_norms(edge_b200_ctx *ctx, double t, int n_waves, const doubl
     if (l2) l2[i] = std::sqrt(h[9 * R + i]);
     if (linf) linf[i] = h[18 * R + i];
   }
+  return EDGE_B200_OK;
+}
+
+int edge_b200_wavefield(edge_b200_ctx *ctx, float *out) {
+  if (!ctx || !out) return EDGE_B200_EINVAL;
+  const size_t n = (size_t)ctx->nEl * 9 * ctx->cfg.n_runs;
+  cudaStream_t s = ctx->stream;
+  EDGE_CUDA(ctx->norms.fit(n * sizeof(float)), "wave field");
+  const int grid = (int)std::min<size_t>((n + 255) / 256, 148 * 16);
+  if (ctx->cfg.precision == 64)
+    kWaveField<double><<<grid, 256, 0, s>>>((const double *)ctx->dofsE, ctx->nEl, ctx->cfg.n_runs, ctx->GB,
+                                            ctx->norms.as<float>());
+  else
+    kWaveField<float><<<grid, 256, 0, s>>>((const float *)ctx->dofsE, ctx->nEl, ctx->cfg.n_runs, ctx->GB,
+                                           ctx->norms.as<float>());
+  EDGE_CUDA(cudaGetLastError(), "wave field");
+  EDGE_CUDA(cudaMemcpyAsync(out, ctx->norms.p, n * sizeof(float), cudaMemcpyDeviceToHost, s), "wave field");
+  EDGE_CUDA(cudaStreamSynchronize(s), "wave field");
   return EDGE_B200_OK;
 }
 

@@ -93,6 +93,12 @@ class Solver:
         self._chk(lib().edge_b200_step_lts(self._h, t0, dt_fun, n_cycles), "step_lts")
         self.t = t0 + float(n_cycles * (1 << (self.n_groups - 1))) * dt_fun
 
+    def wavefield(self):
+        """Mode-0 coefficients [R][9][nEl] (FP32) of the device DOFs."""
+        out = np.zeros((self.prob.runs, 9, self.prob.n_el), np.float32)
+        self._chk(lib().edge_b200_wavefield(self._h, ptr(out)), "wavefield")
+        return out
+
     def upload_geometry(self):
         crds = np.ascontiguousarray(self.prob.mesh.el_ve_crds(), np.float64)
         self._chk(lib().edge_b200_upload_geometry(self._h, ptr(crds)), "upload_geometry")

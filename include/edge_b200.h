@@ -209,6 +209,10 @@ int edge_b200_upload_geometry(edge_b200_ctx *ctx, const double *el_ve_crds);
 int edge_b200_error_norms(edge_b200_ctx *ctx, double t, int n_waves, const double *waves, int n_qp,
                           const double *qp_xi, const double *qp_w, const double *qp_basis, double *l1, double *l2,
                           double *linf);
+/* Wave-field snapshot (io::WaveField / io::Vtk::write, src/io/Vtk.cpp:83-121): the mode-0
+ * coefficient of every element, quantity and run, as FP32 in the reference's output order
+ * out[run][quantity][element] ([n_runs][9][nEl]); the DOFs stay on the device. */
+int edge_b200_wavefield(edge_b200_ctx *ctx, float *out);
 /* Halo exchange between the halves of a step (EDGE's MPI path: the local step packs the
  * face-projected time integrals of the send faces, AderDg.hpp:419-473, the neighbour step reads
  * the received ones, 675-684). With edge_b200_set_owned the kernels update only the elements

@@ -48,3 +48,21 @@ def test_norms_match_numpy(precision, order, runs):
     # the DG solution stays close to the wave: x-velocity error well below its norm
     # (amplitude n_x = 1/sqrt(2), rms over the box ext^3 of a sine: 1/2)
     assert np.all(l2[6] < 0.05 * 0.5 * ext ** 1.5)
+
+
+def test_wavefield_is_mode_zero(tmp_path):
+    from edge_b200 import vtk
+    prob = host.build_problem(3, 4, 16, seed=6, n_receivers=0, source="random", n_steps=10)
+    s = Solver(prob, precision=32)
+    try:
+        s.upload_dofs(prob.zero_dofs(np.float32)[0])
+        s.step(10)
+        wf = s.wavefield()
+        e, _ = s.download_dofs()
+    finally:
+        s.close()
+    np.testing.assert_array_equal(wf, np.transpose(e[:, :, 0, :], (2, 1, 0)))
+    assert np.abs(wf).max() > 0
+    path = str(tmp_path / "wf.vtk")
+    vtk.write(path, prob.mesh.ve, prob.mesh.el_ve, wf)
+    np.testing.assert_array_equal(vtk.read_cell_data(path)["crun_3_var_6"], wf[3, 6])
