@@ -43,6 +43,9 @@ _SIGS = {
     "edge_b200_upload_dofs": (C.c_int, [vp] * 3),
     "edge_b200_download_dofs": (C.c_int, [vp] * 3),
     "edge_b200_download_tdofs": (C.c_int, [vp] * 2),
+    "edge_b200_upload_dofs_async": (C.c_int, [vp] * 3),
+    "edge_b200_download_dofs_async": (C.c_int, [vp] * 3),
+    "edge_b200_join_transfers": (C.c_int, [vp, C.c_int]),
     "edge_b200_keep_tdofs": (C.c_int, [vp, C.c_int]),
     "edge_b200_set_run_dofs": (C.c_int, [vp, C.c_int, vp, vp]),
     "edge_b200_rewind_receivers": (C.c_int, [vp, dbl]),

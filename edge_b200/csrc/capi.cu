@@ -280,6 +280,47 @@ struct edge_b200_ctx {
     return cudaStreamSynchronize(stream);
   }
 
+  // asynchronous transfers: their own copy streams and staging buffers; events order them with
+  // the context stream (H2D -> layout kernel -> step kernels -> layout kernel -> D2H) on the device
+  cudaStream_t h2d = nullptr, d2h = nullptr;
+  cudaEvent_t evH2D = nullptr, evToRows = nullptr, evFromRows = nullptr, evD2H = nullptr;
+  void *stageOut = nullptr;
+  bool d2hPending = false, toRowsPending = false;
+  cudaError_t ensureAsync() {
+    cudaError_t e;
+    if (h2d) return cudaSuccess;
+    if ((e = ensureStage())) return e;
+    const size_t n = std::max(refCount(9), refCount(6 * cfg.n_rms));
+    if ((e = cudaMalloc(&stageOut, n * realSize))) return e;
+    if ((e = cudaStreamCreateWithFlags(&h2d, cudaStreamNonBlocking))) return e;
+    if ((e = cudaStreamCreateWithFlags(&d2h, cudaStreamNonBlocking))) return e;
+    for (cudaEvent_t *ev : {&evH2D, &evToRows, &evFromRows, &evD2H})
+      if ((e = cudaEventCreateWithFlags(ev, cudaEventDisableTiming))) return e;
+    return cudaSuccess;
+  }
+  cudaError_t uploadRowsAsync(void *rows, const void *host, int rowsPerEl) {
+    cudaError_t e;
+    // the staging buffer is free once the previous layout kernel read it
+    if (toRowsPending && (e = cudaStreamWaitEvent(h2d, evToRows, 0))) return e;
+    if ((e = cudaMemcpyAsync(stage, host, refCount(rowsPerEl) * realSize, cudaMemcpyHostToDevice, h2d))) return e;
+    if ((e = cudaEventRecord(evH2D, h2d))) return e;
+    if ((e = cudaStreamWaitEvent(stream, evH2D, 0))) return e;
+    if ((e = convertLayout(true, cfg.precision, stage, rows, nEl * rowsPerEl, B, cfg.n_runs, GB, stream))) return e;
+    toRowsPending = true;
+    return cudaEventRecord(evToRows, stream);
+  }
+  cudaError_t downloadRowsAsync(void *host, const void *rows, int rowsPerEl) {
+    cudaError_t e;
+    // the output staging buffer is free once the previous copy to the host finished
+    if (d2hPending && (e = cudaStreamWaitEvent(stream, evD2H, 0))) return e;
+    if ((e = convertLayout(false, cfg.precision, rows, stageOut, nEl * rowsPerEl, B, cfg.n_runs, GB, stream))) return e;
+    if ((e = cudaEventRecord(evFromRows, stream))) return e;
+    if ((e = cudaStreamWaitEvent(d2h, evFromRows, 0))) return e;
+    if ((e = cudaMemcpyAsync(host, stageOut, refCount(rowsPerEl) * realSize, cudaMemcpyDeviceToHost, d2h))) return e;
+    d2hPending = true;
+    return cudaEventRecord(evD2H, d2h);
+  }
+
   int fail(cudaError_t e, const char *what) {
     err = std::string(what) + ": " + cudaGetErrorString(e);
     return EDGE_B200_EDEVICE;
@@ -310,7 +351,11 @@ struct edge_b200_ctx {
     dfree(dofsE); dfree(dofsA); dfree(tDofs); dfree(face);
     dfree(starE); dfree(starA); dfree(srcA); dfree(fsE); dfree(fsA);
     dfree(elFaEl); dfree(fId); dfree(vId); dfree(faType);
-    dfree(dTau); dfree(dSlot); dfree(stage);
+    dfree(dTau); dfree(dSlot); dfree(stage); dfree(stageOut);
+    if (h2d) cudaStreamSynchronize(h2d), cudaStreamDestroy(h2d);
+    if (d2h) cudaStreamSynchronize(d2h), cudaStreamDestroy(d2h);
+    for (cudaEvent_t ev : {evH2D, evToRows, evFromRows, evD2H})
+      if (ev) cudaEventDestroy(ev);
     for (auto &t : timed) {
       cudaEventDestroy(t.a);
       cudaEventDestroy(t.b);
@@ -439,6 +484,37 @@ int edge_b200_download_dofs(edge_b200_ctx *ctx, void *dofs_e, void *dofs_a) {
   if (!ctx || !dofs_e) return EDGE_B200_EINVAL;
   EDGE_CUDA(ctx->downloadRows(dofs_e, ctx->dofsE, 9), "download dofsE");
   if (ctx->cfg.n_rms && dofs_a) EDGE_CUDA(ctx->downloadRows(dofs_a, ctx->dofsA, 6 * ctx->cfg.n_rms), "download dofsA");
+  return EDGE_B200_OK;
+}
+
+int edge_b200_upload_dofs_async(edge_b200_ctx *ctx, const void *dofs_e, const void *dofs_a) {
+  if (!ctx || !dofs_e || (ctx->cfg.n_rms && !dofs_a)) return EDGE_B200_EINVAL;
+  EDGE_CUDA(ctx->ensureAsync(), "async transfers");
+  EDGE_CUDA(ctx->uploadRowsAsync(ctx->dofsE, dofs_e, 9), "upload dofsE");
+  if (ctx->cfg.n_rms) EDGE_CUDA(ctx->uploadRowsAsync(ctx->dofsA, dofs_a, 6 * ctx->cfg.n_rms), "upload dofsA");
+  return EDGE_B200_OK;
+}
+
+int edge_b200_download_dofs_async(edge_b200_ctx *ctx, void *dofs_e, void *dofs_a) {
+  if (!ctx || !dofs_e) return EDGE_B200_EINVAL;
+  EDGE_CUDA(ctx->ensureAsync(), "async transfers");
+  EDGE_CUDA(ctx->downloadRowsAsync(dofs_e, ctx->dofsE, 9), "download dofsE");
+  if (ctx->cfg.n_rms && dofs_a)
+    EDGE_CUDA(ctx->downloadRowsAsync(dofs_a, ctx->dofsA, 6 * ctx->cfg.n_rms), "download dofsA");
+  return EDGE_B200_OK;
+}
+
+int edge_b200_join_transfers(edge_b200_ctx *ctx, int after_stream) {
+  if (!ctx) return EDGE_B200_EINVAL;
+  if (after_stream) {
+    // the copy streams start after what the context stream holds now
+    EDGE_CUDA(ctx->ensureAsync(), "join transfers");
+    EDGE_CUDA(cudaEventRecord(ctx->evFromRows, ctx->stream), "join transfers");
+    EDGE_CUDA(cudaStreamWaitEvent(ctx->h2d, ctx->evFromRows, 0), "join transfers");
+    EDGE_CUDA(cudaStreamWaitEvent(ctx->d2h, ctx->evFromRows, 0), "join transfers");
+  } else if (ctx->d2hPending) {
+    EDGE_CUDA(cudaStreamWaitEvent(ctx->stream, ctx->evD2H, 0), "join transfers");
+  }
   return EDGE_B200_OK;
 }
 
@@ -971,6 +1047,8 @@ int edge_b200_wavefield(edge_b200_ctx *ctx, float *out) {
 
 int edge_b200_sync(edge_b200_ctx *ctx) {
   if (!ctx) return EDGE_B200_EINVAL;
+  if (ctx->h2d) EDGE_CUDA(cudaStreamSynchronize(ctx->h2d), "sync");
+  if (ctx->d2h) EDGE_CUDA(cudaStreamSynchronize(ctx->d2h), "sync");
   EDGE_CUDA(cudaStreamSynchronize(ctx->stream), "sync");
   return EDGE_B200_OK;
 }

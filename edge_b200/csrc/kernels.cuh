@@ -569,10 +569,10 @@ __device__ __forceinline__ void localFace(const StepArgs<T> &a, const T *TI, T *
     FluxLMul<O, FA>::template run<T>(OwnRow<T>{rowPtr<T, SB>(TI, q, l)}, s);
     {
       // the row padded to GF with zeros, then the warp's rows of each element as coalesced stores
-      T sp[G::GF];
+      T *p = rowPtr<T, SF>(S0, q, l);
+      stRow<T, F>(p, s);
 #pragma unroll
-      for (int j = 0; j < G::GF; j++) sp[j] = j < F ? s[j] : T(0);
-      stRow<T, G::GF>(rowPtr<T, SF>(S0, q, l), sp);
+      for (int j = F; j < G::GF; j++) p[j] = T(0);
     }
     __syncwarp();
     if (valid)
@@ -778,10 +778,10 @@ __global__ void __launch_bounds__(Geo<T, O, R, RM>::NT, LTS ? 1 : Geo<T, O, R, R
     if constexpr (G::tiSmem) {
       // the updated rows through the (now unused) time-integral tile, stored coalesced
       if (q < 9) {
-        T ap[G::GB];
+        T *p = rowPtr<T, SB>(TI, q, l);
+        stRow<T, B>(p, acc);
 #pragma unroll
-        for (int n = 0; n < G::GB; n++) ap[n] = n < B ? acc[n] : T(0);
-        stRow<T, G::GB>(rowPtr<T, SB>(TI, q, l), ap);
+        for (int n = B; n < G::GB; n++) p[n] = T(0);
         __syncwarp();
         if (valid)
           storeRowsCoalesced<T, R, G::GB, SB>(TI, a.dofsE + (e * 9 + q) * int64_t(R * G::GB), q, eo, r);
@@ -1071,10 +1071,10 @@ __global__ void __launch_bounds__(Geo<T, O, R, RM>::NT, Geo<T, O, R, RM>::minCta
       // the updated rows through the DOF tile (this warp's rows only), stored coalesced; then the
       // next group's DOF rows into the tile
       if (q < 9) {
-        T ap[G::GB];
+        T *p = rowPtr<T, G::SB>(NS::dofTile(smem), q, l);
+        stRow<T, B>(p, acc);
 #pragma unroll
-        for (int n = 0; n < G::GB; n++) ap[n] = n < B ? acc[n] : T(0);
-        stRow<T, G::GB>(rowPtr<T, G::SB>(NS::dofTile(smem), q, l), ap);
+        for (int n = B; n < G::GB; n++) p[n] = T(0);
         __syncwarp();
         if (valid)
           storeRowsCoalesced<T, R, G::GB, G::SB>(NS::dofTile(smem), a.dofsE + (e * 9 + q) * int64_t(R * G::GB), q,
