@@ -48,6 +48,8 @@ def parse():
     ap.add_argument("--serve-requests", type=int, default=160,
                     help="requests of the serving run (Poisson arrivals); 0 skips it")
     ap.add_argument("--serve-rate", type=float, default=40.0, help="mean arrivals per second")
+    ap.add_argument("--lts-report", action="store_true",
+                    help="also time rate-2 LTS against GTS on a layered box (adds about a minute)")
     return ap.parse_args()
 
 
@@ -274,6 +276,55 @@ def run_serve(n_req, rate, device, seed=3343):
     return out
 
 
+def run_lts(device, n_cubes=48, order=5, runs=16, n_groups=3, cycles=2):
+    """Rate-2 LTS against GTS on a layered box (vp 1500 / 3000 / 6000 m/s from the top, free surface
+    on top): elements sorted into EDGE-V time groups; both advance the same simulated time (GTS at
+    the fundamental step). Reports the element updates each performs per second of wall time and
+    the wall-time ratio."""
+    import numpy as np
+    import torch
+    from edge_b200 import host
+    from edge_b200.solver import Solver
+    layers = [1500.0, 3000.0, 6000.0]
+    base = host.build_problem(n_cubes, order, runs, layers=layers, seed=3343, source="random", n_receivers=8,
+                              n_steps=64)
+    dt_el = host.dt_cfl_el(base.mesh, order, base.rho, base.lam, base.mu)
+    tg = host.time_groups(base.mesh, dt_el, n_groups)
+    mesh, perm, gf = host.sort_by_groups(base.mesh, tg)
+    prob = host.build_problem(n_cubes, order, runs, layers=layers, seed=3343, source="random", n_receivers=8,
+                              n_steps=64, mesh=mesh)
+    counts = np.diff(gf)
+    n_fun = cycles * (1 << (n_groups - 1))
+    st = torch.cuda.Stream(device=device)
+    out = {"tets": prob.n_el, "order": order, "runs": runs, "groups": counts.tolist(),
+           "fundamental_steps": n_fun}
+    for mode in ("gts", "lts"):
+        s = Solver(prob, precision=32, stream=st.cuda_stream, device=device)
+        s.upload_dofs(prob.zero_dofs(np.float32)[0])
+        if mode == "lts":
+            s.set_time_groups(gf)
+            s.step_lts(1)
+        else:
+            s.step(2)
+        s.sync()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(st)
+        if mode == "lts":
+            s.step_lts(cycles)
+        else:
+            s.step(n_fun)
+        e1.record(st)
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1)
+        s.close()
+        upd = (sum(int(c) * (n_fun >> g) for g, c in enumerate(counts)) if mode == "lts" else prob.n_el * n_fun)
+        out[mode] = {"ms": ms, "element_updates_per_s": upd * runs / (ms / 1e3),
+                     "gts_equivalent_element_updates_per_s": prob.n_el * n_fun * runs / (ms / 1e3)}
+    out["speedup_lts_over_gts"] = out["gts"]["ms"] / out["lts"]["ms"]
+    out["ideal_speedup"] = prob.n_el * n_fun / sum(int(c) * (n_fun >> g) for g, c in enumerate(counts))
+    return out
+
+
 def run_reference(a, ws, rank):
     if rank != 0:
         return
@@ -440,6 +491,7 @@ def main():
     serving = None
     if a.serve_requests > 0:
         serving = run_serve(a.serve_requests, a.serve_rate, local)
+    lts = run_lts(local) if a.lts_report else None
 
     if rank == 0:
         out = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": a.steps,
@@ -453,7 +505,7 @@ def main():
                "step_ms_p50": step_ms[len(step_ms) // 2], "step_ms_p99": step_ms[min(len(step_ms) - 1,
                                                                                       int(0.99 * len(step_ms)))],
                "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": int(launches),
-               "clocks": clk, "fp64_plain": fp64, "serving": serving, "roofline_neighbour": roofline_neighbour}
+               "clocks": clk, "fp64_plain": fp64, "serving": serving, "roofline_neighbour": roofline_neighbour, "lts": lts}
         print(json.dumps(out), flush=True)
     barrier(ws)
     if ws > 1:

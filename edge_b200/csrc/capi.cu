@@ -195,6 +195,7 @@ struct edge_b200_ctx {
   // clocks; compact face buffers of the elements at group interfaces
   int nTg = 0;
   std::vector<int64_t> tgFirst;
+  std::vector<int64_t> tgHalfEnd;  // group g: elements [tgFirst[g], tgHalfEnd[g]) hold every one with a smaller neighbour
   std::vector<double> tgRecvTime;
   std::vector<int32_t> tgRecvCount;
   DevBuf ltsFlags, ltsRel, sumIdx, halfIdx, faceSum, faceHalf1, faceHalf2;
@@ -819,6 +820,15 @@ int edge_b200_set_time_groups(edge_b200_ctx *ctx, int n_groups, const int64_t *g
   EDGE_CUDA(cudaStreamSynchronize(s), "time groups");
   ctx->nTg = n_groups;
   ctx->tgFirst.assign(group_first, group_first + n_groups + 1);
+  // the local step needs the half-step tile only up to the last element with a smaller neighbour
+  // of each group (a group sorted with those elements first keeps the rest on the faster kernel)
+  ctx->tgHalfEnd.assign(n_groups, 0);
+  for (int g = 0; g < n_groups; g++) {
+    int64_t end = group_first[g];
+    for (int64_t e = group_first[g]; e < group_first[g + 1]; e++)
+      if (flags[e] & LTS_HAS_SMALLER) end = e + 1;
+    ctx->tgHalfEnd[g] = end;
+  }
   ctx->tgRecvTime.assign(n_groups, ctx->recvTime);
   ctx->tgRecvCount.assign(n_groups, ctx->recvCount);
   return EDGE_B200_OK;
@@ -921,8 +931,18 @@ int edge_b200_step_lts(edge_b200_ctx *ctx, double t, double dt_fun, int n_cycles
         EDGE_CUDA(ctx->launch(3, [&] { return ctx->ks->recv(a, r, s); }), "receiver kernel");
         ctx->launches++;
       }
-      EDGE_CUDA(ctx->launch(0, [&] { return ctx->ks->localLts(a, s); }), "local kernel");
-      ctx->launches++;
+      StepArgsRaw aHalf = a, aSums = a;
+      aHalf.elCount = ctx->tgHalfEnd[w.g] - a.elFirst;
+      aSums.elFirst = ctx->tgHalfEnd[w.g];
+      aSums.elCount = a.elFirst + a.elCount - aSums.elFirst;
+      if (aHalf.elCount > 0) {
+        EDGE_CUDA(ctx->launch(0, [&] { return ctx->ks->localLts(aHalf, s); }), "local kernel");
+        ctx->launches++;
+      }
+      if (aSums.elCount > 0) {
+        EDGE_CUDA(ctx->launch(0, [&] { return ctx->ks->localLtsSums(aSums, s); }), "local kernel");
+        ctx->launches++;
+      }
       if (sE[w.g] > sB[w.g]) {
         SrcArgs sa = ctx->src;
         sa.grpOff += sB[w.g];

@@ -8,7 +8,7 @@ namespace edge_b200 {
 template <typename T, int O, int R, int RM>
 class KernelSetImpl final : public KernelSet {
   using G = Geo<T, O, R, RM>;
-  int numSms_ = 0, occLocal_ = 1, occNeigh_ = 1, occRecv_ = 1, occLocalLts_ = 1;
+  int numSms_ = 0, occLocal_ = 1, occNeigh_ = 1, occRecv_ = 1, occLocalLts_ = 1, occLocalSum_ = 1;
 
   static StepArgs<T> cast(const StepArgsRaw &a) {
     StepArgs<T> b;
@@ -48,24 +48,31 @@ class KernelSetImpl final : public KernelSet {
   cudaError_t init(int device) override {
     cudaError_t e;
     if ((e = cudaDeviceGetAttribute(&numSms_, cudaDevAttrMultiProcessorCount, device))) return e;
-    if ((e = cudaFuncSetAttribute(kLocal<T, O, R, RM, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smemLocal())))
+    if ((e = cudaFuncSetAttribute(kLocal<T, O, R, RM, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smemLocal())))
       return e;
     if ((e = cudaFuncSetAttribute(kNeigh<T, O, R, RM>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smemNeigh())))
       return e;
     if ((e = cudaFuncSetAttribute(kRecv<T, O, R, RM>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smemRecv())))
       return e;
-    if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occLocal_, kLocal<T, O, R, RM, false>, G::NT, smemLocal())))
+    if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occLocal_, kLocal<T, O, R, RM, 0>, G::NT, smemLocal())))
       return e;
     if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occNeigh_, kNeigh<T, O, R, RM>, G::NT, smemNeigh())))
       return e;
     if constexpr (G::ltsOk) {
-      if ((e = cudaFuncSetAttribute(kLocal<T, O, R, RM, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+      if ((e = cudaFuncSetAttribute(kLocal<T, O, R, RM, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                     (int)G::smemLocalLts)))
         return e;
-      if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occLocalLts_, kLocal<T, O, R, RM, true>, G::NT,
+      if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occLocalLts_, kLocal<T, O, R, RM, 2>, G::NT,
                                                              G::smemLocalLts)))
         return e;
       occLocalLts_ = occLocalLts_ < 1 ? 1 : occLocalLts_;
+      if ((e = cudaFuncSetAttribute(kLocal<T, O, R, RM, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    (int)smemLocal())))
+        return e;
+      if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occLocalSum_, kLocal<T, O, R, RM, 1>, G::NT,
+                                                             smemLocal())))
+        return e;
+      occLocalSum_ = occLocalSum_ < 1 ? 1 : occLocalSum_;
     }
     occLocal_ = occLocal_ < 1 ? 1 : occLocal_;
     occNeigh_ = occNeigh_ < 1 ? 1 : occNeigh_;
@@ -82,13 +89,22 @@ class KernelSetImpl final : public KernelSet {
 
   cudaError_t local(const StepArgsRaw &a, cudaStream_t s) override {
     if (a.elCount < 1) return cudaSuccess;
-    kLocal<T, O, R, RM, false><<<grid(a.elCount, ctasLocal()), G::NT, smemLocal(), s>>>(cast(a));
+    kLocal<T, O, R, RM, 0><<<grid(a.elCount, ctasLocal()), G::NT, smemLocal(), s>>>(cast(a));
     return cudaGetLastError();
   }
   cudaError_t localLts(const StepArgsRaw &a, cudaStream_t s) override {
     if constexpr (G::ltsOk) {
       if (a.elCount < 1) return cudaSuccess;
-      kLocal<T, O, R, RM, true><<<grid(a.elCount, numSms_ * occLocalLts_), G::NT, G::smemLocalLts, s>>>(cast(a));
+      kLocal<T, O, R, RM, 2><<<grid(a.elCount, numSms_ * occLocalLts_), G::NT, G::smemLocalLts, s>>>(cast(a));
+      return cudaGetLastError();
+    } else {
+      return cudaErrorNotSupported;
+    }
+  }
+  cudaError_t localLtsSums(const StepArgsRaw &a, cudaStream_t s) override {
+    if constexpr (G::ltsOk) {
+      if (a.elCount < 1) return cudaSuccess;
+      kLocal<T, O, R, RM, 1><<<grid(a.elCount, numSms_ * occLocalSum_), G::NT, smemLocal(), s>>>(cast(a));
       return cudaGetLastError();
     } else {
       return cudaErrorNotSupported;

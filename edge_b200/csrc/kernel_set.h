@@ -33,6 +33,8 @@ class KernelSet {
   virtual cudaError_t local(const StepArgsRaw &a, cudaStream_t s) = 0;
   // local step with the LTS face buffers (the half-step time integral needs one more tile)
   virtual cudaError_t localLts(const StepArgsRaw &a, cudaStream_t s) = 0;
+  // the same without half-step integrals, for elements without a smaller neighbour (no extra tile)
+  virtual cudaError_t localLtsSums(const StepArgsRaw &a, cudaStream_t s) = 0;
   virtual bool ltsSupported() const = 0;
   virtual cudaError_t neigh(const StepArgsRaw &a, cudaStream_t s) = 0;
   virtual cudaError_t recv(const StepArgsRaw &a, const RecvArgs &r, cudaStream_t s) = 0;

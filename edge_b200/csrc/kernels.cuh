@@ -557,7 +557,9 @@ __device__ __forceinline__ void faceMix(const T *S0, int l, const T (&fr)[9], T 
 // ------------------------------------------------------------------------------------------------
 // TAIL: a barrier after the quantity mix, before the face tile is written again (not needed when
 // consecutive faces alternate between two tiles)
-template <typename T, int O, int R, int RM, int FA, bool LTS = false, bool TAIL = true>
+// LTS: 0 none, 1 the two-step sums of elements with a larger neighbour, 2 also the half-step
+// projections of elements with a smaller neighbour (needs TIh)
+template <typename T, int O, int R, int RM, int FA, int LTS = 0, bool TAIL = true>
 __device__ __forceinline__ void localFace(const StepArgs<T> &a, const T *TI, T *S0, int q, int l, int64_t e,
                                           int r, bool valid, T *acc, T *upA, const T *TIh = nullptr) {
   using G = Geo<T, O, R, RM>;
@@ -590,7 +592,7 @@ __device__ __forceinline__ void localFace(const StepArgs<T> &a, const T *TI, T *
           for (int j = 0; j < F; j++) v[j] += s[j];
           stRowG<T, F>(p, v);
         }
-        if (fl & LTS_HAS_SMALLER) {
+        if (LTS == 2 && (fl & LTS_HAS_SMALLER)) {
           // face projections of the integrals over [0, dt/2] and [dt/2, dt]
           T h[F];
 #pragma unroll
@@ -625,8 +627,10 @@ __device__ __forceinline__ void localFace(const StepArgs<T> &a, const T *TI, T *
   if constexpr (TAIL) __syncthreads();
 }
 
-template <typename T, int O, int R, int RM, bool LTS>
-__global__ void __launch_bounds__(Geo<T, O, R, RM>::NT, LTS ? 1 : Geo<T, O, R, RM>::minCtasLocal)
+// LTS as in localFace; mode 2 keeps the half-step integral in one more tile (one CTA per SM), mode
+// 1 runs on the elements of a time group without a smaller neighbour
+template <typename T, int O, int R, int RM, int LTS>
+__global__ void __launch_bounds__(Geo<T, O, R, RM>::NT, LTS == 2 ? 1 : Geo<T, O, R, RM>::minCtasLocal)
     kLocal(StepArgs<T> a) {
   using G = Geo<T, O, R, RM>;
   constexpr int B = G::B, E = G::E, SB = G::SB;
@@ -644,7 +648,7 @@ __global__ void __launch_bounds__(Geo<T, O, R, RM>::NT, LTS ? 1 : Geo<T, O, R, R
   T *TI = G::tiSmem ? X + G::nX : X;
   T *TIA = G::tiSmem ? XA + G::nXA : XA;
   T *S0 = AS ? TIA + G::nTIA : (G::tiSmem ? X : X + G::nX);
-  T *TIh = LTS ? reinterpret_cast<T *>(smem + G::smemLocal) : nullptr;
+  T *TIh = LTS == 2 ? reinterpret_cast<T *>(smem + G::smemLocal) : nullptr;
   const int q = threadIdx.x >> 5, l = threadIdx.x & 31;
   const int eo = l / R, r = l % R;
   const int64_t nGroups = (a.elCount + E - 1) / E;
@@ -678,7 +682,7 @@ __global__ void __launch_bounds__(Geo<T, O, R, RM>::NT, LTS ? 1 : Geo<T, O, R, R
         ldRowG<T, B>(gRow<T, R, G::GB>(a.dofsE, ev, 9, q, r), v, valid);
         stRow<T, B>(rowPtr<T, SB>(X, q, l), v);
       }
-      if constexpr (LTS) {
+      if constexpr (LTS == 2) {
         T h[B];
 #pragma unroll
         for (int n = 0; n < B; n++) h[n] = (dt * T(0.5)) * v[n];
@@ -713,7 +717,7 @@ __global__ void __launch_bounds__(Geo<T, O, R, RM>::NT, LTS ? 1 : Geo<T, O, R, R
     c.load(a, ev, valid, q);
     __syncthreads();
     // Cauchy-Kowalevski (TimePredVanilla::ck, TimePredVanilla.hpp:200-306)
-    ckAll<T, O, R, RM, 1, LTS, G::ckPingPong>(X, TI, XA, TIA, q, l, c, a.omega, dt, dt, tIr, tIAr, TIh,
+    ckAll<T, O, R, RM, 1, LTS == 2, G::ckPingPong>(X, TI, XA, TIA, q, l, c, a.omega, dt, dt, tIr, tIAr, TIh,
                                               dt * T(0.5), S0);
     if constexpr (!G::tiSmem) {
       if (q < 9) {

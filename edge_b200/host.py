@@ -209,10 +209,12 @@ def lts_tables(mesh, el_tg):
 
 
 def sort_by_groups(mesh, el_tg):
-    """The mesh with its elements ordered by time group (stable), the input index of each new
+    """The mesh with its elements ordered by time group and, within a group, elements with a
+    smaller neighbour first (they need the half-step integrals), the input index of each new
     element, and group_first [G+1] (element ranges of the groups)."""
     el_tg = np.asarray(el_tg)
-    perm = np.argsort(el_tg, kind="stable")
+    flags, _ = lts_tables(mesh, el_tg)
+    perm = np.lexsort(((flags & 2) == 0, el_tg))
     bf_ve, tag = mesh.boundary_faces()
     m = Mesh.from_arrays(mesh.ve, mesh.el_ve[perm], bf_ve, tag, reorder=False)
     n_groups = int(el_tg.max()) + 1
