@@ -39,17 +39,23 @@ def test_headline_size_linearity_and_run_independence():
             s.sync()
             return rows.clone()
 
+        # (each array is 13.8 GB; in-place arithmetic keeps the peak near 125 GB with the solver)
         x, y = rand(), rand()
         fx, fy = step(x), step(y)
-        fxy = step(2.0 * x - 0.5 * y)
-        lin = fxy - (2.0 * fx - 0.5 * fy)
+        z = x.clone().mul_(2.0).add_(y, alpha=-0.5)
+        del y
+        fxy = step(z)
+        del z
         assert torch.isfinite(fxy).all()
-        rel = (lin.norm() / fxy.norm()).item()
+        norm = fxy.norm().item()
+        fxy.add_(fx, alpha=-2.0).add_(fy, alpha=0.5)
+        rel = fxy.norm().item() / norm
         assert rel < 1e-5, rel
+        del fxy, fy
         # permuting the fused runs permutes the results exactly
         perm = torch.randperm(runs, generator=torch.Generator().manual_seed(3)).to("cuda")
-        fp = step(x[:, :, perm])
+        fp = step(x[:, :, perm].contiguous())
         assert torch.equal(fp, fx[:, :, perm])
-        del x, y, fx, fy, fxy, lin, fp
+        del x, fx, fp
     finally:
         s.close()
