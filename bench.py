@@ -150,9 +150,12 @@ def host_n_modes(order):
     return order * (order + 1) * (order + 2) // 6
 
 
-def algorithmic(prob, prec):
+def algorithmic(prob, prec, premix=False, fs_pair=84):
     """Per-element algorithmic bytes and flops of one step (dense-in-modes counts as in the
-    roofline model of the path) for each kernel."""
+    roofline model of the path) for each kernel. premix: the local kernel mixes the face
+    projections with the reading element's flux solver and reads per face the padded pair
+    [2][fs_pair] of flux solvers in the compute precision instead of its own fsE[0] block; the
+    neighbour kernel then reads no flux solvers."""
     from edge_b200.host import n_face_modes, n_modes
     O, R, rm = prob.order, prob.runs, prob.rm
     B, F, p = n_modes(O), n_face_modes(O), (8 if prec == 64 else 4)
@@ -162,10 +165,12 @@ def algorithmic(prob, prec):
     surf = 4 * (2 * 9 * F * B + 2 * 81 * F + 2 * 9 * B * F)
     dofs = (9 + 6 * rm) * B * R * p
     face = 4 * 9 * F * R * p
-    local_bytes = 2 * dofs + face + 3 * 24 * 8 + 4 * 81 * 8 + (rm * 12 * 8 + 27 * 8 + 4 * 54 * 8 if rm else 0)
-    neigh_bytes = 2 * dofs + face + 4 * 81 * 8 + 4 * (4 + 1 + 1 + 1) + (4 * 54 * 8 if rm else 0)
+    fs_local = 4 * 2 * fs_pair * p if premix else 4 * 81 * 8
+    local_bytes = 2 * dofs + face + 3 * 24 * 8 + fs_local + (rm * 12 * 8 + 27 * 8 + 4 * 54 * 8 if rm else 0)
+    neigh_bytes = 2 * dofs + face + (0 if premix else 4 * 81 * 8) + 4 * (4 + 1 + 1 + 1) + (4 * 54 * 8 if rm else 0)
+    mix = 4 * 2 * 81 * F if premix else 0
     return dict(local_bytes=local_bytes, neigh_bytes=neigh_bytes,
-                local_flops=(ck + vol + surf) * R, neigh_flops=surf * R)
+                local_flops=(ck + vol + surf + mix) * R, neigh_flops=(surf - mix) * R)
 
 
 def measured_peaks():
@@ -403,7 +408,9 @@ def main():
     L.edge_b200_set_timing(sv._h, 0)
     names = ["local", "neighbour", "sources", "receivers"]
     shares = {names[i]: float(kms[i] / kms.sum()) for i in range(4) if kn[i]}
-    alg = algorithmic(prob, prec)
+    kc = np.zeros(5, np.int32)
+    L.edge_b200_kernel_config(sv._h, _lib.ptr(kc))
+    alg = algorithmic(prob, prec, premix=bool(kc[1]), fs_pair=int(kc[2]))
     top = int(np.argmax(kms[:2]))
     avg_ms = kms[top] / max(kn[top], 1)
     bytes_launch = (alg["local_bytes"] if top == 0 else alg["neigh_bytes"]) * prob.n_el

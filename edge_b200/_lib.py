@@ -37,6 +37,7 @@ _SIGS = {
     "edge_setup_trafo": (C.c_int, [vp] * 5),
     "edge_setup_fs_pair": (C.c_int, [dbl] * 6 + [vp, vp, vp, C.c_int, vp, vp, vp, vp]),
     "edge_b200_create": (C.c_int, [vp, i64, vp]),
+    "edge_b200_kernel_config": (C.c_int, [vp, vp]),
     "edge_b200_destroy": (C.c_int, [vp]),
     "edge_b200_upload_mesh": (C.c_int, [vp] * 5),
     "edge_b200_upload_element_data": (C.c_int, [vp] * 7),

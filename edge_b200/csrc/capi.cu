@@ -66,6 +66,35 @@ struct DevBuf {
   ~DevBuf() { dfree(p); }
 };
 
+// flux-solver pairs of the pre-mixed face projections: per element face fsE[0] of the element and
+// the fsE[1] block its face reader applies (the face neighbour's at its own face id for inner faces,
+// the element's own for a free surface, zeros for outflow), 81 values padded to P, in the
+// configuration's precision: out[nEl][4][2][P]
+template <typename T>
+__global__ void kBuildFsLR(const double *fsE, const int32_t *elFaEl, const uint8_t *fId, const uint8_t *faType,
+                           int64_t nEl, int P, T *out) {
+  const int64_t total = nEl * 4 * 2 * P;
+  for (int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < total; i += int64_t(gridDim.x) * blockDim.x) {
+    const int64_t ef = i / (2 * P);
+    const int w = int(i % (2 * P)) / P, j = int(i % P);
+    double v = 0;
+    if (j < 81) {
+      if (w == 0) {
+        v = fsE[ef * 81 + j];
+      } else {
+        const int ty = faType[ef];
+        const int64_t e = ef / 4;
+        const int fa = int(ef % 4);
+        if (ty == EDGE_FACE_INNER)
+          v = fsE[((nEl + elFaEl[ef]) * 4 + fId[ef]) * 81 + j];
+        else if (ty == EDGE_FACE_FREE_SURFACE)
+          v = fsE[((nEl + e) * 4 + fa) * 81 + j];
+      }
+    }
+    out[i] = T(v);
+  }
+}
+
 // halo exchange: blocks [9][R][GF] of face slots (element * 4 + face) to / from a packed buffer,
 // 16 bytes per thread; slots outside the face buffer are skipped
 __global__ void kFacePack(uint4 *face, uint4 *buf, const int32_t *slots, int n, int64_t blk16, int64_t nSlots,
@@ -175,6 +204,10 @@ struct edge_b200_ctx {
   uint8_t *fId = nullptr, *vId = nullptr, *faType = nullptr;
   double omega[3] = {0, 0, 0};
   bool meshSet = false, dataSet = false, keepTDofs = false;
+  // flux-solver pairs of the pre-mixed face projections (configurations with KernelSet::premix),
+  // rebuilt before the next GTS step after the mesh or the element data changed
+  DevBuf fsLR;
+  bool fsLRStale = true;
   // sources
   SrcArgs src{};
   DevBuf srcMem[10];
@@ -322,6 +355,22 @@ struct edge_b200_ctx {
     return cudaEventRecord(evD2H, d2h);
   }
 
+  cudaError_t ensureFsLR() {
+    if (!ks->premix() || !fsLRStale) return cudaSuccess;
+    const int P = ks->fsPairStride();
+    cudaError_t e = fsLR.fit(size_t(nEl) * 4 * 2 * P * realSize);
+    if (e) return e;
+    const int64_t total = nEl * 4 * 2 * P;
+    const int grid = (int)std::min<int64_t>((total + 255) / 256, 148 * 16);
+    if (cfg.precision == 64)
+      kBuildFsLR<double><<<grid, 256, 0, stream>>>(fsE, elFaEl, fId, faType, nEl, P, fsLR.as<double>());
+    else
+      kBuildFsLR<float><<<grid, 256, 0, stream>>>(fsE, elFaEl, fId, faType, nEl, P, fsLR.as<float>());
+    if ((e = cudaGetLastError())) return e;
+    fsLRStale = false;
+    return cudaSuccess;
+  }
+
   int fail(cudaError_t e, const char *what) {
     err = std::string(what) + ": " + cudaGetErrorString(e);
     return EDGE_B200_EDEVICE;
@@ -341,6 +390,7 @@ struct edge_b200_ctx {
     a.fId = fId;
     a.vId = vId;
     a.faType = faType;
+    a.fsLR = (ks->premix() && !fsLRStale) ? fsLR.p : nullptr;
     a.nEl = nEl;
     a.elFirst = 0;
     a.elCount = nOwned;
@@ -450,6 +500,7 @@ int edge_b200_upload_mesh(edge_b200_ctx *ctx, const int32_t *el_fa_el, const uin
   ctx->hFId.assign(fid_el_fa_el, fid_el_fa_el + n);
   ctx->hFaType.assign(el_fa_type, el_fa_type + n);
   ctx->meshSet = true;
+  ctx->fsLRStale = true;
   return EDGE_B200_OK;
 }
 
@@ -471,6 +522,7 @@ int edge_b200_upload_element_data(edge_b200_ctx *ctx, const double *star_e, cons
   }
   EDGE_CUDA(cudaStreamSynchronize(s), "upload element data");
   ctx->dataSet = true;
+  ctx->fsLRStale = true;
   return EDGE_B200_OK;
 }
 
@@ -663,6 +715,7 @@ static int runSteps(edge_b200_ctx *ctx, double t, double dt, int n_steps, int ph
   if (!ctx->meshSet || !ctx->dataSet) return EDGE_B200_EINVAL;
   ctx->lastLts = false;
   cudaStream_t s = ctx->stream;
+  EDGE_CUDA(ctx->ensureFsLR(), "flux-solver pairs");
   // receiver samples of every step (Receivers::getRecvTimeRel, io/Receivers.cpp:235-248)
   std::vector<int> stepFirst(n_steps + 1, 0);
   std::vector<double> tau;
@@ -953,7 +1006,7 @@ int edge_b200_step_lts(edge_b200_ctx *ctx, double t, double dt_fun, int n_cycles
         ctx->launches++;
       }
     } else {
-      EDGE_CUDA(ctx->launch(1, [&] { return ctx->ks->neigh(a, s); }), "neighbour kernel");
+      EDGE_CUDA(ctx->launch(1, [&] { return ctx->ks->neighLts(a, s); }), "neighbour kernel");
       ctx->launches++;
     }
   }
@@ -1082,6 +1135,16 @@ int edge_b200_device_dofs(edge_b200_ctx *ctx, void **dofs_e, void **dofs_a, void
 }
 
 int64_t edge_b200_last_launches(const edge_b200_ctx *ctx) { return ctx ? ctx->launches : -1; }
+
+int edge_b200_kernel_config(const edge_b200_ctx *ctx, int32_t info[5]) {
+  if (!ctx || !info) return EDGE_B200_EINVAL;
+  info[0] = ctx->ks->elementsPerCta();
+  info[1] = ctx->ks->premix() ? 1 : 0;
+  info[2] = ctx->ks->fsPairStride();
+  info[3] = ctx->ks->ctasLocal();
+  info[4] = ctx->ks->ctasNeigh();
+  return EDGE_B200_OK;
+}
 
 int edge_b200_set_timing(edge_b200_ctx *ctx, int enable) {
   if (!ctx) return EDGE_B200_EINVAL;

@@ -8,7 +8,8 @@ namespace edge_b200 {
 template <typename T, int O, int R, int RM>
 class KernelSetImpl final : public KernelSet {
   using G = Geo<T, O, R, RM>;
-  int numSms_ = 0, occLocal_ = 1, occNeigh_ = 1, occRecv_ = 1, occLocalLts_ = 1, occLocalSum_ = 1;
+  int numSms_ = 0, occLocal_ = 1, occNeigh_ = 1, occRecv_ = 1, occLocalLts_ = 1, occLocalSum_ = 1,
+      occNeighLts_ = 1;
 
   static StepArgs<T> cast(const StepArgsRaw &a) {
     StepArgs<T> b;
@@ -38,9 +39,10 @@ class KernelSetImpl final : public KernelSet {
     b.sumIdx = a.sumIdx;
     b.halfIdx = a.halfIdx;
     b.firstTs = a.firstTs;
+    b.fsLR = static_cast<const T *>(a.fsLR);
     return b;
   }
-  static constexpr size_t smemLocal() { return G::smemLocal; }
+  static constexpr size_t smemLocal() { return G::smemLocalGts; }
   static constexpr size_t smemNeigh() { return G::smemNeigh; }
   static constexpr size_t smemRecv() { return G::smemLocal; }
 
@@ -50,14 +52,25 @@ class KernelSetImpl final : public KernelSet {
     if ((e = cudaDeviceGetAttribute(&numSms_, cudaDevAttrMultiProcessorCount, device))) return e;
     if ((e = cudaFuncSetAttribute(kLocal<T, O, R, RM, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smemLocal())))
       return e;
-    if ((e = cudaFuncSetAttribute(kNeigh<T, O, R, RM>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smemNeigh())))
+    if ((e = cudaFuncSetAttribute(kNeigh<T, O, R, RM, G::premix>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smemNeigh())))
       return e;
     if ((e = cudaFuncSetAttribute(kRecv<T, O, R, RM>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smemRecv())))
       return e;
     if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occLocal_, kLocal<T, O, R, RM, 0>, G::NT, smemLocal())))
       return e;
-    if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occNeigh_, kNeigh<T, O, R, RM>, G::NT, smemNeigh())))
+    if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occNeigh_, kNeigh<T, O, R, RM, G::premix>, G::NT, smemNeigh())))
       return e;
+    if constexpr (G::premix) {
+      if ((e = cudaFuncSetAttribute(kNeigh<T, O, R, RM, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    (int)smemNeigh())))
+        return e;
+      if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occNeighLts_, kNeigh<T, O, R, RM, false>, G::NT,
+                                                             smemNeigh())))
+        return e;
+    } else {
+      occNeighLts_ = occNeigh_;
+    }
+    occNeighLts_ = occNeighLts_ < 1 ? 1 : occNeighLts_;
     if constexpr (G::ltsOk) {
       if ((e = cudaFuncSetAttribute(kLocal<T, O, R, RM, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                     (int)G::smemLocalLts)))
@@ -67,10 +80,10 @@ class KernelSetImpl final : public KernelSet {
         return e;
       occLocalLts_ = occLocalLts_ < 1 ? 1 : occLocalLts_;
       if ((e = cudaFuncSetAttribute(kLocal<T, O, R, RM, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                    (int)smemLocal())))
+                                    (int)G::smemLocal)))
         return e;
       if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occLocalSum_, kLocal<T, O, R, RM, 1>, G::NT,
-                                                             smemLocal())))
+                                                             G::smemLocal)))
         return e;
       occLocalSum_ = occLocalSum_ < 1 ? 1 : occLocalSum_;
     }
@@ -104,16 +117,23 @@ class KernelSetImpl final : public KernelSet {
   cudaError_t localLtsSums(const StepArgsRaw &a, cudaStream_t s) override {
     if constexpr (G::ltsOk) {
       if (a.elCount < 1) return cudaSuccess;
-      kLocal<T, O, R, RM, 1><<<grid(a.elCount, numSms_ * occLocalSum_), G::NT, smemLocal(), s>>>(cast(a));
+      kLocal<T, O, R, RM, 1><<<grid(a.elCount, numSms_ * occLocalSum_), G::NT, G::smemLocal, s>>>(cast(a));
       return cudaGetLastError();
     } else {
       return cudaErrorNotSupported;
     }
   }
   bool ltsSupported() const override { return G::ltsOk; }
+  bool premix() const override { return G::premix; }
+  int fsPairStride() const override { return G::FSP; }
   cudaError_t neigh(const StepArgsRaw &a, cudaStream_t s) override {
     if (a.elCount < 1) return cudaSuccess;
-    kNeigh<T, O, R, RM><<<grid(a.elCount, ctasNeigh()), G::NT, smemNeigh(), s>>>(cast(a));
+    kNeigh<T, O, R, RM, G::premix><<<grid(a.elCount, ctasNeigh()), G::NT, smemNeigh(), s>>>(cast(a));
+    return cudaGetLastError();
+  }
+  cudaError_t neighLts(const StepArgsRaw &a, cudaStream_t s) override {
+    if (a.elCount < 1) return cudaSuccess;
+    kNeigh<T, O, R, RM, false><<<grid(a.elCount, occNeighLts_ * numSms_), G::NT, smemNeigh(), s>>>(cast(a));
     return cudaGetLastError();
   }
   cudaError_t recv(const StepArgsRaw &a, const RecvArgs &r, cudaStream_t s) override {

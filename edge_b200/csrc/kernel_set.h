@@ -24,6 +24,9 @@ struct StepArgsRaw {
   const uint8_t *ltsFlags = nullptr, *ltsRel = nullptr;
   const int32_t *sumIdx = nullptr, *halfIdx = nullptr;
   int firstTs = 0;
+  // per element face fsE[0] and the face reader's fsE[1] in the configuration's precision, each
+  // padded to 16 bytes: [nEl][4][2][fsPairStride()] (premix)
+  const void *fsLR = nullptr;
 };
 
 class KernelSet {
@@ -36,7 +39,12 @@ class KernelSet {
   // the same without half-step integrals, for elements without a smaller neighbour (no extra tile)
   virtual cudaError_t localLtsSums(const StepArgsRaw &a, cudaStream_t s) = 0;
   virtual bool ltsSupported() const = 0;
+  // GTS face projections leave the local kernel mixed with the reader's flux solver (fsLR)
+  virtual bool premix() const = 0;
+  virtual int fsPairStride() const = 0;
   virtual cudaError_t neigh(const StepArgsRaw &a, cudaStream_t s) = 0;
+  // the neighbour step over face buffers the LTS local kernels wrote (not pre-mixed)
+  virtual cudaError_t neighLts(const StepArgsRaw &a, cudaStream_t s) = 0;
   virtual cudaError_t recv(const StepArgsRaw &a, const RecvArgs &r, cudaStream_t s) = 0;
   virtual cudaError_t sources(void *dofsE, const SrcArgs &sa, cudaStream_t s) = 0;
   virtual int elementsPerCta() const = 0;

@@ -51,6 +51,11 @@ struct StepArgs {
   const uint8_t *ltsRel;    // [nEl][4] 0 equal, 1 this element larger, 2 this element smaller
   const int32_t *sumIdx, *halfIdx;
   int firstTs;              // first step of a rate-2 pair of this group
+  // elastic GTS (Geo::premix): per element face the element's own flux solver fsE[0] and the one
+  // its face reader applies (fsE[1] of the face neighbour at its face, or the element's own for a
+  // free surface; zeros for outflow) in T, each padded to 16 bytes (Geo::FSP): [nEl][4][2][FSP];
+  // null: gathered through the connectivity
+  const T *fsLR;
 };
 enum { LTS_HAS_LARGER = 1, LTS_HAS_SMALLER = 2 };
 enum { LTS_EQ = 0, LTS_GT = 1, LTS_LT = 2 };
@@ -284,6 +289,16 @@ struct Geo {
       (sizeof(T) == 4 && RM == 0 && baseLocal <= 110 * 1024) ? 110 * 1024 : 227 * 1024;
   static constexpr bool asyncLocal = tiSmem && baseLocal + nS0 * sizeof(T) <= localBudget;
   static constexpr size_t smemLocal = baseLocal + (asyncLocal ? nS0 * sizeof(T) : 0);
+  // elastic GTS: the local kernel stores each face projection already mixed with the reading
+  // element's flux solver (fsE[1] of the face neighbour, or its own for a free surface), so the
+  // neighbour kernel only rotates its own quantity row and applies fluxT (no shared mix, no
+  // barrier). The two flux-solver blocks of every face arrive one face ahead by cp.async into two
+  // buffers [E][2][FSP] behind the face tile; configurations without room for them keep the mix in
+  // the neighbour kernel.
+  static constexpr int FSP = padGlobal<T>(81);  // a 9x9 block padded to 16 bytes
+  static constexpr size_t premixBytes = size_t(2) * E * 2 * FSP * sizeof(T);
+  static constexpr bool premix = RM == 0 && asyncLocal && smemLocal + premixBytes <= localBudget;
+  static constexpr size_t smemLocalGts = smemLocal + (premix ? premixBytes : 0);
   // elastic CK with ping-pong derivatives between X and the separate face tile
   static constexpr bool ckPingPong = asyncLocal && RM == 0 && nModes(O - 1) <= SF;
   // LTS local step: one more [9][32][SB] tile for the half-step time integral (behind the rest);
@@ -552,6 +567,84 @@ __device__ __forceinline__ void faceMix(const T *S0, int l, const T (&fr)[9], T 
   }
 }
 
+// two mixes of the same rows: s[j] = sum_i fr[i] S0[i][l][j] into registers, t[j] = sum_i fr1[i]
+// S0[i][l][j] written to tRow[0, G) chunk by chunk (skipped when tRow is null); S0's rows are zero
+// in [F, G), so is t there
+template <typename T, int F, int SF, int G>
+__device__ __forceinline__ void faceMix2(const T *S0, int l, const T (&fr)[9], const T (&fr1)[9], T *s,
+                                         T *tRow) {
+#pragma unroll
+  for (int j0 = 0; j0 < F; j0 += 4) {
+    T v[4];
+    ld4<T>(rowPtr<T, SF>(S0, 0, l) + j0, v);
+    T o[4], p[4];
+#pragma unroll
+    for (int u = 0; u < 4; u++) {
+      o[u] = fr[0] * v[u];
+      p[u] = fr1[0] * v[u];
+    }
+#pragma unroll
+    for (int i = 1; i < 9; i++) {
+      ld4<T>(rowPtr<T, SF>(S0, i, l) + j0, v);
+#pragma unroll
+      for (int u = 0; u < 4; u++) {
+        o[u] = fmaT(fr[i], v[u], o[u]);
+        p[u] = fmaT(fr1[i], v[u], p[u]);
+      }
+    }
+#pragma unroll
+    for (int u = 0; u < 4; u++)
+      if (j0 + u < F) s[j0 + u] = o[u];
+    if (tRow) {
+      if (j0 + 4 <= G) {
+        st4<T>(tRow + j0, p);
+      } else {
+#pragma unroll
+        for (int u = 0; u < 4; u++)
+          if (j0 + u < G) tRow[j0 + u] = p[u];
+      }
+    }
+  }
+}
+
+// the flux-solver blocks of face FA of group g's elements (pre-mixed projections) into buf
+// [E][2][FSP]: 16-byte copies from fsLR, or (without it) loads gathered through the connectivity
+// and stored in T, visible after the next barrier like the copies
+template <typename T>
+struct MixFs {
+  T *buf;  // two buffers [2][E][2][FSP]
+  int64_t g, nGroups;
+};
+template <typename T, int O, int R, int RM, int FA>
+__device__ __forceinline__ void issueMixFs(const StepArgs<T> &a, T *buf, int64_t g, int64_t nGroups) {
+  using G = Geo<T, O, R, RM>;
+  constexpr int E = G::E, FSP = G::FSP, W = 16 / int(sizeof(T)), NC = FSP / W;
+  if (g >= nGroups) return;
+  if (a.fsLR) {
+    for (int i = threadIdx.x; i < E * 2 * NC; i += G::NT) {
+      const int eo = i / (2 * NC), k = i % (2 * NC);
+      if (g * E + eo >= a.elCount) continue;
+      const int64_t e = a.elFirst + g * E + eo;
+      cpAsync16(buf + eo * 2 * FSP + k * W, a.fsLR + (e * 4 + FA) * (2 * FSP) + k * W);
+    }
+  } else {
+    for (int i = threadIdx.x; i < E * 2 * 81; i += G::NT) {
+      const int eo = i / 162, k = i % 162, w = k / 81, j = k % 81;
+      if (g * E + eo >= a.elCount) continue;
+      const int64_t e = a.elFirst + g * E + eo;
+      int64_t src = (e * 4 + FA) * 81 + j;
+      if (w == 1) {
+        const int ty = a.faType[e * 4 + FA];
+        if (ty == FT_OUTFLOW) continue;
+        const int64_t rd = ty == FT_INNER ? int64_t(a.elFaEl[e * 4 + FA]) : e;
+        const int rf = ty == FT_INNER ? int(a.fId[e * 4 + FA]) : FA;
+        src = ((a.nEl + rd) * 4 + rf) * 81 + j;
+      }
+      buf[eo * 2 * FSP + w * FSP + j] = T(__ldg(a.fsE + src));
+    }
+  }
+}
+
 // ------------------------------------------------------------------------------------------------
 // local step: CK, volume, local surface, face projections (AderDg::local, AderDg.hpp:338-534)
 // ------------------------------------------------------------------------------------------------
@@ -559,27 +652,33 @@ __device__ __forceinline__ void faceMix(const T *S0, int l, const T (&fr)[9], T 
 // consecutive faces alternate between two tiles)
 // LTS: 0 none, 1 the two-step sums of elements with a larger neighbour, 2 also the half-step
 // projections of elements with a smaller neighbour (needs TIh)
+// pre-mixed projections (LTS 0, Geo::premix): S0alt is a tile free for this warp's own rows,
+// through which the mixed projection leaves as coalesced stores; mf the flux-solver buffers
 template <typename T, int O, int R, int RM, int FA, int LTS = 0, bool TAIL = true>
 __device__ __forceinline__ void localFace(const StepArgs<T> &a, const T *TI, T *S0, int q, int l, int64_t e,
-                                          int r, bool valid, T *acc, T *upA, const T *TIh = nullptr) {
+                                          int r, bool valid, T *acc, T *upA, const T *TIh = nullptr,
+                                          T *S0alt = nullptr, const MixFs<T> &mf = MixFs<T>{nullptr, 0, 0}) {
   using G = Geo<T, O, R, RM>;
   constexpr int F = G::F, SF = G::SF, SB = G::SB;
+  constexpr bool PM = LTS == 0 && G::premix;
   T s[F];
   if (q < 9) {
 #pragma unroll
     for (int j = 0; j < F; j++) s[j] = T(0);
     FluxLMul<O, FA>::template run<T>(OwnRow<T>{rowPtr<T, SB>(TI, q, l)}, s);
     {
-      // the row padded to GF with zeros, then the warp's rows of each element as coalesced stores
+      // the row padded to GF with zeros (for the coalesced stores of the warp's rows)
       T *p = rowPtr<T, SF>(S0, q, l);
       stRow<T, F>(p, s);
 #pragma unroll
       for (int j = F; j < G::GF; j++) p[j] = T(0);
     }
-    __syncwarp();
-    if (valid)
-      storeRowsCoalesced<T, R, G::GF, SF>(S0, a.face + ((e * 4 + FA) * 9 + q) * int64_t(R * G::GF), q, l / R,
-                                          l % R);
+    if constexpr (!PM) {
+      __syncwarp();
+      if (valid)
+        storeRowsCoalesced<T, R, G::GF, SF>(S0, a.face + ((e * 4 + FA) * 9 + q) * int64_t(R * G::GF), q, l / R,
+                                            l % R);
+    }
     if constexpr (LTS) {
       if (valid) {
         const int fl = a.ltsFlags[e];
@@ -606,6 +705,39 @@ __device__ __forceinline__ void localFace(const StepArgs<T> &a, const T *TI, T *
         }
       }
     }
+  }
+  if constexpr (PM) {
+    constexpr int E = G::E, FSP = G::FSP;
+    // this face's flux-solver blocks (issued one face ahead) for every thread after the barrier
+    cpAsyncWait<0>();
+    const int ty = valid ? a.faType[e * 4 + FA] : FT_OUTFLOW;
+    __syncthreads();
+    // the next face's blocks into the other buffer, whose readers (two faces back) all passed the
+    // barrier; after the last face the next group's first
+    if constexpr (FA < 3)
+      issueMixFs<T, O, R, RM, FA + 1>(a, mf.buf + ((FA + 1) % 2) * (E * 2 * FSP), mf.g, mf.nGroups);
+    else
+      issueMixFs<T, O, R, RM, 0>(a, mf.buf, mf.g + gridDim.x, mf.nGroups);
+    cpAsyncCommit();
+    T fr[9], fr1[9];
+    {
+      const T *fb = mf.buf + (FA % 2) * (E * 2 * FSP) + (l / R) * (2 * FSP) + q * 9;
+#pragma unroll
+      for (int i = 0; i < 9; i++) {
+        fr[i] = fb[i];
+        fr1[i] = fb[FSP + i];
+      }
+    }
+    faceMix2<T, F, SF, G::GF>(S0, l, fr, fr1, s, rowPtr<T, SF>(S0alt, q, l));
+    __syncwarp();
+    if (ty != FT_OUTFLOW)
+      storeRowsCoalesced<T, R, G::GF, SF>(S0alt, a.face + ((e * 4 + FA) * 9 + q) * int64_t(R * G::GF), q, l / R,
+                                          l % R);
+    // the next face writes this warp's rows of the tile again
+    __syncwarp();
+    FluxTMul<O, FA>::template run<T>(s, acc);
+    if constexpr (TAIL) __syncthreads();
+    return;
   }
   // flux-solver row of this thread (elastic 9x9 or anelastic 6x9), loaded before the barrier
   T fr[9];
@@ -649,15 +781,19 @@ __global__ void __launch_bounds__(Geo<T, O, R, RM>::NT, LTS == 2 ? 1 : Geo<T, O,
   T *TIA = G::tiSmem ? XA + G::nXA : XA;
   T *S0 = AS ? TIA + G::nTIA : (G::tiSmem ? X : X + G::nX);
   T *TIh = LTS == 2 ? reinterpret_cast<T *>(smem + G::smemLocal) : nullptr;
+  // pre-mixed face projections: flux-solver buffers behind the face tile
+  constexpr bool PM = LTS == 0 && G::premix;
+  T *fsb = PM ? reinterpret_cast<T *>(smem + G::smemLocal) : nullptr;
   const int q = threadIdx.x >> 5, l = threadIdx.x & 31;
   const int eo = l / R, r = l % R;
   const int64_t nGroups = (a.elCount + E - 1) / E;
   const T dt = T(a.dt);
   if constexpr (AS) {
-    // the first group's DOF rows
+    // the first group's DOF rows (and flux-solver blocks of its first face)
     const int64_t g0 = blockIdx.x;
     if (q < 9 && g0 < nGroups && g0 * E + eo < a.elCount)
       copyDofRows<T, R, G::GB, SB>(TI, a.dofsE, a.elFirst + g0 * E + eo, q, eo, r);
+    if constexpr (PM) issueMixFs<T, O, R, RM, 0>(a, fsb, g0, nGroups);
     cpAsyncCommit();
   }
   for (int64_t g = blockIdx.x; g < nGroups; g += gridDim.x) {
@@ -768,11 +904,12 @@ __global__ void __launch_bounds__(Geo<T, O, R, RM>::NT, LTS == 2 ? 1 : Geo<T, O,
     }
     // local surface integral (SurfIntVanilla::local, SurfIntVanilla.hpp:212-262) + face projections
     if constexpr (AS) {
-      localFace<T, O, R, RM, 0, LTS, false>(a, TI, S0, q, l, ev, r, valid, acc, upA, TIh);
-      localFace<T, O, R, RM, 1, LTS, false>(a, TI, X, q, l, ev, r, valid, acc, upA, TIh);
-      localFace<T, O, R, RM, 2, LTS, false>(a, TI, S0, q, l, ev, r, valid, acc, upA, TIh);
+      const MixFs<T> mf{fsb, g, nGroups};
+      localFace<T, O, R, RM, 0, LTS, false>(a, TI, S0, q, l, ev, r, valid, acc, upA, TIh, X, mf);
+      localFace<T, O, R, RM, 1, LTS, false>(a, TI, X, q, l, ev, r, valid, acc, upA, TIh, S0, mf);
+      localFace<T, O, R, RM, 2, LTS, false>(a, TI, S0, q, l, ev, r, valid, acc, upA, TIh, X, mf);
       // the barrier after the last face orders its readers of X before the next group writes X
-      localFace<T, O, R, RM, 3, LTS, true>(a, TI, X, q, l, ev, r, valid, acc, upA, TIh);
+      localFace<T, O, R, RM, 3, LTS, true>(a, TI, X, q, l, ev, r, valid, acc, upA, TIh, S0, mf);
     } else {
       localFace<T, O, R, RM, 0, LTS>(a, TI, S0, q, l, ev, r, valid, acc, upA, TIh);
       localFace<T, O, R, RM, 1, LTS>(a, TI, S0, q, l, ev, r, valid, acc, upA, TIh);
@@ -908,8 +1045,9 @@ struct NeighSlots {
     }
   }
 
-  // copies of item (group g, face FA) into `slot`; m = connectivity of this lane's element
-  template <int FA>
+  // copies of item (group g, face FA) into `slot`; m = connectivity of this lane's element; PM: the
+  // rows are pre-mixed (no flux-solver blocks)
+  template <int FA, bool PM>
   __device__ __forceinline__ static void issue(const StepArgs<T> &a, unsigned char *base, int slot, int q, int l,
                                                int64_t g, bool groupValid, const FaceMeta &m) {
     if (groupValid) {
@@ -934,7 +1072,7 @@ struct NeighSlots {
           cpAsync16(dst + row * SF + col * W, blk + row * GF + col * W);
         }
       }
-      if constexpr (G::fsSmem) {
+      if constexpr (G::fsSmem && !PM) {
         // flux-solver blocks fsE[1][e][FA] (and fsA[1][e][FA]) of the group's elements
         double *fsDst = fs(base, slot);
         for (int i = threadIdx.x; i < E * NFS; i += NT) {
@@ -999,14 +1137,58 @@ __device__ __forceinline__ void neighApply(const StepArgs<T> &a, const T *S, con
     FluxTMul<O, FA>::template run<T>(s, upA);
 }
 
-// item (local group k, face FA): item index i = 4k + FA lives in slot i % NSN; after the barrier the
-// item i + NSN - 1 is issued into slot (i - 1) % NSN, which the barrier has released
+// pre-mixed rows: this warp's own quantity row of the neighbour's projection, rotated into this
+// element's face orientation (inner faces), then fluxT
 template <typename T, int O, int R, int RM, int FA>
+__device__ __forceinline__ void neighApplyMixed(const T *S, int q, int l, bool valid, const FaceMeta &m, T *acc) {
+  using G = Geo<T, O, R, RM>;
+  constexpr int F = G::F, SF = G::SF;
+  const int ty = m.type(FA);
+  if (!valid || ty == FT_OUTFLOW || q >= 9) return;
+  T x[F];
+  ldRow<T, F>(rowPtr<T, SF>(S, q, l), x);
+  if (ty == FT_INNER) {
+    T o[F];
+#pragma unroll
+    for (int j = 0; j < F; j++) o[j] = T(0);
+    const int v = m.vert(FA);
+    if (v == 0)
+      OriMul<O, 0>::template run<T>(x, o);
+    else if (v == 1)
+      OriMul<O, 1>::template run<T>(x, o);
+    else
+      OriMul<O, 2>::template run<T>(x, o);
+    FluxTMul<O, FA>::template run<T>(o, acc);
+  } else {
+    FluxTMul<O, FA>::template run<T>(x, acc);
+  }
+}
+
+// item (local group k, face FA): item index i = 4k + FA lives in slot i % NSN; after the barrier the
+// item i + NSN - 1 is issued into slot (i - 1) % NSN, which the barrier has released. PM: every warp
+// touches only its own quantity rows, so a warp-level order replaces the barrier.
+template <typename T, int O, int R, int RM, int FA, bool PM>
 __device__ __forceinline__ void neighItem(const StepArgs<T> &a, unsigned char *base, int q, int l, int64_t e,
                                           bool valid, const FaceMeta &cur, const FaceMeta &nxt, int64_t g,
                                           bool nextValid, int64_t k, T *acc, T *upA) {
   using NS = NeighSlots<T, O, R, RM>;
   constexpr int NSN = Geo<T, O, R, RM>::NSN;
+  if constexpr (PM) {
+    cpAsyncWait<NSN - 2>();
+    __syncwarp();
+    const int64_t item = k * 4 + FA;
+    const int slot = int(item % NSN);
+    T *S = NS::rows(base, slot);
+    neighApplyMixed<T, O, R, RM, FA>(S, q, l, valid, cur, acc);
+    __syncwarp();
+    constexpr int AHEAD = FA + NSN - 1;
+    const int slotNext = int((item + NSN - 1) % NSN);
+    if constexpr (AHEAD < 4)
+      NS::template issue<AHEAD, true>(a, base, slotNext, q, l, g, true, cur);
+    else
+      NS::template issue<AHEAD - 4, true>(a, base, slotNext, q, l, g + gridDim.x, nextValid, nxt);
+    return;
+  }
   cpAsyncWait<NSN - 2>();
   __syncwarp();
   const int64_t item = k * 4 + FA;
@@ -1019,13 +1201,15 @@ __device__ __forceinline__ void neighItem(const StepArgs<T> &a, unsigned char *b
   // the next group's DOF rows join the copies committed now (the barrier ordered this group's
   // reads of the tile before them)
   if constexpr (AHEAD < 4)
-    NS::template issue<AHEAD>(a, base, slotNext, q, l, g, true, cur);
+    NS::template issue<AHEAD, false>(a, base, slotNext, q, l, g, true, cur);
   else
-    NS::template issue<AHEAD - 4>(a, base, slotNext, q, l, g + gridDim.x, nextValid, nxt);
+    NS::template issue<AHEAD - 4, false>(a, base, slotNext, q, l, g + gridDim.x, nextValid, nxt);
   neighApply<T, O, R, RM, FA>(a, S, NS::fs(base, slot), q, l, e, valid, cur, acc, upA);
 }
 
-template <typename T, int O, int R, int RM>
+// PM: the face buffers hold projections pre-mixed with this element's flux solvers (the GTS local
+// kernel writes them so); otherwise the mix happens here (LTS, attenuation)
+template <typename T, int O, int R, int RM, bool PM>
 __global__ void __launch_bounds__(Geo<T, O, R, RM>::NT, Geo<T, O, R, RM>::minCtasNeigh) kNeigh(StepArgs<T> a) {
   using G = Geo<T, O, R, RM>;
   using NS = NeighSlots<T, O, R, RM>;
@@ -1039,9 +1223,9 @@ __global__ void __launch_bounds__(Geo<T, O, R, RM>::NT, Geo<T, O, R, RM>::minCta
   cur.load(a, a.elFirst + g * E + eo, g * E + eo < a.elCount);
   // prologue: the first group's DOF rows and items 0 .. NSN-2 (its first faces)
   NS::issueDofs(a, smem, q, l, g, g < nGroups);
-  NS::template issue<0>(a, smem, 0, q, l, g, g < nGroups, cur);
-  if constexpr (NSN > 2) NS::template issue<1>(a, smem, 1, q, l, g, g < nGroups, cur);
-  if constexpr (NSN > 3) NS::template issue<2>(a, smem, 2, q, l, g, g < nGroups, cur);
+  NS::template issue<0, PM>(a, smem, 0, q, l, g, g < nGroups, cur);
+  if constexpr (NSN > 2) NS::template issue<1, PM>(a, smem, 1, q, l, g, g < nGroups, cur);
+  if constexpr (NSN > 3) NS::template issue<2, PM>(a, smem, 2, q, l, g, g < nGroups, cur);
   for (int64_t k = 0; g < nGroups; g += gridDim.x, k++) {
     const int64_t e = a.elFirst + g * E + eo;
     const bool valid = g * E + eo < a.elCount;
@@ -1067,10 +1251,10 @@ __global__ void __launch_bounds__(Geo<T, O, R, RM>::NT, Geo<T, O, R, RM>::minCta
 #pragma unroll
       for (int n = 0; n < B; n++) upA[n] = T(0);
     }
-    neighItem<T, O, R, RM, 0>(a, smem, q, l, e, valid, cur, nxt, g, nextValid, k, acc, upA);
-    neighItem<T, O, R, RM, 1>(a, smem, q, l, e, valid, cur, nxt, g, nextValid, k, acc, upA);
-    neighItem<T, O, R, RM, 2>(a, smem, q, l, e, valid, cur, nxt, g, nextValid, k, acc, upA);
-    neighItem<T, O, R, RM, 3>(a, smem, q, l, e, valid, cur, nxt, g, nextValid, k, acc, upA);
+    neighItem<T, O, R, RM, 0, PM>(a, smem, q, l, e, valid, cur, nxt, g, nextValid, k, acc, upA);
+    neighItem<T, O, R, RM, 1, PM>(a, smem, q, l, e, valid, cur, nxt, g, nextValid, k, acc, upA);
+    neighItem<T, O, R, RM, 2, PM>(a, smem, q, l, e, valid, cur, nxt, g, nextValid, k, acc, upA);
+    neighItem<T, O, R, RM, 3, PM>(a, smem, q, l, e, valid, cur, nxt, g, nextValid, k, acc, upA);
     if constexpr (G::dofTile) {
       // the updated rows through the DOF tile (this warp's rows only), stored coalesced; then the
       // next group's DOF rows into the tile

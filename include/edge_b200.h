@@ -272,6 +272,13 @@ int64_t edge_b200_last_launches(const edge_b200_ctx *ctx);
  * (synchronises the stream). */
 int edge_b200_set_timing(edge_b200_ctx *ctx, int enable);
 int edge_b200_kernel_times(edge_b200_ctx *ctx, double *ms, int64_t *launches);
+/* Launch shape of the context's compiled configuration (no counterpart in the reference, whose
+ * kernels run one element per thread team): info[0] elements per CTA, info[1] 1 when GTS face
+ * projections leave the local kernel pre-mixed with the reading element's flux solver (the local
+ * kernel then reads per element face the padded pair [2][info[2]] of flux solvers in the
+ * configuration's precision, the neighbour kernel none), info[3] / info[4] persistent CTAs of the
+ * local / neighbour kernel. */
+int edge_b200_kernel_config(const edge_b200_ctx *ctx, int32_t info[5]);
 
 /* No counterpart in the reference. n_steps GTS steps (local kernel, then neighbour kernel; no
  * sources, no receivers) over caller-owned DEVICE arrays, without allocating anything: no

@@ -110,3 +110,29 @@ def test_runs_are_independent():
         s1.step(2, t=0.0)
         e1, _ = s1.download_dofs()
         assert rel_l2(e16[..., r:r + 1], e1) < 1e-6
+
+
+@pytest.mark.parametrize("order,runs", [(4, 16), (5, 16)])
+def test_fp32_heterogeneous_premixed_faces(order, runs):
+    """Layered, log-normally perturbed materials: the face projections the local kernel pre-mixes
+    with the reading element's flux solver differ from ones mixed with the element's own."""
+    prob = small_problem(n=3, order=order, runs=runs, jitter=0.15, n_steps=3, source="random",
+                         layers=[3000.0, 6000.0], lognormal_sigma=0.2)
+    s, orc, e, a, t, (rb, rt, rc) = _run_both(prob, 32, 3)
+    assert rel_l2(e, orc.state["dofsE"]) < TOL32
+    k = int(rc[0])
+    assert rel_l2(rb[:, :k], orc.recv["buf"][:, :k]) < TOL32
+
+
+def test_kernel_config_reports_premix():
+    from edge_b200._lib import lib, ptr
+    cases = [((32, 5, 16, 0), (2, 1, 84)), ((32, 4, 16, 0), (2, 1, 84)), ((32, 5, 8, 0), (4, 1, 84)), ((32, 5, 4, 0), (8, 0, 84)),
+             ((64, 5, 1, 0), (32, 0, 82)), ((32, 4, 8, 3), (4, 0, 84))]
+    for (prec, order, runs, rm), want in cases:
+        prob = small_problem(n=2, order=order, runs=runs, rm=rm, n_steps=1, source=None, n_receivers=0)
+        s = Solver(prob, precision=prec)
+        info = np.zeros(5, np.int32)
+        assert lib().edge_b200_kernel_config(s._h, ptr(info)) == 0
+        assert tuple(int(x) for x in info[:3]) == want, (prec, order, runs, rm, info)
+        assert info[3] >= 148 and info[4] >= 148
+        s.close()
