@@ -183,6 +183,14 @@ def measured_peaks():
         return 6650.0, "of fallback"
 
 
+def peak_clock_mhz():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            return float(json.load(f)["sm_max_mhz"])
+    except (OSError, KeyError, ValueError):
+        return 1965.0
+
+
 def traffic_from_profiles(workload):
     """Per-launch DRAM bytes of the dominant kernel from the committed ncu summary, if present."""
     path = os.path.join(ROOT, "profiles", f"kLocal_{workload}.txt")
@@ -424,6 +432,15 @@ def main():
                 "achieved_tflops": flops_launch / (avg_ms / 1e3) / 1e12,
                 "kernel_avg_ms": {names[i]: float(kms[i] / kn[i]) for i in range(4) if kn[i]},
                 "kernel_share": shares}
+    # the local kernel is bound by the FP32 pipe, not HBM: its dense-equivalent flops (the DG
+    # products counted dense; the kernel executes FMAs for the non-zeros only) against the nominal
+    # FP32 CUDA-core peak (SMs x 128 FMA lanes x 2 flops x max SM clock)
+    if prec == 32:
+        sms = torch.cuda.get_device_properties(torch.cuda.current_device()).multi_processor_count
+        fp32_peak = sms * 128 * 2 * peak_clock_mhz() * 1e6 / 1e12
+        roofline["fp32_pipe"] = {"dense_equivalent_tflops": roofline["achieved_tflops"],
+                                 "nominal_peak_tflops": fp32_peak,
+                                 "frac": roofline["achieved_tflops"] / fp32_peak}
     # the neighbour-flux kernel (the HBM-bound one) on its own: bytes this design moves (face
     # projections read, DOFs read + written, flux solvers, connectivity) and the reference algorithm's
     # count (neighbours' time-integrated DOFs instead of face projections)
