@@ -1008,6 +1008,13 @@ struct FaceMeta {
   __device__ __forceinline__ int vert(int f) const { return (vi >> (8 * f)) & 0xff; }
 };
 
+// the reflection (OriMul index) taking the neighbour's projection at its face fo (in that face's
+// basis) to this element's face FA basis, for the neighbour's vertex id at FA (kFacePerm)
+template <int O, int FA>
+__device__ __forceinline__ int neighOri(const FaceMeta &m) {
+  return kFacePerm[O - 2][m.src[FA] & 3][FA][m.vert(FA)];
+}
+
 template <typename T, int O, int R, int RM>
 struct NeighSlots {
   using G = Geo<T, O, R, RM>;
@@ -1099,7 +1106,7 @@ __device__ __forceinline__ void neighOrient(T *S, int q, int l, bool valid, cons
     ldRow<T, F>(rowPtr<T, SF>(S, q, l), x);
 #pragma unroll
     for (int j = 0; j < F; j++) s[j] = T(0);
-    const int v = m.vert(FA);
+    const int v = neighOri<O, FA>(m);
     if (v == 0)
       OriMul<O, 0>::template run<T>(x, s);
     else if (v == 1)
@@ -1151,7 +1158,7 @@ __device__ __forceinline__ void neighApplyMixed(const T *S, int q, int l, bool v
     T o[F];
 #pragma unroll
     for (int j = 0; j < F; j++) o[j] = T(0);
-    const int v = m.vert(FA);
+    const int v = neighOri<O, FA>(m);
     if (v == 0)
       OriMul<O, 0>::template run<T>(x, o);
     else if (v == 1)

@@ -9,15 +9,26 @@ matrix entries as literals. Per thread the operand and accumulator rows live in 
                       (derivative D of the Cauchy-Kowalevski recursion; D=1 also serves the
                       viscoelastic case, which never truncates: k < B, n < B(O-1))
 * ``VolMul<O>``       acc[n] += sum_dim sum_k z_dim(k) * K_dim M^-1 [k][n], k < B(O-1)
-* ``FluxLMul<O,FA>``  s[j]   += sum_k z(k) * fluxL_FA[k][j]          (projection to face FA)
+* ``FluxLMul<O,FA>``  s[j]   += sum_k z(k) * fluxL'_FA[k][j]         (projection to face FA)
 
 The first three take the operand as a callable that fills four rows at a time
 (``z.template load<k0>(zz)``, zz[dim][i] = operand of row k0+i in direction dim); the caller forms
 it from shared memory with 128-bit loads (e.g. a star-matrix mix whose loads serve all three
 directions), and groups of rows without non-zeros are skipped entirely. The other two take
 register arrays:
-* ``FluxTMul<O,FA>``  acc[n] += sum_j s[j] * fluxT_FA[j][n]          (lift from face FA)
-* ``OriMul<O,V>``     s[j]   += sum_k x[k] * (Mface^-1 Ori_V)[k][j]  (neighbour face orientation)
+* ``FluxTMul<O,FA>``  acc[n] += sum_j s[j] * fluxT'_FA[j][n]         (lift from face FA)
+* ``OriMul<O,V>``     s[j]   += sum_k x[k] * (Mface^-1 Ori_V)[k][j]  (V: reflection of the face)
+
+Face bases. Each local face FA of every element keeps its projections in the hierarchical triangle
+basis composed with a fixed rotation sigma_FA of the reference triangle's vertices (psi_m o
+sigma_FA, orthogonal with the same masses), chosen per order and face to make fluxL'_FA / fluxT'_FA
+as sparse as possible: at order 5 the face matrices hold 748 instead of 880 non-zeros (face 0 35
+instead of 103, faces 2 and 3 304 instead of 363 / 309). A neighbour's projections at its face fo
+reach this element's face FA through sigma_fo o sigma_v o sigma_FA^-1, sigma_v being the
+reference's vertex-id map (a reflection, tools/edge_pre/types/Tet.py faToFa); with rotations for
+the sigma_FA that is again one of the three reflections, V = ``kFacePerm[O-2][fo][FA][v]``. The
+flux operators are the reference's up to this change of face basis, which the lifted flux does
+not see.
 
 Every accumulator receives its terms in ascending k, as the reference's vanilla kernels sum.
 
@@ -122,6 +133,7 @@ def main(out=None):
          "template <int O, int FA> struct FluxTMul;",
          "template <int O, int V> struct OriMul;", ""]
     nm = dgmat.n_modes_tet
+    tables = []
     for o in ORDERS:
         ex = dgmat.exact_matrices(o)
         B, F = nm(o), dgmat.n_modes_tri(o)
@@ -131,29 +143,123 @@ def main(out=None):
             s += struct_fused("CkMul", f"{o}, {d}", body, "acc")
         body = block_rows4(ex["stiffV"], nm(o - 1), B, "acc")
         s += struct_fused("VolMul", f"{o}", body, "acc")
+        fb = face_bases(o)
+        sig = [b[0] for b in fb]
         for f in range(4):
-            s += struct_fused("FluxLMul", f"{o}, {f}", block_rows4([ex["fluxL"][f]], B, F, "s"), "s")
-            s += struct("FluxTMul", f"{o}, {f}", block("", None, None, ex["fluxT"][f], F, B, "s", "acc"), "s", "acc")
-        # face orientation: Mface^-1 Ori_v from fluxN = P_f Mface^-1 Ori_v
+            s += struct_fused("FluxLMul", f"{o}, {f}", block_rows4([fb[f][1]], B, F, "s"), "s")
+            s += struct("FluxTMul", f"{o}, {f}", block("", None, None, fb[f][2], F, B, "s", "acc"), "s", "acc")
+        # face orientation: Mface^-1 Ori_v of the three reflections
         ori = exact_orientations(o)
         for v in range(3):
-            s += struct("OriMul", f"{o}, {v}", block("", None, None, ori[v], F, F, "x", "s"), "x", "s")
+            s += struct("OriMul", f"{o}, {v}", block("", None, None, ori[3 + v], F, F, "x", "s"), "x", "s")
+        tables.append((o, sig, face_perm_table(sig)))
+    s.append("// orientation (OriMul index) from a neighbour's face fo to this element's face FA with vertex")
+    s.append("// id v: kFacePerm[O - 2][fo][FA][v]; face bases sigma_FA per order: " +
+             ", ".join(f"O{o} {sig}" for o, sig, _ in tables))
+    rows = []
+    for o, _, tab in tables:
+        rows.append("{" + ", ".join("{" + ", ".join("{" + ", ".join(str(x) for x in tab[fo][fa]) + "}"
+                                                   for fa in range(4)) + "}" for fo in range(4)) + "}")
+    s.append("__constant__ int8_t kFacePerm[5][4][4][3] = {" + ",\n    ".join(rows) + "};")
     os.makedirs(os.path.dirname(out), exist_ok=True)
     with open(out, "w") as fh:
         fh.write("\n".join(s) + "\n")
     return out
 
 
+# the six vertex permutations of the reference triangle (0,0), (1,0), (0,1) as affine maps
+# chi -> A chi + b, given by the images of chi1 and chi2 (dgmat's FA_TO_FA form); index 0 is the
+# identity, 3..5 are the reference's vertex-id maps FA_TO_FA[0..2]
+PERMS = [
+    [([1, 0], 0), ([0, 1], 0)],
+    [([0, 1], 0), ([-1, -1], 1)],
+    [([-1, -1], 1), ([1, 0], 0)],
+] + [list(m) for m in dgmat.FA_TO_FA]
+
+
+def _perm_of(maps):
+    """Vertex permutation (image index of each reference vertex) of an affine map."""
+    verts = [(0, 0), (1, 0), (0, 1)]
+    out = []
+    for x, y in verts:
+        img = tuple(c[0] * x + c[1] * y + k for c, k in maps)
+        out.append(verts.index(img))
+    return tuple(out)
+
+
+PERM_VERTS = [_perm_of(m) for m in PERMS]
+
+
+def compose(*idx):
+    """Index of the map idx[0] o idx[1] o ... (the last applied first)."""
+    p = (0, 1, 2)
+    for i in reversed(idx):
+        q = PERM_VERTS[i]
+        p = tuple(q[a] for a in p)
+    return PERM_VERTS.index(p)
+
+
+def inverse(i):
+    q = PERM_VERTS[i]
+    inv = [0, 0, 0]
+    for a, b in enumerate(q):
+        inv[b] = a
+    return PERM_VERTS.index(tuple(inv))
+
+
+def perm_matrix(order, i):
+    """Q[m][j] = int psi_m(sigma_i(chi)) psi_j(chi) / int psi_j^2 (psi_m o sigma_i in the basis)."""
+    bfa = dgmat.basis_tri(order - 1)
+    nf = len(bfa)
+    mfa = [dgmat._int_tri(dgmat._pmul(bfa[j], bfa[j])) for j in range(nf)]
+    maps = [dgmat._lin(c, k, 2) for c, k in PERMS[i]]
+    tr = [dgmat._subs_affine(p, maps, 2) for p in bfa]
+    return [[dgmat._int_tri(dgmat._pmul(tr[m], bfa[j])) / mfa[j] for j in range(nf)] for m in range(nf)]
+
+
+def face_bases(order):
+    """Per face FA: (sigma_FA, fluxL'_FA [B][F], fluxT'_FA [F][B]) with the sparsest face matrices
+    (ties: the lowest permutation index)."""
+    ex = dgmat.exact_matrices(order)
+    nb, nf = dgmat.n_modes_tet(order), dgmat.n_modes_tri(order)
+    out = []
+    for f in range(4):
+        proj = ex["fluxL"][f]
+        best = None
+        for i in range(3):  # rotations: the neighbour's map stays a reflection
+            q = perm_matrix(order, i)
+            pp = [[sum(q[m][j] * proj[k][j] for j in range(nf) if q[m][j]) for m in range(nf)] for k in range(nb)]
+            nnz = sum(1 for k in range(nb) for m in range(nf) if pp[k][m] != 0)
+            if best is None or nnz < best[0]:
+                best = (nnz, i, pp)
+        _, i, pp = best
+        # fluxT'[m][n] = fluxL'[n][m] / |psi_m|^2 / |phi_n|^2 (same masses: sigma preserves area)
+        minv = ex["massInv"]
+        bfa = dgmat.basis_tri(order - 1)
+        mfa_inv = [Fraction(1) / dgmat._int_tri(dgmat._pmul(bfa[m], bfa[m])) for m in range(nf)]
+        ft = [[pp[n][m] * mfa_inv[m] * minv[n] for n in range(nb)] for m in range(nf)]
+        out.append((i, pp, ft))
+    return out
+
+
+def face_perm_table(sig):
+    """V[fo][FA][v]: sigma_fo o sigma_v o sigma_FA^-1 = sigma_V (sigma_v = PERMS[3 + v], a reflection)."""
+    out = [[[compose(sig[fo], 3 + v, inverse(sig[fa])) for v in range(3)] for fa in range(4)] for fo in range(4)]
+    assert all(x >= 3 for a in out for b in a for x in b), "face permutations must stay reflections"
+    return [[[x - 3 for x in b] for b in a] for a in out]
+
+
 def exact_orientations(order):
-    """(Mface^-1 Ori_v)[k][j] for v = 0..2, exact (same construction as dgmat.exact_matrices)."""
+    """(Mface^-1 Ori_P)[k][j] for the permutations P of PERMS, exact (same construction as
+    dgmat.exact_matrices)."""
     deg = order - 1
     bfa = dgmat.basis_tri(deg)
     nf = len(bfa)
     mass_fa = [[dgmat._int_tri(dgmat._pmul(bfa[i], bfa[j])) for j in range(nf)] for i in range(nf)]
     minv = [Fraction(1) / mass_fa[i][i] for i in range(nf)]
     out = []
-    for v in range(3):
-        maps = [dgmat._lin(c, k, 2) for c, k in dgmat.FA_TO_FA[v]]
+    for mp in PERMS:
+        maps = [dgmat._lin(c, k, 2) for c, k in mp]
         tr = [dgmat._subs_affine(p, maps, 2) for p in bfa]
         ori = [[dgmat._int_tri(dgmat._pmul(tr[i], bfa[j])) for j in range(nf)] for i in range(nf)]
         out.append([[minv[k] * ori[k][j] for j in range(nf)] for k in range(nf)])
