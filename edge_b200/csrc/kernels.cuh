@@ -400,6 +400,34 @@ struct Mix3 {
       for (int i = 0; i < 4; i++) zz[d][i] = fmaT(c[d][2], v2[i], fmaT(c[d][1], v1[i], c[d][0] * v0[i]));
   }
 };
+// FP32: the same products on packed pairs of modes (sm_100 FFMA2: half the issue slots; each lane
+// of a pair rounds as the scalar chain does, so the results are bit-identical)
+template <int S>
+struct Mix3<float, S> {
+  const float *r0, *r1, *r2;
+  const float (*c)[3];
+  template <int K0>
+  __device__ __forceinline__ void load(float (&zz)[3][4]) const {
+    const float4 a = *reinterpret_cast<const float4 *>(r0 + K0);
+    const float4 b = *reinterpret_cast<const float4 *>(r1 + K0);
+    const float4 e = *reinterpret_cast<const float4 *>(r2 + K0);
+#pragma unroll
+    for (int d = 0; d < 3; d++) {
+      const float2 k0 = make_float2(c[d][0], c[d][0]), k1 = make_float2(c[d][1], c[d][1]),
+                   k2 = make_float2(c[d][2], c[d][2]);
+      float2 lo = __fmul2_rn(k0, make_float2(a.x, a.y));
+      float2 hi = __fmul2_rn(k0, make_float2(a.z, a.w));
+      lo = __ffma2_rn(k1, make_float2(b.x, b.y), lo);
+      hi = __ffma2_rn(k1, make_float2(b.z, b.w), hi);
+      lo = __ffma2_rn(k2, make_float2(e.x, e.y), lo);
+      hi = __ffma2_rn(k2, make_float2(e.z, e.w), hi);
+      zz[d][0] = lo.x;
+      zz[d][1] = lo.y;
+      zz[d][2] = hi.x;
+      zz[d][3] = hi.y;
+    }
+  }
+};
 // anelastic star: two velocity rows
 template <typename T, int S>
 struct Mix2 {
@@ -414,6 +442,28 @@ struct Mix2 {
     for (int d = 0; d < 3; d++)
 #pragma unroll
       for (int i = 0; i < 4; i++) zz[d][i] = fmaT(c[d][1], v1[i], c[d][0] * v0[i]);
+  }
+};
+template <int S>
+struct Mix2<float, S> {
+  const float *r0, *r1;
+  const float (*c)[2];
+  template <int K0>
+  __device__ __forceinline__ void load(float (&zz)[3][4]) const {
+    const float4 a = *reinterpret_cast<const float4 *>(r0 + K0);
+    const float4 b = *reinterpret_cast<const float4 *>(r1 + K0);
+#pragma unroll
+    for (int d = 0; d < 3; d++) {
+      const float2 k0 = make_float2(c[d][0], c[d][0]), k1 = make_float2(c[d][1], c[d][1]);
+      float2 lo = __fmul2_rn(k0, make_float2(a.x, a.y));
+      float2 hi = __fmul2_rn(k0, make_float2(a.z, a.w));
+      lo = __ffma2_rn(k1, make_float2(b.x, b.y), lo);
+      hi = __ffma2_rn(k1, make_float2(b.z, b.w), hi);
+      zz[d][0] = lo.x;
+      zz[d][1] = lo.y;
+      zz[d][2] = hi.x;
+      zz[d][3] = hi.y;
+    }
   }
 };
 // the thread's own row
