@@ -314,45 +314,79 @@ struct edge_b200_ctx {
     return cudaStreamSynchronize(stream);
   }
 
-  // asynchronous transfers: their own copy streams and staging buffers; events order them with
-  // the context stream (H2D -> layout kernel -> step kernels -> layout kernel -> D2H) on the device
+  // asynchronous transfers on their own copy streams. Uploads move element chunks of about
+  // kChunkBytes through a ring of kSlots staging slots: per chunk the copy and its layout kernel (on
+  // the context stream) are ordered by events, and a slot is reused once the kernel of its previous
+  // chunk read it, so the copies run back to back while the layout kernels trail them. Downloads
+  // convert all rows at once (the next step rewrites them) into one of two full-size buffers and
+  // copy that out; a buffer is reused once its copy from two downloads back finished, so the context
+  // stream never waits for the copy of the step just before.
+  static constexpr int kSlots = 3;
+  static constexpr size_t kChunkBytes = size_t(1) << 30;
   cudaStream_t h2d = nullptr, d2h = nullptr;
-  cudaEvent_t evH2D = nullptr, evToRows = nullptr, evFromRows = nullptr, evD2H = nullptr;
-  void *stageOut = nullptr;
-  bool d2hPending = false, toRowsPending = false;
+  cudaEvent_t evH2D[kSlots] = {}, evToRows[kSlots] = {}, evFromRows[2] = {}, evD2H[2] = {};
+  cudaEvent_t evMark = nullptr;
+  void *slotIn[kSlots] = {}, *bufOut[2] = {};
+  bool toRowsPending[kSlots] = {}, d2hPending[2] = {};
+  int inNext = 0, outNext = 0, outLast = -1;
+  int64_t chunkEls = 1;
   cudaError_t ensureAsync() {
     cudaError_t e;
     if (h2d) return cudaSuccess;
-    if ((e = ensureStage())) return e;
-    const size_t n = std::max(refCount(9), refCount(6 * cfg.n_rms));
-    if ((e = cudaMalloc(&stageOut, n * realSize))) return e;
+    const size_t perEl = size_t(std::max(9, 6 * cfg.n_rms)) * B * cfg.n_runs * realSize;
+    chunkEls = std::max<int64_t>(1, std::min<int64_t>(nEl, int64_t(kChunkBytes / perEl)));
+    for (int i = 0; i < kSlots; i++) {
+      if ((e = cudaMalloc(&slotIn[i], chunkEls * perEl))) return e;
+      for (cudaEvent_t *ev : {&evH2D[i], &evToRows[i]})
+        if ((e = cudaEventCreateWithFlags(ev, cudaEventDisableTiming))) return e;
+    }
+    for (int i = 0; i < 2; i++) {
+      if ((e = cudaMalloc(&bufOut[i], nEl * perEl))) return e;
+      for (cudaEvent_t *ev : {&evFromRows[i], &evD2H[i]})
+        if ((e = cudaEventCreateWithFlags(ev, cudaEventDisableTiming))) return e;
+    }
+    if ((e = cudaEventCreateWithFlags(&evMark, cudaEventDisableTiming))) return e;
     if ((e = cudaStreamCreateWithFlags(&h2d, cudaStreamNonBlocking))) return e;
-    if ((e = cudaStreamCreateWithFlags(&d2h, cudaStreamNonBlocking))) return e;
-    for (cudaEvent_t *ev : {&evH2D, &evToRows, &evFromRows, &evD2H})
-      if ((e = cudaEventCreateWithFlags(ev, cudaEventDisableTiming))) return e;
-    return cudaSuccess;
+    return cudaStreamCreateWithFlags(&d2h, cudaStreamNonBlocking);
   }
   cudaError_t uploadRowsAsync(void *rows, const void *host, int rowsPerEl) {
     cudaError_t e;
-    // the staging buffer is free once the previous layout kernel read it
-    if (toRowsPending && (e = cudaStreamWaitEvent(h2d, evToRows, 0))) return e;
-    if ((e = cudaMemcpyAsync(stage, host, refCount(rowsPerEl) * realSize, cudaMemcpyHostToDevice, h2d))) return e;
-    if ((e = cudaEventRecord(evH2D, h2d))) return e;
-    if ((e = cudaStreamWaitEvent(stream, evH2D, 0))) return e;
-    if ((e = convertLayout(true, cfg.precision, stage, rows, nEl * rowsPerEl, B, cfg.n_runs, GB, stream))) return e;
-    toRowsPending = true;
-    return cudaEventRecord(evToRows, stream);
+    const size_t refEl = size_t(rowsPerEl) * B * cfg.n_runs * realSize;
+    const size_t rowEl = size_t(rowsPerEl) * cfg.n_runs * GB * realSize;
+    for (int64_t e0 = 0; e0 < nEl; e0 += chunkEls) {
+      const int64_t n = std::min(chunkEls, nEl - e0);
+      const int k = inNext;
+      inNext = (inNext + 1) % kSlots;
+      // the slot is free once the layout kernel of its previous chunk read it
+      if (toRowsPending[k] && (e = cudaStreamWaitEvent(h2d, evToRows[k], 0))) return e;
+      if ((e = cudaMemcpyAsync(slotIn[k], static_cast<const char *>(host) + e0 * refEl, n * refEl,
+                               cudaMemcpyHostToDevice, h2d)))
+        return e;
+      if ((e = cudaEventRecord(evH2D[k], h2d))) return e;
+      if ((e = cudaStreamWaitEvent(stream, evH2D[k], 0))) return e;
+      if ((e = convertLayout(true, cfg.precision, slotIn[k], static_cast<char *>(rows) + e0 * rowEl,
+                             n * rowsPerEl, B, cfg.n_runs, GB, stream)))
+        return e;
+      toRowsPending[k] = true;
+      if ((e = cudaEventRecord(evToRows[k], stream))) return e;
+    }
+    return cudaSuccess;
   }
   cudaError_t downloadRowsAsync(void *host, const void *rows, int rowsPerEl) {
     cudaError_t e;
-    // the output staging buffer is free once the previous copy to the host finished
-    if (d2hPending && (e = cudaStreamWaitEvent(stream, evD2H, 0))) return e;
-    if ((e = convertLayout(false, cfg.precision, rows, stageOut, nEl * rowsPerEl, B, cfg.n_runs, GB, stream))) return e;
-    if ((e = cudaEventRecord(evFromRows, stream))) return e;
-    if ((e = cudaStreamWaitEvent(d2h, evFromRows, 0))) return e;
-    if ((e = cudaMemcpyAsync(host, stageOut, refCount(rowsPerEl) * realSize, cudaMemcpyDeviceToHost, d2h))) return e;
-    d2hPending = true;
-    return cudaEventRecord(evD2H, d2h);
+    const int k = outNext;
+    outNext ^= 1;
+    // the buffer is free once its copy to the host from two downloads back finished
+    if (d2hPending[k] && (e = cudaStreamWaitEvent(stream, evD2H[k], 0))) return e;
+    if ((e = convertLayout(false, cfg.precision, rows, bufOut[k], nEl * rowsPerEl, B, cfg.n_runs, GB, stream)))
+      return e;
+    if ((e = cudaEventRecord(evFromRows[k], stream))) return e;
+    if ((e = cudaStreamWaitEvent(d2h, evFromRows[k], 0))) return e;
+    if ((e = cudaMemcpyAsync(host, bufOut[k], refCount(rowsPerEl) * realSize, cudaMemcpyDeviceToHost, d2h)))
+      return e;
+    d2hPending[k] = true;
+    outLast = k;
+    return cudaEventRecord(evD2H[k], d2h);
   }
 
   cudaError_t ensureFsLR() {
@@ -402,11 +436,18 @@ struct edge_b200_ctx {
     dfree(dofsE); dfree(dofsA); dfree(tDofs); dfree(face);
     dfree(starE); dfree(starA); dfree(srcA); dfree(fsE); dfree(fsA);
     dfree(elFaEl); dfree(fId); dfree(vId); dfree(faType);
-    dfree(dTau); dfree(dSlot); dfree(stage); dfree(stageOut);
+    dfree(dTau); dfree(dSlot); dfree(stage);
+    for (int i = 0; i < kSlots; i++) dfree(slotIn[i]);
+    for (int i = 0; i < 2; i++) dfree(bufOut[i]);
     if (h2d) cudaStreamSynchronize(h2d), cudaStreamDestroy(h2d);
     if (d2h) cudaStreamSynchronize(d2h), cudaStreamDestroy(d2h);
-    for (cudaEvent_t ev : {evH2D, evToRows, evFromRows, evD2H})
-      if (ev) cudaEventDestroy(ev);
+    for (int i = 0; i < kSlots; i++)
+      for (cudaEvent_t ev : {evH2D[i], evToRows[i]})
+        if (ev) cudaEventDestroy(ev);
+    for (int i = 0; i < 2; i++)
+      for (cudaEvent_t ev : {evFromRows[i], evD2H[i]})
+        if (ev) cudaEventDestroy(ev);
+    if (evMark) cudaEventDestroy(evMark);
     for (auto &t : timed) {
       cudaEventDestroy(t.a);
       cudaEventDestroy(t.b);
@@ -562,11 +603,12 @@ int edge_b200_join_transfers(edge_b200_ctx *ctx, int after_stream) {
   if (after_stream) {
     // the copy streams start after what the context stream holds now
     EDGE_CUDA(ctx->ensureAsync(), "join transfers");
-    EDGE_CUDA(cudaEventRecord(ctx->evFromRows, ctx->stream), "join transfers");
-    EDGE_CUDA(cudaStreamWaitEvent(ctx->h2d, ctx->evFromRows, 0), "join transfers");
-    EDGE_CUDA(cudaStreamWaitEvent(ctx->d2h, ctx->evFromRows, 0), "join transfers");
-  } else if (ctx->d2hPending) {
-    EDGE_CUDA(cudaStreamWaitEvent(ctx->stream, ctx->evD2H, 0), "join transfers");
+    EDGE_CUDA(cudaEventRecord(ctx->evMark, ctx->stream), "join transfers");
+    EDGE_CUDA(cudaStreamWaitEvent(ctx->h2d, ctx->evMark, 0), "join transfers");
+    EDGE_CUDA(cudaStreamWaitEvent(ctx->d2h, ctx->evMark, 0), "join transfers");
+  } else if (ctx->outLast >= 0) {
+    // the copies to the host run in order on one stream: the last one covers the others
+    EDGE_CUDA(cudaStreamWaitEvent(ctx->stream, ctx->evD2H[ctx->outLast], 0), "join transfers");
   }
   return EDGE_B200_OK;
 }

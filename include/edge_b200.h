@@ -169,13 +169,15 @@ int edge_b200_upload_dofs(edge_b200_ctx *ctx, const void *dofs_e, const void *do
 int edge_b200_download_dofs(edge_b200_ctx *ctx, void *dofs_e, void *dofs_a);
 /* Asynchronous forms for host-resident DOFs that change every step: the copies run on two copy
  * streams of the context (one per direction) and overlap each other and the kernels, ordered with
- * the step kernels on the device by events; they use their own staging buffers. Host buffers must
- * be pinned (cudaHostAlloc / cudaHostRegister) and left alone until edge_b200_sync returns.
- * edge_b200_join_transfers(ctx, 0) makes the context stream wait (on the device) for the last
- * download, e.g. before an event that should cover it; (ctx, 1) makes the copy streams start after
- * the work the context stream holds now. Do not mix with the synchronous forms while transfers are
- * in flight (they share the input staging buffer). No counterpart in the reference (its DOFs are
- * host arrays). */
+ * the step kernels on the device by events. Uploads move chunks of about 1 GB through a ring of
+ * three staging slots, so each chunk's layout kernel overlaps the next chunk's copy; downloads
+ * convert the rows at once into one of two full-size buffers (allocated on first use), so the next
+ * step need not wait for the previous download's copy. Host buffers must be pinned (cudaHostAlloc / cudaHostRegister)
+ * and left alone until edge_b200_sync returns. edge_b200_join_transfers(ctx, 0) makes the context
+ * stream wait (on the device) for the last download, e.g. before an event that should cover it;
+ * (ctx, 1) makes the copy streams start after the work the context stream holds now. The
+ * synchronous forms do not wait for the copy streams: join (or sync) before mixing them. No
+ * counterpart in the reference (its DOFs are host arrays). */
 int edge_b200_upload_dofs_async(edge_b200_ctx *ctx, const void *dofs_e, const void *dofs_a);
 int edge_b200_download_dofs_async(edge_b200_ctx *ctx, void *dofs_e, void *dofs_a);
 int edge_b200_join_transfers(edge_b200_ctx *ctx, int after_stream);
