@@ -627,20 +627,22 @@ __device__ __forceinline__ void faceMix2(const T *S0, int l, const T (&fr)[9], c
   for (int j0 = 0; j0 < F; j0 += 4) {
     T v[4];
     ld4<T>(rowPtr<T, SF>(S0, 0, l) + j0, v);
+    // modes past F (the zero padding of the last chunk) are not mixed: t is zero there
     T o[4], p[4];
 #pragma unroll
     for (int u = 0; u < 4; u++) {
-      o[u] = fr[0] * v[u];
-      p[u] = fr1[0] * v[u];
+      o[u] = j0 + u < F ? fr[0] * v[u] : T(0);
+      p[u] = j0 + u < F ? fr1[0] * v[u] : T(0);
     }
 #pragma unroll
     for (int i = 1; i < 9; i++) {
       ld4<T>(rowPtr<T, SF>(S0, i, l) + j0, v);
 #pragma unroll
-      for (int u = 0; u < 4; u++) {
-        o[u] = fmaT(fr[i], v[u], o[u]);
-        p[u] = fmaT(fr1[i], v[u], p[u]);
-      }
+      for (int u = 0; u < 4; u++)
+        if (j0 + u < F) {
+          o[u] = fmaT(fr[i], v[u], o[u]);
+          p[u] = fmaT(fr1[i], v[u], p[u]);
+        }
     }
 #pragma unroll
     for (int u = 0; u < 4; u++)
