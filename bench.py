@@ -50,6 +50,8 @@ def parse():
     ap.add_argument("--serve-rate", type=float, default=40.0, help="mean arrivals per second")
     ap.add_argument("--lts-report", action="store_true",
                     help="also time rate-2 LTS against GTS on a layered box (adds about a minute)")
+    ap.add_argument("--batch-sims", type=int, default=32,
+                    help="simulations of the uneven-batch run (graph-captured batch steps); 0 skips it")
     return ap.parse_args()
 
 
@@ -289,6 +291,96 @@ def run_serve(n_req, rate, device, seed=3343):
     return out
 
 
+# compiled FP32 configurations the uneven batch draws from: (order, runs, mechanisms)
+BATCH_CFGS = [(o, r, 0) for o in (3, 4, 5) for r in (1, 4, 8, 16)] + [(6, r, 0) for r in (4, 8, 16)] + \
+    [(3, 8, 3), (4, 8, 3)]
+
+
+def run_batch(n_sims, device, seed=3343, mem_fraction=0.6):
+    """Uneven batch in the shape of the 64-simulation batch configuration, scaled to a bounded run:
+    n_sims simulations over four seeded jittered boxes (9^3 .. 21^3 cubes x 6 = 4,374 .. 55,566 tets,
+    jitter 0 / 5 / 10 / 20%), each with its own order, fused runs and physics (compiled FP32
+    configurations, viscoelastic at 8 runs, orders 3-4), own random sources and 20-100 steps,
+    stepped together by graph-captured batch steps with autotuned launch shapes. Reported against
+    the same simulations run one after another through edge_b200_step (FP32), and against each
+    simulation alone on the plain FP64 path (one run per fused run; FP64 ms per step measured per
+    mesh, order and physics, times runs x steps)."""
+    import time
+
+    import numpy as np
+    import torch
+    from edge_b200 import host
+    from edge_b200.batch import Batch
+    from edge_b200.solver import Solver
+    rng = np.random.default_rng(seed)
+    boxes = [(9, 0.0), (13, 0.05), (17, 0.1), (21, 0.2)]
+    meshes = [host.Mesh.box(n, (1e4, 1e4, 1e4), jitter=j, seed=seed + i) for i, (n, j) in enumerate(boxes)]
+    free, _ = torch.cuda.mem_get_info(device)
+    budget, used = free * mem_fraction, 0.0
+    sims = []
+    for k in range(n_sims):
+        mi = int(rng.integers(len(meshes)))
+        o, r, rm = BATCH_CFGS[int(rng.integers(len(BATCH_CFGS)))]
+        steps = int(rng.integers(20, 101))
+        mesh = meshes[mi]
+        B, F = host.n_modes(o), o * (o + 1) // 2
+        need = mesh.n_el * r * 4 * ((9 + 6 * rm) * (B + 4) * 2 + 36 * (F + 4)) + mesh.n_el * 4000
+        if used + need > budget:
+            continue
+        prob = host.build_problem(0, o, r, rm=rm, mesh=mesh, seed=seed + 17 * k, source="random", n_receivers=0,
+                                  n_steps=steps, f0=1.5)
+        e0, a0 = prob.zero_dofs()
+        s = Solver(prob, precision=32, device=device)
+        s.upload_dofs(e0, a0)
+        sims.append((mi, o, r, rm, steps, prob, s))
+        used += need
+    solvers = [x[6] for x in sims]
+    steps = [x[4] for x in sims]
+    upd = sum(x[5].n_el * x[2] * x[4] for x in sims)
+    torch.cuda.synchronize()
+    b = Batch(solvers, autotune=True)
+    b.run(1)  # captures the graph once outside the timing
+    t0 = time.perf_counter()
+    segs = b.run(steps)
+    t_batch = time.perf_counter() - t0
+    b.close()
+    # the same simulations one after another, each through its own steps
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for s, k in zip(solvers, steps):
+        s.step(k)
+    torch.cuda.synchronize()
+    t_seq = time.perf_counter() - t0
+    # plain FP64, one run: ms per step per (mesh, order, mechanisms)
+    ms64 = {}
+    for mi, o, r, rm, k, prob, s in sims:
+        key = (mi, o, rm)
+        if key in ms64:
+            continue
+        p = host.build_problem(0, o, 1, rm=rm, mesh=meshes[mi], seed=seed, source=None, n_receivers=0)
+        s64 = Solver(p, precision=64, device=device)
+        z, za = p.zero_dofs()
+        s64.upload_dofs(z, za)
+        s64.step(2)
+        s64.sync()
+        t1 = time.perf_counter()
+        s64.step(10)
+        s64.sync()
+        ms64[key] = (time.perf_counter() - t1) / 10 * 1e3
+        s64.close()
+    t64 = sum(ms64[(mi, o, rm)] * r * k for mi, o, r, rm, k, _, _ in sims) / 1e3
+    for s in solvers:
+        s.close()
+    return {"simulations": len(sims), "tets": [m.n_el for m in meshes],
+            "configs": sorted({(o, r, rm) for _, o, r, rm, _, _, _ in sims}),
+            "element_updates": upd, "graph_segments": len(segs), "batch_s": t_batch,
+            "element_updates_per_s": upd / t_batch, "one_after_another_fp32_s": t_seq,
+            "speedup_vs_one_after_another_fp32": t_seq / t_batch, "plain_fp64_alone_s": t64,
+            "speedup_vs_plain_fp64_alone": t64 / t_batch,
+            "note": "wall clock (host timer after a device sync); FP64 extrapolated from 10 timed steps per "
+                    "mesh / order / physics"}
+
+
 def run_lts(device, n_cubes=48, order=5, runs=16, n_groups=3, cycles=2):
     """Rate-2 LTS against GTS on a layered box (vp 1500 / 3000 / 6000 m/s from the top, free surface
     on top): elements sorted into EDGE-V time groups; both advance the same simulated time (GTS at
@@ -516,6 +608,7 @@ def main():
     if a.serve_requests > 0:
         serving = run_serve(a.serve_requests, a.serve_rate, local)
     lts = run_lts(local) if a.lts_report else None
+    batch = run_batch(a.batch_sims, local) if (a.batch_sims > 0 and rank == 0) else None
 
     if rank == 0:
         out = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": a.steps,
@@ -529,7 +622,8 @@ def main():
                "step_ms_p50": step_ms[len(step_ms) // 2], "step_ms_p99": step_ms[min(len(step_ms) - 1,
                                                                                       int(0.99 * len(step_ms)))],
                "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": int(launches),
-               "clocks": clk, "fp64_plain": fp64, "serving": serving, "roofline_neighbour": roofline_neighbour, "lts": lts}
+               "clocks": clk, "fp64_plain": fp64, "serving": serving, "roofline_neighbour": roofline_neighbour, "lts": lts,
+               "batch": batch}
         print(json.dumps(out), flush=True)
     barrier(ws)
     if ws > 1:

@@ -38,6 +38,13 @@ _SIGS = {
     "edge_setup_fs_pair": (C.c_int, [dbl] * 6 + [vp, vp, vp, C.c_int, vp, vp, vp, vp]),
     "edge_b200_create": (C.c_int, [vp, i64, vp]),
     "edge_b200_kernel_config": (C.c_int, [vp, vp]),
+    "edge_b200_batch_create": (C.c_int, [vp, C.c_int, vp, vp, vp]),
+    "edge_b200_batch_set_active": (C.c_int, [vp, vp]),
+    "edge_b200_batch_step": (C.c_int, [vp, C.c_int]),
+    "edge_b200_batch_sync": (C.c_int, [vp, vp]),
+    "edge_b200_batch_last_error": (C.c_char_p, [vp]),
+    "edge_b200_batch_destroy": (C.c_int, [vp]),
+    "edge_b200_autotune": (C.c_int, [vp, dbl, vp]),
     "edge_b200_destroy": (C.c_int, [vp]),
     "edge_b200_upload_mesh": (C.c_int, [vp] * 5),
     "edge_b200_upload_element_data": (C.c_int, [vp] * 7),

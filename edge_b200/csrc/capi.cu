@@ -1212,3 +1212,242 @@ int edge_b200_kernel_times(edge_b200_ctx *ctx, double *ms, int64_t *launches) {
 const char *edge_b200_last_error(const edge_b200_ctx *ctx) { return ctx ? ctx->err.c_str() : "null context"; }
 
 }  // extern "C"
+
+// ------------------------------------------------------------------------------------------------
+// batches of contexts stepped together through one captured CUDA graph, and the launch-shape
+// autotuner
+// ------------------------------------------------------------------------------------------------
+namespace {
+__global__ void kAdvanceSteps(int64_t *steps, const int32_t *active, int n) {
+  for (int k = threadIdx.x; k < n; k += blockDim.x)
+    if (active[k]) steps[k]++;
+}
+}  // namespace
+
+struct edge_b200_batch {
+  std::vector<edge_b200_ctx *> ctxs;
+  std::vector<double> t0, dt;
+  std::vector<int32_t> active;
+  std::vector<cudaStream_t> streams;  // one per context, forked from `origin` inside the capture
+  std::vector<cudaEvent_t> joins;
+  cudaStream_t origin = nullptr;
+  cudaEvent_t fork = nullptr;
+  int64_t *steps = nullptr;    // device: steps taken per context
+  int32_t *activeDev = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  bool dirty = true;
+  std::string err;
+  ~edge_b200_batch() {
+    if (origin) cudaStreamSynchronize(origin);
+    if (exec) cudaGraphExecDestroy(exec);
+    for (cudaStream_t s : streams)
+      if (s) cudaStreamDestroy(s);
+    for (cudaEvent_t e : joins)
+      if (e) cudaEventDestroy(e);
+    if (fork) cudaEventDestroy(fork);
+    if (origin) cudaStreamDestroy(origin);
+    dfree(steps);
+    dfree(activeDev);
+  }
+  // one GTS step of every active context (local, sources, neighbour), each on its own stream
+  cudaError_t capture() {
+    cudaError_t e;
+    if (exec) {
+      cudaGraphExecDestroy(exec);
+      exec = nullptr;
+    }
+    if ((e = cudaMemcpyAsync(activeDev, active.data(), active.size() * sizeof(int32_t), cudaMemcpyHostToDevice,
+                             origin)))
+      return e;
+    if ((e = cudaStreamSynchronize(origin))) return e;
+    if ((e = cudaStreamBeginCapture(origin, cudaStreamCaptureModeThreadLocal))) return e;
+    cudaError_t c = cudaEventRecord(fork, origin);
+    for (size_t k = 0; k < ctxs.size() && !c; k++) {
+      if (!active[k]) continue;
+      edge_b200_ctx *ctx = ctxs[k];
+      cudaStream_t s = streams[k];
+      if ((c = cudaStreamWaitEvent(s, fork, 0))) break;
+      StepArgsRaw a = ctx->args(dt[k]);
+      if ((c = ctx->ks->local(a, s))) break;
+      if (ctx->src.nGrp > 0) {
+        SrcArgs sa = ctx->src;
+        sa.t = t0[k];
+        sa.dt = dt[k];
+        sa.stepDev = steps + k;
+        if ((c = ctx->ks->sources(ctx->dofsE, sa, s))) break;
+      }
+      if ((c = ctx->ks->neigh(a, s))) break;
+      if ((c = cudaEventRecord(joins[k], s))) break;
+      c = cudaStreamWaitEvent(origin, joins[k], 0);
+    }
+    if (!c) {
+      kAdvanceSteps<<<1, 256, 0, origin>>>(steps, activeDev, (int)ctxs.size());
+      c = cudaGetLastError();
+    }
+    cudaGraph_t graph = nullptr;
+    e = cudaStreamEndCapture(origin, &graph);
+    if (c) {
+      if (graph) cudaGraphDestroy(graph);
+      return c;
+    }
+    if (e) return e;
+    e = cudaGraphInstantiate(&exec, graph, 0);
+    cudaGraphDestroy(graph);
+    if (e) return e;
+    dirty = false;
+    return cudaSuccess;
+  }
+};
+
+#define EDGE_BATCH_CUDA(call, what)                                 \
+  do {                                                              \
+    cudaError_t e_ = (call);                                        \
+    if (e_ != cudaSuccess) {                                        \
+      b->err = std::string(what) + ": " + cudaGetErrorString(e_);   \
+      return EDGE_B200_EDEVICE;                                     \
+    }                                                               \
+  } while (0)
+
+int edge_b200_batch_create(edge_b200_ctx *const *ctxs, int n, const double *t0, const double *dt,
+                           edge_b200_batch **out) {
+  if (!ctxs || n < 1 || !t0 || !dt || !out) return EDGE_B200_EINVAL;
+  for (int k = 0; k < n; k++) {
+    edge_b200_ctx *c = ctxs[k];
+    if (!c || !c->meshSet || !c->dataSet || !(dt[k] > 0)) return EDGE_B200_EINVAL;
+    if (c->nRecv > 0 || c->nOwned != c->nEl || c->timing) return EDGE_B200_ENOTSUP;
+    if (c->cfg.device != ctxs[0]->cfg.device) return EDGE_B200_EINVAL;
+    for (int j = 0; j < k; j++)
+      if (ctxs[j] == c) return EDGE_B200_EINVAL;
+  }
+  edge_b200_batch *b = new (std::nothrow) edge_b200_batch();
+  if (!b) return EDGE_B200_ENOMEM;
+  b->ctxs.assign(ctxs, ctxs + n);
+  b->t0.assign(t0, t0 + n);
+  b->dt.assign(dt, dt + n);
+  b->active.assign(n, 1);
+  b->streams.assign(n, nullptr);
+  b->joins.assign(n, nullptr);
+  cudaError_t e = cudaStreamCreateWithFlags(&b->origin, cudaStreamNonBlocking);
+  if (!e) e = cudaEventCreateWithFlags(&b->fork, cudaEventDisableTiming);
+  for (int k = 0; k < n && !e; k++) {
+    e = cudaStreamCreateWithFlags(&b->streams[k], cudaStreamNonBlocking);
+    if (!e) e = cudaEventCreateWithFlags(&b->joins[k], cudaEventDisableTiming);
+  }
+  if (!e) e = cudaMalloc(&b->steps, n * sizeof(int64_t));
+  if (!e) e = cudaMalloc(&b->activeDev, n * sizeof(int32_t));
+  if (!e) e = cudaMemsetAsync(b->steps, 0, n * sizeof(int64_t), b->origin);
+  // the contexts' pending work (uploads) and their flux-solver pairs come before the first step
+  for (int k = 0; k < n && !e; k++) {
+    edge_b200_ctx *c = ctxs[k];
+    e = c->ensureFsLR();
+    if (!e) e = cudaEventRecord(b->joins[k], c->stream);
+    if (!e) e = cudaStreamWaitEvent(b->origin, b->joins[k], 0);
+  }
+  if (e) {
+    delete b;
+    return e == cudaErrorMemoryAllocation ? EDGE_B200_ENOMEM : EDGE_B200_EDEVICE;
+  }
+  *out = b;
+  return EDGE_B200_OK;
+}
+
+int edge_b200_batch_set_active(edge_b200_batch *b, const int32_t *active) {
+  if (!b || !active) return EDGE_B200_EINVAL;
+  for (size_t k = 0; k < b->active.size(); k++) {
+    const int32_t v = active[k] ? 1 : 0;
+    if (v != b->active[k]) b->dirty = true;
+    b->active[k] = v;
+  }
+  return EDGE_B200_OK;
+}
+
+int edge_b200_batch_step(edge_b200_batch *b, int n_steps) {
+  if (!b || n_steps < 0) return EDGE_B200_EINVAL;
+  if (n_steps == 0) return EDGE_B200_OK;
+  if (b->dirty) EDGE_BATCH_CUDA(b->capture(), "capture batch step");
+  for (int i = 0; i < n_steps; i++) EDGE_BATCH_CUDA(cudaGraphLaunch(b->exec, b->origin), "batch step");
+  return EDGE_B200_OK;
+}
+
+int edge_b200_batch_sync(edge_b200_batch *b, int64_t *steps) {
+  if (!b) return EDGE_B200_EINVAL;
+  EDGE_BATCH_CUDA(cudaStreamSynchronize(b->origin), "batch sync");
+  if (steps)
+    EDGE_BATCH_CUDA(cudaMemcpy(steps, b->steps, b->ctxs.size() * sizeof(int64_t), cudaMemcpyDeviceToHost),
+                    "batch steps");
+  return EDGE_B200_OK;
+}
+
+const char *edge_b200_batch_last_error(const edge_b200_batch *b) { return b ? b->err.c_str() : ""; }
+
+int edge_b200_batch_destroy(edge_b200_batch *b) {
+  if (!b) return EDGE_B200_EINVAL;
+  delete b;
+  return EDGE_B200_OK;
+}
+
+int edge_b200_autotune(edge_b200_ctx *ctx, double dt, int32_t caps[2]) {
+  if (!ctx || !(dt > 0)) return EDGE_B200_EINVAL;
+  if (!ctx->meshSet || !ctx->dataSet || ctx->timing) return EDGE_B200_EINVAL;
+  cudaStream_t s = ctx->stream;
+  EDGE_CUDA(ctx->ensureFsLR(), "flux-solver pairs");
+  const size_t rs = ctx->realSize;
+  const size_t bytesE = ctx->dofsCount() * rs, bytesA = ctx->dofsACount() * rs;
+  DevBuf save;
+  if (save.fit(bytesE + bytesA) != cudaSuccess) return EDGE_B200_ENOMEM;
+  EDGE_CUDA(cudaMemcpyAsync(save.p, ctx->dofsE, bytesE, cudaMemcpyDeviceToDevice, s), "autotune save");
+  if (bytesA)
+    EDGE_CUDA(cudaMemcpyAsync(static_cast<char *>(save.p) + bytesE, ctx->dofsA, bytesA, cudaMemcpyDeviceToDevice, s),
+              "autotune save");
+  KernelSet *ks = ctx->ks;
+  ks->setGridCaps(0, 0);
+  const int64_t groups = (ctx->nOwned + ks->elementsPerCta() - 1) / ks->elementsPerCta();
+  const int defL = ks->ctasLocal(), defN = ks->ctasNeigh();
+  cudaEvent_t ev[2];
+  EDGE_CUDA(cudaEventCreate(&ev[0]), "autotune");
+  EDGE_CUDA(cudaEventCreate(&ev[1]), "autotune");
+  StepArgsRaw a = ctx->args(dt);
+  int best[2] = {0, 0};
+  cudaError_t err = cudaSuccess;
+  for (int kind = 0; kind < 2 && !err; kind++) {
+    const int def = kind == 0 ? defL : defN;
+    // candidates: the persistent default, half of it, one CTA per element group (when more)
+    const int64_t cand[3] = {0, def / 2, groups > def ? std::min<int64_t>(groups, 1 << 30) : 0};
+    float bestMs = 1e30f;
+    for (int c = 0; c < 3 && !err; c++) {
+      if (c > 0 && cand[c] <= 0) continue;
+      if (kind == 0)
+        ks->setGridCaps((int)cand[c], 0);
+      else
+        ks->setGridCaps(best[0], (int)cand[c]);
+      float ms = 1e30f;
+      for (int rep = 0; rep < 4 && !err; rep++) {
+        if ((err = cudaEventRecord(ev[0], s))) break;
+        err = kind == 0 ? ks->local(a, s) : ks->neigh(a, s);
+        if (!err) err = cudaEventRecord(ev[1], s);
+        if (!err) err = cudaEventSynchronize(ev[1]);
+        float t = 0;
+        if (!err) err = cudaEventElapsedTime(&t, ev[0], ev[1]);
+        if (rep > 0) ms = std::min(ms, t);  // the first launch warms up
+      }
+      if (!err && ms < bestMs) {
+        bestMs = ms;
+        best[kind] = (int)cand[c];
+      }
+    }
+  }
+  cudaEventDestroy(ev[0]);
+  cudaEventDestroy(ev[1]);
+  EDGE_CUDA(err, "autotune");
+  ks->setGridCaps(best[0], best[1]);
+  EDGE_CUDA(cudaMemcpyAsync(ctx->dofsE, save.p, bytesE, cudaMemcpyDeviceToDevice, s), "autotune restore");
+  if (bytesA)
+    EDGE_CUDA(cudaMemcpyAsync(ctx->dofsA, static_cast<char *>(save.p) + bytesE, bytesA, cudaMemcpyDeviceToDevice, s),
+              "autotune restore");
+  EDGE_CUDA(cudaStreamSynchronize(s), "autotune restore");
+  if (caps) {
+    caps[0] = best[0];
+    caps[1] = best[1];
+  }
+  return EDGE_B200_OK;
+}

@@ -9,7 +9,7 @@ template <typename T, int O, int R, int RM>
 class KernelSetImpl final : public KernelSet {
   using G = Geo<T, O, R, RM>;
   int numSms_ = 0, occLocal_ = 1, occNeigh_ = 1, occRecv_ = 1, occLocalLts_ = 1, occLocalSum_ = 1,
-      occNeighLts_ = 1;
+      occNeighLts_ = 1, capLocal_ = 0, capNeigh_ = 0;
 
   static StepArgs<T> cast(const StepArgsRaw &a) {
     StepArgs<T> b;
@@ -92,8 +92,12 @@ class KernelSetImpl final : public KernelSet {
     return cudaSuccess;
   }
   int elementsPerCta() const override { return G::E; }
-  int ctasLocal() const override { return numSms_ * occLocal_; }
-  int ctasNeigh() const override { return numSms_ * occNeigh_; }
+  int ctasLocal() const override { return capLocal_ > 0 ? capLocal_ : numSms_ * occLocal_; }
+  int ctasNeigh() const override { return capNeigh_ > 0 ? capNeigh_ : numSms_ * occNeigh_; }
+  void setGridCaps(int local, int neigh) override {
+    capLocal_ = local;
+    capNeigh_ = neigh;
+  }
 
   static int grid(int64_t nEl, int cap) {
     int64_t groups = (nEl + G::E - 1) / G::E;

@@ -50,6 +50,9 @@ class KernelSet {
   virtual int elementsPerCta() const = 0;
   virtual int ctasLocal() const = 0;
   virtual int ctasNeigh() const = 0;
+  // caps on the persistent grids of the GTS local / neighbour kernels (0: resident CTAs per SM x
+  // SMs, the default; a larger cap gives one CTA per element group up to it)
+  virtual void setGridCaps(int local, int neigh) = 0;
 };
 
 // returns nullptr when the configuration is not compiled in

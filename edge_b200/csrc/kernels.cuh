@@ -1466,6 +1466,9 @@ struct SrcArgs {
   const int64_t *tsOff, *nPts;
   const double *ts;
   double t, dt, tol;
+  // replayed launches (a captured batch step): the step starts at t + (*stepDev) * dt, the step
+  // counter advancing on the device after each step; null: at t
+  const int64_t *stepDev;
 };
 
 __device__ inline double seriesIntegral(double dx, double xStart, int64_t nPts, const double *vals, double x1,
@@ -1501,10 +1504,11 @@ __global__ void kSources(T *dofsE, SrcArgs s) {
   constexpr int B = nModes(O);
   const int g = blockIdx.x;
   if (g >= s.nGrp) return;
+  const double t1 = s.stepDev ? s.t + double(*s.stepDev) * s.dt : s.t;
   for (int t = threadIdx.x; t < 9 * B; t += blockDim.x) {
     const int q = t / B, md = t % B;
     for (int i = s.grpOff[g]; i < s.grpOff[g + 1]; i++) {
-      const double in = seriesIntegral(s.dts[i], s.t0[i], s.nPts[i], s.ts + s.tsOff[i], s.t, s.t + s.dt, s.tol);
+      const double in = seriesIntegral(s.dts[i], s.t0[i], s.nPts[i], s.ts + s.tsOff[i], t1, t1 + s.dt, s.tol);
       const double sc = in * s.scal[i * 9 + q];
       T *p = dofsE + ((s.el[i] * 9 + q) * R + s.run[i]) * int64_t(padGlobal<T>(B)) + md;
       *p = T(double(*p) + sc * s.bEval[i * B + md]);

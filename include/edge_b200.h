@@ -309,6 +309,37 @@ int edge_b200_step_noalloc(const edge_b200_cfg *cfg, int64_t n_el, double dt, in
                            const double *omega, const int32_t *el_fa_el,
                            const uint8_t *fid_el_fa_el, const uint8_t *vid_el_fa_el,
                            const uint8_t *el_fa_type);
+/* ---------------------------- batches of simulations, autotuner --------------------------- */
+
+/* A batch of contexts (different meshes, orders, fused runs, physics; one device) stepped
+ * together: one batch step is every active context's GTS step (local, sources, neighbour), each
+ * context's kernels on a stream of its own, captured once into a CUDA graph and replayed per step,
+ * so the independent contexts' kernels run side by side. Context k steps from time t0[k] by dt[k];
+ * a device counter per context gives its sources the step's time. The contexts keep their data;
+ * upload DOFs and element data before creating the batch, and call edge_b200_batch_sync before
+ * using a context on its own again. Contexts with receivers, halo parts or kernel timing on are
+ * refused (EDGE_B200_ENOTSUP): those run through edge_b200_step. No counterpart in the reference
+ * (one solver per process; cfg4-style uneven batches). */
+typedef struct edge_b200_batch edge_b200_batch;
+int edge_b200_batch_create(edge_b200_ctx *const *ctxs, int n, const double *t0, const double *dt,
+                           edge_b200_batch **out);
+/* active[k] != 0: context k takes part in the following steps (all do after create); the graph is
+ * captured again at the next step when the set changed, e.g. when a simulation finished. */
+int edge_b200_batch_set_active(edge_b200_batch *b, const int32_t *active);
+/* n_steps batch steps (graph launches) on the batch's own stream; returns without waiting. */
+int edge_b200_batch_step(edge_b200_batch *b, int n_steps);
+/* Waits for the batch; steps[n] (may be NULL) receives the steps each context has taken. */
+int edge_b200_batch_sync(edge_b200_batch *b, int64_t *steps);
+const char *edge_b200_batch_last_error(const edge_b200_batch *b);
+int edge_b200_batch_destroy(edge_b200_batch *b);
+/* Launch-shape autotuner for this context's mesh: times the local and then the neighbour kernel
+ * with its grid at the persistent default (resident CTAs per SM x SMs), half of it, and one CTA
+ * per element group, keeps the fastest for later GTS steps, and restores the DOFs it stepped
+ * (needs device memory for one copy of them). caps[2] (may be NULL) receives the chosen grid caps
+ * (0 = the default). The element-group shape itself (32 / runs elements per CTA) is fixed per
+ * compiled configuration. No counterpart in the reference. */
+int edge_b200_autotune(edge_b200_ctx *ctx, double dt, int32_t caps[2]);
+
 /* Last CUDA error string of the context (static storage). */
 const char *edge_b200_last_error(const edge_b200_ctx *ctx);
 
