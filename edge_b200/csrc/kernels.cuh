@@ -331,9 +331,9 @@ struct Geo {
 // per-thread element coefficients
 template <typename T, int RM>
 struct ElemCoef {
-  T cs[3][3];     // star row q, 3 slots, per dim
+  T cs[3][3];     // star row q, 3 slots, per derivative direction (kStarDir)
   int cols[3];
-  T ca[3][2];     // anelastic star row s, per dim
+  T ca[3][2];     // anelastic star row s, per derivative direction
   int colsA[2];
   T csrc[3][3];   // source matrices row q (< 6), per mechanism
   int colsSrc[3];
@@ -342,13 +342,17 @@ struct ElemCoef {
     if (q < 9) {
 #pragma unroll
       for (int i = 0; i < 3; i++) cols[i] = kStarCol[q][i];
+      // star_dim -> star of the derivative directions of the generated stiffness products (FP64)
 #pragma unroll
-      for (int d = 0; d < 3; d++)
+      for (int i = 0; i < 3; i++) {
+        const int idx = kStarIdx[q][i];
+        double v[3] = {0, 0, 0};
+        if (valid && idx >= 0)
 #pragma unroll
-        for (int i = 0; i < 3; i++) {
-          int idx = kStarIdx[q][i];
-          cs[d][i] = valid && idx >= 0 ? T(__ldg(&a.starE[(e * 3 + d) * 24 + idx])) : T(0);
-        }
+          for (int d = 0; d < 3; d++) v[d] = __ldg(&a.starE[(e * 3 + d) * 24 + idx]);
+#pragma unroll
+        for (int d = 0; d < 3; d++) cs[d][i] = T(kStarDir[0][d] * v[0] + kStarDir[1][d] * v[1] + kStarDir[2][d] * v[2]);
+      }
       if (RM && q < 6) {
 #pragma unroll
         for (int i = 0; i < 3; i++) colsSrc[i] = kSrcCol[q][i];
@@ -372,12 +376,15 @@ struct ElemCoef {
 #pragma unroll
       for (int i = 0; i < 2; i++) colsA[i] = kStarACol[s][i];
 #pragma unroll
-      for (int d = 0; d < 3; d++)
+      for (int i = 0; i < 2; i++) {
+        const int idx = kStarAIdx[s][i];
+        double v[3] = {0, 0, 0};
+        if (valid && idx >= 0)
 #pragma unroll
-        for (int i = 0; i < 2; i++) {
-          int idx = kStarAIdx[s][i];
-          ca[d][i] = valid && idx >= 0 ? T(__ldg(&a.starA[(e * 3 + d) * 9 + idx])) : T(0);
-        }
+          for (int d = 0; d < 3; d++) v[d] = __ldg(&a.starA[(e * 3 + d) * 9 + idx]);
+#pragma unroll
+        for (int d = 0; d < 3; d++) ca[d][i] = T(kStarDir[0][d] * v[0] + kStarDir[1][d] * v[1] + kStarDir[2][d] * v[2]);
+      }
     }
   }
 };

@@ -30,6 +30,13 @@ the sigma_FA that is again one of the three reflections, V = ``kFacePerm[O-2][fo
 flux operators are the reference's up to this change of face basis, which the lifted flux does
 not see.
 
+Derivative directions. The stiffness products run in the reference-coordinate derivative directions
+a = 0, 1, 2 given by the rows of ``DIRS`` (K'_a = sum_dim DIRS[a][dim] K_dim) instead of xi1, xi2,
+xi3: in the hierarchical basis these combinations cancel exactly where the axis directions do not,
+so at order 5 the recursion's products hold 565 instead of 901 non-zeros and the volume's 394
+instead of 647. The star matrices change accordingly, star'_a = sum_dim DIRS^-1[dim][a] star_dim
+(``kStarDir``, applied when the kernels load them), which keeps sum_dim star_dim K_dim unchanged.
+
 Every accumulator receives its terms in ascending k, as the reference's vanilla kernels sum.
 
 Usage: python -m edge_b200.gen_kernels
@@ -40,6 +47,33 @@ from fractions import Fraction
 from edge_b200 import dgmat
 
 ORDERS = range(2, 7)
+
+# derivative directions of the stiffness products (rows: combinations of the xi1, xi2, xi3
+# derivatives), chosen for the fewest non-zeros at orders 4-6 among combinations with
+# coefficients in {-1, 0, 1}
+DIRS = [(-1, 0, 0), (-1, 1, 1), (0, -1, 1)]
+
+
+def dirs_inverse():
+    """DIRS^-1 as Fractions (3x3 Gauss-Jordan)."""
+    m = [[Fraction(x) for x in row] + [Fraction(int(i == j)) for j in range(3)] for i, row in enumerate(DIRS)]
+    for c in range(3):
+        p = next(r for r in range(c, 3) if m[r][c] != 0)
+        m[c], m[p] = m[p], m[c]
+        piv = m[c][c]
+        m[c] = [x / piv for x in m[c]]
+        for r in range(3):
+            if r != c and m[r][c] != 0:
+                f = m[r][c]
+                m[r] = [x - f * y for x, y in zip(m[r], m[c])]
+    return [row[3:] for row in m]
+
+
+def combine_dirs(mats):
+    """K'_a = sum_dim DIRS[a][dim] K_dim for three [k][n] matrices."""
+    kk, nn = len(mats[0]), len(mats[0][0])
+    return [[[sum(Fraction(DIRS[a][d]) * mats[d][k][n] for d in range(3)) for n in range(nn)] for k in range(kk)]
+            for a in range(3)]
 
 
 def lit(x):
@@ -138,10 +172,11 @@ def main(out=None):
         ex = dgmat.exact_matrices(o)
         B, F = nm(o), dgmat.n_modes_tri(o)
         s.append(f"// ---------------- order {o}: B = {B}, F = {F} ----------------")
+        stiffT, stiffV = combine_dirs(ex["stiffT"]), combine_dirs(ex["stiffV"])
         for d in range(1, o):
-            body = block_rows4(ex["stiffT"], nm(o - d + 1), nm(o - d), "acc", neg=True)
+            body = block_rows4(stiffT, nm(o - d + 1), nm(o - d), "acc", neg=True)
             s += struct_fused("CkMul", f"{o}, {d}", body, "acc")
-        body = block_rows4(ex["stiffV"], nm(o - 1), B, "acc")
+        body = block_rows4(stiffV, nm(o - 1), B, "acc")
         s += struct_fused("VolMul", f"{o}", body, "acc")
         fb = face_bases(o)
         sig = [b[0] for b in fb]
@@ -153,6 +188,10 @@ def main(out=None):
         for v in range(3):
             s += struct("OriMul", f"{o}, {v}", block("", None, None, ori[3 + v], F, F, "x", "s"), "x", "s")
         tables.append((o, sig, face_perm_table(sig)))
+    inv = dirs_inverse()
+    s.append("// star matrices of the derivative directions: star'_a = sum_dim kStarDir[dim][a] * star_dim")
+    s.append("__constant__ double kStarDir[3][3] = {" +
+             ", ".join("{" + ", ".join(repr(float(inv[d][a])) for a in range(3)) + "}" for d in range(3)) + "};")
     s.append("// orientation (OriMul index) from a neighbour's face fo to this element's face FA with vertex")
     s.append("// id v: kFacePerm[O - 2][fo][FA][v]; face bases sigma_FA per order: " +
              ", ".join(f"O{o} {sig}" for o, sig, _ in tables))

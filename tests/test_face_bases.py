@@ -55,3 +55,22 @@ def test_generated_table_matches_generator():
         tab = gk.face_perm_table([b[0] for b in gk.face_bases(o)])
         want += [tab[fo][fa][v] for fo in range(4) for fa in range(4) for v in range(3)]
     assert nums == want
+
+
+@pytest.mark.parametrize("order", [2, 3, 4, 5, 6])
+def test_derivative_directions_keep_the_star_stiffness_sum(order):
+    """sum_a star'_a (x) K'_a == sum_dim star_dim (x) K_dim for the generated direction basis
+    (stiffT of the recursion and stiffV of the volume), with star'_a = sum_dim DIRS^-1[dim][a]."""
+    ex = dgmat.exact_matrices(order)
+    inv = np.array([[float(x) for x in row] for row in gk.dirs_inverse()])
+    np.testing.assert_allclose(np.array(gk.DIRS, float) @ inv, np.eye(3), atol=0)
+    rng = np.random.default_rng(order)
+    star = rng.normal(size=(3, 9, 9))
+    star2 = np.einsum("da,dij->aij", inv, star)
+    for key in ("stiffT", "stiffV"):
+        K = np.array([_f(m) for m in ex[key]])
+        K2 = np.array([_f(m) for m in gk.combine_dirs(ex[key])])
+        ref = np.einsum("dij,dkn->ikjn", star, K)
+        got = np.einsum("aij,akn->ikjn", star2, K2)
+        np.testing.assert_allclose(got, ref, rtol=0, atol=1e-10 * np.abs(ref).max())
+        assert np.count_nonzero(K2) < np.count_nonzero(K)
