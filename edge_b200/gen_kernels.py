@@ -33,7 +33,7 @@ not see.
 Derivative directions. The stiffness products run in the reference-coordinate derivative directions
 a = 0, 1, 2 given by the rows of ``DIRS`` (K'_a = sum_dim DIRS[a][dim] K_dim) instead of xi1, xi2,
 xi3: in the hierarchical basis these combinations cancel exactly where the axis directions do not,
-so at order 5 the recursion's products hold 565 instead of 901 non-zeros and the volume's 394
+so at order 5 the recursion's products hold 516 instead of 901 non-zeros and the volume's 364
 instead of 647. The star matrices change accordingly, star'_a = sum_dim DIRS^-1[dim][a] star_dim
 (``kStarDir``, applied when the kernels load them), which keeps sum_dim star_dim K_dim unchanged.
 
@@ -49,9 +49,9 @@ from edge_b200 import dgmat
 ORDERS = range(2, 7)
 
 # derivative directions of the stiffness products (rows: combinations of the xi1, xi2, xi3
-# derivatives), chosen for the fewest non-zeros at orders 4-6 among combinations with
-# coefficients in {-1, 0, 1}
-DIRS = [(-1, 0, 0), (-1, 1, 1), (0, -1, 1)]
+# derivatives), chosen for the fewest non-zeros at orders 2-6 among combinations with integer
+# coefficients in [-4, 4] (every order picks the same three)
+DIRS = [(1, 0, 0), (0, 1, -1), (1, -2, 0)]
 
 
 def dirs_inverse():
