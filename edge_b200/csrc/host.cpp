@@ -420,6 +420,14 @@ int edge_mesh_box(int nx, int ny, int nz, const double ext[3], double jitter, ui
     auto draw = [&](int64_t v) {
       for (int d = 0; d < 3; d++) m->ve[3 * v + d] = base[3 * v + d] + (2 * rng.uniform() - 1) * jitter * h[d];
     };
+    // orientation of every tet before the jitter (the six tets of a cube alternate in sign; the
+    // element normalisation orients them later): a jittered tet is inverted when its sign flips
+    std::vector<int8_t> sign0(nEl);
+    for (int64_t e = 0; e < nEl; e++) {
+      double j3[3][3];
+      m->jac(e, j3);
+      sign0[e] = det3(j3) > 0 ? 1 : -1;
+    }
     for (int64_t v = 0; v < vx * vy * vz; v++)
       if (interior(v)) draw(v);
     for (int it = 0; it < 64; it++) {
@@ -427,8 +435,8 @@ int edge_mesh_box(int nx, int ny, int nz, const double ext[3], double jitter, ui
       for (int64_t e = 0; e < nEl; e++) {
         double j3[3][3];
         m->jac(e, j3);
-        double vol = std::abs(det3(j3));
-        if (det3(j3) <= 0 || vol < 1e-3 * h[0] * h[1] * h[2])
+        const double sv = sign0[e] * det3(j3);
+        if (sv <= 1e-3 * h[0] * h[1] * h[2])
           for (int a = 0; a < 4; a++)
             if (interior(m->elVe[4 * e + a])) bad.push_back(m->elVe[4 * e + a]);
       }
