@@ -933,6 +933,7 @@ int edge_b200_step_lts(edge_b200_ctx *ctx, double t, double dt_fun, int n_cycles
   if (!ctx || !(dt_fun > 0) || n_cycles < 0 || ctx->nTg < 1) return EDGE_B200_EINVAL;
   if (!ctx->meshSet || !ctx->dataSet) return EDGE_B200_EINVAL;
   if (!ctx->ks->ltsSupported()) return EDGE_B200_ENOTSUP;
+  EDGE_CUDA(ctx->ensureFsLR(), "flux-solver pairs");
   ctx->lastLts = true;
   const int G = ctx->nTg;
   const int64_t nFun = int64_t(1) << (G - 1);  // fundamental steps per cycle (largest group's step)

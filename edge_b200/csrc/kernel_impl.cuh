@@ -9,7 +9,7 @@ template <typename T, int O, int R, int RM>
 class KernelSetImpl final : public KernelSet {
   using G = Geo<T, O, R, RM>;
   int numSms_ = 0, occLocal_ = 1, occNeigh_ = 1, occRecv_ = 1, occLocalLts_ = 1, occLocalSum_ = 1,
-      occNeighLts_ = 1, capLocal_ = 0, capNeigh_ = 0;
+      capLocal_ = 0, capNeigh_ = 0;
 
   static StepArgs<T> cast(const StepArgsRaw &a) {
     StepArgs<T> b;
@@ -60,17 +60,11 @@ class KernelSetImpl final : public KernelSet {
       return e;
     if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occNeigh_, kNeigh<T, O, R, RM, G::premix>, G::NT, smemNeigh())))
       return e;
-    if constexpr (G::premix) {
-      if ((e = cudaFuncSetAttribute(kNeigh<T, O, R, RM, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    if constexpr (G::premixLts != G::premix) {
+      if ((e = cudaFuncSetAttribute(kNeigh<T, O, R, RM, G::premixLts>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                     (int)smemNeigh())))
         return e;
-      if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occNeighLts_, kNeigh<T, O, R, RM, false>, G::NT,
-                                                             smemNeigh())))
-        return e;
-    } else {
-      occNeighLts_ = occNeigh_;
     }
-    occNeighLts_ = occNeighLts_ < 1 ? 1 : occNeighLts_;
     if constexpr (G::ltsOk) {
       if ((e = cudaFuncSetAttribute(kLocal<T, O, R, RM, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                     (int)G::smemLocalLts)))
@@ -80,10 +74,10 @@ class KernelSetImpl final : public KernelSet {
         return e;
       occLocalLts_ = occLocalLts_ < 1 ? 1 : occLocalLts_;
       if ((e = cudaFuncSetAttribute(kLocal<T, O, R, RM, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                    (int)G::smemLocal)))
+                                    (int)G::smemLocalSums)))
         return e;
       if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occLocalSum_, kLocal<T, O, R, RM, 1>, G::NT,
-                                                             G::smemLocal)))
+                                                             G::smemLocalSums)))
         return e;
       occLocalSum_ = occLocalSum_ < 1 ? 1 : occLocalSum_;
     }
@@ -121,7 +115,7 @@ class KernelSetImpl final : public KernelSet {
   cudaError_t localLtsSums(const StepArgsRaw &a, cudaStream_t s) override {
     if constexpr (G::ltsOk) {
       if (a.elCount < 1) return cudaSuccess;
-      kLocal<T, O, R, RM, 1><<<grid(a.elCount, numSms_ * occLocalSum_), G::NT, G::smemLocal, s>>>(cast(a));
+      kLocal<T, O, R, RM, 1><<<grid(a.elCount, numSms_ * occLocalSum_), G::NT, G::smemLocalSums, s>>>(cast(a));
       return cudaGetLastError();
     } else {
       return cudaErrorNotSupported;
@@ -137,7 +131,7 @@ class KernelSetImpl final : public KernelSet {
   }
   cudaError_t neighLts(const StepArgsRaw &a, cudaStream_t s) override {
     if (a.elCount < 1) return cudaSuccess;
-    kNeigh<T, O, R, RM, false><<<grid(a.elCount, occNeighLts_ * numSms_), G::NT, smemNeigh(), s>>>(cast(a));
+    kNeigh<T, O, R, RM, G::premixLts><<<grid(a.elCount, ctasNeigh()), G::NT, smemNeigh(), s>>>(cast(a));
     return cudaGetLastError();
   }
   cudaError_t recv(const StepArgsRaw &a, const RecvArgs &r, cudaStream_t s) override {

@@ -43,7 +43,8 @@ class KernelSet {
   virtual bool premix() const = 0;
   virtual int fsPairStride() const = 0;
   virtual cudaError_t neigh(const StepArgsRaw &a, cudaStream_t s) = 0;
-  // the neighbour step over face buffers the LTS local kernels wrote (not pre-mixed)
+  // the neighbour step over the buffers the LTS local kernels wrote (pre-mixed where those
+  // kernels have room for it)
   virtual cudaError_t neighLts(const StepArgsRaw &a, cudaStream_t s) = 0;
   virtual cudaError_t recv(const StepArgsRaw &a, const RecvArgs &r, cudaStream_t s) = 0;
   virtual cudaError_t sources(void *dofsE, const SrcArgs &sa, cudaStream_t s) = 0;

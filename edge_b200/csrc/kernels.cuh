@@ -301,9 +301,15 @@ struct Geo {
   static constexpr size_t smemLocalGts = smemLocal + (premix ? premixBytes : 0);
   // elastic CK with ping-pong derivatives between X and the separate face tile
   static constexpr bool ckPingPong = asyncLocal && RM == 0 && nModes(O - 1) <= SF;
-  // LTS local step: one more [9][32][SB] tile for the half-step time integral (behind the rest);
+  // LTS local step: one more [9][32][SB] tile for the half-step time integral (behind the rest)
+  // and, pre-mixing, the flux-solver buffers and two face tiles for the half-step projections;
   // configurations whose time integrals do not fit shared memory have no LTS kernels
-  static constexpr size_t smemLocalLts = smemLocal + nX * sizeof(T);
+  static constexpr bool premixLts =
+      premix && smemLocal + nX * sizeof(T) + premixBytes + 2 * nS0 * sizeof(T) <= 227 * 1024;
+  static constexpr size_t smemLocalLts =
+      smemLocal + nX * sizeof(T) + (premixLts ? premixBytes + 2 * nS0 * sizeof(T) : 0);
+  // the LTS local kernel without half-step integrals (mode 1)
+  static constexpr size_t smemLocalSums = smemLocal + (premixLts ? premixBytes : 0);
   static constexpr bool ltsOk = tiSmem && smemLocalLts <= 227 * 1024;
   // neighbour kernel: a ring of NSN slots, each [9][32][SF] face rows and, for E <= 4, the E
   // elements' flux-solver blocks (81 + 54 doubles); as many slots (2..4) as fit the shared memory
@@ -716,10 +722,15 @@ __device__ __forceinline__ void issueMixFs(const StepArgs<T> &a, T *buf, int64_t
 template <typename T, int O, int R, int RM, int FA, int LTS = 0, bool TAIL = true>
 __device__ __forceinline__ void localFace(const StepArgs<T> &a, const T *TI, T *S0, int q, int l, int64_t e,
                                           int r, bool valid, T *acc, T *upA, const T *TIh = nullptr,
-                                          T *S0alt = nullptr, const MixFs<T> &mf = MixFs<T>{nullptr, 0, 0}) {
+                                          T *S0alt = nullptr, const MixFs<T> &mf = MixFs<T>{nullptr, 0, 0},
+                                          T *Sh = nullptr) {
   using G = Geo<T, O, R, RM>;
   constexpr int F = G::F, SF = G::SF, SB = G::SB;
-  constexpr bool PM = LTS == 0 && G::premix;
+  constexpr bool PM = LTS == 0 ? G::premix : G::premixLts;
+  // pre-mixing LTS mode 2: the half-step projection rows of elements with a smaller neighbour go
+  // through a face tile of their own (two, alternating with the faces) for their quantity mix
+  T *ShF = (PM && LTS == 2) ? Sh + (FA % 2) * G::nS0 : nullptr;
+  const bool half = LTS == 2 && valid && (a.ltsFlags[e] & LTS_HAS_SMALLER);
   T s[F];
   if (q < 9) {
 #pragma unroll
@@ -738,7 +749,16 @@ __device__ __forceinline__ void localFace(const StepArgs<T> &a, const T *TI, T *
         storeRowsCoalesced<T, R, G::GF, SF>(S0, a.face + ((e * 4 + FA) * 9 + q) * int64_t(R * G::GF), q, l / R,
                                             l % R);
     }
-    if constexpr (LTS) {
+    if constexpr (PM && LTS == 2) {
+      if (half) {
+        T h[F];
+#pragma unroll
+        for (int j = 0; j < F; j++) h[j] = T(0);
+        FluxLMul<O, FA>::template run<T>(OwnRow<T>{rowPtr<T, SB>(TIh, q, l)}, h);
+        stRow<T, F>(rowPtr<T, SF>(ShF, q, l), h);
+      }
+    }
+    if constexpr (LTS && !PM) {
       if (valid) {
         const int fl = a.ltsFlags[e];
         if (fl & LTS_HAS_LARGER) {
@@ -787,11 +807,38 @@ __device__ __forceinline__ void localFace(const StepArgs<T> &a, const T *TI, T *
         fr1[i] = fb[FSP + i];
       }
     }
-    faceMix2<T, F, SF, G::GF>(S0, l, fr, fr1, s, rowPtr<T, SF>(S0alt, q, l));
+    T *tRow = rowPtr<T, SF>(S0alt, q, l);
+    faceMix2<T, F, SF, G::GF>(S0, l, fr, fr1, s, tRow);
     __syncwarp();
     if (ty != FT_OUTFLOW)
       storeRowsCoalesced<T, R, G::GF, SF>(S0alt, a.face + ((e * 4 + FA) * 9 + q) * int64_t(R * G::GF), q, l / R,
                                           l % R);
+    if constexpr (LTS) {
+      // the LTS buffers of the (pre-mixed) projection t: its sum over the two steps of a pair for a
+      // larger neighbour, the half-step projections (mixed alike) for a smaller one
+      if (valid) {
+        const int fl = a.ltsFlags[e];
+        if (fl & LTS_HAS_LARGER) {
+          T *p = gRow<T, R, G::GF>(a.faceSum, int64_t(a.sumIdx[e]) * 4 + FA, 9, q, r);
+          T v[F], t[F];
+          ldRowG<T, F>(p, v, !a.firstTs);
+          ldRow<T, F>(tRow, t);
+#pragma unroll
+          for (int j = 0; j < F; j++) v[j] += t[j];
+          stRowG<T, F>(p, v);
+        }
+        if (LTS == 2 && half) {
+          T h[F], t[F];
+          faceMix<T, F, SF>(ShF, l, fr1, h);
+          const int64_t slot = int64_t(a.halfIdx[e]) * 4 + FA;
+          stRowG<T, F>(gRow<T, R, G::GF>(a.faceHalf1, slot, 9, q, r), h);
+          ldRow<T, F>(tRow, t);
+#pragma unroll
+          for (int j = 0; j < F; j++) h[j] = t[j] - h[j];
+          stRowG<T, F>(gRow<T, R, G::GF>(a.faceHalf2, slot, 9, q, r), h);
+        }
+      }
+    }
     // the next face writes this warp's rows of the tile again
     __syncwarp();
     FluxTMul<O, FA>::template run<T>(s, acc);
@@ -840,9 +887,12 @@ __global__ void __launch_bounds__(Geo<T, O, R, RM>::NT, LTS == 2 ? 1 : Geo<T, O,
   T *TIA = G::tiSmem ? XA + G::nXA : XA;
   T *S0 = AS ? TIA + G::nTIA : (G::tiSmem ? X : X + G::nX);
   T *TIh = LTS == 2 ? reinterpret_cast<T *>(smem + G::smemLocal) : nullptr;
-  // pre-mixed face projections: flux-solver buffers behind the face tile
-  constexpr bool PM = LTS == 0 && G::premix;
-  T *fsb = PM ? reinterpret_cast<T *>(smem + G::smemLocal) : nullptr;
+  // pre-mixed face projections: flux-solver buffers behind the face tile (behind TIh with LTS
+  // mode 2, followed by its two half-step face tiles)
+  constexpr bool PM = LTS == 0 ? G::premix : G::premixLts;
+  constexpr size_t fsOff = G::smemLocal + (LTS == 2 ? G::nX * sizeof(T) : 0);
+  T *fsb = PM ? reinterpret_cast<T *>(smem + fsOff) : nullptr;
+  T *Sh = (PM && LTS == 2) ? reinterpret_cast<T *>(smem + fsOff + G::premixBytes) : nullptr;
   const int q = threadIdx.x >> 5, l = threadIdx.x & 31;
   const int eo = l / R, r = l % R;
   const int64_t nGroups = (a.elCount + E - 1) / E;
@@ -964,11 +1014,11 @@ __global__ void __launch_bounds__(Geo<T, O, R, RM>::NT, LTS == 2 ? 1 : Geo<T, O,
     // local surface integral (SurfIntVanilla::local, SurfIntVanilla.hpp:212-262) + face projections
     if constexpr (AS) {
       const MixFs<T> mf{fsb, g, nGroups};
-      localFace<T, O, R, RM, 0, LTS, false>(a, TI, S0, q, l, ev, r, valid, acc, upA, TIh, X, mf);
-      localFace<T, O, R, RM, 1, LTS, false>(a, TI, X, q, l, ev, r, valid, acc, upA, TIh, S0, mf);
-      localFace<T, O, R, RM, 2, LTS, false>(a, TI, S0, q, l, ev, r, valid, acc, upA, TIh, X, mf);
+      localFace<T, O, R, RM, 0, LTS, false>(a, TI, S0, q, l, ev, r, valid, acc, upA, TIh, X, mf, Sh);
+      localFace<T, O, R, RM, 1, LTS, false>(a, TI, X, q, l, ev, r, valid, acc, upA, TIh, S0, mf, Sh);
+      localFace<T, O, R, RM, 2, LTS, false>(a, TI, S0, q, l, ev, r, valid, acc, upA, TIh, X, mf, Sh);
       // the barrier after the last face orders its readers of X before the next group writes X
-      localFace<T, O, R, RM, 3, LTS, true>(a, TI, X, q, l, ev, r, valid, acc, upA, TIh, S0, mf);
+      localFace<T, O, R, RM, 3, LTS, true>(a, TI, X, q, l, ev, r, valid, acc, upA, TIh, S0, mf, Sh);
     } else {
       localFace<T, O, R, RM, 0, LTS>(a, TI, S0, q, l, ev, r, valid, acc, upA, TIh);
       localFace<T, O, R, RM, 1, LTS>(a, TI, S0, q, l, ev, r, valid, acc, upA, TIh);
