@@ -1323,8 +1323,9 @@ __device__ __forceinline__ void neighItem(const StepArgs<T> &a, unsigned char *b
   neighApply<T, O, R, RM, FA>(a, S, NS::fs(base, slot), q, l, e, valid, cur, acc, upA);
 }
 
-// PM: the face buffers hold projections pre-mixed with this element's flux solvers (the GTS local
-// kernel writes them so); otherwise the mix happens here (LTS, attenuation)
+// PM: the face buffers hold projections pre-mixed with this element's flux solvers (the local
+// kernels write them so where their buffers fit); otherwise the mix happens here (attenuation,
+// configurations without room for pre-mixing)
 template <typename T, int O, int R, int RM, bool PM>
 __global__ void __launch_bounds__(Geo<T, O, R, RM>::NT, Geo<T, O, R, RM>::minCtasNeigh) kNeigh(StepArgs<T> a) {
   using G = Geo<T, O, R, RM>;
