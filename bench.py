@@ -596,6 +596,15 @@ def main():
         fp64 = {"value": v64 * ws, "unit": UNIT, "ms_per_step": y0.elapsed_time(y1) / k64,
                 "config": {"order": prob.order, "runs": 1, "precision": "fp64"},
                 "batched_fp32_over_plain_fp64": value / (v64 * ws)}
+        # the plain path against both ceilings: HBM (its algorithmic bytes per element) and the FP64
+        # pipe (dense-equivalent flops over the nominal SMs x 64 FP64 FMA lanes x 2 x max SM clock)
+        alg64 = algorithmic(p64, 64)
+        sms = torch.cuda.get_device_properties(torch.cuda.current_device()).multi_processor_count
+        fp64_peak = sms * 64 * 2 * peak_clock_mhz() * 1e6 / 1e12
+        tfl = (alg64["local_flops"] + alg64["neigh_flops"]) * v64 / 1e12
+        gbs = (alg64["local_bytes"] + alg64["neigh_bytes"]) * v64 / 1e9
+        fp64["fp64_pipe"] = {"dense_equivalent_tflops": tfl, "nominal_peak_tflops": fp64_peak, "frac": tfl / fp64_peak}
+        fp64["hbm"] = {"achieved_gbs": gbs, "peak": peak, "frac": gbs / peak, "peak_source": peak_src}
         s64.close()
 
     cpu = None
