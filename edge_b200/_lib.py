@@ -38,6 +38,7 @@ _SIGS = {
     "edge_setup_fs_pair": (C.c_int, [dbl] * 6 + [vp, vp, vp, C.c_int, vp, vp, vp, vp]),
     "edge_b200_create": (C.c_int, [vp, i64, vp]),
     "edge_b200_kernel_config": (C.c_int, [vp, vp]),
+    "edge_b200_set_fused": (C.c_int, [vp, C.c_int]),
     "edge_b200_batch_create": (C.c_int, [vp, C.c_int, vp, vp, vp]),
     "edge_b200_batch_set_active": (C.c_int, [vp, vp]),
     "edge_b200_batch_step": (C.c_int, [vp, C.c_int]),

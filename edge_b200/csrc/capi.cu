@@ -208,6 +208,14 @@ struct edge_b200_ctx {
   // rebuilt before the next GTS step after the mesh or the element data changed
   DevBuf fsLR;
   bool fsLRStale = true;
+  // fused GTS steps (pre-mixing configurations, no halo): within one multi-step call each local
+  // step also runs the previous step's neighbour step, so the face projections alternate between
+  // two buffers (faceCur holds the last written); the last step's neighbour step runs on its own at
+  // the end of the call (flush), so between calls nothing is pending
+  DevBuf faceAlt;
+  int faceCur = 0;
+  bool pending = false, fusedOn = true;
+  void *faceBuf(int i) const { return i ? faceAlt.p : face; }
   // sources
   SrcArgs src{};
   DevBuf srcMem[10];
@@ -389,6 +397,16 @@ struct edge_b200_ctx {
     return cudaEventRecord(evD2H[k], d2h);
   }
 
+  // runs the pending neighbour step of the last fused step
+  cudaError_t flush() {
+    if (!pending) return cudaSuccess;
+    StepArgsRaw a = args(0);
+    cudaError_t e = launch(1, [&] { return ks->neigh(a, stream); });
+    if (e) return e;
+    pending = false;
+    return cudaSuccess;
+  }
+
   cudaError_t ensureFsLR() {
     if (!ks->premix() || !fsLRStale) return cudaSuccess;
     const int P = ks->fsPairStride();
@@ -414,7 +432,7 @@ struct edge_b200_ctx {
     a.dofsE = dofsE;
     a.dofsA = dofsA;
     a.tDofs = keepTDofs ? tDofs : nullptr;
-    a.face = face;
+    a.face = faceBuf(faceCur);
     a.starE = starE;
     a.starA = starA;
     a.srcA = srcA;
@@ -569,6 +587,7 @@ int edge_b200_upload_element_data(edge_b200_ctx *ctx, const double *star_e, cons
 
 int edge_b200_upload_dofs(edge_b200_ctx *ctx, const void *dofs_e, const void *dofs_a) {
   if (!ctx || !dofs_e || (ctx->cfg.n_rms && !dofs_a)) return EDGE_B200_EINVAL;
+  ctx->pending = false;  // the new DOFs replace the ones a pending neighbour step would complete
   EDGE_CUDA(ctx->uploadRows(ctx->dofsE, dofs_e, 9), "upload dofsE");
   if (ctx->cfg.n_rms) EDGE_CUDA(ctx->uploadRows(ctx->dofsA, dofs_a, 6 * ctx->cfg.n_rms), "upload dofsA");
   return EDGE_B200_OK;
@@ -576,6 +595,7 @@ int edge_b200_upload_dofs(edge_b200_ctx *ctx, const void *dofs_e, const void *do
 
 int edge_b200_download_dofs(edge_b200_ctx *ctx, void *dofs_e, void *dofs_a) {
   if (!ctx || !dofs_e) return EDGE_B200_EINVAL;
+  EDGE_CUDA(ctx->flush(), "pending neighbour step");
   EDGE_CUDA(ctx->downloadRows(dofs_e, ctx->dofsE, 9), "download dofsE");
   if (ctx->cfg.n_rms && dofs_a) EDGE_CUDA(ctx->downloadRows(dofs_a, ctx->dofsA, 6 * ctx->cfg.n_rms), "download dofsA");
   return EDGE_B200_OK;
@@ -584,6 +604,7 @@ int edge_b200_download_dofs(edge_b200_ctx *ctx, void *dofs_e, void *dofs_a) {
 int edge_b200_upload_dofs_async(edge_b200_ctx *ctx, const void *dofs_e, const void *dofs_a) {
   if (!ctx || !dofs_e || (ctx->cfg.n_rms && !dofs_a)) return EDGE_B200_EINVAL;
   EDGE_CUDA(ctx->ensureAsync(), "async transfers");
+  ctx->pending = false;
   EDGE_CUDA(ctx->uploadRowsAsync(ctx->dofsE, dofs_e, 9), "upload dofsE");
   if (ctx->cfg.n_rms) EDGE_CUDA(ctx->uploadRowsAsync(ctx->dofsA, dofs_a, 6 * ctx->cfg.n_rms), "upload dofsA");
   return EDGE_B200_OK;
@@ -592,6 +613,7 @@ int edge_b200_upload_dofs_async(edge_b200_ctx *ctx, const void *dofs_e, const vo
 int edge_b200_download_dofs_async(edge_b200_ctx *ctx, void *dofs_e, void *dofs_a) {
   if (!ctx || !dofs_e) return EDGE_B200_EINVAL;
   EDGE_CUDA(ctx->ensureAsync(), "async transfers");
+  EDGE_CUDA(ctx->flush(), "pending neighbour step");
   EDGE_CUDA(ctx->downloadRowsAsync(dofs_e, ctx->dofsE, 9), "download dofsE");
   if (ctx->cfg.n_rms && dofs_a)
     EDGE_CUDA(ctx->downloadRowsAsync(dofs_a, ctx->dofsA, 6 * ctx->cfg.n_rms), "download dofsA");
@@ -615,6 +637,7 @@ int edge_b200_join_transfers(edge_b200_ctx *ctx, int after_stream) {
 
 int edge_b200_set_run_dofs(edge_b200_ctx *ctx, int run, const void *dofs_e, const void *dofs_a) {
   if (!ctx || run < 0 || run >= ctx->cfg.n_runs) return EDGE_B200_EINVAL;
+  EDGE_CUDA(ctx->flush(), "pending neighbour step");
   EDGE_CUDA(ctx->ensureStage(), "set run dofs");
   const int rm = ctx->cfg.n_rms;
   for (int part = 0; part < (rm ? 2 : 1); part++) {
@@ -758,6 +781,17 @@ static int runSteps(edge_b200_ctx *ctx, double t, double dt, int n_steps, int ph
   ctx->lastLts = false;
   cudaStream_t s = ctx->stream;
   EDGE_CUDA(ctx->ensureFsLR(), "flux-solver pairs");
+  // whole GTS steps of a pre-mixing configuration without halo parts fold each neighbour step
+  // into the next local step; the split phases run the neighbour step on its own
+  const bool fused = phases == 3 && ctx->fusedOn && ctx->ks->fusedSupported() && ctx->nOwned == ctx->nEl;
+  if (fused) {
+    if (!ctx->faceAlt.p) {
+      EDGE_CUDA(ctx->faceAlt.fit(ctx->faceCount() * ctx->realSize), "second face buffer");
+      EDGE_CUDA(cudaMemsetAsync(ctx->faceAlt.p, 0, ctx->faceCount() * ctx->realSize, s), "second face buffer");
+    }
+  } else {
+    EDGE_CUDA(ctx->flush(), "pending neighbour step");
+  }
   // receiver samples of every step (Receivers::getRecvTimeRel, io/Receivers.cpp:235-248)
   std::vector<int> stepFirst(n_steps + 1, 0);
   std::vector<double> tau;
@@ -798,6 +832,11 @@ static int runSteps(edge_b200_ctx *ctx, double t, double dt, int n_steps, int ph
   double ts = t;
   for (int st = 0; st < n_steps; st++) {
     const int ns = stepFirst[st + 1] - stepFirst[st];
+    if (fused) {
+      // the previous step's projections (their neighbour step still pending) in, this step's out
+      a.faceIn = ctx->pending ? ctx->faceBuf(ctx->faceCur) : nullptr;
+      a.face = ctx->faceBuf(ctx->faceCur ^ 1);
+    }
     if ((phases & 1) && ns > 0 && ctx->nRecvGrp > 0) {
       RecvArgs r;
       r.grpEl = ctx->grpEl.as<int64_t>();
@@ -813,7 +852,8 @@ static int runSteps(edge_b200_ctx *ctx, double t, double dt, int n_steps, int ph
       ctx->launches++;
     }
     if (phases & 1) {
-      EDGE_CUDA(ctx->launch(0, [&] { return ctx->ks->local(a, s); }), "local kernel");
+      EDGE_CUDA(ctx->launch(0, [&] { return fused ? ctx->ks->localFused(a, s) : ctx->ks->local(a, s); }),
+                "local kernel");
       ctx->launches++;
       if (ctx->src.nGrp > 0) {
         SrcArgs sa = ctx->src;
@@ -823,12 +863,27 @@ static int runSteps(edge_b200_ctx *ctx, double t, double dt, int n_steps, int ph
         ctx->launches++;
       }
     }
-    if (phases & 2) {
+    if (fused) {
+      ctx->faceCur ^= 1;
+      ctx->pending = true;
+    } else if (phases & 2) {
       EDGE_CUDA(ctx->launch(1, [&] { return ctx->ks->neigh(a, s); }), "neighbour kernel");
       ctx->launches++;
     }
     ts += dt;
   }
+  // the last step's neighbour step on its own: the DOFs are complete when the call returns
+  if (fused && ctx->pending) {
+    EDGE_CUDA(ctx->flush(), "neighbour kernel");
+    ctx->launches++;
+  }
+  return EDGE_B200_OK;
+}
+
+int edge_b200_set_fused(edge_b200_ctx *ctx, int enable) {
+  if (!ctx) return EDGE_B200_EINVAL;
+  if (!enable) EDGE_CUDA(ctx->flush(), "pending neighbour step");
+  ctx->fusedOn = enable != 0;
   return EDGE_B200_OK;
 }
 
@@ -843,6 +898,7 @@ int edge_b200_step_phase(edge_b200_ctx *ctx, double t, double dt, int phase) {
 
 int edge_b200_set_owned(edge_b200_ctx *ctx, int64_t n_owned) {
   if (!ctx || n_owned < 0 || n_owned > ctx->nEl || ctx->nTg > 1) return EDGE_B200_EINVAL;
+  EDGE_CUDA(ctx->flush(), "pending neighbour step");
   ctx->nOwned = n_owned;
   return EDGE_B200_OK;
 }
@@ -857,7 +913,7 @@ static int packFaces(edge_b200_ctx *ctx, int n, const int32_t *slots, void *buf,
   const int64_t blk16 = edge_b200_face_block_bytes(ctx) / 16;
   const int64_t total = (int64_t)n * blk16;
   const int grid = (int)std::min<int64_t>((total + 255) / 256, 148 * 16);
-  kFacePack<<<grid, 256, 0, ctx->stream>>>(static_cast<uint4 *>(ctx->face), static_cast<uint4 *>(buf), slots,
+  kFacePack<<<grid, 256, 0, ctx->stream>>>(static_cast<uint4 *>(ctx->faceBuf(ctx->faceCur)), static_cast<uint4 *>(buf), slots,
                                              n, blk16, ctx->nEl * 4, pack);
   EDGE_CUDA(cudaGetLastError(), pack ? "pack faces" : "unpack faces");
   return EDGE_B200_OK;
@@ -933,6 +989,7 @@ int edge_b200_step_lts(edge_b200_ctx *ctx, double t, double dt_fun, int n_cycles
   if (!ctx || !(dt_fun > 0) || n_cycles < 0 || ctx->nTg < 1) return EDGE_B200_EINVAL;
   if (!ctx->meshSet || !ctx->dataSet) return EDGE_B200_EINVAL;
   if (!ctx->ks->ltsSupported()) return EDGE_B200_ENOTSUP;
+  EDGE_CUDA(ctx->flush(), "pending neighbour step");
   EDGE_CUDA(ctx->ensureFsLR(), "flux-solver pairs");
   ctx->lastLts = true;
   const int G = ctx->nTg;
@@ -1091,6 +1148,7 @@ int edge_b200_error_norms(edge_b200_ctx *ctx, double t, int n_waves, const doubl
       !qp_xi || !qp_w || !qp_basis || ctx->B > 64)
     return EDGE_B200_EINVAL;
   const int B = ctx->B, R = ctx->cfg.n_runs;
+  EDGE_CUDA(ctx->flush(), "pending neighbour step");
   std::vector<PlaneWave> pw(std::max(n_waves, 1));
   for (int w = 0; w < n_waves; w++) {
     const double *src = waves + 15 * w;  // k[3], omega, phase, amp[9], run
@@ -1145,6 +1203,7 @@ int edge_b200_error_norms(edge_b200_ctx *ctx, double t, int n_waves, const doubl
 
 int edge_b200_wavefield(edge_b200_ctx *ctx, float *out) {
   if (!ctx || !out) return EDGE_B200_EINVAL;
+  EDGE_CUDA(ctx->flush(), "pending neighbour step");
   const size_t n = (size_t)ctx->nEl * 9 * ctx->cfg.n_runs;
   cudaStream_t s = ctx->stream;
   EDGE_CUDA(ctx->norms.fit(n * sizeof(float)), "wave field");
@@ -1171,6 +1230,7 @@ int edge_b200_sync(edge_b200_ctx *ctx) {
 
 int edge_b200_device_dofs(edge_b200_ctx *ctx, void **dofs_e, void **dofs_a, void **tdofs) {
   if (!ctx) return EDGE_B200_EINVAL;
+  EDGE_CUDA(ctx->flush(), "pending neighbour step");
   if (dofs_e) *dofs_e = ctx->dofsE;
   if (dofs_a) *dofs_a = ctx->dofsA;
   if (tdofs) *tdofs = ctx->tDofs;
@@ -1179,8 +1239,9 @@ int edge_b200_device_dofs(edge_b200_ctx *ctx, void **dofs_e, void **dofs_a, void
 
 int64_t edge_b200_last_launches(const edge_b200_ctx *ctx) { return ctx ? ctx->launches : -1; }
 
-int edge_b200_kernel_config(const edge_b200_ctx *ctx, int32_t info[5]) {
+int edge_b200_kernel_config(const edge_b200_ctx *ctx, int32_t info[6]) {
   if (!ctx || !info) return EDGE_B200_EINVAL;
+  info[5] = (ctx->fusedOn && ctx->ks->fusedSupported() && ctx->nOwned == ctx->nEl) ? 1 : 0;
   info[0] = ctx->ks->elementsPerCta();
   info[1] = ctx->ks->premix() ? 1 : 0;
   info[2] = ctx->ks->fsPairStride();
@@ -1340,7 +1401,8 @@ int edge_b200_batch_create(edge_b200_ctx *const *ctxs, int n, const double *t0, 
   // the contexts' pending work (uploads) and their flux-solver pairs come before the first step
   for (int k = 0; k < n && !e; k++) {
     edge_b200_ctx *c = ctxs[k];
-    e = c->ensureFsLR();
+    e = c->flush();
+    if (!e) e = c->ensureFsLR();
     if (!e) e = cudaEventRecord(b->joins[k], c->stream);
     if (!e) e = cudaStreamWaitEvent(b->origin, b->joins[k], 0);
   }
@@ -1391,6 +1453,7 @@ int edge_b200_autotune(edge_b200_ctx *ctx, double dt, int32_t caps[2]) {
   if (!ctx || !(dt > 0)) return EDGE_B200_EINVAL;
   if (!ctx->meshSet || !ctx->dataSet || ctx->timing) return EDGE_B200_EINVAL;
   cudaStream_t s = ctx->stream;
+  EDGE_CUDA(ctx->flush(), "pending neighbour step");
   EDGE_CUDA(ctx->ensureFsLR(), "flux-solver pairs");
   const size_t rs = ctx->realSize;
   const size_t bytesE = ctx->dofsCount() * rs, bytesA = ctx->dofsACount() * rs;

@@ -40,6 +40,7 @@ class KernelSetImpl final : public KernelSet {
     b.halfIdx = a.halfIdx;
     b.firstTs = a.firstTs;
     b.fsLR = static_cast<const T *>(a.fsLR);
+    b.faceIn = static_cast<const T *>(a.faceIn);
     return b;
   }
   static constexpr size_t smemLocal() { return G::smemLocalGts; }
@@ -58,6 +59,11 @@ class KernelSetImpl final : public KernelSet {
       return e;
     if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occLocal_, kLocal<T, O, R, RM, 0>, G::NT, smemLocal())))
       return e;
+    if constexpr (G::premix) {
+      if ((e = cudaFuncSetAttribute(kLocal<T, O, R, RM, 0, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    (int)smemLocal())))
+        return e;
+    }
     if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occNeigh_, kNeigh<T, O, R, RM, G::premix>, G::NT, smemNeigh())))
       return e;
     if constexpr (G::premixLts != G::premix) {
@@ -103,6 +109,16 @@ class KernelSetImpl final : public KernelSet {
     kLocal<T, O, R, RM, 0><<<grid(a.elCount, ctasLocal()), G::NT, smemLocal(), s>>>(cast(a));
     return cudaGetLastError();
   }
+  cudaError_t localFused(const StepArgsRaw &a, cudaStream_t s) override {
+    if constexpr (G::premix) {
+      if (a.elCount < 1) return cudaSuccess;
+      kLocal<T, O, R, RM, 0, true><<<grid(a.elCount, ctasLocal()), G::NT, smemLocal(), s>>>(cast(a));
+      return cudaGetLastError();
+    } else {
+      return cudaErrorNotSupported;
+    }
+  }
+  bool fusedSupported() const override { return G::premix; }
   cudaError_t localLts(const StepArgsRaw &a, cudaStream_t s) override {
     if constexpr (G::ltsOk) {
       if (a.elCount < 1) return cudaSuccess;

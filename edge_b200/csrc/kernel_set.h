@@ -27,6 +27,8 @@ struct StepArgsRaw {
   // per element face fsE[0] and the face reader's fsE[1] in the configuration's precision, each
   // padded to 16 bytes: [nEl][4][2][fsPairStride()] (premix)
   const void *fsLR = nullptr;
+  // fused GTS steps: the previous step's face projections whose neighbour step is still pending
+  const void *faceIn = nullptr;
 };
 
 class KernelSet {
@@ -34,6 +36,9 @@ class KernelSet {
   virtual ~KernelSet() {}
   virtual cudaError_t init(int device) = 0;  // sets smem attributes, sizes the persistent grids
   virtual cudaError_t local(const StepArgsRaw &a, cudaStream_t s) = 0;
+  // the local step with the pending neighbour step of the previous one folded in (a.faceIn)
+  virtual cudaError_t localFused(const StepArgsRaw &a, cudaStream_t s) = 0;
+  virtual bool fusedSupported() const = 0;
   // local step with the LTS face buffers (the half-step time integral needs one more tile)
   virtual cudaError_t localLts(const StepArgsRaw &a, cudaStream_t s) = 0;
   // the same without half-step integrals, for elements without a smaller neighbour (no extra tile)

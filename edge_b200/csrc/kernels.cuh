@@ -56,6 +56,10 @@ struct StepArgs {
   // free surface; zeros for outflow) in T, each padded to 16 bytes (Geo::FSP): [nEl][4][2][FSP];
   // null: gathered through the connectivity
   const T *fsLR;
+  // fused GTS steps (kLocal<..., FUSED>, kRecv): the previous step's pre-mixed face projections,
+  // whose neighbour fluxes are added to the DOF rows before the recursion (the previous step's
+  // neighbour step runs here), or null when none are pending
+  const T *faceIn;
 };
 enum { LTS_HAS_LARGER = 1, LTS_HAS_SMALLER = 2 };
 enum { LTS_EQ = 0, LTS_GT = 1, LTS_LT = 2 };
@@ -710,6 +714,88 @@ __device__ __forceinline__ void issueMixFs(const StepArgs<T> &a, T *buf, int64_t
   }
 }
 
+// face connectivity of one element (all four faces): the face slot each face gathers from
+// (neighbour * 4 + its face id, or a compact LTS slot * 4 + face id), and one byte per face for the
+// buffer (LTS relation), the vertex id and the face type
+struct FaceMeta {
+  int32_t src[4];
+  uint32_t rel, vi, ty;
+  template <typename T>
+  __device__ __forceinline__ void load(const StepArgs<T> &a, int64_t e, bool valid) {
+    if (valid) {
+      const int4 n = __ldg(reinterpret_cast<const int4 *>(a.elFaEl) + e);
+      const uint32_t fo = __ldg(reinterpret_cast<const uint32_t *>(a.fId) + e);
+      vi = __ldg(reinterpret_cast<const uint32_t *>(a.vId) + e);
+      ty = __ldg(reinterpret_cast<const uint32_t *>(a.faType) + e);
+      rel = a.ltsRel ? __ldg(reinterpret_cast<const uint32_t *>(a.ltsRel) + e) : 0u;
+      const int32_t ne[4] = {n.x, n.y, n.z, n.w};
+#pragma unroll
+      for (int f = 0; f < 4; f++) {
+        int32_t slotEl = ne[f];
+        const int rf = (rel >> (8 * f)) & 0xff;
+        if (((ty >> (8 * f)) & 0xff) == FT_INNER && rf != LTS_EQ)
+          slotEl = __ldg((rf == LTS_GT ? a.sumIdx : a.halfIdx) + ne[f]);
+        src[f] = slotEl * 4 + int32_t((fo >> (8 * f)) & 0xff);
+      }
+    } else {
+      src[0] = src[1] = src[2] = src[3] = 0;
+      rel = vi = 0;
+      ty = 0x02020202u;  // outflow on every face: nothing to gather or add
+    }
+  }
+  __device__ __forceinline__ int type(int f) const { return (ty >> (8 * f)) & 0xff; }
+  __device__ __forceinline__ int relation(int f) const { return (rel >> (8 * f)) & 0xff; }
+  __device__ __forceinline__ int vert(int f) const { return (vi >> (8 * f)) & 0xff; }
+};
+
+// the reflection (OriMul index) taking the neighbour's projection at its face fo (in that face's
+// basis) to this element's face FA basis, for the neighbour's vertex id at FA (kFacePerm)
+template <int O, int FA>
+__device__ __forceinline__ int neighOri(const FaceMeta &m) {
+  return kFacePerm[O - 2][m.src[FA] & 3][FA][m.vert(FA)];
+}
+
+
+// the neighbour flux of face FA through pre-mixed projections read straight from global memory
+// (this warp's quantity row, this lane's run): the arithmetic of the neighbour kernel's
+// neighApplyMixed, for kernels that fold a pending neighbour step into their DOF rows
+template <typename T, int O, int R, int RM, int FA>
+__device__ __forceinline__ void neighFluxFace(const T *faceIn, const FaceMeta &m, int64_t e, int q, int r,
+                                              bool valid, T *acc) {
+  using G = Geo<T, O, R, RM>;
+  constexpr int F = G::F;
+  const int ty = m.type(FA);
+  if (!valid || ty == FT_OUTFLOW || q >= 9) return;
+  const int64_t src = ty == FT_INNER ? int64_t(m.src[FA]) : e * 4 + FA;
+  T x[F];
+  ldRowG<T, F>(gRow<T, R, G::GF>(faceIn, src, 9, q, r), x, true);
+  if (ty == FT_INNER) {
+    T o[F];
+#pragma unroll
+    for (int j = 0; j < F; j++) o[j] = T(0);
+    const int v = neighOri<O, FA>(m);
+    if (v == 0)
+      OriMul<O, 0>::template run<T>(x, o);
+    else if (v == 1)
+      OriMul<O, 1>::template run<T>(x, o);
+    else
+      OriMul<O, 2>::template run<T>(x, o);
+    FluxTMul<O, FA>::template run<T>(o, acc);
+  } else {
+    FluxTMul<O, FA>::template run<T>(x, acc);
+  }
+}
+template <typename T, int O, int R, int RM>
+__device__ __forceinline__ void neighFluxDirect(const StepArgs<T> &a, const T *faceIn, int64_t e, int q, int r,
+                                                bool valid, T *acc) {
+  FaceMeta m;
+  m.load(a, e, valid);
+  neighFluxFace<T, O, R, RM, 0>(faceIn, m, e, q, r, valid, acc);
+  neighFluxFace<T, O, R, RM, 1>(faceIn, m, e, q, r, valid, acc);
+  neighFluxFace<T, O, R, RM, 2>(faceIn, m, e, q, r, valid, acc);
+  neighFluxFace<T, O, R, RM, 3>(faceIn, m, e, q, r, valid, acc);
+}
+
 // ------------------------------------------------------------------------------------------------
 // local step: CK, volume, local surface, face projections (AderDg::local, AderDg.hpp:338-534)
 // ------------------------------------------------------------------------------------------------
@@ -867,7 +953,9 @@ __device__ __forceinline__ void localFace(const StepArgs<T> &a, const T *TI, T *
 
 // LTS as in localFace; mode 2 keeps the half-step integral in one more tile (one CTA per SM), mode
 // 1 runs on the elements of a time group without a smaller neighbour
-template <typename T, int O, int R, int RM, int LTS>
+// FUSED (GTS, pre-mixing configurations): the previous step's neighbour fluxes (a.faceIn, when
+// pending) are added to each group's DOF rows first, and the completed rows stored back
+template <typename T, int O, int R, int RM, int LTS, bool FUSED = false>
 __global__ void __launch_bounds__(Geo<T, O, R, RM>::NT, LTS == 2 ? 1 : Geo<T, O, R, RM>::minCtasLocal)
     kLocal(StepArgs<T> a) {
   using G = Geo<T, O, R, RM>;
@@ -922,6 +1010,20 @@ __global__ void __launch_bounds__(Geo<T, O, R, RM>::NT, LTS == 2 ? 1 : Geo<T, O,
         else
 #pragma unroll
           for (int n = 0; n < B; n++) v[n] = T(0);
+        if constexpr (FUSED) {
+          if (a.faceIn) {
+            neighFluxDirect<T, O, R, RM>(a, a.faceIn, ev, q, r, valid, v);
+            // the completed rows back to the DOFs (the volume integral reads them again)
+            T *p = rowPtr<T, SB>(X, q, l);
+            stRow<T, B>(p, v);
+#pragma unroll
+            for (int n = B; n < G::GB; n++) p[n] = T(0);
+            __syncwarp();
+            if (valid)
+              storeRowsCoalesced<T, R, G::GB, SB>(X, a.dofsE + (e * 9 + q) * int64_t(R * G::GB), q, eo, r);
+            __syncwarp();
+          }
+        }
         stRow<T, B>(rowPtr<T, SB>(X, q, l), v);
       } else {
         ldRowG<T, B>(gRow<T, R, G::GB>(a.dofsE, ev, 9, q, r), v, valid);
@@ -1082,47 +1184,6 @@ __global__ void __launch_bounds__(Geo<T, O, R, RM>::NT, LTS == 2 ? 1 : Geo<T, O,
 // coalesced stores and the next group's DOF rows arrive in it asynchronously. Per item: wait for its copies, rotate the neighbour's rows into this element's face
 // orientation in place, one CTA barrier, issue the copies of the item NSN - 1 ahead into the slot
 // the previous item released, then mix quantities and apply fluxT.
-
-// face connectivity of one element (all four faces): the face slot each face gathers from
-// (neighbour * 4 + its face id, or a compact LTS slot * 4 + face id), and one byte per face for the
-// buffer (LTS relation), the vertex id and the face type
-struct FaceMeta {
-  int32_t src[4];
-  uint32_t rel, vi, ty;
-  template <typename T>
-  __device__ __forceinline__ void load(const StepArgs<T> &a, int64_t e, bool valid) {
-    if (valid) {
-      const int4 n = __ldg(reinterpret_cast<const int4 *>(a.elFaEl) + e);
-      const uint32_t fo = __ldg(reinterpret_cast<const uint32_t *>(a.fId) + e);
-      vi = __ldg(reinterpret_cast<const uint32_t *>(a.vId) + e);
-      ty = __ldg(reinterpret_cast<const uint32_t *>(a.faType) + e);
-      rel = a.ltsRel ? __ldg(reinterpret_cast<const uint32_t *>(a.ltsRel) + e) : 0u;
-      const int32_t ne[4] = {n.x, n.y, n.z, n.w};
-#pragma unroll
-      for (int f = 0; f < 4; f++) {
-        int32_t slotEl = ne[f];
-        const int rf = (rel >> (8 * f)) & 0xff;
-        if (((ty >> (8 * f)) & 0xff) == FT_INNER && rf != LTS_EQ)
-          slotEl = __ldg((rf == LTS_GT ? a.sumIdx : a.halfIdx) + ne[f]);
-        src[f] = slotEl * 4 + int32_t((fo >> (8 * f)) & 0xff);
-      }
-    } else {
-      src[0] = src[1] = src[2] = src[3] = 0;
-      rel = vi = 0;
-      ty = 0x02020202u;  // outflow on every face: nothing to gather or add
-    }
-  }
-  __device__ __forceinline__ int type(int f) const { return (ty >> (8 * f)) & 0xff; }
-  __device__ __forceinline__ int relation(int f) const { return (rel >> (8 * f)) & 0xff; }
-  __device__ __forceinline__ int vert(int f) const { return (vi >> (8 * f)) & 0xff; }
-};
-
-// the reflection (OriMul index) taking the neighbour's projection at its face fo (in that face's
-// basis) to this element's face FA basis, for the neighbour's vertex id at FA (kFacePerm)
-template <int O, int FA>
-__device__ __forceinline__ int neighOri(const FaceMeta &m) {
-  return kFacePerm[O - 2][m.src[FA] & 3][FA][m.vert(FA)];
-}
 
 template <typename T, int O, int R, int RM>
 struct NeighSlots {
@@ -1481,6 +1542,9 @@ __global__ void __launch_bounds__(Geo<T, O, R, RM>::NT) kRecv(StepArgs<T> a, Rec
   if (q < 9) {
     T v[B];
     ldRowG<T, B>(gRow<T, R, G::GB>(a.dofsE, ev, 9, q, r), v, valid);
+    // a pending neighbour step (fused GTS steps) completes the rows first
+    if constexpr (RM == 0)
+      if (a.faceIn) neighFluxDirect<T, O, R, RM>(a, a.faceIn, ev, q, r, valid, v);
     stRow<T, B>(rowPtr<T, SB>(X, q, l), v);
     if constexpr (G::tiSmem)
       stRow<T, B>(rowPtr<T, SB>(TI, q, l), zero);

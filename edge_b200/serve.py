@@ -80,13 +80,14 @@ class MeshCache:
 
 
 def pool_bytes(n_el, order, runs, precision):
-    """Device memory of a pool context (DOFs, face projections, staging, element data: star
-    matrices, flux solvers and the flux-solver pairs of the pre-mixed face projections)."""
+    """Device memory of a pool context (DOFs, two face-projection buffers of the fused steps,
+    staging, element data: star matrices, flux solvers and the flux-solver pairs of the pre-mixed
+    face projections)."""
     p = 8 if precision == 64 else 4
     w = 16 // p
     gb = math.ceil(host.n_modes(order) / w) * w
     gf = math.ceil(host.n_face_modes(order) / w) * w
-    return n_el * (9 * runs * gb * p * 2 + 36 * runs * gf * p + 9 * host.n_modes(order) * runs * p
+    return n_el * (9 * runs * gb * p * 2 + 2 * 36 * runs * gf * p + 9 * host.n_modes(order) * runs * p
                    + (72 + 648) * 8 + 4 * 2 * 84 * p + 28)
 
 

@@ -273,14 +273,24 @@ int64_t edge_b200_last_launches(const edge_b200_ctx *ctx);
  * 2 = sources, 3 = receivers, the summed milliseconds and launch counts since timing was enabled
  * (synchronises the stream). */
 int edge_b200_set_timing(edge_b200_ctx *ctx, int enable);
+/* Fused GTS steps (1, the default; 0 turns them off): in configurations that pre-mix their face
+ * projections and without halo parts, edge_b200_step with n_steps > 1 runs each step's neighbour
+ * step inside the next step's local kernel (which adds the previous projections' lifted fluxes to
+ * each element's DOF rows before its recursion; the receiver kernel does the same for its
+ * elements), with the face projections alternating between two buffers; the last step's
+ * neighbour step runs on its own before the call returns, so the DOFs are complete between calls.
+ * Same arithmetic as the separate neighbour kernel: the results are identical. No counterpart in
+ * the reference. */
+int edge_b200_set_fused(edge_b200_ctx *ctx, int enable);
 int edge_b200_kernel_times(edge_b200_ctx *ctx, double *ms, int64_t *launches);
 /* Launch shape of the context's compiled configuration (no counterpart in the reference, whose
  * kernels run one element per thread team): info[0] elements per CTA, info[1] 1 when GTS face
  * projections leave the local kernel pre-mixed with the reading element's flux solver (the local
  * kernel then reads per element face the padded pair [2][info[2]] of flux solvers in the
  * configuration's precision, the neighbour kernel none), info[3] / info[4] persistent CTAs of the
- * local / neighbour kernel. */
-int edge_b200_kernel_config(const edge_b200_ctx *ctx, int32_t info[5]);
+ * local / neighbour kernel, info[5] 1 when multi-step calls fuse each neighbour step into the next
+ * local kernel (edge_b200_set_fused). */
+int edge_b200_kernel_config(const edge_b200_ctx *ctx, int32_t info[6]);
 
 /* No counterpart in the reference. n_steps GTS steps (local kernel, then neighbour kernel; no
  * sources, no receivers) over caller-owned DEVICE arrays, without allocating anything: no

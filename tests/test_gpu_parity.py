@@ -131,8 +131,9 @@ def test_kernel_config_reports_premix():
     for (prec, order, runs, rm), want in cases:
         prob = small_problem(n=2, order=order, runs=runs, rm=rm, n_steps=1, source=None, n_receivers=0)
         s = Solver(prob, precision=prec)
-        info = np.zeros(5, np.int32)
+        info = np.zeros(6, np.int32)
         assert lib().edge_b200_kernel_config(s._h, ptr(info)) == 0
         assert tuple(int(x) for x in info[:3]) == want, (prec, order, runs, rm, info)
         assert info[3] >= 148 and info[4] >= 148
+        assert info[5] == info[1]  # multi-step calls fuse the neighbour step where projections are pre-mixed
         s.close()
