@@ -2,9 +2,9 @@
 simulations over different meshes, orders, fused-run counts and physics on one GPU).
 
 Each simulation keeps its own context (``Solver``); ``Batch`` hands the contexts to
-``edge_b200_batch_create``, which captures one batch step (every active context's local, source
-and neighbour kernels, each context on a stream of its own) into a CUDA graph and replays it per
-step. Simulations of different lengths drop out as they finish: ``schedule`` splits a run into
+``edge_b200_batch_create``, which captures two batch steps (every active context's kernels, each
+context on a stream of its own; fused steps where the context's own steps are fused) into a CUDA
+graph and replays it. Simulations of different lengths drop out as they finish: ``schedule`` splits a run into
 segments with a fixed active set (the graph is captured again at each change). Optionally each
 context's launch shape is autotuned first (``edge_b200_autotune``).
 

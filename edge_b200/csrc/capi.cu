@@ -1280,9 +1280,9 @@ const char *edge_b200_last_error(const edge_b200_ctx *ctx) { return ctx ? ctx->e
 // autotuner
 // ------------------------------------------------------------------------------------------------
 namespace {
-__global__ void kAdvanceSteps(int64_t *steps, const int32_t *active, int n) {
+__global__ void kAdvanceSteps(int64_t *steps, const int32_t *active, int n, int by) {
   for (int k = threadIdx.x; k < n; k += blockDim.x)
-    if (active[k]) steps[k]++;
+    if (active[k]) steps[k] += by;
 }
 }  // namespace
 
@@ -1296,7 +1296,7 @@ struct edge_b200_batch {
   cudaEvent_t fork = nullptr;
   int64_t *steps = nullptr;    // device: steps taken per context
   int32_t *activeDev = nullptr;
-  cudaGraphExec_t exec = nullptr;
+  cudaGraphExec_t exec = nullptr;  // two batch steps
   bool dirty = true;
   std::string err;
   ~edge_b200_batch() {
@@ -1311,7 +1311,56 @@ struct edge_b200_batch {
     dfree(steps);
     dfree(activeDev);
   }
-  // one GTS step of every active context (local, sources, neighbour), each on its own stream
+  // contexts whose GTS steps fold each neighbour step into the next local step (as edge_b200_step
+  // does): within a call their steps alternate between the two face buffers
+  static bool fused(const edge_b200_ctx *c) { return c->fusedOn && c->ks->fusedSupported(); }
+  // one GTS step of context k on its stream, its sources at t0 + tOff + steps[k] * dt. kind 0: a
+  // call's first step (fused contexts: nothing pending, projections out to faceAlt); 1: fused,
+  // pending projections in faceAlt, out to face; 2: in face, out to faceAlt. Other contexts take
+  // a whole separate-kernel step (local, sources, neighbour) in each kind.
+  cudaError_t issueStep(size_t k, int kind, double tOff) {
+    edge_b200_ctx *ctx = ctxs[k];
+    cudaStream_t s = streams[k];
+    StepArgsRaw a = ctx->args(dt[k]);
+    const bool fu = fused(ctx);
+    cudaError_t c;
+    if (fu) {
+      a.faceIn = kind == 0 ? nullptr : ctx->faceBuf(kind == 1 ? 1 : 0);
+      a.face = ctx->faceBuf(kind == 1 ? 0 : 1);
+      c = ctx->ks->localFused(a, s);
+    } else {
+      c = ctx->ks->local(a, s);
+    }
+    if (c) return c;
+    if (ctx->src.nGrp > 0) {
+      SrcArgs sa = ctx->src;
+      sa.t = t0[k] + tOff;
+      sa.dt = dt[k];
+      sa.stepDev = steps + k;
+      if ((c = ctx->ks->sources(ctx->dofsE, sa, s))) return c;
+    }
+    return fu ? cudaSuccess : ctx->ks->neigh(a, s);
+  }
+  // body(k) on every active context's stream, forked from and joined back into `origin`
+  template <class F>
+  cudaError_t forkJoin(F body) {
+    cudaError_t c = cudaEventRecord(fork, origin);
+    for (size_t k = 0; k < ctxs.size() && !c; k++) {
+      if (!active[k]) continue;
+      cudaStream_t s = streams[k];
+      if ((c = cudaStreamWaitEvent(s, fork, 0))) break;
+      if ((c = body(k))) break;
+      if ((c = cudaEventRecord(joins[k], s))) break;
+      c = cudaStreamWaitEvent(origin, joins[k], 0);
+    }
+    return c;
+  }
+  cudaError_t advance(int by) {
+    kAdvanceSteps<<<1, 256, 0, origin>>>(steps, activeDev, (int)ctxs.size(), by);
+    return cudaGetLastError();
+  }
+  // the replayed unit: two GTS steps of every active context (fused ones: kinds 1 then 2, which
+  // leaves the pending projections where they were), each context on its own stream
   cudaError_t capture() {
     cudaError_t e;
     if (exec) {
@@ -1323,29 +1372,11 @@ struct edge_b200_batch {
       return e;
     if ((e = cudaStreamSynchronize(origin))) return e;
     if ((e = cudaStreamBeginCapture(origin, cudaStreamCaptureModeThreadLocal))) return e;
-    cudaError_t c = cudaEventRecord(fork, origin);
-    for (size_t k = 0; k < ctxs.size() && !c; k++) {
-      if (!active[k]) continue;
-      edge_b200_ctx *ctx = ctxs[k];
-      cudaStream_t s = streams[k];
-      if ((c = cudaStreamWaitEvent(s, fork, 0))) break;
-      StepArgsRaw a = ctx->args(dt[k]);
-      if ((c = ctx->ks->local(a, s))) break;
-      if (ctx->src.nGrp > 0) {
-        SrcArgs sa = ctx->src;
-        sa.t = t0[k];
-        sa.dt = dt[k];
-        sa.stepDev = steps + k;
-        if ((c = ctx->ks->sources(ctx->dofsE, sa, s))) break;
-      }
-      if ((c = ctx->ks->neigh(a, s))) break;
-      if ((c = cudaEventRecord(joins[k], s))) break;
-      c = cudaStreamWaitEvent(origin, joins[k], 0);
-    }
-    if (!c) {
-      kAdvanceSteps<<<1, 256, 0, origin>>>(steps, activeDev, (int)ctxs.size());
-      c = cudaGetLastError();
-    }
+    cudaError_t c = forkJoin([&](size_t k) {
+      cudaError_t r = issueStep(k, 1, 0.0);
+      return r ? r : issueStep(k, 2, dt[k]);
+    });
+    if (!c) c = advance(2);
     cudaGraph_t graph = nullptr;
     e = cudaStreamEndCapture(origin, &graph);
     if (c) {
@@ -1357,6 +1388,37 @@ struct edge_b200_batch {
     cudaGraphDestroy(graph);
     if (e) return e;
     dirty = false;
+    return cudaSuccess;
+  }
+  // n GTS steps of every active context: the first launched directly (kind 0), then pairs by
+  // graph, an odd one left directly (kind 1), then the fused contexts' last neighbour step, so
+  // that nothing is pending when the call returns
+  cudaError_t run(int n) {
+    cudaError_t c;
+    if (dirty && (c = capture())) return c;
+    for (size_t k = 0; k < ctxs.size(); k++)
+      if (active[k] && fused(ctxs[k])) ctxs[k]->faceCur = 0;  // nothing pending: only a relabelling
+    if ((c = forkJoin([&](size_t k) { return issueStep(k, 0, 0.0); }))) return c;
+    if ((c = advance(1))) return c;
+    for (int i = 0; i < (n - 1) / 2; i++)
+      if ((c = cudaGraphLaunch(exec, origin))) return c;
+    const bool odd = (n - 1) % 2 == 1;
+    if (odd) {
+      if ((c = forkJoin([&](size_t k) { return issueStep(k, 1, 0.0); }))) return c;
+      if ((c = advance(1))) return c;
+    }
+    // last written: faceAlt after kinds 0 and 2, face after kind 1
+    const int last = odd ? 0 : 1;
+    c = forkJoin([&](size_t k) {
+      edge_b200_ctx *ctx = ctxs[k];
+      if (!fused(ctx)) return cudaSuccess;
+      StepArgsRaw a = ctx->args(dt[k]);
+      a.face = ctx->faceBuf(last);
+      return ctx->ks->neigh(a, streams[k]);
+    });
+    if (c) return c;
+    for (size_t k = 0; k < ctxs.size(); k++)
+      if (active[k] && fused(ctxs[k])) ctxs[k]->faceCur = last;
     return cudaSuccess;
   }
 };
@@ -1403,6 +1465,10 @@ int edge_b200_batch_create(edge_b200_ctx *const *ctxs, int n, const double *t0, 
     edge_b200_ctx *c = ctxs[k];
     e = c->flush();
     if (!e) e = c->ensureFsLR();
+    if (!e && edge_b200_batch::fused(c) && !c->faceAlt.p) {
+      e = c->faceAlt.fit(c->faceCount() * c->realSize);
+      if (!e) e = cudaMemsetAsync(c->faceAlt.p, 0, c->faceCount() * c->realSize, c->stream);
+    }
     if (!e) e = cudaEventRecord(b->joins[k], c->stream);
     if (!e) e = cudaStreamWaitEvent(b->origin, b->joins[k], 0);
   }
@@ -1427,8 +1493,7 @@ int edge_b200_batch_set_active(edge_b200_batch *b, const int32_t *active) {
 int edge_b200_batch_step(edge_b200_batch *b, int n_steps) {
   if (!b || n_steps < 0) return EDGE_B200_EINVAL;
   if (n_steps == 0) return EDGE_B200_OK;
-  if (b->dirty) EDGE_BATCH_CUDA(b->capture(), "capture batch step");
-  for (int i = 0; i < n_steps; i++) EDGE_BATCH_CUDA(cudaGraphLaunch(b->exec, b->origin), "batch step");
+  EDGE_BATCH_CUDA(b->run(n_steps), "batch steps");
   return EDGE_B200_OK;
 }
 

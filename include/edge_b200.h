@@ -323,8 +323,11 @@ int edge_b200_step_noalloc(const edge_b200_cfg *cfg, int64_t n_el, double dt, in
 
 /* A batch of contexts (different meshes, orders, fused runs, physics; one device) stepped
  * together: one batch step is every active context's GTS step (local, sources, neighbour), each
- * context's kernels on a stream of its own, captured once into a CUDA graph and replayed per step,
- * so the independent contexts' kernels run side by side. Context k steps from time t0[k] by dt[k];
+ * context's kernels on a stream of its own, so the independent contexts' kernels run side by side.
+ * Two batch steps are captured once into a CUDA graph and replayed; contexts whose edge_b200_step
+ * folds each neighbour step into the next local step do the same here (the first step of a call and
+ * an odd last one are launched directly, and every call ends with the fused contexts' last
+ * neighbour step, so nothing is pending between calls). Context k steps from time t0[k] by dt[k];
  * a device counter per context gives its sources the step's time. The contexts keep their data;
  * upload DOFs and element data before creating the batch, and call edge_b200_batch_sync before
  * using a context on its own again. Contexts with receivers, halo parts or kernel timing on are
@@ -336,7 +339,7 @@ int edge_b200_batch_create(edge_b200_ctx *const *ctxs, int n, const double *t0, 
 /* active[k] != 0: context k takes part in the following steps (all do after create); the graph is
  * captured again at the next step when the set changed, e.g. when a simulation finished. */
 int edge_b200_batch_set_active(edge_b200_batch *b, const int32_t *active);
-/* n_steps batch steps (graph launches) on the batch's own stream; returns without waiting. */
+/* n_steps batch steps on the batch's own stream; returns without waiting. */
 int edge_b200_batch_step(edge_b200_batch *b, int n_steps);
 /* Waits for the batch; steps[n] (may be NULL) receives the steps each context has taken. */
 int edge_b200_batch_sync(edge_b200_batch *b, int64_t *steps);

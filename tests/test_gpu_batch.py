@@ -1,4 +1,4 @@
-"""Uneven batches through one captured CUDA graph per batch step (edge_b200_batch_*), and the
+"""Uneven batches through captured CUDA graphs of two batch steps (edge_b200_batch_*), and the
 launch-shape autotuner: every simulation of a batch ends where it ends when stepped alone."""
 import numpy as np
 import pytest
@@ -45,6 +45,33 @@ def test_batch_matches_each_simulation_alone():
         if c[2]:
             assert rel_l2(ab, aa) < c[6], c
     b.close()
+    for p in pairs:
+        for s in p:
+            s.close()
+
+
+def test_batch_segments_of_fused_steps():
+    """Segments of 1, 6 and 5 steps (a call's first step alone; graph pairs with and without an
+    odd step left), over fused and separate-kernel contexts, then a second call and a step of each
+    context on its own after it."""
+    cases = [(5, 16, 0, 32, 3), (4, 8, 3, 32, 2), (3, 1, 0, 64, 2)]
+    steps = [1, 7, 12]
+    pairs = [_pair(o, r, rm, p, n, 31 + i) for i, (o, r, rm, p, n) in enumerate(cases)]
+    b = Batch([p[0] for p in pairs])
+    segs = b.run(steps)
+    assert [k for _, k in segs] == [1, 6, 5]
+    b.run([2, 3, 0])
+    np.testing.assert_array_equal(b.sync(), [3, 10, 12])
+    b.close()
+    for (sb, sa), c, k in zip(pairs, cases, [3, 10, 12]):
+        sb.step(1)
+        sa.step(k + 1)
+        eb, ab = sb.download_dofs()
+        ea, aa = sa.download_dofs()
+        tol = 1e-12 if c[3] == 64 else 1e-6
+        assert rel_l2(eb, ea) < tol, c
+        if c[2]:
+            assert rel_l2(ab, aa) < tol, c
     for p in pairs:
         for s in p:
             s.close()
