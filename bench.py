@@ -32,6 +32,8 @@ WORKLOADS = {
     "box60j_o4_r8_m3_fp32": (60, 4, 8, 3, 32, "random", 2.0),
     # small case of the headline kernels for ncu captures (24,576 tets; DOFs 0.5 GB > L2)
     "box16_o5_r16_fp32": (16, 5, 16, 0, 32, "random", 1.5),
+    # small case of the attenuation kernels (20^3 cubes x 6 = 48,000 tets; DOFs 0.83 GB > L2)
+    "box20j_o4_r8_m3_fp32": (20, 4, 8, 3, 32, "random", 2.0),
 }
 
 

@@ -227,13 +227,12 @@ __device__ __forceinline__ void cpAsyncWait() {
   asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
 }
 
-// cooperative copy of the DOF rows [R][GB] of quantity q of an element into the tile rows
-// (q, eo * R + row) with stride S: warp q moves its quantity's rows, consecutive lanes consecutive
-// 16-byte chunks
+// cooperative copy of the rows [R][GB] of quantity row q (of nRows per element) of element e into
+// the tile rows (q, eo * R + row) with stride S, consecutive lanes moving consecutive 16-byte chunks
 template <typename T, int R, int GB, int S>
-__device__ __forceinline__ void copyDofRows(T *tile, const T *dofsE, int64_t e, int q, int eo, int r) {
+__device__ __forceinline__ void copyRows(T *tile, const T *base, int64_t e, int nRows, int q, int eo, int r) {
   constexpr int W = 16 / int(sizeof(T)), CPRB = GB / W;
-  const T *blk = dofsE + (e * 9 + q) * int64_t(R * GB);
+  const T *blk = base + (e * nRows + q) * int64_t(R * GB);
   T *dst = tile + (q * 32 + eo * R) * S;
 #pragma unroll
   for (int it = 0; it < CPRB; it++) {
@@ -241,6 +240,14 @@ __device__ __forceinline__ void copyDofRows(T *tile, const T *dofsE, int64_t e, 
     const int row = k / CPRB, col = k % CPRB;
     cpAsync16(dst + row * S + col * W, blk + row * GB + col * W);
   }
+}
+
+// cooperative copy of the DOF rows [R][GB] of quantity q of an element into the tile rows
+// (q, eo * R + row) with stride S: warp q moves its quantity's rows, consecutive lanes consecutive
+// 16-byte chunks
+template <typename T, int R, int GB, int S>
+__device__ __forceinline__ void copyDofRows(T *tile, const T *dofsE, int64_t e, int q, int eo, int r) {
+  copyRows<T, R, GB, S>(tile, dofsE, e, 9, q, eo, r);
 }
 
 // the reverse for results: tile rows (q, eo * R + row), stride S -> the [R][G] rows of row block
@@ -302,7 +309,13 @@ struct Geo {
   static constexpr int FSP = padGlobal<T>(81);  // a 9x9 block padded to 16 bytes
   static constexpr size_t premixBytes = size_t(2) * E * 2 * FSP * sizeof(T);
   static constexpr bool premix = RM == 0 && asyncLocal && smemLocal + premixBytes <= localBudget;
-  static constexpr size_t smemLocalGts = smemLocal + (premix ? premixBytes : 0);
+  // configurations that mix in the neighbour kernel (attenuation among them): the local flux-solver
+  // blocks fsE[0] (and fsA[0]) of every face arrive one face ahead by cp.async into two buffers
+  // [E][NFL] of doubles behind the face tile, where they fit
+  static constexpr int NFL = 81 + (RM ? 54 : 0);
+  static constexpr size_t fsLocalBytes = size_t(2) * E * NFL * sizeof(double);
+  static constexpr bool fsLocal = !premix && asyncLocal && smemLocal + fsLocalBytes <= localBudget;
+  static constexpr size_t smemLocalGts = smemLocal + (premix ? premixBytes : fsLocal ? fsLocalBytes : 0);
   // elastic CK with ping-pong derivatives between X and the separate face tile
   static constexpr bool ckPingPong = asyncLocal && RM == 0 && nModes(O - 1) <= SF;
   // LTS local step: one more [9][32][SB] tile for the half-step time integral (behind the rest)
@@ -714,6 +727,25 @@ __device__ __forceinline__ void issueMixFs(const StepArgs<T> &a, T *buf, int64_t
   }
 }
 
+// local flux-solver blocks fsE[0] (and fsA[0]) of face FA of group g's elements into buf [E][NFL]
+// (Geo::fsLocal)
+struct LocalFs {
+  double *buf;  // two buffers [2][E][NFL]
+  int64_t g, nGroups;
+};
+template <typename T, int O, int R, int RM, int FA>
+__device__ __forceinline__ void issueLocalFs(const StepArgs<T> &a, double *buf, int64_t g, int64_t nGroups) {
+  using G = Geo<T, O, R, RM>;
+  constexpr int E = G::E, NFL = G::NFL;
+  if (g >= nGroups) return;
+  for (int i = threadIdx.x; i < E * NFL; i += G::NT) {
+    const int eo = i / NFL, j = i % NFL;
+    if (g * E + eo >= a.elCount) continue;
+    const int64_t e = a.elFirst + g * E + eo;
+    cpAsync8(buf + i, j < 81 ? a.fsE + (e * 4 + FA) * 81 + j : a.fsA + (e * 4 + FA) * 54 + (j - 81));
+  }
+}
+
 // face connectivity of one element (all four faces): the face slot each face gathers from
 // (neighbour * 4 + its face id, or a compact LTS slot * 4 + face id), and one byte per face for the
 // buffer (LTS relation), the vertex id and the face type
@@ -809,7 +841,7 @@ template <typename T, int O, int R, int RM, int FA, int LTS = 0, bool TAIL = tru
 __device__ __forceinline__ void localFace(const StepArgs<T> &a, const T *TI, T *S0, int q, int l, int64_t e,
                                           int r, bool valid, T *acc, T *upA, const T *TIh = nullptr,
                                           T *S0alt = nullptr, const MixFs<T> &mf = MixFs<T>{nullptr, 0, 0},
-                                          T *Sh = nullptr) {
+                                          T *Sh = nullptr, const LocalFs &lf = LocalFs{nullptr, 0, 0}) {
   using G = Geo<T, O, R, RM>;
   constexpr int F = G::F, SF = G::SF, SB = G::SB;
   constexpr bool PM = LTS == 0 ? G::premix : G::premixLts;
@@ -931,18 +963,35 @@ __device__ __forceinline__ void localFace(const StepArgs<T> &a, const T *TI, T *
     if constexpr (TAIL) __syncthreads();
     return;
   }
-  // flux-solver row of this thread (elastic 9x9 or anelastic 6x9), loaded before the barrier
+  // flux-solver row of this thread (elastic 9x9 or anelastic 6x9): from the buffer filled one face
+  // ahead (Geo::fsLocal), else loaded before the barrier
   T fr[9];
-  if (q < 9) {
-    const double *fp = a.fsE + ((e * 4 + FA) * 81 + q * 9);
+  if constexpr (LTS == 0 && G::fsLocal) {
+    constexpr int E = G::E, NFL = G::NFL;
+    cpAsyncWait<0>();
+    __syncthreads();
+    // the next face's blocks into the other buffer, whose readers (one face back) all passed the
+    // barrier; after the last face the next group's first
+    if constexpr (FA < 3)
+      issueLocalFs<T, O, R, RM, FA + 1>(a, lf.buf + ((FA + 1) % 2) * (E * NFL), lf.g, lf.nGroups);
+    else
+      issueLocalFs<T, O, R, RM, 0>(a, lf.buf, lf.g + gridDim.x, lf.nGroups);
+    cpAsyncCommit();
+    const double *fp = lf.buf + (FA % 2) * (E * NFL) + (l / R) * NFL + (q < 9 ? q * 9 : 81 + (q - 9) * 9);
 #pragma unroll
-    for (int i = 0; i < 9; i++) fr[i] = valid ? T(__ldg(fp + i)) : T(0);
-  } else if constexpr (RM > 0) {
-    const double *fp = a.fsA + ((e * 4 + FA) * 54 + (q - 9) * 9);
+    for (int i = 0; i < 9; i++) fr[i] = valid ? T(fp[i]) : T(0);
+  } else {
+    if (q < 9) {
+      const double *fp = a.fsE + ((e * 4 + FA) * 81 + q * 9);
 #pragma unroll
-    for (int i = 0; i < 9; i++) fr[i] = valid ? T(__ldg(fp + i)) : T(0);
+      for (int i = 0; i < 9; i++) fr[i] = valid ? T(__ldg(fp + i)) : T(0);
+    } else if constexpr (RM > 0) {
+      const double *fp = a.fsA + ((e * 4 + FA) * 54 + (q - 9) * 9);
+#pragma unroll
+      for (int i = 0; i < 9; i++) fr[i] = valid ? T(__ldg(fp + i)) : T(0);
+    }
+    __syncthreads();
   }
-  __syncthreads();
   faceMix<T, F, SF>(S0, l, fr, s);
   if (q < 9)
     FluxTMul<O, FA>::template run<T>(s, acc);
@@ -981,6 +1030,13 @@ __global__ void __launch_bounds__(Geo<T, O, R, RM>::NT, LTS == 2 ? 1 : Geo<T, O,
   constexpr size_t fsOff = G::smemLocal + (LTS == 2 ? G::nX * sizeof(T) : 0);
   T *fsb = PM ? reinterpret_cast<T *>(smem + fsOff) : nullptr;
   T *Sh = (PM && LTS == 2) ? reinterpret_cast<T *>(smem + fsOff + G::premixBytes) : nullptr;
+  // local flux-solver buffers one face ahead (Geo::fsLocal) in the same place
+  constexpr bool FL = LTS == 0 && G::fsLocal;
+  double *fsl = FL ? reinterpret_cast<double *>(smem + G::smemLocal) : nullptr;
+  // AP (GTS): the anelastic rows arrive by cp.async too (the next group's into this warp's TIA
+  // rows at the end of a group, the current group's into its XA rows after the recursion, for the
+  // update)
+  constexpr bool AP = AS && RM > 0 && LTS == 0;
   const int q = threadIdx.x >> 5, l = threadIdx.x & 31;
   const int eo = l / R, r = l % R;
   const int64_t nGroups = (a.elCount + E - 1) / E;
@@ -990,7 +1046,14 @@ __global__ void __launch_bounds__(Geo<T, O, R, RM>::NT, LTS == 2 ? 1 : Geo<T, O,
     const int64_t g0 = blockIdx.x;
     if (q < 9 && g0 < nGroups && g0 * E + eo < a.elCount)
       copyDofRows<T, R, G::GB, SB>(TI, a.dofsE, a.elFirst + g0 * E + eo, q, eo, r);
+    if constexpr (AP) {
+      if (q >= 9 && g0 < nGroups && g0 * E + eo < a.elCount)
+#pragma unroll
+        for (int m = 0; m < RM; m++)
+          copyRows<T, R, G::GB, SB>(TIA, a.dofsA, a.elFirst + g0 * E + eo, RM * 6, m * 6 + q - 9, eo, r);
+    }
     if constexpr (PM) issueMixFs<T, O, R, RM, 0>(a, fsb, g0, nGroups);
+    if constexpr (FL) issueLocalFs<T, O, R, RM, 0>(a, fsl, g0, nGroups);
     cpAsyncCommit();
   }
   for (int64_t g = blockIdx.x; g < nGroups; g += gridDim.x) {
@@ -1045,10 +1108,22 @@ __global__ void __launch_bounds__(Geo<T, O, R, RM>::NT, LTS == 2 ? 1 : Geo<T, O,
       }
     } else if constexpr (RM > 0) {
       const int s = q - 9;
+      if constexpr (AP) {
+        cpAsyncWait<0>();
+        __syncwarp();
+      }
 #pragma unroll
       for (int m = 0; m < RM; m++) {
         T v[B];
-        ldRowG<T, B>(gRow<T, R, G::GB>(a.dofsA, ev, RM * 6, m * 6 + s, r), v, valid);
+        if constexpr (AP) {
+          if (valid)
+            ldRow<T, B>(rowPtr<T, SB>(TIA, m * 6 + s, l), v);
+          else
+#pragma unroll
+            for (int n = 0; n < B; n++) v[n] = T(0);
+        } else {
+          ldRowG<T, B>(gRow<T, R, G::GB>(a.dofsA, ev, RM * 6, m * 6 + s, r), v, valid);
+        }
         stRow<T, B>(rowPtr<T, SB>(XA, m * 6 + s, l), v);
 #pragma unroll
         for (int n = 0; n < B; n++) v[n] = dt * v[n];
@@ -1105,6 +1180,13 @@ __global__ void __launch_bounds__(Geo<T, O, R, RM>::NT, LTS == 2 ? 1 : Geo<T, O,
       if constexpr (RM > 0)
         if (q < 6) addSrc<T, B, SB, RM>(c, TIA, l, acc);
     } else if constexpr (RM > 0) {
+      if constexpr (AP) {
+        // this group's anelastic rows into this warp's XA rows (free after the recursion)
+        if (valid)
+#pragma unroll
+          for (int m = 0; m < RM; m++) copyRows<T, R, G::GB, SB>(XA, a.dofsA, e, RM * 6, m * 6 + q - 9, eo, r);
+        cpAsyncCommit();
+      }
 #pragma unroll
       for (int n = 0; n < B; n++) {
         acc[n] = T(0);
@@ -1116,11 +1198,12 @@ __global__ void __launch_bounds__(Geo<T, O, R, RM>::NT, LTS == 2 ? 1 : Geo<T, O,
     // local surface integral (SurfIntVanilla::local, SurfIntVanilla.hpp:212-262) + face projections
     if constexpr (AS) {
       const MixFs<T> mf{fsb, g, nGroups};
-      localFace<T, O, R, RM, 0, LTS, false>(a, TI, S0, q, l, ev, r, valid, acc, upA, TIh, X, mf, Sh);
-      localFace<T, O, R, RM, 1, LTS, false>(a, TI, X, q, l, ev, r, valid, acc, upA, TIh, S0, mf, Sh);
-      localFace<T, O, R, RM, 2, LTS, false>(a, TI, S0, q, l, ev, r, valid, acc, upA, TIh, X, mf, Sh);
+      const LocalFs lf{fsl, g, nGroups};
+      localFace<T, O, R, RM, 0, LTS, false>(a, TI, S0, q, l, ev, r, valid, acc, upA, TIh, X, mf, Sh, lf);
+      localFace<T, O, R, RM, 1, LTS, false>(a, TI, X, q, l, ev, r, valid, acc, upA, TIh, S0, mf, Sh, lf);
+      localFace<T, O, R, RM, 2, LTS, false>(a, TI, S0, q, l, ev, r, valid, acc, upA, TIh, X, mf, Sh, lf);
       // the barrier after the last face orders its readers of X before the next group writes X
-      localFace<T, O, R, RM, 3, LTS, true>(a, TI, X, q, l, ev, r, valid, acc, upA, TIh, S0, mf, Sh);
+      localFace<T, O, R, RM, 3, LTS, true>(a, TI, X, q, l, ev, r, valid, acc, upA, TIh, S0, mf, Sh, lf);
     } else {
       localFace<T, O, R, RM, 0, LTS>(a, TI, S0, q, l, ev, r, valid, acc, upA, TIh);
       localFace<T, O, R, RM, 1, LTS>(a, TI, S0, q, l, ev, r, valid, acc, upA, TIh);
@@ -1147,6 +1230,12 @@ __global__ void __launch_bounds__(Geo<T, O, R, RM>::NT, LTS == 2 ? 1 : Geo<T, O,
       }
       if constexpr (AS) cpAsyncCommit();
     }
+    if constexpr (AP) {
+      if (q >= 9) {
+        cpAsyncWait<0>();
+        __syncwarp();
+      }
+    }
     if (valid) {
       if (q < 9) {
         if constexpr (!G::tiSmem) stRowG<T, B>(gRow<T, R, G::GB>(a.dofsE, e, 9, q, r), acc);
@@ -1160,7 +1249,10 @@ __global__ void __launch_bounds__(Geo<T, O, R, RM>::NT, LTS == 2 ? 1 : Geo<T, O,
           ldRow<T, B>(rowPtr<T, SB>(TIA, m * 6 + s, l), ti);
           T *dst = gRow<T, R, G::GB>(a.dofsA, e, RM * 6, m * 6 + s, r);
           T v[B];
-          ldRowG<T, B>(dst, v, true);
+          if constexpr (AP)
+            ldRow<T, B>(rowPtr<T, SB>(XA, m * 6 + s, l), v);
+          else
+            ldRowG<T, B>(dst, v, true);
 #pragma unroll
           for (int n = 0; n < B; n++) {
             v[n] = fmaT(om, acc[n] - ti[n], v[n]);
@@ -1168,6 +1260,18 @@ __global__ void __launch_bounds__(Geo<T, O, R, RM>::NT, LTS == 2 ? 1 : Geo<T, O,
           }
           stRowG<T, B>(dst, v);
         }
+      }
+    }
+    if constexpr (AP) {
+      // the next group's anelastic rows into this warp's TIA rows (read above by their lanes)
+      if (q >= 9) {
+        __syncwarp();
+        const int64_t gn = g + gridDim.x;
+        if (gn < nGroups && gn * E + eo < a.elCount)
+#pragma unroll
+          for (int m = 0; m < RM; m++)
+            copyRows<T, R, G::GB, SB>(TIA, a.dofsA, a.elFirst + gn * E + eo, RM * 6, m * 6 + q - 9, eo, r);
+        cpAsyncCommit();
       }
     }
   }
