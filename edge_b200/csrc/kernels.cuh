@@ -315,7 +315,13 @@ struct Geo {
   static constexpr int NFL = 81 + (RM ? 54 : 0);
   static constexpr size_t fsLocalBytes = size_t(2) * E * NFL * sizeof(double);
   static constexpr bool fsLocal = !premix && asyncLocal && smemLocal + fsLocalBytes <= localBudget;
-  static constexpr size_t smemLocalGts = smemLocal + (premix ? premixBytes : fsLocal ? fsLocalBytes : 0);
+  // with attenuation the next group's element coefficients (star, starA, srcA: NCO doubles per
+  // element) arrive by cp.async as well, into a buffer behind those
+  static constexpr int NCO = 72 + 27 + 12 * RM;
+  static constexpr size_t coefBytes = size_t(E) * NCO * sizeof(double);
+  static constexpr bool coefSmem = fsLocal && RM > 0 && smemLocal + fsLocalBytes + coefBytes <= localBudget;
+  static constexpr size_t smemLocalGts =
+      smemLocal + (premix ? premixBytes : fsLocal ? fsLocalBytes + (coefSmem ? coefBytes : 0) : 0);
   // elastic CK with ping-pong derivatives between X and the separate face tile
   static constexpr bool ckPingPong = asyncLocal && RM == 0 && nModes(O - 1) <= SF;
   // LTS local step: one more [9][32][SB] tile for the half-step time integral (behind the rest)
@@ -344,7 +350,13 @@ struct Geo {
   static constexpr int NSN = slotRoom / slotNeigh >= 4 ? 4 : int(slotRoom / slotNeigh);
   static_assert(NSN >= 2, "neighbour kernel needs two slots");
   static_assert(slotNeigh % 16 == 0, "slots start on 16-byte boundaries (cp.async targets)");
-  static constexpr size_t smemNeigh = NSN * slotNeigh + (dofTile ? dofTileBytes : 0);
+  // with attenuation the group's anelastic rows [RM * 6][32][SB] arrive in a tile of their own
+  // (with the DOF rows, one group ahead) where it fits
+  static constexpr size_t dofATileBytes = size_t(RM) * 6 * 32 * SB * sizeof(T);
+  static constexpr bool dofATile =
+      RM > 0 && dofTile && NSN * slotNeigh + dofTileBytes + dofATileBytes <= budgetNeigh;
+  static constexpr size_t smemNeigh =
+      NSN * slotNeigh + (dofTile ? dofTileBytes : 0) + (dofATile ? dofATileBytes : 0);
   // resident CTAs per SM the register allocation targets (65,536 registers per SM): FP32 keeps
   // two 288-thread CTAs of each kernel (<= 113 registers); FP64 rows need twice the registers
   // and keep one
@@ -362,6 +374,20 @@ struct ElemCoef {
   int colsSrc[3];
 
   __device__ __forceinline__ void load(const StepArgs<T> &a, int64_t e, bool valid, int q) {
+    loadFrom<true>(a.starE + e * 72, a.starA + e * 27, a.srcA + e * (RM * 12), valid, q);
+  }
+  template <bool GLOBAL>
+  __device__ __forceinline__ static double rd(const double *p) {
+    if constexpr (GLOBAL)
+      return __ldg(p);
+    else
+      return *p;
+  }
+  // from the element's blocks star [3][24], starA [3][9], srcA [RM][12] (global memory, or a copy in
+  // shared memory)
+  template <bool GLOBAL>
+  __device__ __forceinline__ void loadFrom(const double *sE, const double *sA, const double *sS, bool valid,
+                                           int q) {
     if (q < 9) {
 #pragma unroll
       for (int i = 0; i < 3; i++) cols[i] = kStarCol[q][i];
@@ -372,7 +398,7 @@ struct ElemCoef {
         double v[3] = {0, 0, 0};
         if (valid && idx >= 0)
 #pragma unroll
-          for (int d = 0; d < 3; d++) v[d] = __ldg(&a.starE[(e * 3 + d) * 24 + idx]);
+          for (int d = 0; d < 3; d++) v[d] = rd<GLOBAL>(sE + d * 24 + idx);
 #pragma unroll
         for (int d = 0; d < 3; d++) cs[d][i] = T(kStarDir[0][d] * v[0] + kStarDir[1][d] * v[1] + kStarDir[2][d] * v[2]);
       }
@@ -384,7 +410,7 @@ struct ElemCoef {
 #pragma unroll
           for (int i = 0; i < 3; i++) {
             int idx = kSrcIdx[q][i];
-            csrc[m][i] = valid && m < RM && idx >= 0 ? T(__ldg(&a.srcA[(e * RM + m) * 12 + idx])) : T(0);
+            csrc[m][i] = valid && m < RM && idx >= 0 ? T(rd<GLOBAL>(sS + m * 12 + idx)) : T(0);
           }
       } else {
 #pragma unroll
@@ -404,7 +430,7 @@ struct ElemCoef {
         double v[3] = {0, 0, 0};
         if (valid && idx >= 0)
 #pragma unroll
-          for (int d = 0; d < 3; d++) v[d] = __ldg(&a.starA[(e * 3 + d) * 9 + idx]);
+          for (int d = 0; d < 3; d++) v[d] = rd<GLOBAL>(sA + d * 9 + idx);
 #pragma unroll
         for (int d = 0; d < 3; d++) ca[d][i] = T(kStarDir[0][d] * v[0] + kStarDir[1][d] * v[1] + kStarDir[2][d] * v[2]);
       }
@@ -746,6 +772,23 @@ __device__ __forceinline__ void issueLocalFs(const StepArgs<T> &a, double *buf, 
   }
 }
 
+// element coefficients of group g's elements into buf [E][NCO]: star [3][24], starA [3][9],
+// srcA [RM][12] (Geo::coefSmem)
+template <typename T, int O, int R, int RM>
+__device__ __forceinline__ void issueCoef(const StepArgs<T> &a, double *buf, int64_t g, int64_t nGroups) {
+  using G = Geo<T, O, R, RM>;
+  constexpr int E = G::E, NCO = G::NCO;
+  if (g >= nGroups) return;
+  for (int i = threadIdx.x; i < E * NCO; i += G::NT) {
+    const int eo = i / NCO, j = i % NCO;
+    if (g * E + eo >= a.elCount) continue;
+    const int64_t e = a.elFirst + g * E + eo;
+    cpAsync8(buf + i, j < 72   ? a.starE + e * 72 + j
+                      : j < 99 ? a.starA + e * 27 + (j - 72)
+                               : a.srcA + e * (RM * 12) + (j - 99));
+  }
+}
+
 // face connectivity of one element (all four faces): the face slot each face gathers from
 // (neighbour * 4 + its face id, or a compact LTS slot * 4 + face id), and one byte per face for the
 // buffer (LTS relation), the vertex id and the face type
@@ -1037,6 +1080,9 @@ __global__ void __launch_bounds__(Geo<T, O, R, RM>::NT, LTS == 2 ? 1 : Geo<T, O,
   // rows at the end of a group, the current group's into its XA rows after the recursion, for the
   // update)
   constexpr bool AP = AS && RM > 0 && LTS == 0;
+  // element coefficients one group ahead (Geo::coefSmem), behind the flux-solver buffers
+  constexpr bool CS = FL && G::coefSmem;
+  double *coefBuf = CS ? fsl + 2 * E * G::NFL : nullptr;
   const int q = threadIdx.x >> 5, l = threadIdx.x & 31;
   const int eo = l / R, r = l % R;
   const int64_t nGroups = (a.elCount + E - 1) / E;
@@ -1054,6 +1100,7 @@ __global__ void __launch_bounds__(Geo<T, O, R, RM>::NT, LTS == 2 ? 1 : Geo<T, O,
     }
     if constexpr (PM) issueMixFs<T, O, R, RM, 0>(a, fsb, g0, nGroups);
     if constexpr (FL) issueLocalFs<T, O, R, RM, 0>(a, fsl, g0, nGroups);
+    if constexpr (CS) issueCoef<T, O, R, RM>(a, coefBuf, g0, nGroups);
     cpAsyncCommit();
   }
   for (int64_t g = blockIdx.x; g < nGroups; g += gridDim.x) {
@@ -1136,8 +1183,15 @@ __global__ void __launch_bounds__(Geo<T, O, R, RM>::NT, LTS == 2 ? 1 : Geo<T, O,
       }
     }
     ElemCoef<T, RM> c;
-    c.load(a, ev, valid, q);
-    __syncthreads();
+    if constexpr (CS) {
+      // every thread waited for its copies above; the barrier makes all of them visible
+      __syncthreads();
+      const double *cb = coefBuf + eo * G::NCO;
+      c.template loadFrom<false>(cb, cb + 72, cb + 99, valid, q);
+    } else {
+      c.load(a, ev, valid, q);
+      __syncthreads();
+    }
     // Cauchy-Kowalevski (TimePredVanilla::ck, TimePredVanilla.hpp:200-306)
     ckAll<T, O, R, RM, 1, LTS == 2, G::ckPingPong>(X, TI, XA, TIA, q, l, c, a.omega, dt, dt, tIr, tIAr, TIh,
                                               dt * T(0.5), S0);
@@ -1204,6 +1258,11 @@ __global__ void __launch_bounds__(Geo<T, O, R, RM>::NT, LTS == 2 ? 1 : Geo<T, O,
       localFace<T, O, R, RM, 2, LTS, false>(a, TI, S0, q, l, ev, r, valid, acc, upA, TIh, X, mf, Sh, lf);
       // the barrier after the last face orders its readers of X before the next group writes X
       localFace<T, O, R, RM, 3, LTS, true>(a, TI, X, q, l, ev, r, valid, acc, upA, TIh, S0, mf, Sh, lf);
+      if constexpr (CS) {
+        // the next group's coefficients (every thread read this group's before the barriers above)
+        issueCoef<T, O, R, RM>(a, coefBuf, g + gridDim.x, nGroups);
+        cpAsyncCommit();
+      }
     } else {
       localFace<T, O, R, RM, 0, LTS>(a, TI, S0, q, l, ev, r, valid, acc, upA, TIh);
       localFace<T, O, R, RM, 1, LTS>(a, TI, S0, q, l, ev, r, valid, acc, upA, TIh);
@@ -1323,6 +1382,22 @@ struct NeighSlots {
         const int row = k / CPRB, col = k % CPRB;
         cpAsync16(dst + row * G::SB + col * W, blk + row * G::GB + col * W);
       }
+    }
+  }
+
+  __device__ __forceinline__ static T *dofATile(unsigned char *base) {
+    return reinterpret_cast<T *>(base + G::NSN * G::slotNeigh + G::dofTileBytes);
+  }
+  // the anelastic rows of group g into their tile (anelastic warp s copies rows m * 6 + s)
+  __device__ __forceinline__ static void issueDofsA(const StepArgs<T> &a, unsigned char *base, int q, int l,
+                                                    int64_t g, bool groupValid) {
+    if constexpr (G::dofATile) {
+      const int eo = l / R, r = l % R;
+      if (!groupValid || q < 9 || g * E + eo >= a.elCount) return;
+      const int64_t e = a.elFirst + g * E + eo;
+#pragma unroll
+      for (int m = 0; m < RM; m++)
+        copyRows<T, R, G::GB, G::SB>(dofATile(base), a.dofsA, e, RM * 6, m * 6 + q - 9, eo, r);
     }
   }
 
@@ -1505,6 +1580,7 @@ __global__ void __launch_bounds__(Geo<T, O, R, RM>::NT, Geo<T, O, R, RM>::minCta
   cur.load(a, a.elFirst + g * E + eo, g * E + eo < a.elCount);
   // prologue: the first group's DOF rows and items 0 .. NSN-2 (its first faces)
   NS::issueDofs(a, smem, q, l, g, g < nGroups);
+  NS::issueDofsA(a, smem, q, l, g, g < nGroups);
   NS::template issue<0, PM>(a, smem, 0, q, l, g, g < nGroups, cur);
   if constexpr (NSN > 2) NS::template issue<1, PM>(a, smem, 1, q, l, g, g < nGroups, cur);
   if constexpr (NSN > 3) NS::template issue<2, PM>(a, smem, 2, q, l, g, g < nGroups, cur);
@@ -1530,6 +1606,11 @@ __global__ void __launch_bounds__(Geo<T, O, R, RM>::NT, Geo<T, O, R, RM>::minCta
         ldRowG<T, B>(gRow<T, R, G::GB>(a.dofsE, valid ? e : 0, 9, q, r), acc, valid);
       }
     } else if constexpr (RM > 0) {
+      if constexpr (G::dofATile) {
+        // the group's anelastic rows (committed with the DOF rows), read back at the group's end
+        cpAsyncWait<0>();
+        __syncwarp();
+      }
 #pragma unroll
       for (int n = 0; n < B; n++) upA[n] = T(0);
     }
@@ -1537,6 +1618,29 @@ __global__ void __launch_bounds__(Geo<T, O, R, RM>::NT, Geo<T, O, R, RM>::minCta
     neighItem<T, O, R, RM, 1, PM>(a, smem, q, l, e, valid, cur, nxt, g, nextValid, k, acc, upA);
     neighItem<T, O, R, RM, 2, PM>(a, smem, q, l, e, valid, cur, nxt, g, nextValid, k, acc, upA);
     neighItem<T, O, R, RM, 3, PM>(a, smem, q, l, e, valid, cur, nxt, g, nextValid, k, acc, upA);
+    if constexpr (RM > 0) {
+      if (q >= 9) {
+        if (valid) {
+          // scatterUpdateA (SurfInt.hpp:139-156)
+          const int s = q - 9;
+#pragma unroll
+          for (int m = 0; m < RM; m++) {
+            const T om = T(a.omega[m]);
+            T *dst = gRow<T, R, G::GB>(a.dofsA, e, RM * 6, m * 6 + s, r);
+            T v[B];
+            if constexpr (G::dofATile)
+              ldRow<T, B>(rowPtr<T, G::SB>(NS::dofATile(smem), m * 6 + s, l), v);
+            else
+              ldRowG<T, B>(dst, v, true);
+#pragma unroll
+            for (int n = 0; n < B; n++) v[n] = fmaT(om, upA[n], v[n]);
+            stRowG<T, B>(dst, v);
+          }
+        }
+        // the tile rows read above before the next group's copies into them
+        if constexpr (G::dofATile) __syncwarp();
+      }
+    }
     if constexpr (G::dofTile) {
       // the updated rows through the DOF tile (this warp's rows only), stored coalesced; then the
       // next group's DOF rows into the tile
@@ -1552,26 +1656,11 @@ __global__ void __launch_bounds__(Geo<T, O, R, RM>::NT, Geo<T, O, R, RM>::minCta
         __syncwarp();
       }
       NS::issueDofs(a, smem, q, l, g + gridDim.x, nextValid);
+      NS::issueDofsA(a, smem, q, l, g + gridDim.x, nextValid);
       cpAsyncCommit();
     }
-    if (valid) {
-      if (q < 9) {
-        if constexpr (!G::dofTile) stRowG<T, B>(gRow<T, R, G::GB>(a.dofsE, e, 9, q, r), acc);
-      } else if constexpr (RM > 0) {
-        // scatterUpdateA (SurfInt.hpp:139-156)
-        const int s = q - 9;
-#pragma unroll
-        for (int m = 0; m < RM; m++) {
-          const T om = T(a.omega[m]);
-          T *dst = gRow<T, R, G::GB>(a.dofsA, e, RM * 6, m * 6 + s, r);
-          T v[B];
-          ldRowG<T, B>(dst, v, true);
-#pragma unroll
-          for (int n = 0; n < B; n++) v[n] = fmaT(om, upA[n], v[n]);
-          stRowG<T, B>(dst, v);
-        }
-      }
-    }
+    if constexpr (!G::dofTile)
+      if (valid && q < 9) stRowG<T, B>(gRow<T, R, G::GB>(a.dofsE, e, 9, q, r), acc);
     cur = nxt;
   }
   cpAsyncWait<0>();
