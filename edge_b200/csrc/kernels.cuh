@@ -320,8 +320,15 @@ struct Geo {
   static constexpr int NCO = 72 + 27 + 12 * RM;
   static constexpr size_t coefBytes = size_t(E) * NCO * sizeof(double);
   static constexpr bool coefSmem = fsLocal && RM > 0 && smemLocal + fsLocalBytes + coefBytes <= localBudget;
-  static constexpr size_t smemLocalGts =
-      smemLocal + (premix ? premixBytes : fsLocal ? fsLocalBytes + (coefSmem ? coefBytes : 0) : 0);
+  // and the anelastic warps compute the anelastic source terms of the elastic rows, handed over in a
+  // tile [9][32][SB] behind the coefficients (srcShare)
+  static constexpr size_t srcOff = (smemLocal + fsLocalBytes + coefBytes + 15) / 16 * 16;
+  static constexpr size_t srcBytes = size_t(9) * 32 * SB * sizeof(T);
+  static constexpr bool srcSplit = coefSmem && srcOff + srcBytes <= localBudget;
+  static constexpr size_t smemLocalGts = premix     ? smemLocal + premixBytes
+                                         : srcSplit ? srcOff + srcBytes
+                                         : fsLocal  ? smemLocal + fsLocalBytes + (coefSmem ? coefBytes : 0)
+                                                    : smemLocal;
   // elastic CK with ping-pong derivatives between X and the separate face tile
   static constexpr bool ckPingPong = asyncLocal && RM == 0 && nModes(O - 1) <= SF;
   // LTS local step: one more [9][32][SB] tile for the half-step time integral (behind the rest)
@@ -385,7 +392,9 @@ struct ElemCoef {
   }
   // from the element's blocks star [3][24], starA [3][9], srcA [RM][12] (global memory, or a copy in
   // shared memory)
-  template <bool GLOBAL>
+  // SPLIT: the anelastic warps compute the anelastic source terms of the elastic rows (srcShare)
+  // and hold their coefficients; the elastic warps hold none
+  template <bool GLOBAL, bool SPLIT = false>
   __device__ __forceinline__ void loadFrom(const double *sE, const double *sA, const double *sS, bool valid,
                                            int q) {
     if (q < 9) {
@@ -402,7 +411,7 @@ struct ElemCoef {
 #pragma unroll
         for (int d = 0; d < 3; d++) cs[d][i] = T(kStarDir[0][d] * v[0] + kStarDir[1][d] * v[1] + kStarDir[2][d] * v[2]);
       }
-      if (RM && q < 6) {
+      if (RM && q < 6 && !SPLIT) {
 #pragma unroll
         for (int i = 0; i < 3; i++) colsSrc[i] = kSrcCol[q][i];
 #pragma unroll
@@ -433,6 +442,25 @@ struct ElemCoef {
           for (int d = 0; d < 3; d++) v[d] = rd<GLOBAL>(sA + d * 9 + idx);
 #pragma unroll
         for (int d = 0; d < 3; d++) ca[d][i] = T(kStarDir[0][d] * v[0] + kStarDir[1][d] * v[1] + kStarDir[2][d] * v[2]);
+      }
+      if constexpr (SPLIT && RM > 0) {
+        // s < 3: srcA_m[s][i] of mechanisms m < RM - 1 (csrc[m][i]); s >= 3: srcA_{RM-1}[s - 3][i]
+        // (csrc[0][i]) and srcA_m[s][s] of every mechanism (csrc[1][m])
+#pragma unroll
+        for (int m = 0; m < 3; m++)
+#pragma unroll
+          for (int i = 0; i < 3; i++) csrc[m][i] = T(0);
+        if (s < 3) {
+#pragma unroll
+          for (int m = 0; m + 1 < RM; m++)
+#pragma unroll
+            for (int i = 0; i < 3; i++) csrc[m][i] = valid ? T(rd<GLOBAL>(sS + m * 12 + kSrcIdx[s][i])) : T(0);
+        } else {
+#pragma unroll
+          for (int i = 0; i < 3; i++) csrc[0][i] = valid ? T(rd<GLOBAL>(sS + (RM - 1) * 12 + kSrcIdx[s - 3][i])) : T(0);
+#pragma unroll
+          for (int m = 0; m < RM; m++) csrc[1][m] = valid ? T(rd<GLOBAL>(sS + m * 12 + kSrcIdx[s][0])) : T(0);
+        }
       }
     }
   }
@@ -553,6 +581,59 @@ __device__ __forceinline__ void addSrc(const ElemCoef<T, RM> &c, const T *Y, int
     }
 }
 
+// the same source terms computed by the anelastic warps (ElemCoef SPLIT), into the rows of SRC
+// [9][32][S]: warp s < 3 the terms of mechanisms m < RM - 1 of elastic row s (row s); warp s >= 3
+// those of elastic row s (row s) and the last mechanism's of elastic row s - 3 (row s + 3). Elastic
+// row q < 6 then adds row q, and q < 3 row q + 6 too: six source rows per anelastic warp instead of
+// nine per elastic warp 0-2.
+template <typename T, int B, int S, int RM>
+__device__ __forceinline__ void srcShare(const ElemCoef<T, RM> &c, const T *Y, int l, int s, T *SRC) {
+  T o[B], y[B];
+#pragma unroll
+  for (int n = 0; n < B; n++) o[n] = T(0);
+  if (s < 3) {
+#pragma unroll
+    for (int m = 0; m + 1 < RM; m++)
+#pragma unroll
+      for (int i = 0; i < 3; i++) {
+        ldRow<T, B>(rowPtr<T, S>(Y, m * 6 + i, l), y);
+#pragma unroll
+        for (int n = 0; n < B; n++) o[n] = fmaT(c.csrc[m][i], y[n], o[n]);
+      }
+    stRow<T, B>(rowPtr<T, S>(SRC, s, l), o);
+  } else {
+#pragma unroll
+    for (int i = 0; i < 3; i++) {
+      ldRow<T, B>(rowPtr<T, S>(Y, (RM - 1) * 6 + i, l), y);
+#pragma unroll
+      for (int n = 0; n < B; n++) o[n] = fmaT(c.csrc[0][i], y[n], o[n]);
+    }
+    stRow<T, B>(rowPtr<T, S>(SRC, s + 3, l), o);
+#pragma unroll
+    for (int n = 0; n < B; n++) o[n] = T(0);
+#pragma unroll
+    for (int m = 0; m < RM; m++) {
+      ldRow<T, B>(rowPtr<T, S>(Y, m * 6 + s, l), y);
+#pragma unroll
+      for (int n = 0; n < B; n++) o[n] = fmaT(c.csrc[1][m], y[n], o[n]);
+    }
+    stRow<T, B>(rowPtr<T, S>(SRC, s, l), o);
+  }
+}
+// elastic row q < 6: acc += its source rows of SRC
+template <typename T, int B, int S>
+__device__ __forceinline__ void addSrcRows(const T *SRC, int q, int l, T *acc) {
+  T y[B];
+  ldRow<T, B>(rowPtr<T, S>(SRC, q, l), y);
+#pragma unroll
+  for (int n = 0; n < B; n++) acc[n] += y[n];
+  if (q < 3) {
+    ldRow<T, B>(rowPtr<T, S>(SRC, q + 6, l), y);
+#pragma unroll
+    for (int n = 0; n < B; n++) acc[n] += y[n];
+  }
+}
+
 // ---------------------------------------- CK recursion -----------------------------------------
 // derivative D of TimePredVanilla::ck (TimePredVanilla.hpp:229-303) with the star matrix applied
 // before the stiffness product; der[D] replaces der[D-1] in X, TI += sca * der[D] (rows owned by
@@ -571,9 +652,10 @@ struct CkStep {
   static_assert(!PP || (RM == 0 && NN <= G::SF), "ping-pong derivatives must fit the face tile");
 
   // H: also TIh += scaH * der[D] (the time integral over the first half of the step, for LTS)
+  // SRC (attenuation, ElemCoef SPLIT): the anelastic warps compute the source terms (srcShare)
   __device__ __forceinline__ static void run(T *X, T *TI, T *XA, T *TIA, int q, int l, const ElemCoef<T, RM> &c,
                                              const double *omega, T sca, T *tIr, T (*tIAr)[B], T *TIh = nullptr,
-                                             T scaH = T(0), T *XP = nullptr) {
+                                             T scaH = T(0), T *XP = nullptr, T *SRC = nullptr) {
     T *Xin = IN_P ? XP : X;
     T *Xout = OUT_P ? XP : X;
     T acc[B];
@@ -584,12 +666,15 @@ struct CkStep {
                     rowPtr<T, SI>(Xin, c.cols[2], l), c.cs};
       CkMul<O, DK>::template run<T>(z, acc);
       if constexpr (RM > 0)
-        if (q < 6) addSrc<T, B, S, RM>(c, XA, l, acc);
+        if (q < 6 && !SRC) addSrc<T, B, S, RM>(c, XA, l, acc);
     } else if constexpr (RM > 0) {
+      if (SRC) srcShare<T, B, S, RM>(c, XA, l, q - 9, SRC);
       Mix2<T, S> z{rowPtr<T, S>(X, 6 + c.colsA[0], l), rowPtr<T, S>(X, 6 + c.colsA[1], l), c.ca};
       CkMul<O, DK>::template run<T>(z, acc);
     }
     if constexpr (!PP) __syncthreads();
+    if constexpr (RM > 0)
+      if (SRC && q < 6) addSrcRows<T, B, S>(SRC, q, l, acc);
     if (q < 9) {
       constexpr int NW = RM ? B : NN;  // modes beyond NN stay zero without anelasticity
       stRow<T, NW>(rowPtr<T, SO>(Xout, q, l), acc);
@@ -642,12 +727,12 @@ struct CkStep {
 template <typename T, int O, int R, int RM, int D, bool H = false, bool PP = false>
 __device__ __forceinline__ void ckAll(T *X, T *TI, T *XA, T *TIA, int q, int l, const ElemCoef<T, RM> &c,
                                       const double *omega, T dt, T sca, T *tIr, T (*tIAr)[nModes(O)],
-                                      T *TIh = nullptr, T scaH = T(0), T *XP = nullptr) {
+                                      T *TIh = nullptr, T scaH = T(0), T *XP = nullptr, T *SRC = nullptr) {
   if constexpr (D < O) {
     sca = sca * dt / T(D + 1);
     if constexpr (H) scaH = scaH * (dt * T(0.5)) / T(D + 1);
-    CkStep<T, O, R, RM, D, H, PP>::run(X, TI, XA, TIA, q, l, c, omega, sca, tIr, tIAr, TIh, scaH, XP);
-    ckAll<T, O, R, RM, D + 1, H, PP>(X, TI, XA, TIA, q, l, c, omega, dt, sca, tIr, tIAr, TIh, scaH, XP);
+    CkStep<T, O, R, RM, D, H, PP>::run(X, TI, XA, TIA, q, l, c, omega, sca, tIr, tIAr, TIh, scaH, XP, SRC);
+    ckAll<T, O, R, RM, D + 1, H, PP>(X, TI, XA, TIA, q, l, c, omega, dt, sca, tIr, tIAr, TIh, scaH, XP, SRC);
   }
 }
 
@@ -1083,6 +1168,9 @@ __global__ void __launch_bounds__(Geo<T, O, R, RM>::NT, LTS == 2 ? 1 : Geo<T, O,
   // element coefficients one group ahead (Geo::coefSmem), behind the flux-solver buffers
   constexpr bool CS = FL && G::coefSmem;
   double *coefBuf = CS ? fsl + 2 * E * G::NFL : nullptr;
+  // anelastic source terms from the anelastic warps (Geo::srcSplit)
+  constexpr bool SS = CS && G::srcSplit;
+  T *srcBuf = SS ? reinterpret_cast<T *>(smem + G::srcOff) : nullptr;
   const int q = threadIdx.x >> 5, l = threadIdx.x & 31;
   const int eo = l / R, r = l % R;
   const int64_t nGroups = (a.elCount + E - 1) / E;
@@ -1187,14 +1275,14 @@ __global__ void __launch_bounds__(Geo<T, O, R, RM>::NT, LTS == 2 ? 1 : Geo<T, O,
       // every thread waited for its copies above; the barrier makes all of them visible
       __syncthreads();
       const double *cb = coefBuf + eo * G::NCO;
-      c.template loadFrom<false>(cb, cb + 72, cb + 99, valid, q);
+      c.template loadFrom<false, SS>(cb, cb + 72, cb + 99, valid, q);
     } else {
       c.load(a, ev, valid, q);
       __syncthreads();
     }
     // Cauchy-Kowalevski (TimePredVanilla::ck, TimePredVanilla.hpp:200-306)
     ckAll<T, O, R, RM, 1, LTS == 2, G::ckPingPong>(X, TI, XA, TIA, q, l, c, a.omega, dt, dt, tIr, tIAr, TIh,
-                                              dt * T(0.5), S0);
+                                              dt * T(0.5), S0, srcBuf);
     if constexpr (!G::tiSmem) {
       if (q < 9) {
         stRow<T, B>(rowPtr<T, SB>(X, q, l), tIr);
@@ -1231,9 +1319,11 @@ __global__ void __launch_bounds__(Geo<T, O, R, RM>::NT, LTS == 2 ? 1 : Geo<T, O,
       Mix3<T, SB> z{rowPtr<T, SB>(TI, c.cols[0], l), rowPtr<T, SB>(TI, c.cols[1], l),
                     rowPtr<T, SB>(TI, c.cols[2], l), c.cs};
       VolMul<O>::template run<T>(z, acc);
-      if constexpr (RM > 0)
+      if constexpr (RM > 0 && !SS)
         if (q < 6) addSrc<T, B, SB, RM>(c, TIA, l, acc);
     } else if constexpr (RM > 0) {
+      // (SS: the source terms of the time integrals, added to the elastic rows after the faces)
+      if constexpr (SS) srcShare<T, B, SB, RM>(c, TIA, l, q - 9, srcBuf);
       if constexpr (AP) {
         // this group's anelastic rows into this warp's XA rows (free after the recursion)
         if (valid)
@@ -1258,6 +1348,8 @@ __global__ void __launch_bounds__(Geo<T, O, R, RM>::NT, LTS == 2 ? 1 : Geo<T, O,
       localFace<T, O, R, RM, 2, LTS, false>(a, TI, S0, q, l, ev, r, valid, acc, upA, TIh, X, mf, Sh, lf);
       // the barrier after the last face orders its readers of X before the next group writes X
       localFace<T, O, R, RM, 3, LTS, true>(a, TI, X, q, l, ev, r, valid, acc, upA, TIh, S0, mf, Sh, lf);
+      if constexpr (SS)
+        if (q < 6) addSrcRows<T, B, SB>(srcBuf, q, l, acc);
       if constexpr (CS) {
         // the next group's coefficients (every thread read this group's before the barriers above)
         issueCoef<T, O, R, RM>(a, coefBuf, g + gridDim.x, nGroups);
