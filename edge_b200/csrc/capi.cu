@@ -1297,6 +1297,7 @@ struct edge_b200_batch {
   int64_t *steps = nullptr;    // device: steps taken per context
   int32_t *activeDev = nullptr;
   cudaGraphExec_t exec = nullptr;  // two batch steps
+  std::vector<char> fu;            // per context: fused steps, fixed when the graph is captured
   bool dirty = true;
   std::string err;
   ~edge_b200_batch() {
@@ -1322,9 +1323,8 @@ struct edge_b200_batch {
     edge_b200_ctx *ctx = ctxs[k];
     cudaStream_t s = streams[k];
     StepArgsRaw a = ctx->args(dt[k]);
-    const bool fu = fused(ctx);
     cudaError_t c;
-    if (fu) {
+    if (fu[k]) {
       a.faceIn = kind == 0 ? nullptr : ctx->faceBuf(kind == 1 ? 1 : 0);
       a.face = ctx->faceBuf(kind == 1 ? 0 : 1);
       c = ctx->ks->localFused(a, s);
@@ -1339,7 +1339,7 @@ struct edge_b200_batch {
       sa.stepDev = steps + k;
       if ((c = ctx->ks->sources(ctx->dofsE, sa, s))) return c;
     }
-    return fu ? cudaSuccess : ctx->ks->neigh(a, s);
+    return fu[k] ? cudaSuccess : ctx->ks->neigh(a, s);
   }
   // body(k) on every active context's stream, forked from and joined back into `origin`
   template <class F>
@@ -1371,6 +1371,10 @@ struct edge_b200_batch {
                              origin)))
       return e;
     if ((e = cudaStreamSynchronize(origin))) return e;
+    // each context's step form for this graph and the direct launches around it (a context switched
+    // to fused steps after the batch was created, without its second face buffer, stays separate)
+    fu.assign(ctxs.size(), 0);
+    for (size_t k = 0; k < ctxs.size(); k++) fu[k] = fused(ctxs[k]) && ctxs[k]->faceAlt.p != nullptr;
     if ((e = cudaStreamBeginCapture(origin, cudaStreamCaptureModeThreadLocal))) return e;
     cudaError_t c = forkJoin([&](size_t k) {
       cudaError_t r = issueStep(k, 1, 0.0);
@@ -1397,7 +1401,7 @@ struct edge_b200_batch {
     cudaError_t c;
     if (dirty && (c = capture())) return c;
     for (size_t k = 0; k < ctxs.size(); k++)
-      if (active[k] && fused(ctxs[k])) ctxs[k]->faceCur = 0;  // nothing pending: only a relabelling
+      if (active[k] && fu[k]) ctxs[k]->faceCur = 0;  // nothing pending: only a relabelling
     if ((c = forkJoin([&](size_t k) { return issueStep(k, 0, 0.0); }))) return c;
     if ((c = advance(1))) return c;
     for (int i = 0; i < (n - 1) / 2; i++)
@@ -1411,14 +1415,14 @@ struct edge_b200_batch {
     const int last = odd ? 0 : 1;
     c = forkJoin([&](size_t k) {
       edge_b200_ctx *ctx = ctxs[k];
-      if (!fused(ctx)) return cudaSuccess;
+      if (!fu[k]) return cudaSuccess;
       StepArgsRaw a = ctx->args(dt[k]);
       a.face = ctx->faceBuf(last);
       return ctx->ks->neigh(a, streams[k]);
     });
     if (c) return c;
     for (size_t k = 0; k < ctxs.size(); k++)
-      if (active[k] && fused(ctxs[k])) ctxs[k]->faceCur = last;
+      if (active[k] && fu[k]) ctxs[k]->faceCur = last;
     return cudaSuccess;
   }
 };

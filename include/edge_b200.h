@@ -327,7 +327,8 @@ int edge_b200_step_noalloc(const edge_b200_cfg *cfg, int64_t n_el, double dt, in
  * Two batch steps are captured once into a CUDA graph and replayed; contexts whose edge_b200_step
  * folds each neighbour step into the next local step do the same here (the first step of a call and
  * an odd last one are launched directly, and every call ends with the fused contexts' last
- * neighbour step, so nothing is pending between calls). Context k steps from time t0[k] by dt[k];
+ * neighbour step, so nothing is pending between calls; each context's step form is fixed when the
+ * graph is captured). Context k steps from time t0[k] by dt[k];
  * a device counter per context gives its sources the step's time. The contexts keep their data;
  * upload DOFs and element data before creating the batch, and call edge_b200_batch_sync before
  * using a context on its own again. Contexts with receivers, halo parts or kernel timing on are

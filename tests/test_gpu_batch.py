@@ -77,6 +77,27 @@ def test_batch_segments_of_fused_steps():
             s.close()
 
 
+def test_batch_step_form_fixed_at_capture():
+    """A context created with separate-kernel steps and switched to fused ones afterwards (no second
+    face buffer) keeps separate steps in the batch; a context switched off stays consistent too."""
+    from edge_b200._lib import lib
+    pairs = [_pair(5, 16, 0, 32, 2, 41), _pair(5, 16, 0, 32, 2, 43)]
+    assert lib().edge_b200_set_fused(pairs[0][0]._h, 0) == 0
+    b = Batch([p[0] for p in pairs])
+    assert lib().edge_b200_set_fused(pairs[0][0]._h, 1) == 0
+    b.run([5, 4])
+    assert lib().edge_b200_set_fused(pairs[1][0]._h, 0) == 0
+    b.run([2, 3])
+    np.testing.assert_array_equal(b.sync(), [7, 7])
+    b.close()
+    for sb, sa in pairs:
+        sa.step(7)
+        assert rel_l2(sb.download_dofs()[0], sa.download_dofs()[0]) < 1e-6
+    for p in pairs:
+        for s in p:
+            s.close()
+
+
 def test_batch_refuses_receivers():
     from edge_b200._lib import lib
     import ctypes as C
