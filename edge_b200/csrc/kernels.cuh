@@ -325,8 +325,16 @@ struct Geo {
   static constexpr size_t srcOff = (smemLocal + fsLocalBytes + coefBytes + 15) / 16 * 16;
   static constexpr size_t srcBytes = size_t(9) * 32 * SB * sizeof(T);
   static constexpr bool srcSplit = coefSmem && srcOff + srcBytes <= localBudget;
-  static constexpr size_t smemLocalGts = premix     ? smemLocal + premixBytes
-                                         : srcSplit ? srcOff + srcBytes
+  // and the group's 36 face projections (9 rows x 4 faces) are spread over all fifteen warps into
+  // four face tiles (the face tile, X, and two behind the source tile), with the flux-solver blocks
+  // of all four faces at hand (faces 2 and 3 behind the source tile): one barrier before the four
+  // faces' mixes instead of one per face (facesSplit)
+  static constexpr size_t fsExtraOff = srcOff + srcBytes;
+  static constexpr size_t tilesOff = (fsExtraOff + fsLocalBytes + 15) / 16 * 16;
+  static constexpr bool projSplit = srcSplit && tilesOff + 2 * nS0 * sizeof(T) <= localBudget;
+  static constexpr size_t smemLocalGts = premix      ? smemLocal + premixBytes
+                                         : projSplit ? tilesOff + 2 * nS0 * sizeof(T)
+                                         : srcSplit  ? srcOff + srcBytes
                                          : fsLocal  ? smemLocal + fsLocalBytes + (coefSmem ? coefBytes : 0)
                                                     : smemLocal;
   // elastic CK with ping-pong derivatives between X and the separate face tile
@@ -1128,6 +1136,73 @@ __device__ __forceinline__ void localFace(const StepArgs<T> &a, const T *TI, T *
   if constexpr (TAIL) __syncthreads();
 }
 
+// quantity mix of face FA's tile with this thread's flux-solver row fp, lifted into acc (elastic
+// rows) or upA (anelastic rows)
+template <typename T, int O, int R, int RM, int FA>
+__device__ __forceinline__ void faceLift(const T *tile, const double *fp, int q, int l, bool valid, T *acc,
+                                         T *upA) {
+  using G = Geo<T, O, R, RM>;
+  constexpr int F = G::F, SF = G::SF;
+  T fr[9];
+#pragma unroll
+  for (int i = 0; i < 9; i++) fr[i] = valid ? T(fp[i]) : T(0);
+  T s[F];
+  faceMix<T, F, SF>(tile, l, fr, s);
+  if (q < 9)
+    FluxTMul<O, FA>::template run<T>(s, acc);
+  else if constexpr (RM > 0)
+    FluxTMul<O, FA>::template run<T>(s, upA);
+}
+
+// the four local faces with the projections spread over all warps (Geo::projSplit, attenuation,
+// GTS): elastic warp q projects its row onto faces 0 and 1, anelastic warp s takes tasks 18 + s,
+// 24 + s and 30 + s of the 18 (face 2 and 3) row projections (task t: row t % 9, face t / 9); each
+// projection goes to its face tile and to the face buffer. After one barrier every warp mixes and
+// lifts its own row for the four faces (fs4: the flux-solver blocks of the four faces). A barrier
+// at the end orders the tiles' readers before X is written again.
+template <typename T, int O, int R, int RM>
+__device__ __forceinline__ void facesSplit(const StepArgs<T> &a, const T *TI, T *const (&tiles)[4],
+                                           const double *const (&fs4)[4], int q, int l, int64_t e, bool valid,
+                                           T *acc, T *upA) {
+  using G = Geo<T, O, R, RM>;
+  constexpr int F = G::F, SF = G::SF, SB = G::SB, NFL = G::NFL;
+  const int eo = l / R, r = l % R;
+  const int nTasks = q < 9 ? 2 : 3;
+  for (int j = 0; j < nTasks; j++) {
+    const int t = q < 9 ? q + 9 * j : 18 + (q - 9) + 6 * j;
+    const int row = t % 9, fa = t / 9;
+    T s[F];
+#pragma unroll
+    for (int i = 0; i < F; i++) s[i] = T(0);
+    const OwnRow<T> src{rowPtr<T, SB>(TI, row, l)};
+    if (fa == 0)
+      FluxLMul<O, 0>::template run<T>(src, s);
+    else if (fa == 1)
+      FluxLMul<O, 1>::template run<T>(src, s);
+    else if (fa == 2)
+      FluxLMul<O, 2>::template run<T>(src, s);
+    else
+      FluxLMul<O, 3>::template run<T>(src, s);
+    T *tile = fa == 0 ? tiles[0] : fa == 1 ? tiles[1] : fa == 2 ? tiles[2] : tiles[3];
+    T *p = rowPtr<T, SF>(tile, row, l);
+    stRow<T, F>(p, s);
+#pragma unroll
+    for (int i = F; i < G::GF; i++) p[i] = T(0);
+    __syncwarp();
+    if (valid)
+      storeRowsCoalesced<T, R, G::GF, SF>(tile, a.face + ((e * 4 + fa) * 9 + row) * int64_t(R * G::GF), row, eo,
+                                          r);
+  }
+  cpAsyncWait<0>();
+  __syncthreads();
+  const int fo = (l / R) * NFL + (q < 9 ? q * 9 : 81 + (q - 9) * 9);
+  faceLift<T, O, R, RM, 0>(tiles[0], fs4[0] + fo, q, l, valid, acc, upA);
+  faceLift<T, O, R, RM, 1>(tiles[1], fs4[1] + fo, q, l, valid, acc, upA);
+  faceLift<T, O, R, RM, 2>(tiles[2], fs4[2] + fo, q, l, valid, acc, upA);
+  faceLift<T, O, R, RM, 3>(tiles[3], fs4[3] + fo, q, l, valid, acc, upA);
+  __syncthreads();
+}
+
 // LTS as in localFace; mode 2 keeps the half-step integral in one more tile (one CTA per SM), mode
 // 1 runs on the elements of a time group without a smaller neighbour
 // FUSED (GTS, pre-mixing configurations): the previous step's neighbour fluxes (a.faceIn, when
@@ -1171,6 +1246,10 @@ __global__ void __launch_bounds__(Geo<T, O, R, RM>::NT, LTS == 2 ? 1 : Geo<T, O,
   // anelastic source terms from the anelastic warps (Geo::srcSplit)
   constexpr bool SS = CS && G::srcSplit;
   T *srcBuf = SS ? reinterpret_cast<T *>(smem + G::srcOff) : nullptr;
+  // projections spread over all warps (Geo::projSplit): the flux-solver blocks of the four faces of
+  // a group arrive together, one group ahead
+  constexpr bool PSP = SS && G::projSplit;
+  double *fsExtra = PSP ? reinterpret_cast<double *>(smem + G::fsExtraOff) : nullptr;
   const int q = threadIdx.x >> 5, l = threadIdx.x & 31;
   const int eo = l / R, r = l % R;
   const int64_t nGroups = (a.elCount + E - 1) / E;
@@ -1188,6 +1267,11 @@ __global__ void __launch_bounds__(Geo<T, O, R, RM>::NT, LTS == 2 ? 1 : Geo<T, O,
     }
     if constexpr (PM) issueMixFs<T, O, R, RM, 0>(a, fsb, g0, nGroups);
     if constexpr (FL) issueLocalFs<T, O, R, RM, 0>(a, fsl, g0, nGroups);
+    if constexpr (PSP) {
+      issueLocalFs<T, O, R, RM, 1>(a, fsl + E * G::NFL, g0, nGroups);
+      issueLocalFs<T, O, R, RM, 2>(a, fsExtra, g0, nGroups);
+      issueLocalFs<T, O, R, RM, 3>(a, fsExtra + E * G::NFL, g0, nGroups);
+    }
     if constexpr (CS) issueCoef<T, O, R, RM>(a, coefBuf, g0, nGroups);
     cpAsyncCommit();
   }
@@ -1343,11 +1427,25 @@ __global__ void __launch_bounds__(Geo<T, O, R, RM>::NT, LTS == 2 ? 1 : Geo<T, O,
     if constexpr (AS) {
       const MixFs<T> mf{fsb, g, nGroups};
       const LocalFs lf{fsl, g, nGroups};
-      localFace<T, O, R, RM, 0, LTS, false>(a, TI, S0, q, l, ev, r, valid, acc, upA, TIh, X, mf, Sh, lf);
-      localFace<T, O, R, RM, 1, LTS, false>(a, TI, X, q, l, ev, r, valid, acc, upA, TIh, S0, mf, Sh, lf);
-      localFace<T, O, R, RM, 2, LTS, false>(a, TI, S0, q, l, ev, r, valid, acc, upA, TIh, X, mf, Sh, lf);
-      // the barrier after the last face orders its readers of X before the next group writes X
-      localFace<T, O, R, RM, 3, LTS, true>(a, TI, X, q, l, ev, r, valid, acc, upA, TIh, S0, mf, Sh, lf);
+      if constexpr (PSP) {
+        T *const tiles[4] = {S0, X, reinterpret_cast<T *>(smem + G::tilesOff),
+                             reinterpret_cast<T *>(smem + G::tilesOff) + G::nS0};
+        const double *const fs4[4] = {fsl, fsl + E * G::NFL, fsExtra, fsExtra + E * G::NFL};
+        facesSplit<T, O, R, RM>(a, TI, tiles, fs4, q, l, ev, valid, acc, upA);
+        // the next group's flux-solver blocks (every thread read this group's before the barrier)
+        const int64_t gn = g + gridDim.x;
+        issueLocalFs<T, O, R, RM, 0>(a, fsl, gn, nGroups);
+        issueLocalFs<T, O, R, RM, 1>(a, fsl + E * G::NFL, gn, nGroups);
+        issueLocalFs<T, O, R, RM, 2>(a, fsExtra, gn, nGroups);
+        issueLocalFs<T, O, R, RM, 3>(a, fsExtra + E * G::NFL, gn, nGroups);
+        cpAsyncCommit();
+      } else {
+        localFace<T, O, R, RM, 0, LTS, false>(a, TI, S0, q, l, ev, r, valid, acc, upA, TIh, X, mf, Sh, lf);
+        localFace<T, O, R, RM, 1, LTS, false>(a, TI, X, q, l, ev, r, valid, acc, upA, TIh, S0, mf, Sh, lf);
+        localFace<T, O, R, RM, 2, LTS, false>(a, TI, S0, q, l, ev, r, valid, acc, upA, TIh, X, mf, Sh, lf);
+        // the barrier after the last face orders its readers of X before the next group writes X
+        localFace<T, O, R, RM, 3, LTS, true>(a, TI, X, q, l, ev, r, valid, acc, upA, TIh, S0, mf, Sh, lf);
+      }
       if constexpr (SS)
         if (q < 6) addSrcRows<T, B, SB>(srcBuf, q, l, acc);
       if constexpr (CS) {
