@@ -337,6 +337,14 @@ struct Geo {
                                          : srcSplit  ? srcOff + srcBytes
                                          : fsLocal  ? smemLocal + fsLocalBytes + (coefSmem ? coefBytes : 0)
                                                     : smemLocal;
+  // the local kernel's shared-memory regions: in order, 16-byte aligned where 128-bit accesses or
+  // 16-byte copies reach them, within the 227 KB a CTA may hold
+  static_assert(smemLocal % 16 == 0, "buffers behind the tiles start on 16-byte boundaries");
+  static_assert(!srcSplit || (srcOff % 16 == 0 && srcOff >= smemLocal + fsLocalBytes + coefBytes),
+                "source tile behind the coefficients");
+  static_assert(!projSplit || (tilesOff % 16 == 0 && tilesOff >= fsExtraOff + fsLocalBytes),
+                "face tiles behind the flux-solver blocks of faces 2 and 3");
+  static_assert(smemLocalGts <= 227 * 1024, "local kernel within a CTA's shared memory");
   // elastic CK with ping-pong derivatives between X and the separate face tile
   static constexpr bool ckPingPong = asyncLocal && RM == 0 && nModes(O - 1) <= SF;
   // LTS local step: one more [9][32][SB] tile for the half-step time integral (behind the rest)
