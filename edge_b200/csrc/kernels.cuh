@@ -95,6 +95,13 @@ __host__ __device__ constexpr int padRow(int n) {
   if (m % 2 == 0) m++;
   return m * w;
 }
+// the same without the odd-chunk padding (rows of four-mode groups only), for tiles that would not
+// fit shared memory otherwise; 128-bit accesses then meet two-way bank conflicts
+template <typename T>
+__host__ __device__ constexpr int padRowTight(int n) {
+  const int w = 16 / int(sizeof(T));
+  return ((((n + 3) / 4) * 4 + w - 1) / w) * w;
+}
 
 template <typename T>
 __device__ __forceinline__ void ld4(const T *p, T (&v)[4]);
@@ -278,7 +285,12 @@ struct Geo {
   static constexpr int B = nModes(O), F = nFaceModes(O), E = 32 / R;
   static constexpr int NW = 9 + (RM ? 6 : 0);
   static constexpr int NT = NW * 32;
-  static constexpr int SB = padRow<T>(B), SF = padRow<T>(F);
+  // rows padded for conflict-free 128-bit accesses, unless the derivative, anelastic and face tiles
+  // would then exceed the 227 KB of a CTA (order 6 with attenuation): tight rows instead
+  static constexpr bool tightRows =
+      (size_t(9) * 32 * padRow<T>(B) * (1 + 2 * RM) + size_t(9) * 32 * padRow<T>(F)) * sizeof(T) > 227 * 1024;
+  static constexpr int SB = tightRows ? padRowTight<T>(B) : padRow<T>(B);
+  static constexpr int SF = tightRows ? padRowTight<T>(F) : padRow<T>(F);
   // X [9][32][SB]   derivatives during the CK recursion
   // TI [9][32][SB]  time-integrated DOFs
   // XA / TIA [RM][6][32][SB]  anelastic derivatives / time integrals
@@ -1165,9 +1177,10 @@ __device__ __forceinline__ void faceLift(const T *tile, const double *fp, int q,
 // the four local faces with the projections spread over all warps (Geo::projSplit, attenuation,
 // GTS): elastic warp q projects its row onto faces 0 and 1, anelastic warp s takes tasks 18 + s,
 // 24 + s and 30 + s of the 18 (face 2 and 3) row projections (task t: row t % 9, face t / 9); each
-// projection goes to its face tile and to the face buffer. After one barrier every warp mixes and
-// lifts its own row for the four faces (fs4: the flux-solver blocks of the four faces). A barrier
-// at the end orders the tiles' readers before X is written again.
+// projection goes to its face tile and to the face buffer. A barrier after every warp's first task
+// keeps the face-1 projections out of X until all DOF rows there have been read; after one more
+// barrier every warp mixes and lifts its own row for the four faces (fs4: the flux-solver blocks of
+// the four faces). A barrier at the end orders the tiles' readers before X is written again.
 template <typename T, int O, int R, int RM>
 __device__ __forceinline__ void facesSplit(const StepArgs<T> &a, const T *TI, T *const (&tiles)[4],
                                            const double *const (&fs4)[4], int q, int l, int64_t e, bool valid,
@@ -1177,6 +1190,10 @@ __device__ __forceinline__ void facesSplit(const StepArgs<T> &a, const T *TI, T 
   const int eo = l / R, r = l % R;
   const int nTasks = q < 9 ? 2 : 3;
   for (int j = 0; j < nTasks; j++) {
+    // face 1's tile is X, where the elastic warps have just reloaded and read their DOF rows (row
+    // stride SB, not SF): every warp passes this barrier after its first task, so no projection
+    // reaches X while another warp's DOF rows are still arriving there or being read
+    if (j == 1) __syncthreads();
     const int t = q < 9 ? q + 9 * j : 18 + (q - 9) + 6 * j;
     const int row = t % 9, fa = t / 9;
     T s[F];

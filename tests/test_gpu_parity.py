@@ -83,7 +83,10 @@ def test_fp64_all_boundary_types():
 @pytest.mark.parametrize("order,runs,rm", [(3, 16, 0), (4, 16, 0), (5, 16, 0), (6, 16, 0), (4, 8, 3),
                                            (3, 1, 0), (4, 1, 0), (5, 1, 0),
                                            (3, 4, 0), (4, 4, 0), (5, 4, 0), (6, 4, 0),
-                                           (3, 8, 0), (4, 8, 0), (5, 8, 0), (6, 8, 0), (3, 8, 3), (5, 8, 3)])
+                                           (3, 8, 0), (4, 8, 0), (5, 8, 0), (6, 8, 0), (3, 8, 3), (5, 8, 3),
+                                           (6, 1, 0), (3, 1, 3), (3, 4, 3), (3, 16, 3), (4, 1, 3), (4, 4, 3),
+                                           (4, 16, 3), (5, 1, 3), (5, 4, 3), (5, 16, 3), (6, 1, 3), (6, 4, 3),
+                                           (6, 8, 3), (6, 16, 3)])
 def test_fp32_fused_runs_vs_fp64_oracle(order, runs, rm):
     prob = small_problem(n=2, order=order, runs=runs, rm=rm, jitter=0.15, n_steps=3, source="random")
     s, orc, e, a, t, (rb, rt, rc) = _run_both(prob, 32, 3)
@@ -137,3 +140,33 @@ def test_kernel_config_reports_premix():
         assert info[3] >= 148 and info[4] >= 148
         assert info[5] == info[1]  # multi-step calls fuse the neighbour step where projections are pre-mixed
         s.close()
+
+
+def _per_range(a, b, chunks=4):
+    n = len(b)
+    return [rel_l2(a[n * i // chunks:n * (i + 1) // chunks], b[n * i // chunks:n * (i + 1) // chunks])
+            for i in range(chunks)]
+
+
+@pytest.mark.parametrize("n,order,runs,rm,prec", [(12, 4, 8, 3, 32), (12, 4, 1, 3, 64), (12, 3, 8, 3, 32),
+                                                  (10, 5, 16, 0, 32), (12, 4, 16, 0, 32)])
+def test_medium_mesh_vs_oracle(n, order, runs, rm, prec):
+    """Meshes with many element groups per persistent CTA (10,368 and 6,000 tets; the small cases
+    above have one group per CTA), so the kernels' one-group-ahead prefetches all take part:
+    jittered layered materials, random DOFs, 4 steps; every quarter of the element range within the
+    tolerance, and two runs of the device path bit-identical."""
+    prob = small_problem(n=n, order=order, runs=runs, rm=rm, jitter=0.2, n_steps=8, source="random",
+                         layers=[4000.0, 5500.0, 6500.0], lognormal_sigma=0.1)
+    tol = TOL64 if prec == 64 else TOL32
+    s, orc, e, a, t, (rb, rt, rc) = _run_both(prob, prec, 4)
+    errs = _per_range(e, orc.state["dofsE"])
+    if rm:
+        errs += _per_range(a, orc.state["dofsA"])
+    assert max(errs) < tol, errs
+    e0, a0 = random_dofs(prob, seed=1)
+    s.upload_dofs(e0, a0)
+    s.step(4, t=0.0)
+    e2, a2 = s.download_dofs()
+    assert np.array_equal(e, e2)
+    if rm:
+        assert np.array_equal(a, a2)
