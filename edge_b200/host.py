@@ -295,6 +295,22 @@ class Problem:
         a = np.zeros((self.n_el, self.rm, 6, self.B, self.runs), dtype) if self.rm else None
         return e, a
 
+    def single_run(self, r):
+        """The one-run problem of fused run r: same mesh, element data and receivers, with only
+        run r's point sources (EDGE runs a fused build's runs independently: no kernel mixes runs)."""
+        src = {}
+        s = self.sources
+        if s and s.get("n", 0):
+            keep = [i for i in range(s["n"]) if s["run"][i] == r]
+            pick = lambda k: np.ascontiguousarray(s[k][keep])
+            src = dict(n=len(keep), el=pick("el"), run=np.zeros(len(keep), np.int32), scal=pick("scal"),
+                       bEval=pick("bEval"), t0=pick("t0"), dt=pick("dt"), tsOff=pick("tsOff"), nPts=pick("nPts"),
+                       ts=s["ts"])
+        return Problem(order=self.order, runs=1, rm=self.rm, mesh=self.mesh, rho=self.rho, lam=self.lam,
+                       mu=self.mu, starE=self.starE, fsE=self.fsE, dt=self.dt, starA=self.starA, srcA=self.srcA,
+                       fsA=self.fsA, omega=self.omega, sources=src, receivers=self.receivers,
+                       name=self.name + f"_run{r}")
+
     def oracle_dict(self):
         """Element data in the oracle's layout (tests only)."""
         from . import dgmat
@@ -344,9 +360,13 @@ def build_problem(n_cubes, order, runs, rm=0, ext=1e4, jitter=0.0, seed=3343, vp
                   vs=3464.0, rho=2670.0, layers=None, lognormal_sigma=0.0, q_range=None,
                   freq_cen=1.0, freq_rat=100.0, n_receivers=8, source="explosive", f0=2.0,
                   n_steps=200, period=None, cfl=1.0, bc_top=FACE_FREE_SURFACE,
-                  bc_sides=FACE_OUTFLOW, name="", mesh=None):
+                  bc_sides=FACE_OUTFLOW, name="", mesh=None, f0_window=None, receivers_near=None):
     """Synthetic setups of the element update (box meshes, homogeneous or layered materials).
-    A given ``mesh`` (e.g. Mesh.from_gmsh of a box [0, ext]^3) replaces the generated box."""
+    A given ``mesh`` (e.g. Mesh.from_gmsh of a box [0, ext]^3) replaces the generated box.
+    Sources are Ricker moment rates peaking at 1.2 / f0; with ``f0_window`` the peak is put at that
+    fraction of the simulated time n_steps * dt instead (f0 follows), for runs too short for the
+    given f0. With ``receivers_near`` (metres) receiver i sits that far from run (i mod runs)'s
+    source in a seeded random direction instead of at a uniform position."""
     rng = np.random.default_rng(seed)
     if mesh is None:
         mesh = Mesh.box(n_cubes, (ext, ext, ext), jitter=jitter, seed=seed, bc_top=bc_top, bc_sides=bc_sides)
@@ -391,10 +411,18 @@ def build_problem(n_cubes, order, runs, rm=0, ext=1e4, jitter=0.0, seed=3343, vp
     if pos is not None:
         dts = dt / 10.0
         n_series = int(np.ceil(t_end / dts)) + 4
-        src = make_sources(mesh, order, runs, pos, scal, f0, 1.2 / f0, dts, n_series)
+        t_onset = 1.2 / f0
+        if f0_window:
+            t_onset = f0_window * t_end
+            f0 = 1.2 / t_onset
+        src = make_sources(mesh, order, runs, pos, scal, f0, t_onset, dts, n_series)
     rec = {}
     if n_receivers:
         rpos = rng.uniform(0.1 * ext, 0.9 * ext, (n_receivers, 3))
+        if receivers_near and pos is not None:
+            u = rng.normal(size=(n_receivers, 3))
+            u /= np.linalg.norm(u, axis=1)[:, None]
+            rpos = pos[np.arange(n_receivers) % runs] + receivers_near * u
         per = period if period else dt * 0.37
         rec = make_receivers(mesh, order, rpos, per, t_end)
     return Problem(order=order, runs=runs, rm=rm, mesh=mesh, rho=rhoe, lam=lam, mu=mu, starE=starE,

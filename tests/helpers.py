@@ -54,19 +54,7 @@ class OracleRun:
 
 def single_run(prob, r):
     """The one-run problem of fused run r (same mesh and element data, run r's sources)."""
-    src = {}
-    s = prob.sources
-    if s and s.get("n", 0):
-        keep = [i for i in range(s["n"]) if s["run"][i] == r]
-        src = dict(n=len(keep), el=np.ascontiguousarray(s["el"][keep]), run=np.zeros(len(keep), np.int32),
-                   scal=np.ascontiguousarray(s["scal"][keep]), bEval=np.ascontiguousarray(s["bEval"][keep]),
-                   t0=np.ascontiguousarray(s["t0"][keep]), dt=np.ascontiguousarray(s["dt"][keep]),
-                   tsOff=np.ascontiguousarray(s["tsOff"][keep]), nPts=np.ascontiguousarray(s["nPts"][keep]),
-                   ts=s["ts"])
-    return host.Problem(order=prob.order, runs=1, rm=prob.rm, mesh=prob.mesh, rho=prob.rho, lam=prob.lam,
-                        mu=prob.mu, starE=prob.starE, fsE=prob.fsE, dt=prob.dt, starA=prob.starA,
-                        srcA=prob.srcA, fsA=prob.fsA, omega=prob.omega, sources=src,
-                        receivers=prob.receivers, name=prob.name + f"_run{r}")
+    return prob.single_run(r)
 
 
 def rel_l2(a, b):
