@@ -7,13 +7,14 @@ KernelSet *makeKernelSet_o2(int precision, int order, int runs, int rms) {
   return nullptr;
 }
 
-// process-wide instances for callers that must not allocate (edge_b200_step_noalloc)
-KernelSet *staticKernelSet_o2(int precision, int order, int runs, int rms) {
+// process-wide instances, one per device, for callers that must not allocate
+// (edge_b200_step_noalloc); device < kStaticDevices
+KernelSet *staticKernelSet_o2(int precision, int order, int runs, int rms, int device) {
 #undef EDGE_B200_CFG
 #define EDGE_B200_CFG(T, O, R, RM, prec)                          \
   if (precision == prec && order == O && runs == R && rms == RM) { \
-    static KernelSetImpl<T, O, R, RM> inst;                       \
-    return &inst;                                                 \
+    static KernelSetImpl<T, O, R, RM> inst[kStaticDevices];       \
+    return &inst[device];                                         \
   }
 #include "inst_o2.inc"
   return nullptr;

@@ -59,9 +59,14 @@ class KernelSet {
   // caps on the persistent grids of the GTS local / neighbour kernels (0: resident CTAs per SM x
   // SMs, the default; a larger cap gives one CTA per element group up to it)
   virtual void setGridCaps(int local, int neigh) = 0;
+  // static instances only: init() has run on their device (edge_b200_step_noalloc, under its lock)
+  bool staticReady = false;
 };
 
 // returns nullptr when the configuration is not compiled in
 KernelSet *makeKernelSet(int precision, int order, int runs, int rms);
+
+// devices the allocation-free entry point serves (one static kernel set per device and configuration)
+constexpr int kStaticDevices = 64;
 
 }  // namespace edge_b200

@@ -13,11 +13,11 @@
 #include "layout.cuh"
 
 namespace edge_b200 {
-KernelSet *staticKernelSet_o2(int, int, int, int);
-KernelSet *staticKernelSet_o3(int, int, int, int);
-KernelSet *staticKernelSet_o4(int, int, int, int);
-KernelSet *staticKernelSet_o5(int, int, int, int);
-KernelSet *staticKernelSet_o6(int, int, int, int);
+KernelSet *staticKernelSet_o2(int, int, int, int, int);
+KernelSet *staticKernelSet_o3(int, int, int, int, int);
+KernelSet *staticKernelSet_o4(int, int, int, int, int);
+KernelSet *staticKernelSet_o5(int, int, int, int, int);
+KernelSet *staticKernelSet_o6(int, int, int, int, int);
 }  // namespace edge_b200
 
 using namespace edge_b200;
@@ -25,26 +25,40 @@ using namespace edge_b200;
 namespace {
 
 constexpr size_t kScratchBytes = EDGE_B200_NOALLOC_SCRATCH_BYTES;
-constexpr int kMaxDevices = 64;
+constexpr int kMaxDevices = kStaticDevices;
 
 // Held by every GPU that loads the library, until the process exits.
 __device__ __align__(256) unsigned char g_faceScratch[kScratchBytes];
 
-// per device: the array's device address (host code only sees a stand-in symbol) and whether
-// the kernel set's launch attributes were set on that device
+// per device: the array's device address (host code only sees a stand-in symbol); per device and
+// configuration: whether that kernel set's launch attributes and grid sizes were set (each device
+// has kernel sets of its own, so devices with different SM counts do not share grid sizes)
 std::mutex g_setupMutex;
 void *g_scratchPtr[kMaxDevices] = {};
 
-KernelSet *staticKernelSet(int precision, int order, int runs, int rms) {
+KernelSet *staticKernelSet(int precision, int order, int runs, int rms, int device) {
   switch (order) {
-    case 2: return staticKernelSet_o2(precision, order, runs, rms);
-    case 3: return staticKernelSet_o3(precision, order, runs, rms);
-    case 4: return staticKernelSet_o4(precision, order, runs, rms);
-    case 5: return staticKernelSet_o5(precision, order, runs, rms);
-    case 6: return staticKernelSet_o6(precision, order, runs, rms);
+    case 2: return staticKernelSet_o2(precision, order, runs, rms, device);
+    case 3: return staticKernelSet_o3(precision, order, runs, rms, device);
+    case 4: return staticKernelSet_o4(precision, order, runs, rms, device);
+    case 5: return staticKernelSet_o5(precision, order, runs, rms, device);
+    case 6: return staticKernelSet_o6(precision, order, runs, rms, device);
     default: return nullptr;
   }
 }
+
+// makes `device` current for the call and gives the caller's current device back on every return
+struct DeviceGuard {
+  int prev = -1;
+  bool ok = false;
+  explicit DeviceGuard(int device) {
+    if (cudaGetDevice(&prev) != cudaSuccess) return;
+    ok = prev == device || cudaSetDevice(device) == cudaSuccess;
+  }
+  ~DeviceGuard() {
+    if (ok && prev >= 0) cudaSetDevice(prev);
+  }
+};
 
 }  // namespace
 
@@ -66,21 +80,26 @@ extern "C" int edge_b200_step_noalloc(const edge_b200_cfg *cfg, int64_t n_el, do
       reinterpret_cast<uintptr_t>(vid_el_fa_el) % 4 || reinterpret_cast<uintptr_t>(el_fa_type) % 4)
     return EDGE_B200_EINVAL;
   const size_t realSize = cfg->precision == 64 ? 8 : 4;
-  // scratch: face projections, then the DOFs in the device-resident row layout (256-byte aligned)
+  // scratch: face projections, then the DOFs in the device-resident row layout (256-byte aligned);
+  // n_el is checked against the per-element size first, so the products below cannot wrap
   const int B = nModes(cfg->order), GB = rowPad(B, cfg->precision);
   const int GF = rowPad(nFaceModes(cfg->order), cfg->precision);
+  const size_t perEl = ((size_t)4 * 9 * GF + (size_t)(9 + 6 * cfg->n_rms) * GB) * cfg->n_runs * realSize;
+  if ((uint64_t)n_el > kScratchBytes / perEl) return EDGE_B200_ESCRATCH;
   auto align = [](size_t x) { return (x + 255) / 256 * 256; };
   const size_t faceBytes = align((size_t)n_el * 4 * 9 * cfg->n_runs * GF * realSize);
   const size_t dofsBytes = align((size_t)n_el * 9 * cfg->n_runs * GB * realSize);
   const size_t dofsABytes = align((size_t)n_el * 6 * cfg->n_rms * cfg->n_runs * GB * realSize);
   if (faceBytes + dofsBytes + dofsABytes > kScratchBytes) return EDGE_B200_ESCRATCH;
-  KernelSet *ks = staticKernelSet(cfg->precision, cfg->order, cfg->n_runs, cfg->n_rms);
+  KernelSet *ks = staticKernelSet(cfg->precision, cfg->order, cfg->n_runs, cfg->n_rms, cfg->device);
   if (!ks) return EDGE_B200_ENOTSUP;
 
-  if (cudaSetDevice(cfg->device) != cudaSuccess) return EDGE_B200_EDEVICE;
+  DeviceGuard dev(cfg->device);
+  if (!dev.ok) return EDGE_B200_EDEVICE;
   void *scratch = nullptr;
   {
-    // set-up once per device, with that device current
+    // set-up once per device (the scratch address) and once per device and configuration (the
+    // kernels' dynamic shared-memory limits and persistent grid sizes), with that device current
     std::lock_guard<std::mutex> lock(g_setupMutex);
     if (!g_scratchPtr[cfg->device]) {
       void *p = nullptr;
@@ -88,8 +107,10 @@ extern "C" int edge_b200_step_noalloc(const edge_b200_cfg *cfg, int64_t n_el, do
       g_scratchPtr[cfg->device] = p;
     }
     scratch = g_scratchPtr[cfg->device];
-    // sets the kernels' dynamic shared-memory limits and sizes the persistent grids (no allocation)
-    if (ks->init(cfg->device) != cudaSuccess) return EDGE_B200_EDEVICE;
+    if (!ks->staticReady) {
+      if (ks->init(cfg->device) != cudaSuccess) return EDGE_B200_EDEVICE;
+      ks->staticReady = true;
+    }
   }
 
   StepArgsRaw a;

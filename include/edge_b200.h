@@ -302,11 +302,13 @@ int edge_b200_kernel_config(const edge_b200_ctx *ctx, int32_t info[6]);
  * kernels' row layout (rows of B and F padded to 16 bytes) -- lives in one file-scope device array
  * of EDGE_B200_NOALLOC_SCRATCH_BYTES (32 MiB) that every GPU loading the library holds until exit;
  * a problem needing more (about n_el * R * (4 * 9 * F + (9 + 6 * n_rms) * B) * sizeof(real)
- * bytes) is rejected with EDGE_B200_ESCRATCH. The first call on a device looks up that array's device address (and sets
- * the kernels' shared-memory limits) with the device current; make that first call before any
- * stream capture. Every call shares the array: calls that overlap on the GPU (other streams,
- * other host threads) race and must be serialised by the caller. Nothing in it needs to start at
- * zero: each step writes every face projection before reading it.
+ * bytes) is rejected with EDGE_B200_ESCRATCH. The first call on a device looks up that array's
+ * device address, and the first call of each configuration on a device sets its kernels'
+ * shared-memory limits and grid sizes, with that device current; make those first calls before any
+ * stream capture. The call makes cfg->device current while it runs and restores the caller's
+ * current device before it returns. Every call shares the array: calls that overlap on the GPU
+ * (other streams, other host threads) race and must be serialised by the caller. Nothing in it
+ * needs to start at zero: each step writes every face projection before reading it.
  * Arguments: cfg as for edge_b200_create (order, n_runs, n_rms, precision, stream, device);
  * dofs_e / dofs_a in the cfg precision, element data in FP64 with the layouts of
  * edge_b200_upload_element_data, connectivity as in edge_b200_upload_mesh, all on cfg->device
