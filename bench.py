@@ -25,16 +25,7 @@ sys.path.insert(0, ROOT)
 METRIC = "elastic element-updates/s: batched FP32 vs plain FP64 at rel-L2 1e-4; p50/p99"
 UNIT = "element-updates/s"
 
-WORKLOADS = {
-    # name: (cubes per axis, order, runs, mechanisms, precision, source, f0)
-    "box48_o5_r16_fp32": (48, 5, 16, 0, 32, "random", 1.5),
-    "box12_o4_r1_fp64": (12, 4, 1, 0, 64, "explosive", 2.0),
-    "box60j_o4_r8_m3_fp32": (60, 4, 8, 3, 32, "random", 2.0),
-    # small case of the headline kernels for ncu captures (24,576 tets; DOFs 0.5 GB > L2)
-    "box16_o5_r16_fp32": (16, 5, 16, 0, 32, "random", 1.5),
-    # small case of the attenuation kernels (20^3 cubes x 6 = 48,000 tets; DOFs 0.83 GB > L2)
-    "box20j_o4_r8_m3_fp32": (20, 4, 8, 3, 32, "random", 2.0),
-}
+from edge_b200.workloads import WORKLOADS  # noqa: E402
 
 
 def parse():
@@ -47,6 +38,8 @@ def parse():
     ap.add_argument("--e2e-steps", type=int, default=10)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-fp64", action="store_true")
+    ap.add_argument("--parity", action=argparse.BooleanOptionalAction, default=True,
+                    help="per-run FP32 receiver error against FP64 at the workload's full size and steps")
     ap.add_argument("--serve-requests", type=int, default=160,
                     help="requests of the serving run (Poisson arrivals); 0 skips it")
     ap.add_argument("--serve-rate", type=float, default=40.0, help="mean arrivals per second")
@@ -139,15 +132,9 @@ class Clocks:
 
 
 def build_problem(name):
-    from edge_b200 import host
-    n, order, runs, rm, prec, source, f0 = WORKLOADS[name]
-    kw = {}
-    if rm:
-        kw = dict(jitter=0.2, layers=[4000.0, 5500.0, 6500.0], lognormal_sigma=0.1, q_range=(50.0, 200.0),
-                  freq_cen=1.0, freq_rat=100.0)
-    prob = host.build_problem(n, order, runs, rm=rm, ext=1e4, seed=3343, source=source, f0=f0,
-                              n_receivers=8, n_steps=500, name=name, **kw)
-    return prob, prec
+    from edge_b200 import workloads
+    prob, w = workloads.build(name)
+    return prob, w.precision
 
 
 def host_n_modes(order):
@@ -212,39 +199,91 @@ def traffic_from_profiles(workload):
     return None
 
 
-def cpu_sample_rate(order, runs, rm, n_cubes=12, steps=2):
-    """Reference CPU kernels (oracle/_ref, OpenMP over all host threads) on a bounded sample;
-    falls back to the C oracle port. Returns (element-updates/s, kind, cores, sample text)."""
+def cpu_reference_rate(order, runs, rm, n_cubes=16, steps=3, warm=1, r1=True):
+    """The reference's own vanilla CPU kernels (oracle/_ref, OpenMP over all host threads) on a
+    bounded sample of the workload: a box of n_cubes^3 x 6 tets (16^3: 24,576 tets; FP64 DOFs and
+    time-integrated DOFs of 2 x 9 x B x R x 8 bytes per element, 2.2 GB at order 5 with 16 runs,
+    beyond any L3), with its mesh and elastic element data built by the oracle's numpy mesh code
+    and the reference's compiled Elasticity::star / ::fs. `warm` untimed steps (the first constructs
+    the kernels), then the median of `steps` timed steps (local + neighbour). With r1, the same
+    sample is also timed with the one-run build, the rate of running the R runs one after another.
+    Falls back to the C oracle port (one thread) where oracle/_ref is absent.
+    Returns (element-updates/s, kind, cores, sample text, extra dict)."""
     import numpy as np
-    sys.path.insert(0, os.path.join(ROOT, "oracle"))
-    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    for p in (os.path.join(ROOT, "oracle"),):
+        if p not in sys.path:
+            sys.path.insert(0, p)
+    import mesh as om
     import oracle as orc
     import ref as refmod
-    from edge_b200 import host
-    prob = host.build_problem(n_cubes, order, runs, rm=rm, ext=1e4, seed=3343, source=None, n_receivers=0,
-                              n_steps=steps)
-    d = prob.oracle_dict()
-    rng = np.random.default_rng(0)
-    st = dict(dofsE=rng.normal(size=(prob.n_el, 9, prob.B, runs)),
-              dofsA=rng.normal(size=(prob.n_el, rm, 6, prob.B, runs)) if rm else None,
-              tDofs=np.zeros((prob.n_el, 9, prob.B, runs)))
     L = refmod.load(order, runs, rm)
-    cores = os.cpu_count() or 1
+    m = om.box(n_cubes)
+    ne = m["n_el"]
+    rho = np.full(ne, 2670.0)
+    mu = rho * 3464.0 ** 2
+    lam = rho * 6000.0 ** 2 - 2 * mu
+    extra = {}
+    setup = "mesh: oracle numpy box; element data: reference Elasticity::star/fs"
     if L is not None:
-        kind = "reference"
-        t0 = time.perf_counter()
-        for _ in range(steps):
-            refmod.step(L, d, st, 0.0, prob.dt)
-        el = time.perf_counter() - t0
+        starE, fsE = om.elastic_data(L, m, rho, lam, mu)
     else:
-        kind, cores = "port", 1
-        t0 = time.perf_counter()
-        for _ in range(steps):
-            orc.step(d, st, 0.0, prob.dt)
-        el = time.perf_counter() - t0
-    sample = (f"{n_cubes}^3 cubes x 6 = {prob.n_el} tets, order {order}, {runs} runs, {rm} mechanisms, "
-              f"{steps} steps (local + neighbour), FP64")
-    return prob.n_el * runs * steps / el, kind, cores, sample
+        from edge_b200 import host
+        hm = host.Mesh.box(n_cubes)
+        starE, fsE = host.star(hm, rho, lam, mu), host.flux_solvers(hm, rho, lam, mu)[0]
+        setup = "mesh and element data: host setup (oracle/_ref absent)"
+    d = dict(order=order, runs=runs, rm=rm, nEl=ne, starE=starE, fsE=fsE, elFaEl=m["el_fa_el"],
+             fIdElFaEl=m["fid"], vIdElFaEl=m["vid"], faType=m["el_fa_type"], starA=None, srcA=None, fsA=None,
+             omega=None)
+    if rm:
+        # anelastic coefficients through the host setup (the reference's needs Eigen, absent here)
+        from edge_b200 import host
+        hm = host.Mesh.box(n_cubes)
+        rng = np.random.default_rng(3343)
+        d["srcA"], d["omega"], lam2, mu2 = host.attenuation(rm, 1.0, 100.0, rng.uniform(50, 200, ne),
+                                                            rng.uniform(50, 200, ne), lam.copy(), mu.copy())
+        d["starA"] = host.star_anelastic(hm)
+        d["fsA"] = host.flux_solvers(hm, rho, lam2, mu2, rm)[1]
+        setup += "; anelastic data: host setup"
+    from edge_b200.dgmat import matrices
+    d.update({k: v for k, v in matrices(order).items() if k in ("stiffT", "stiffV", "fluxL", "fluxN", "fluxT")})
+    d = {k: (np.ascontiguousarray(v) if isinstance(v, np.ndarray) else v) for k, v in d.items()}
+    dt = 0.5 * float(m["el_india"].min()) / 6000.0 / (2 * order - 1)
+    B = host_n_modes(order)
+    rng = np.random.default_rng(0)
+
+    def state(r):
+        return dict(dofsE=rng.normal(size=(ne, 9, B, r)), dofsA=rng.normal(size=(ne, rm, 6, B, r)) if rm else None,
+                    tDofs=np.zeros((ne, 9, B, r)))
+
+    def timed(lib, r, n_warm, n_timed):
+        st = state(r)
+        dd = dict(d, runs=r)
+        ts = []
+        for i in range(n_warm + n_timed):
+            t0 = time.perf_counter()
+            if lib is not None:
+                refmod.step(lib, dd, st, 0.0, dt)
+            else:
+                orc.step(dd, st, 0.0, dt)
+            if i >= n_warm:
+                ts.append(time.perf_counter() - t0)
+        return ne * r / statistics.median(ts), ts
+
+    cores = os.cpu_count() or 1
+    kind = "reference" if L is not None else "port"
+    if L is None:
+        cores = 1
+    value, ts = timed(L, runs, warm, steps)
+    sample = (f"{n_cubes}^3 cubes x 6 = {ne} tets, order {order}, {runs} runs, {rm} mechanisms, FP64, "
+              f"{warm} warm-up + median of {steps} timed steps (local + neighbour); {setup}")
+    extra["step_s"] = ts
+    if r1 and runs > 1:
+        L1 = refmod.load(order, 1, rm)
+        if L1 is not None:
+            v1, t1 = timed(L1, 1, 1, max(steps, 3))
+            extra["one_run_build"] = {"value": v1, "unit": UNIT, "step_s": t1,
+                                      "note": f"the {runs} runs one after another with the one-run build"}
+    return value, kind, cores, sample, extra
 
 
 def run_serve(n_req, rate, device, seed=3343):
@@ -438,20 +477,19 @@ def run_lts(device, n_cubes=48, order=5, runs=16, n_groups=3, cycles=2):
 
 
 def run_reference(a, ws, rank):
+    """The reference arm: the reference's own vanilla CPU kernels (oracle/_ref) on the host cores,
+    rank 0 only; each of the warm-up and timed steps is one step over the bounded sample of the
+    workload (cpu_reference_rate). Nothing of the CUDA library is loaded on this path for elastic
+    workloads."""
     if rank != 0:
         return
-    n, order, runs, rm, prec, source, f0 = WORKLOADS[a.workload]
-    vals = []
-    for i in range(a.warmup + a.steps):
-        v, kind, cores, sample = cpu_sample_rate(order, runs, rm, n_cubes=8, steps=1)
-        if i >= a.warmup:
-            vals.append(v)
-    value = statistics.median(vals)
+    w = WORKLOADS[a.workload]
+    value, kind, cores, sample, extra = cpu_reference_rate(w.order, w.runs, w.rm, warm=a.warmup, steps=a.steps)
     out = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": a.gpus,
            "steps": a.steps, "warmup": a.warmup, "higher_is_better": True, "scaling": "weak",
            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
            "config": {"workload": a.workload, "reference_sample": sample},
-           "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": kind, "sample": sample},
+           "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": kind, "sample": sample, **extra},
            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(out), flush=True)
 
@@ -593,7 +631,7 @@ def main():
         s64.upload_dofs(z)
         s64.step(2)
         s64.sync()
-        k64 = max(2, a.steps // 4)
+        k64 = max(20, a.steps)
         y0, y1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         y0.record(stream)
         s64.step(k64)
@@ -616,10 +654,18 @@ def main():
 
     cpu = None
     if rank == 0 and not a.no_cpu_baseline:
-        v, kind, cores, sample = cpu_sample_rate(prob.order, prob.runs, prob.rm, n_cubes=8, steps=1)
-        cpu = {"value": v, "unit": UNIT, "cores": cores, "kind": kind, "sample": sample}
+        v, kind, cores, sample, extra = cpu_reference_rate(prob.order, prob.runs, prob.rm)
+        cpu = {"value": v, "unit": UNIT, "cores": cores, "kind": kind, "sample": sample, **extra}
 
     sv.close()
+    # the FP32 error bar at the workload's full size and stated step count: per fused run, the
+    # receivers against the same run alone on the plain FP64 path (pinned to the oracle to 1e-12)
+    parity = None
+    if a.parity and rank == 0 and prec == 32:
+        from edge_b200 import accuracy
+        parity = accuracy.fused_vs_plain(prob, WORKLOADS[a.workload].steps, device=local)
+        parity["tolerance"] = 1e-4
+        parity["within_tolerance"] = parity["receiver_rel_l2_max"] < 1e-4
     serving = None
     if a.serve_requests > 0:
         serving = run_serve(a.serve_requests, a.serve_rate, local)
@@ -639,7 +685,7 @@ def main():
                                                                                       int(0.99 * len(step_ms)))],
                "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": int(launches),
                "clocks": clk, "fp64_plain": fp64, "serving": serving, "roofline_neighbour": roofline_neighbour, "lts": lts,
-               "batch": batch}
+               "batch": batch, "parity_at_size": parity}
         print(json.dumps(out), flush=True)
     barrier(ws)
     if ws > 1:

@@ -1,9 +1,10 @@
 # Compiles the reference's own vanilla kernels (unchanged, from the reference checkout) into
 # oracle/_ref/libedgeref_O<order>_R<runs>_M<mechanisms>.so, driven by ref_driver.cpp.
-# TEST INFRASTRUCTURE ONLY; needs the reference sources (EDGE_REF, default /root/reference).
+# TEST INFRASTRUCTURE ONLY; needs the reference sources: EDGE_REF (or the EDGE_REFERENCE
+# environment variable), else a checkout named "reference" beside this repository.
 #   make -f ref.mk            builds the default configurations
 #   make -f ref.mk CFGS="4_1_0"
-EDGE_REF ?= /root/reference
+EDGE_REF ?= $(or $(EDGE_REFERENCE),$(abspath $(CURDIR)/../../reference))
 # the image exports CXX without OpenMP runtime files; the system compiler has them
 CXX := $(if $(wildcard /usr/bin/g++),/usr/bin/g++,g++)
 OUT := _ref

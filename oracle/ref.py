@@ -10,7 +10,8 @@ import subprocess
 import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-REF = os.environ.get("EDGE_REFERENCE", "/root/reference")
+# the reference checkout: $EDGE_REFERENCE, else "reference" beside this repository
+REF = os.environ.get("EDGE_REFERENCE", os.path.join(os.path.dirname(os.path.dirname(HERE)), "reference"))
 _cache = {}
 
 

@@ -21,7 +21,7 @@ import types
 
 import numpy as np
 
-REF = os.environ.get("EDGE_REFERENCE", "/root/reference")
+REF = os.environ.get("EDGE_REFERENCE", os.path.abspath(os.path.join(os.path.dirname(__file__), "..", "..", "..", "reference")))
 sys.path.insert(0, os.path.join(REF, "tools", "edge_pre"))
 
 # the triangle basis module imports matplotlib for plotting only; a stub suffices

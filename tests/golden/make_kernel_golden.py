@@ -22,7 +22,7 @@ import sys
 
 import numpy as np
 
-REF = os.environ.get("EDGE_REFERENCE", "/root/reference")
+REF = os.environ.get("EDGE_REFERENCE", os.path.abspath(os.path.join(os.path.dirname(__file__), "..", "..", "..", "reference")))
 KDIR = os.path.join(REF, "src", "impl", "seismic", "kernels")
 NUM = re.compile(r"[-+]?(?:\d+\.\d*|\.\d+|\d+)(?:[eE][-+]?\d+)?")
 
