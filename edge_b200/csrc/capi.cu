@@ -660,6 +660,36 @@ int edge_b200_set_run_dofs(edge_b200_ctx *ctx, int run, const void *dofs_e, cons
   return EDGE_B200_OK;
 }
 
+int edge_b200_copy_run(edge_b200_ctx *dst, int dst_run, edge_b200_ctx *src, int src_run) {
+  if (!dst || !src || dst_run < 0 || dst_run >= dst->cfg.n_runs || src_run < 0 || src_run >= src->cfg.n_runs)
+    return EDGE_B200_EINVAL;
+  if (dst->nEl != src->nEl || dst->cfg.order != src->cfg.order || dst->cfg.n_rms != src->cfg.n_rms ||
+      dst->cfg.precision != src->cfg.precision || dst->cfg.device != src->cfg.device || dst->GB != src->GB)
+    return EDGE_B200_EINVAL;
+  if (dst == src && dst_run == src_run) return EDGE_B200_OK;
+  edge_b200_ctx *ctx = dst;  // errors are recorded on the destination
+  EDGE_CUDA(src->flush(), "pending neighbour step");
+  EDGE_CUDA(dst->flush(), "pending neighbour step");
+  // the source's stream reaches this point before the destination's copies start
+  cudaEvent_t ev;
+  EDGE_CUDA(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming), "copy run");
+  cudaError_t e = cudaEventRecord(ev, src->stream);
+  if (e == cudaSuccess) e = cudaStreamWaitEvent(dst->stream, ev, 0);
+  cudaEventDestroy(ev);
+  EDGE_CUDA(e, "copy run");
+  // one padded row [GB] per (element, quantity row) of the run: a strided 2D copy per DOF array
+  const size_t row = (size_t)dst->GB * dst->realSize;
+  for (int part = 0; part < (dst->cfg.n_rms ? 2 : 1); part++) {
+    const int64_t nRows = dst->nEl * (part == 0 ? 9 : 6 * dst->cfg.n_rms);
+    char *d = static_cast<char *>(part == 0 ? dst->dofsE : dst->dofsA) + dst_run * row;
+    const char *sp = static_cast<const char *>(part == 0 ? src->dofsE : src->dofsA) + src_run * row;
+    EDGE_CUDA(cudaMemcpy2DAsync(d, dst->cfg.n_runs * row, sp, src->cfg.n_runs * row, row, (size_t)nRows,
+                                cudaMemcpyDeviceToDevice, dst->stream),
+              "copy run");
+  }
+  return EDGE_B200_OK;
+}
+
 int edge_b200_keep_tdofs(edge_b200_ctx *ctx, int enable) {
   if (!ctx) return EDGE_B200_EINVAL;
   if (enable && !ctx->tDofs) {

@@ -356,6 +356,38 @@ def make_receivers(mesh, order, positions, period, t_end, t_first=0.0):
                 positions=np.asarray(positions)[order_idx])
 
 
+def materials(mesh, ext, vp=6000.0, vs=3464.0, rho=2670.0, layers=None, lognormal_sigma=0.0, rng=None):
+    """Per-element (rho, lam, mu): homogeneous, or horizontal layers of vp (listed from the top,
+    z = ext, down; vs = vp / sqrt(3)), each element optionally scaled by a seeded lognormal factor."""
+    ne = mesh.n_el
+    if layers is None:
+        vpe = np.full(ne, vp)
+    else:
+        z = mesh.centroids()[:, 2]
+        bounds = np.linspace(0, ext, len(layers) + 1)
+        idx = np.clip(np.searchsorted(bounds, z, side="right") - 1, 0, len(layers) - 1)
+        vpe = np.asarray(layers, np.float64)[::-1][idx]
+    if lognormal_sigma > 0:
+        vpe = vpe * rng.lognormal(0.0, lognormal_sigma, ne)
+    vse = vpe / np.sqrt(3.0) if layers is not None else np.full(ne, vs) * (vpe / vp)
+    rhoe = np.full(ne, rho)
+    mu = rhoe * vse ** 2
+    lam = rhoe * vpe ** 2 - 2 * mu
+    return rhoe, lam, mu
+
+
+def element_data(mesh, rho, lam, mu, rm=0, qp=None, qs=None, freq_cen=1.0, freq_rat=100.0):
+    """Star matrices and flux solvers (and, with rm mechanisms and qualities qp / qs, the anelastic
+    data, with lam / mu replaced by the unrelaxed values first, as AderDgInit.hpp:113-115 does)."""
+    srcA = omega = starA = fsA = None
+    if rm:
+        srcA, omega, lam, mu = attenuation(rm, freq_cen, freq_rat, qp, qs, lam, mu)
+        starA = star_anelastic(mesh)
+    starE = star(mesh, rho, lam, mu)
+    fsE, fsA = flux_solvers(mesh, rho, lam, mu, rm)
+    return dict(lam=lam, mu=mu, starE=starE, fsE=fsE, starA=starA, srcA=srcA, fsA=fsA, omega=omega)
+
+
 def build_problem(n_cubes, order, runs, rm=0, ext=1e4, jitter=0.0, seed=3343, vp=6000.0,
                   vs=3464.0, rho=2670.0, layers=None, lognormal_sigma=0.0, q_range=None,
                   freq_cen=1.0, freq_rat=100.0, n_receivers=8, source="explosive", f0=2.0,
@@ -371,29 +403,15 @@ def build_problem(n_cubes, order, runs, rm=0, ext=1e4, jitter=0.0, seed=3343, vp
     if mesh is None:
         mesh = Mesh.box(n_cubes, (ext, ext, ext), jitter=jitter, seed=seed, bc_top=bc_top, bc_sides=bc_sides)
     ne = mesh.n_el
-    if layers is None:
-        vpe = np.full(ne, vp)
-    else:
-        z = mesh.centroids()[:, 2]
-        bounds = np.linspace(0, ext, len(layers) + 1)
-        idx = np.clip(np.searchsorted(bounds, z, side="right") - 1, 0, len(layers) - 1)
-        # layers are listed top (free surface, z = ext) to bottom
-        vpe = np.asarray(layers, np.float64)[::-1][idx]
-    if lognormal_sigma > 0:
-        vpe = vpe * rng.lognormal(0.0, lognormal_sigma, ne)
-    vse = vpe / np.sqrt(3.0) if layers is not None else np.full(ne, vs) * (vpe / vp)
-    rhoe = np.full(ne, rho)
-    mu = rhoe * vse ** 2
-    lam = rhoe * vpe ** 2 - 2 * mu
-    srcA = omega = starA = fsA = None
+    rhoe, lam, mu = materials(mesh, ext, vp, vs, rho, layers, lognormal_sigma, rng)
+    qp = qs = None
     if rm:
         lo, hi = q_range if q_range else (50.0, 200.0)
         qp = rng.uniform(lo, hi, ne)
         qs = rng.uniform(lo, hi, ne)
-        srcA, omega, lam, mu = attenuation(rm, freq_cen, freq_rat, qp, qs, lam, mu)
-        starA = star_anelastic(mesh)
-    starE = star(mesh, rhoe, lam, mu)
-    fsE, fsA = flux_solvers(mesh, rhoe, lam, mu, rm)
+    ed = element_data(mesh, rhoe, lam, mu, rm, qp, qs, freq_cen, freq_rat)
+    lam, mu = ed["lam"], ed["mu"]
+    starE, fsE, starA, srcA, fsA, omega = (ed[k] for k in ("starE", "fsE", "starA", "srcA", "fsA", "omega"))
     dt = dt_cfl(mesh, order, rhoe, lam, mu) * cfl
     t_end = n_steps * dt
     # sources

@@ -186,6 +186,13 @@ int edge_b200_join_transfers(edge_b200_ctx *ctx, int after_stream);
  * when a run slot is handed to a new simulation while the others continue (no counterpart in the
  * reference, whose fused runs start and end together). */
 int edge_b200_set_run_dofs(edge_b200_ctx *ctx, int run, const void *dofs_e, const void *dofs_a);
+/* Copies fused run src_run of context src into run dst_run of context dst on the device (elastic
+ * and anelastic DOFs; the other runs of dst keep theirs), on dst's stream after the work queued on
+ * src's stream. Both contexts must have the same mesh size, order, mechanisms, precision and
+ * device; their numbers of fused runs may differ. Used to move running simulations between pools
+ * of different run counts (no counterpart in the reference, whose fused runs start and end
+ * together). */
+int edge_b200_copy_run(edge_b200_ctx *dst, int dst_run, edge_b200_ctx *src, int src_run);
 /* Keep the time-integrated DOFs tDofs[nEl][9][B][R] of each local step (the tDofs[0] of
  * steps.inc) in device memory (allocated on first enable; off by default, which saves their HBM
  * writes), and copy the last step's to the host (EDGE_B200_EINVAL unless kept). */
