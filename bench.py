@@ -38,11 +38,13 @@ def parse():
     ap.add_argument("--e2e-steps", type=int, default=10)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-fp64", action="store_true")
+    ap.add_argument("--tc-probe", action=argparse.BooleanOptionalAction, default=True,
+                    help="time tcgen05 tf32 MMAs at the DG products' shapes (the tensor-core alternative)")
     ap.add_argument("--parity", action=argparse.BooleanOptionalAction, default=True,
                     help="per-run FP32 receiver error against FP64 at the workload's full size and steps")
     ap.add_argument("--serve-requests", type=int, default=160,
                     help="requests of the serving run (Poisson arrivals); 0 skips it")
-    ap.add_argument("--serve-rate", type=float, default=40.0, help="mean arrivals per second")
+    ap.add_argument("--serve-rate", type=float, default=20.0, help="mean arrivals per second")
     ap.add_argument("--lts-report", action="store_true",
                     help="also time rate-2 LTS against GTS on a layered box (adds about a minute)")
     ap.add_argument("--batch-sims", type=int, default=32,
@@ -286,39 +288,87 @@ def cpu_reference_rate(order, runs, rm, n_cubes=16, steps=3, warm=1, r1=True):
     return value, kind, cores, sample, extra
 
 
-def run_serve(n_req, rate, device, seed=3343):
-    """The serving form: simulation requests (own point source, 4-16 receivers, 100-300 steps) on
-    two meshes (16^3 and 12^3 cubes x 6 tets) at orders 4 and 5, continuously batched into 16-run
-    FP32 pools. Two passes over the same seeded requests: all arriving at once (capacity: delivered
-    element updates per second against running them one after another as plain FP64 single runs,
-    timed on the same meshes) and Poisson arrivals at `rate` per second (latency percentiles)."""
+# the serving stream: four seeded meshes with their material sets (10,368 to 1,053,696 tets), the
+# orders each serves (elastic; viscoelastic requests at orders 3-4 where listed) and the step range
+# of its requests
+SERVE_MESHES = {
+    "box12": (dict(n_cubes=12, ext=7.5e3, seed=11), (3, 4, 5, 6), (3, 4), (200, 2000)),
+    "box20j": (dict(n_cubes=20, jitter=0.1, layers=(4000.0, 5500.0, 6500.0), lognormal_sigma=0.1, seed=12),
+               (3, 4, 5, 6), (3, 4), (100, 1000)),
+    "box32": (dict(n_cubes=32, layers=(4000.0, 6000.0), lognormal_sigma=0.1, seed=13), (3, 4, 5, 6), (3, 4),
+              (100, 400)),
+    "box56": (dict(n_cubes=56, seed=14), (3, 4, 5, 6), (), (100, 150)),
+}
+
+
+def serve_stream(n_req, rate, seed):
+    """Requests of the bounded serving stream: Poisson(rate) arrivals over SERVE_MESHES, 25%
+    viscoelastic where the mesh serves it, 4-16 receivers, the mesh's step range."""
+    import numpy as np
+    from edge_b200 import serve
+    specs = {k: serve.MeshSpec(**v[0]) for k, v in SERVE_MESHES.items()}
+    rng = np.random.default_rng(seed)
+    reqs = serve.make_stream(n_req, rate, specs, orders=(3, 4, 5, 6), seed=seed, visco=0.25,
+                             mesh_steps={k: v[3] for k, v in SERVE_MESHES.items()})
+    for r in reqs:  # each mesh's own orders and physics
+        _, orders, vorders, _ = SERVE_MESHES[r.mesh]
+        if r.rm and not vorders:
+            r.rm = 0
+        allowed = vorders if r.rm else orders
+        if r.order not in allowed:
+            r.order = int(rng.choice(allowed))
+    return specs, reqs
+
+
+def run_serve(n_req, rate, device, seed=3343, n_check=12):
+    """The serving form on a bounded stream shaped like the serving configuration: n_req requests
+    (Poisson arrivals at `rate` per second) over four meshes of 10,368 to 1,053,696 tets with
+    their own material sets, orders 3-6 (elastic) and 3-4 (viscoelastic, 3 mechanisms), 100-2,000
+    steps, 4-16 receivers and own random sources, continuously batched into 16-run FP32 pools under
+    an 80% HBM budget. Two passes over the same seeded requests: all arriving at once (capacity:
+    delivered element updates per second against running each request alone as a plain FP64
+    single run, timed per mesh / order / physics on the same GPU) and the Poisson stream (latency
+    percentiles). Pools take 1, 4, 8 or 16 fused runs as the waiting requests and the HBM budget
+    allow (the 1 M-tet mesh at orders 5-6 fits 4-8 runs). n_check requests (spread over meshes and
+    physics) are run again alone on the plain FP64 path and their served receiver traces compared
+    by relative L2."""
+    import numpy as np
     import torch
-    from edge_b200 import host, serve
+    from edge_b200 import serve
     from edge_b200.solver import Solver
-    specs = {"box16": serve.MeshSpec(16), "box12": serve.MeshSpec(12, ext=7.5e3)}
-    keys = [(m, o) for m in specs for o in (4, 5)]
     out = {}
-    for name, r in (("burst", 1e6), ("poisson", rate)):
-        reqs = serve.make_stream(n_req, r, specs, orders=(4, 5), steps=(100, 300), seed=seed)
-        srv = serve.Server(specs, runs=16, precision=32, chunk=20, device=device)
-        srv.warm(keys)
+    specs, reqs0 = serve_stream(n_req, rate, seed)
+    keys = sorted({(r.mesh, r.order, r.rm) for r in reqs0})
+    meshes = serve.MeshCache(specs)
+    for k in keys:  # host setup of every mesh, material set and physics outside the timed passes
+        meshes.data(k[0], k[2])
+    served = None
+    for name, r8 in (("burst", None), ("poisson", rate)):
+        _, reqs = serve_stream(n_req, rate, seed)
+        if r8 is None:
+            for r in reqs:
+                r.arrival = 0.0
+        srv = serve.Server(specs, runs=16, precision=32, chunk=40, device=device)
+        srv.meshes = meshes
         done = srv.run(reqs, clock="wall")
-        n_el = {m: srv.meshes.get(m)[0].n_el for m in specs}
-        meshes = srv.meshes
         srv.close()
         lat = serve.latency_stats(done)
-        out[name] = dict(requests=len(done), arrival_rate_per_s=r, wall_s=srv.wall, latency_s_p50=lat["p50"],
-                         latency_s_p99=lat["p99"],
+        n_el = {k: meshes.data(k, 0)["mesh"].n_el for k in specs}
+        out[name] = dict(requests=len(done), arrival_rate_per_s=r8, wall_s=srv.wall, latency_s_p50=lat["p50"],
+                         latency_s_p99=lat["p99"], pools_opened=srv.pools_opened, max_pools=srv.max_pools,
+                         pool_resizes=srv.resizes,
+                         slot_utilisation=srv.slot_updates_used / max(srv.slot_updates_offered, 1),
                          delivered_element_updates_per_s=sum(n_el[x.mesh] * x.n_steps for x in done) / srv.wall)
-    # plain FP64, one run, same mesh and order: ms per step
+        if name == "burst":
+            served = {x.rid: x for x in done}
+    # plain FP64, one run, same mesh, order and physics: ms per step
     ms64 = {}
-    for m, o in keys:
-        mesh, rho, lam, mu, star, fsE = meshes.get(m)
-        dt = host.dt_cfl(mesh, o, rho, lam, mu)
-        p = host.Problem(order=o, runs=1, rm=0, mesh=mesh, rho=rho, lam=lam, mu=mu, starE=star, fsE=fsE, dt=dt)
+    for m, o, rm in keys:
+        p = meshes.problem(m, o, 1, rm)
         st = torch.cuda.Stream(device=device)
         sv = Solver(p, precision=64, stream=st.cuda_stream, device=device)
-        sv.upload_dofs(p.zero_dofs()[0])
+        e, a = p.zero_dofs()
+        sv.upload_dofs(e, a)
         sv.step(3)
         sv.sync()
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -326,15 +376,103 @@ def run_serve(n_req, rate, device, seed=3343):
         sv.step(20)
         e1.record(st)
         torch.cuda.synchronize()
-        ms64[(m, o)] = e0.elapsed_time(e1) / 20
+        ms64[(m, o, rm)] = e0.elapsed_time(e1) / 20
         sv.close()
-    reqs = serve.make_stream(n_req, rate, specs, orders=(4, 5), steps=(100, 300), seed=seed)
-    serial_s = sum(ms64[(x.mesh, x.order)] * x.n_steps for x in reqs) / 1e3
+    # the same keys as 16-run FP32 pools at full occupancy (8 runs where 16 exceed the budget: the
+    # kernel-level ratio the serving form can reach), and the cost of opening such a pool
+    ms32, open_s, runs32 = {}, {}, {}
+    budget = 0.8 * torch.cuda.mem_get_info(device)[1]
+    for m, o, rm in keys:
+        t_open = time.perf_counter()
+        nr = 16 if serve.pool_bytes(meshes.data(m, rm)["mesh"].n_el, o, 16, 32, rm) < budget else 8
+        runs32[(m, o, rm)] = nr
+        p = meshes.problem(m, o, nr, rm)
+        st = torch.cuda.Stream(device=device)
+        sv = Solver(p, precision=32, stream=st.cuda_stream, device=device)
+        sv.step(3)
+        sv.sync()
+        open_s[(m, o, rm)] = time.perf_counter() - t_open
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(st)
+        sv.step(20)
+        e1.record(st)
+        torch.cuda.synchronize()
+        ms32[(m, o, rm)] = e0.elapsed_time(e1) / 20 * 16 / nr  # per 16 runs
+        sv.close()
+    serial_s = sum(ms64[(x.mesh, x.order, x.rm)] * x.n_steps for x in reqs0) / 1e3
+    ideal_s = sum(ms32[(x.mesh, x.order, x.rm)] / 16 * x.n_steps for x in reqs0) / 1e3
     out["burst"]["serial_plain_fp64_s"] = serial_s
     out["burst"]["speedup_vs_serial_plain_fp64"] = serial_s / out["burst"]["wall_s"]
-    out.update(pools=len(keys), slots_per_pool=16, chunk_steps=20,
-               note="wall clock from the first arrival; latency = arrival -> last receiver sample on the host")
+    out["burst"]["full_pools_fp32_s"] = ideal_s
+    out["burst"]["kernel_level_speedup"] = serial_s / ideal_s
+    # per-request error of served results against the plain FP64 path
+    rng = np.random.default_rng(seed + 1)
+    groups = {}
+    for x in reqs0:
+        groups.setdefault((x.mesh, x.rm), []).append(x.rid)
+    pick = []
+    while len(pick) < n_check and any(groups.values()):
+        for g in sorted(groups):
+            if groups[g] and len(pick) < n_check:
+                pick.append(groups[g].pop(int(rng.integers(len(groups[g])))))
+    checks = []
+    for rid in pick:
+        x = served[rid]
+        ref = serve.plain_fp64(x, meshes, device=device)
+        got = x.result()
+        checks.append(dict(rid=rid, mesh=x.mesh, order=x.order, mechanisms=x.rm, steps=x.n_steps,
+                           receivers=len(x.rec_pos),
+                           rel_l2=float(np.linalg.norm(got - ref) / max(np.linalg.norm(ref), 1e-300))))
+    out.update(pools=len(keys), slots_per_pool=16, chunk_steps=40,
+               meshes={k: meshes.data(k, 0)["mesh"].n_el for k in specs},
+               stream=dict(requests=n_req, rate_per_s=rate, viscoelastic=sum(1 for x in reqs0 if x.rm),
+                           orders=sorted({x.order for x in reqs0}),
+                           steps=[min(x.n_steps for x in reqs0), max(x.n_steps for x in reqs0)]),
+               per_request_fp64_check=checks, per_request_rel_l2_max=max(c["rel_l2"] for c in checks),
+               plain_fp64_ms_per_step={f"{m}/o{o}/m{rm}": v for (m, o, rm), v in ms64.items()},
+               fp32_16runs_ms_per_step={f"{m}/o{o}/m{rm}": v for (m, o, rm), v in ms32.items()},
+               pool_open_s={f"{m}/o{o}/m{rm}": v for (m, o, rm), v in open_s.items()},
+               note="wall clock from the first arrival; latency = arrival -> last receiver sample on the host; "
+                    "bounded stream (the 2,000-request, 2 M-tet configuration does not fit one run of the bench: "
+                    "16-run pools of 2 M tets at order 6 need about 430 GB)")
     return out
+
+
+def run_tc_probe(local_ms, n_el, order, runs, device, clock_mhz):
+    """The tensor-core alternative for the local kernel's DG products, measured: tcgen05.mma
+    kind::tf32 (operands in shared memory, accumulator in tensor memory, one CTA per SM) timed per
+    instruction of 128 x N x 8 for the N the products would have, then the instructions one local
+    step needs in the tensor formulation -- rows (quantity, element, run) on M in tiles of 128 (the
+    288 rows of an element group in three tiles), output modes on N (padded to 16), input modes x 3
+    derivative directions (or x 4 faces) on K, each product three times for FP32 accuracy from tf32
+    (split operands) -- at the measured cycles. Only the products: the star and flux-solver mixes,
+    loads, stores and tensor-memory read-back come on top."""
+    from edge_b200 import tcprobe
+    from edge_b200.host import n_face_modes, n_modes
+    errs = {f"{n}x{k}x{it}": tcprobe.check(n, k, it) for n, k, it in ((16, 8, 1), (64, 32, 1), (128, 32, 3))}
+    cyc = {}
+    for n in (16, 32, 48, 64, 96, 128):
+        ms, per_cta = tcprobe.time_shape(n)
+        cyc[n] = ms * 1e-3 * clock_mhz * 1e6 / per_cta
+    pad = lambda x, q: (x + q - 1) // q * q
+    Bm = lambda o: n_modes(o) if o > 0 else 0
+    F = n_face_modes(order)
+    prods = [("ck%d" % d, pad(Bm(order - d), 16), pad(3 * Bm(order - d + 1), 8)) for d in range(1, order)]
+    prods += [("volume", pad(Bm(order), 16), pad(3 * Bm(order - 1), 8)), ("fluxL", pad(4 * F, 16), pad(Bm(order), 8)),
+              ("fluxT", pad(Bm(order), 16), pad(4 * F, 8))]
+    groups_per_sm = n_el * runs / 32 / 148
+    tiles, split = 3, 3
+    est = {}
+    for name, nn, kk in prods:
+        c = cyc[min(x for x in cyc if x >= nn)] if nn <= 128 else cyc[128] * nn / 128
+        est[name] = groups_per_sm * tiles * split * (kk // 8) * c / (clock_mhz * 1e3)
+    total = sum(est.values())
+    return {"check_rel_err": errs, "cycles_per_instruction_128xNx8": cyc, "clock_mhz": clock_mhz,
+            "products": [{"name": a, "N": b, "K": c} for a, b, c in prods],
+            "tensor_ms_per_step_by_product": est, "tensor_ms_per_step": total,
+            "fused_local_kernel_ms": local_ms, "ratio_tensor_products_to_whole_fp32_kernel": total / local_ms,
+            "note": "3xTF32 products only, at the measured per-instruction rate; the FP32 kernel's time includes "
+                    "everything"}
 
 
 # compiled FP32 configurations the uneven batch draws from: (order, runs, mechanisms)
@@ -666,6 +804,13 @@ def main():
         parity = accuracy.fused_vs_plain(prob, WORKLOADS[a.workload].steps, device=local)
         parity["tolerance"] = 1e-4
         parity["within_tolerance"] = parity["receiver_rel_l2_max"] < 1e-4
+    tc = None
+    if a.tc_probe and rank == 0:
+        try:
+            tc = run_tc_probe(roofline["kernel_avg_ms"]["local"], prob.n_el, prob.order, prob.runs, local,
+                              clk["sm_mhz"] or peak_clock_mhz())
+        except (RuntimeError, OSError) as e:
+            tc = {"unavailable": str(e)}
     serving = None
     if a.serve_requests > 0:
         serving = run_serve(a.serve_requests, a.serve_rate, local)
@@ -685,7 +830,7 @@ def main():
                                                                                       int(0.99 * len(step_ms)))],
                "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": int(launches),
                "clocks": clk, "fp64_plain": fp64, "serving": serving, "roofline_neighbour": roofline_neighbour, "lts": lts,
-               "batch": batch, "parity_at_size": parity}
+               "batch": batch, "parity_at_size": parity, "tensor_core_probe": tc}
         print(json.dumps(out), flush=True)
     barrier(ws)
     if ws > 1:

@@ -76,7 +76,23 @@ def build(force=False, jobs=None, verbose=False):
             raise RuntimeError(f"link failed:\n{r.stdout}\n{r.stderr}")
         if verbose:
             print("linked", LIB)
+    build_probe(force=force)
     return LIB
+
+
+PROBE_SRC = os.path.join(CSRC, "probe", "tc_probe.cu")
+PROBE_LIB = os.path.join(HERE, "libedge_b200_probe.so")
+
+
+def build_probe(force=False):
+    """The tensor-core measurement probe (csrc/probe) as a library of its own."""
+    if not force and os.path.exists(PROBE_LIB) and os.path.getmtime(PROBE_LIB) >= os.path.getmtime(PROBE_SRC):
+        return PROBE_LIB
+    cmd = [nvcc()] + NVCC_FLAGS + ["-shared", PROBE_SRC, "-o", PROBE_LIB]
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    if r.returncode != 0:
+        raise RuntimeError(f"nvcc failed for {PROBE_SRC}:\n{r.stdout}\n{r.stderr}")
+    return PROBE_LIB
 
 
 if __name__ == "__main__":

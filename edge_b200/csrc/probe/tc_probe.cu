@@ -1,0 +1,184 @@
+// Measurement probe for the tensor-core question of the element update: how fast does one
+// tcgen05.mma (kind::tf32, one CTA, operands in shared memory, accumulator in tensor memory) run at
+// the small shapes the DG products of the local kernel would have (M = 128 rows of (quantity,
+// element, run), N = 8..256 output modes, K = 8 per instruction), and does its result match the
+// FP32 product. Built into its own library (libedge_b200_probe.so): it is not part of the element
+// update, only the evidence for keeping those products on the FP32 pipe.
+//
+// Operands use the K-major SWIZZLE_NONE canonical layout of the shared-memory matrix descriptor:
+// core matrices of 8 rows x 16 bytes (4 tf32) stored contiguously (128 bytes); the 8-row groups of
+// one 16-byte K chunk follow each other (stride-dimension offset 128 bytes) and the K chunks follow
+// the row groups (leading-dimension offset rows / 8 * 128 bytes).
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+namespace {
+
+constexpr int kThreads = 128;      // four warps: the 128 accumulator lanes, one warp per 32
+constexpr int kMaxRows = 128;      // M (A rows) and N (B rows) at most
+constexpr int kMaxK = 32;          // reduction length staged in shared memory
+constexpr long long kWaitCycles = 4000000000LL;  // about two seconds at the boost clock
+// dynamic shared memory per CTA: the two operand tiles plus padding that keeps one CTA per SM, so
+// the tensor-memory allocations of co-resident CTAs never wait on each other
+constexpr int kSmemBytes = 120 * 1024;
+
+__device__ __forceinline__ uint32_t smemAddr(const void *p) {
+  return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+
+// byte offset of element (row r, k) in the canonical K-major layout of a tile with `rows` rows
+__host__ __device__ __forceinline__ uint32_t canonOffset(int r, int k, int rows) {
+  return (uint32_t)((k / 4) * (rows / 8) * 128 + (r / 8) * 128 + (r % 8) * 16 + (k % 4) * 4);
+}
+
+__device__ __forceinline__ uint64_t smemDesc(uint32_t addr, uint32_t lbo, uint32_t sbo) {
+  uint64_t d = 0;
+  d |= (uint64_t)((addr >> 4) & 0x3FFFu);
+  d |= (uint64_t)((lbo >> 4) & 0x3FFFu) << 16;
+  d |= (uint64_t)((sbo >> 4) & 0x3FFFu) << 32;
+  d |= (uint64_t)1 << 46;  // descriptor version of sm_100; base offset 0, no swizzle
+  return d;
+}
+
+// instruction descriptor: D f32, A and B tf32, both K-major, N / 8 and M / 16
+__host__ __device__ constexpr uint32_t instrDesc(int m, int n) {
+  return (1u << 4) | (2u << 7) | (2u << 10) | ((uint32_t)(n >> 3) << 17) | ((uint32_t)(m >> 4) << 24);
+}
+
+__device__ __forceinline__ void mmaTf32(uint32_t dTmem, uint64_t aDesc, uint64_t bDesc, uint32_t idesc,
+                                        uint32_t accumulate) {
+  asm volatile(
+      "{\n\t"
+      ".reg .pred p;\n\t"
+      "setp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, p;\n\t"
+      "}\n" ::"r"(dTmem),
+      "l"(aDesc), "l"(bDesc), "r"(idesc), "r"(accumulate)
+      : "memory");
+}
+
+__device__ __forceinline__ bool waitParity(uint32_t bar, uint32_t parity) {
+  const long long t0 = clock64();
+  while (clock64() - t0 < kWaitCycles) {
+    uint32_t done;
+    asm volatile(
+        "{\n\t"
+        ".reg .pred P1;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 P1, [%1], %2;\n\t"
+        "selp.b32 %0, 1, 0, P1;\n\t"
+        "}\n"
+        : "=r"(done)
+        : "r"(bar), "r"(parity)
+        : "memory");
+    if (done) return true;
+  }
+  return false;
+}
+
+// One CTA per block: A [m][k] and B [n][k] (row-major in global memory, k <= kMaxK) staged into
+// the canonical layout, `iters` passes of k / 8 instructions accumulating into D [m][n] in tensor
+// memory; D is written back (block 0 only) so the host can check it against the FP32 product.
+// status[blockIdx.x]: 0 ok, 1 the completion wait gave up.
+__global__ void __launch_bounds__(kThreads, 1)
+    kTcProbe(const float *A, const float *B, float *D, int m, int n, int k, int iters, int *status) {
+  extern __shared__ __align__(128) float dyn[];
+  float *sA = dyn, *sB = dyn + kMaxRows * kMaxK;
+  __shared__ __align__(8) uint64_t bar;
+  __shared__ uint32_t tmemBase;
+  const int tid = threadIdx.x, warp = tid >> 5;
+  for (int i = tid; i < m * k; i += kThreads) {
+    const int r = i / k, c = i % k;
+    *reinterpret_cast<float *>(reinterpret_cast<char *>(sA) + canonOffset(r, c, m)) = A[i];
+  }
+  for (int i = tid; i < n * k; i += kThreads) {
+    const int r = i / k, c = i % k;
+    *reinterpret_cast<float *>(reinterpret_cast<char *>(sB) + canonOffset(r, c, n)) = B[i];
+  }
+  const uint32_t barAddr = smemAddr(&bar);
+  uint32_t cols = 32;
+  while (cols < (uint32_t)n) cols <<= 1;
+  if (tid == 0) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" ::"r"(barAddr) : "memory");
+    asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+  }
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;\n" ::"r"(smemAddr(&tmemBase)),
+                 "r"(cols)
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;\n" ::: "memory");
+  }
+  // operands written by threads become visible to the tensor core's (async) proxy
+  asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
+  asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+  const uint32_t tmem = tmemBase;
+  if (tid == 0) {
+    const uint32_t idesc = instrDesc(m, n);
+    const uint32_t aBase = smemAddr(sA), bBase = smemAddr(sB);
+    const uint32_t aLbo = (uint32_t)(m / 8) * 128, bLbo = (uint32_t)(n / 8) * 128;
+    for (int it = 0; it < iters; it++)
+      for (int kb = 0; kb < k / 8; kb++) {
+        const uint64_t ad = smemDesc(aBase + 2 * kb * aLbo, aLbo, 128);
+        const uint64_t bd = smemDesc(bBase + 2 * kb * bLbo, bLbo, 128);
+        mmaTf32(tmem, ad, bd, idesc, (it > 0 || kb > 0) ? 1u : 0u);
+      }
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];\n" ::"r"(barAddr)
+                 : "memory");
+  }
+  bool ok = waitParity(barAddr, 0);
+  if (!ok) ok = waitParity(barAddr, 0);  // second bounded wait for the work in flight before freeing
+  if (!ok && tid == 0) status[blockIdx.x] = 1;
+  asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+  if (ok && blockIdx.x == 0 && D) {
+    // warp w reads accumulator lanes 32 w .. 32 w + 31 (rows of D), 8 columns per load
+    const int row = warp * 32 + (tid & 31);
+    for (int c0 = 0; c0 < n; c0 += 8) {
+      uint32_t v[8];
+      const uint32_t addr = tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)c0;
+      asm volatile(
+          "tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];\n"
+          : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7])
+          : "r"(addr));
+      asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory");
+      if (row < m)
+        for (int j = 0; j < 8 && c0 + j < n; j++) D[row * n + c0 + j] = __uint_as_float(v[j]);
+    }
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
+  __syncthreads();
+  if (warp == 0)
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;\n" ::"r"(tmem), "r"(cols) : "memory");
+}
+
+}  // namespace
+
+extern "C" {
+
+// Runs the probe: `blocks` CTAs, each `iters` x (k / 8) tf32 MMAs of shape m x n x 8 on its own
+// operand copies (A [m][k], B [n][k] device arrays; D [m][n] device array or NULL). m = 128, n a
+// multiple of 16 in [16, 128], k a multiple of 8 in [8, 32]. Returns 0, -1 for invalid shapes,
+// -3 for a CUDA error; *ms receives the kernel time (CUDA events), status[blocks] the per-CTA
+// completion flags (device array).
+int edge_b200_probe_tc(const float *A, const float *B, float *D, int m, int n, int k, int iters, int blocks,
+                       int *status, float *ms) {
+  if (m != 128 || n < 16 || n > kMaxRows || n % 16 || k < 8 || k > kMaxK || k % 8 || iters < 1 || blocks < 1 ||
+      !A || !B || !status || !ms)
+    return -1;
+  if (cudaFuncSetAttribute(kTcProbe, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemBytes) != cudaSuccess)
+    return -3;
+  cudaEvent_t e0, e1;
+  if (cudaEventCreate(&e0) != cudaSuccess || cudaEventCreate(&e1) != cudaSuccess) return -3;
+  cudaEventRecord(e0);
+  kTcProbe<<<blocks, kThreads, kSmemBytes>>>(A, B, D, m, n, k, iters, status);
+  cudaEventRecord(e1);
+  cudaError_t err = cudaEventSynchronize(e1);
+  if (err == cudaSuccess) err = cudaGetLastError();
+  cudaEventElapsedTime(ms, e0, e1);
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  return err == cudaSuccess ? 0 : -3;
+}
+
+}  // extern "C"
