@@ -171,12 +171,12 @@ def lts_neigh(prob, state, first, n, first_ts, rel):
         _ptr(state.get("tDofs2")), _ptr(state["dofsE"]), _ptr(state.get("dofsA")))
 
 
-def lts_cycles(prob, state, group_first, t, dt_fun, n_cycles, flags, rel, recv=None, src=None):
-    """n_cycles steps of the largest time group with the rate-2 schedule: at fundamental step k
-    (t_k = t + k dt_fun) every group g with k % 2^g == 0 runs local + sources over
-    [t_k, t_k + 2^g dt_fun), then every group whose step ends runs neigh; the first step of each
-    pair of a group (its step count even) resets the two-step sums (TimeGroupStatic.cpp:46-111,
-    man_sched.inc:37-206 sequentialised)."""
+def lts_schedule(local, neigh, group_first, t, dt_fun, n_cycles):
+    """The rate-2 order of the work regions over n_cycles steps of the largest time group: at
+    fundamental step k (t_k = t + k dt_fun) every group g with k % 2^g == 0 runs
+    local(lo, n, first_ts, t_k, 2^g dt_fun), then every group whose step ends runs
+    neigh(lo, n, first_ts); the first step of each pair of a group (its step count even) resets the
+    two-step sums (TimeGroupStatic.cpp:46-111, man_sched.inc:37-206 sequentialised)."""
     G = len(group_first) - 1
     n_fun = 1 << (G - 1)
     for c in range(n_cycles):
@@ -187,8 +187,7 @@ def lts_cycles(prob, state, group_first, t, dt_fun, n_cycles, flags, rel, recv=N
                     continue
                 lo, hi = int(group_first[g]), int(group_first[g + 1])
                 if hi > lo:
-                    lts_local(prob, state, lo, hi - lo, ((kk >> g) & 1) == 0, t + float(kk) * dt_fun,
-                              dt_fun * float(1 << g), flags, recv, src)
+                    local(lo, hi - lo, ((kk >> g) & 1) == 0, t + float(kk) * dt_fun, dt_fun * float(1 << g))
             for g in range(G):
                 span = 1 << g
                 if (k + 1) % span:
@@ -196,4 +195,11 @@ def lts_cycles(prob, state, group_first, t, dt_fun, n_cycles, flags, rel, recv=N
                 lo, hi = int(group_first[g]), int(group_first[g + 1])
                 k0 = kk + 1 - span
                 if hi > lo:
-                    lts_neigh(prob, state, lo, hi - lo, ((k0 >> g) & 1) == 0, rel)
+                    neigh(lo, hi - lo, ((k0 >> g) & 1) == 0)
+
+
+def lts_cycles(prob, state, group_first, t, dt_fun, n_cycles, flags, rel, recv=None, src=None):
+    """n_cycles steps of the largest time group with the rate-2 schedule (lts_schedule) of the
+    oracle's LTS work regions."""
+    lts_schedule(lambda lo, n, ft, tk, dt: lts_local(prob, state, lo, n, ft, tk, dt, flags, recv, src),
+                 lambda lo, n, ft: lts_neigh(prob, state, lo, n, ft, rel), group_first, t, dt_fun, n_cycles)

@@ -19,8 +19,16 @@ SRCS := $(EDGE_REF)/src/dg/Basis.cpp $(EDGE_REF)/src/impl/seismic/setups/Elastic
         $(EDGE_REF)/src/data/Dynamic.cpp $(EDGE_REF)/submodules/FastGL/fastgl.cpp
 
 LIBS := $(foreach c,$(CFGS),$(OUT)/libedgeref_O$(word 1,$(subst _, ,$c))_R$(word 2,$(subst _, ,$c))_M$(word 3,$(subst _, ,$c)).so)
+# the reference's AderDg class itself (local / neigh with the LTS branches), elastic
+LTS_CFGS ?= 3_1 4_1 4_4
+LTS_LIBS := $(foreach c,$(LTS_CFGS),$(OUT)/libedgeref_lts_O$(word 1,$(subst _, ,$c))_R$(word 2,$(subst _, ,$c)).so)
 
-all: $(LIBS)
+all: $(LIBS) $(LTS_LIBS)
+
+$(OUT)/libedgeref_lts_O%.so: ref_lts.cpp
+	@mkdir -p $(OUT)
+	$(eval C := $(subst _R,_,$*))
+	$(CXX) $(CXXFLAGS) $(INC) $(call defs,$(C)_0) -shared -o $@ ref_lts.cpp $(SRCS) $(EDGE_REF)/src/parallel/global.cpp
 
 $(OUT)/libedgeref_O%.so: ref_driver.cpp
 	@mkdir -p $(OUT)

@@ -58,3 +58,52 @@ def step(L, prob, state, t, dt, src_apply=None):
         src_apply(state)
     rc = L.ref_step_phase(1, prob["nEl"], dt, *[_p(a) for a in args])
     assert rc == 0
+
+
+def lts_path(order, runs):
+    return os.path.join(HERE, "_ref", f"libedgeref_lts_O{order}_R{runs}.so")
+
+
+def load_lts(order=3, runs=1):
+    """The reference's AderDg class (local / neigh with the LTS branches, elastic) for one
+    configuration, built from the reference checkout when missing; None otherwise."""
+    key = ("lts", order, runs)
+    if key in _cache:
+        return _cache[key]
+    p = lts_path(order, runs)
+    if not os.path.exists(p) and os.path.isdir(os.path.join(REF, "src")):
+        subprocess.run(["make", "-s", "-C", HERE, "-f", "ref.mk", f"LTS_CFGS={order}_{runs}", f"_ref/libedgeref_lts_O{order}_R{runs}.so"],
+                       check=False, capture_output=True)
+    if not os.path.exists(p):
+        _cache[key] = None
+        return None
+    L = C.CDLL(p)
+    vp = C.c_void_p
+    L.ref_lts_setup.argtypes = [C.c_long] + [vp] * 11
+    L.ref_lts_local.argtypes = [C.c_long, C.c_long, C.c_int, C.c_double, C.c_double, vp]
+    L.ref_lts_neigh.argtypes = [C.c_long, C.c_long, C.c_int, vp]
+    _cache[key] = L
+    return L
+
+
+class LtsRun:
+    """The reference's AderDg::local / ::neigh on one mesh with its LTS relations; state arrays
+    (dofsE, tDofs, tDofs1, tDofs2, each [nEl][9][B][R]) are held here and updated in place."""
+
+    def __init__(self, L, prob, flags, rel, dofsE):
+        self.L = L
+        self.st = dict(dofsE=np.ascontiguousarray(dofsE, np.float64))
+        for k in ("tDofs", "tDofs1", "tDofs2"):
+            self.st[k] = np.zeros_like(self.st["dofsE"])
+        self.keep = [np.ascontiguousarray(prob[k]) for k in ("starE", "fsE", "elFaEl", "fIdElFaEl", "vIdElFaEl",
+                                                             "faType")]
+        self.keep += [np.ascontiguousarray(flags, np.uint8), np.ascontiguousarray(rel, np.uint8)]
+        rc = L.ref_lts_setup(prob["nEl"], *[_p(a) for a in self.keep],
+                             *[_p(self.st[k]) for k in ("tDofs", "tDofs1", "tDofs2")])
+        assert rc == 0
+
+    def local(self, first, n, first_ts, t, dt):
+        assert self.L.ref_lts_local(first, n, 1 if first_ts else 0, t, dt, _p(self.st["dofsE"])) == 0
+
+    def neigh(self, first, n, first_ts):
+        assert self.L.ref_lts_neigh(first, n, 1 if first_ts else 0, _p(self.st["dofsE"])) == 0

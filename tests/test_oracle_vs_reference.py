@@ -29,3 +29,28 @@ def test_oracle_step_matches_reference_kernels(order, runs, rm):
     assert rel_l2(orc.state["tDofs"], st["tDofs"]) < 1e-13
     if rm:
         assert rel_l2(orc.state["dofsA"], st["dofsA"]) < 1e-13
+
+
+@pytest.mark.parametrize("order,runs,n_groups", [(3, 1, 2), (3, 1, 3), (4, 1, 3), (4, 4, 3)])
+def test_oracle_lts_matches_reference_aderdg(order, runs, n_groups):
+    """The oracle's LTS work regions (summed and half-step time integrals, the "=", "<" and ">"
+    gathers) against the reference's own AderDg::local / ::neigh on the same grouped mesh, DOFs and
+    rate-2 schedule."""
+    import oracle
+    from test_lts import _grouped
+    L = refmod.load_lts(order, runs)
+    if L is None:
+        pytest.skip("reference build (oracle/_ref) unavailable")
+    prob, gf, flags, rel = _grouped(order=order, n=4, n_groups=n_groups, runs=runs, source=None, n_receivers=0)
+    assert (flags & 1).any() and (flags & 2).any()
+    e0, _ = random_dofs(prob, seed=3)
+    d = prob.oracle_dict()
+    st = dict(dofsE=e0.copy(), dofsA=None, tDofs=np.zeros_like(e0), tDofs1=np.zeros_like(e0),
+              tDofs2=np.zeros_like(e0))
+    oracle.lts_cycles(d, st, gf, 0.0, prob.dt, 2, flags, rel)
+    ref = refmod.LtsRun(L, d, flags, rel, e0)
+    oracle.lts_schedule(ref.local, ref.neigh, gf, 0.0, prob.dt, 2)
+    assert np.abs(st["dofsE"] - e0).max() > 0
+    assert rel_l2(st["dofsE"], ref.st["dofsE"]) < 1e-13
+    for k in ("tDofs", "tDofs1", "tDofs2"):
+        assert rel_l2(st[k], ref.st[k]) < 1e-13, k
