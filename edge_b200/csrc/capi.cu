@@ -193,6 +193,12 @@ struct edge_b200_ctx {
   edge_b200_cfg cfg{};
   int64_t nEl = 0;
   int64_t nOwned = 0;  // the kernels update elements [0, nOwned); the rest are halo ghosts
+  // halo parts: owned elements [0, nSend) have a face neighbour in another part; the local step
+  // can run on them first (their face rows packed and sent while the rest run)
+  int64_t nSend = 0;
+  // local-step range of the next runSteps call (phases 2 / 3 of edge_b200_step_phase)
+  int64_t rangeFirst = 0, rangeCount = -1;
+  bool rangeRecv = true, rangeSrc = true;
   int B = 0, F = 0;
   size_t realSize = 8;
   cudaStream_t stream = nullptr;
@@ -830,7 +836,7 @@ static int runSteps(edge_b200_ctx *ctx, double t, double dt, int n_steps, int ph
     double ts = t;
     for (int st = 0; st < n_steps; st++) {
       stepFirst[st] = (int)tau.size();
-      if (ctx->nRecv && (phases & 1)) {
+      if (ctx->nRecv && (phases & 1) && ctx->rangeRecv) {
         while (ctx->recvTime > ts - kTolTime && ctx->recvTime < ts + dt - kTolTime) {
           if (ctx->recvCount >= ctx->maxBuf) return EDGE_B200_EOVERFLOW;
           tau.push_back(std::abs(ctx->recvTime - ts));
@@ -859,6 +865,10 @@ static int runSteps(edge_b200_ctx *ctx, double t, double dt, int n_steps, int ph
   }
   ctx->launches = 0;
   StepArgsRaw a = ctx->args(dt);
+  if (ctx->rangeCount >= 0) {
+    a.elFirst = ctx->rangeFirst;
+    a.elCount = ctx->rangeCount;
+  }
   double ts = t;
   for (int st = 0; st < n_steps; st++) {
     const int ns = stepFirst[st + 1] - stepFirst[st];
@@ -885,7 +895,7 @@ static int runSteps(edge_b200_ctx *ctx, double t, double dt, int n_steps, int ph
       EDGE_CUDA(ctx->launch(0, [&] { return fused ? ctx->ks->localFused(a, s) : ctx->ks->local(a, s); }),
                 "local kernel");
       ctx->launches++;
-      if (ctx->src.nGrp > 0) {
+      if (ctx->src.nGrp > 0 && ctx->rangeSrc) {
         SrcArgs sa = ctx->src;
         sa.t = ts;
         sa.dt = dt;
@@ -922,8 +932,24 @@ int edge_b200_step(edge_b200_ctx *ctx, double t, double dt, int n_steps) {
 }
 
 int edge_b200_step_phase(edge_b200_ctx *ctx, double t, double dt, int phase) {
-  if (phase != 0 && phase != 1) return EDGE_B200_EINVAL;
-  return runSteps(ctx, t, dt, 1, phase == 0 ? 1 : 2);
+  if (!ctx || phase < 0 || phase > 3) return EDGE_B200_EINVAL;
+  if (phase < 2) return runSteps(ctx, t, dt, 1, phase == 0 ? 1 : 2);
+  // 2: receivers and local step of the send elements; 3: local step of the others and the sources
+  const int64_t nSend = std::min(ctx->nSend, ctx->nOwned);
+  ctx->rangeFirst = phase == 2 ? 0 : nSend;
+  ctx->rangeCount = phase == 2 ? nSend : ctx->nOwned - nSend;
+  ctx->rangeRecv = phase == 2;
+  ctx->rangeSrc = phase == 3;
+  const int rc = runSteps(ctx, t, dt, 1, 1);
+  ctx->rangeCount = -1;
+  ctx->rangeRecv = ctx->rangeSrc = true;
+  return rc;
+}
+
+int edge_b200_set_send_count(edge_b200_ctx *ctx, int64_t n_send) {
+  if (!ctx || n_send < 0 || n_send > ctx->nOwned) return EDGE_B200_EINVAL;
+  ctx->nSend = n_send;
+  return EDGE_B200_OK;
 }
 
 int edge_b200_set_owned(edge_b200_ctx *ctx, int64_t n_owned) {

@@ -22,6 +22,8 @@ class Part:
     rank: int
     lo: int                       # owned elements are the global range [lo, hi)
     hi: int
+    owned: np.ndarray             # global ids of the owned elements in local order: send elements first
+    n_send: int                   # owned elements with a face neighbour in another part (local 0 .. n_send)
     ghosts: np.ndarray            # global ids of the ghost elements (local ids n_owned ...)
     el_fa_el: np.ndarray          # [n_local][4] local neighbour ids (-1 none; ghost rows all -1)
     fid: np.ndarray               # [n_local][4]
@@ -39,7 +41,7 @@ class Part:
         return self.n_owned + len(self.ghosts)
 
     def global_ids(self):
-        return np.concatenate([np.arange(self.lo, self.hi), self.ghosts]).astype(np.int64)
+        return np.concatenate([self.owned, self.ghosts]).astype(np.int64)
 
 
 def ranges(n_el, n_parts):
@@ -48,7 +50,10 @@ def ranges(n_el, n_parts):
 
 
 def plan(mesh, n_parts):
-    """Per-part tables for a partition of the mesh's elements into contiguous ranges."""
+    """Per-part tables for a partition of the mesh's elements into contiguous ranges. Within a part
+    the send elements (a face neighbour in another part) come first, as EDGE's send region follows
+    its inner region in a separate range (setup.inc:337-399), so that their local step can run, and
+    their face rows leave, before the inner elements' local step."""
     from .host import FACE_INNER, FACE_OUTFLOW
     bounds = ranges(mesh.n_el, n_parts)
     ne = mesh.el_fa_el.astype(np.int64)
@@ -58,22 +63,29 @@ def plan(mesh, n_parts):
         lo, hi = int(bounds[p]), int(bounds[p + 1])
         nb = ne[lo:hi]
         remote = inner[lo:hi] & ((nb < lo) | (nb >= hi))
+        is_send = remote.any(axis=1)
+        owned = np.concatenate([np.flatnonzero(is_send), np.flatnonzero(~is_send)]) + lo
+        n_own = hi - lo
+        loc_of = np.empty(n_own, np.int64)
+        loc_of[owned - lo] = np.arange(n_own)
         ghosts = np.unique(nb[remote])
-        g2l = {int(g): (hi - lo) + i for i, g in enumerate(ghosts)}
-        n_local = (hi - lo) + len(ghosts)
+        g2l = {int(g): n_own + i for i, g in enumerate(ghosts)}
+        n_local = n_own + len(ghosts)
+        rows = owned - lo
+        nbo, rmo, ino = nb[rows], remote[rows], inner[lo:hi][rows]
         el_fa_el = np.full((n_local, 4), -1, np.int32)
-        loc = np.where(inner[lo:hi], nb, -1)
-        mapped = np.where((loc >= lo) & (loc < hi), loc - lo, -1)
-        for i, f in zip(*np.nonzero(remote)):
-            mapped[i, f] = g2l[int(nb[i, f])]
-        el_fa_el[:hi - lo] = mapped
+        mapped = np.where(ino & ~rmo, loc_of[np.clip(nbo - lo, 0, n_own - 1)], -1)
+        for i, f in zip(*np.nonzero(rmo)):
+            mapped[i, f] = g2l[int(nbo[i, f])]
+        el_fa_el[:n_own] = mapped
         fid = np.zeros((n_local, 4), np.uint8)
         vid = np.zeros((n_local, 4), np.uint8)
         ty = np.full((n_local, 4), FACE_OUTFLOW, np.uint8)
-        fid[:hi - lo] = mesh.fid[lo:hi]
-        vid[:hi - lo] = mesh.vid[lo:hi]
-        ty[:hi - lo] = mesh.el_fa_type[lo:hi]
-        part = Part(p, lo, hi, ghosts.astype(np.int64), el_fa_el, fid, vid, ty)
+        fid[:n_own] = mesh.fid[owned]
+        vid[:n_own] = mesh.vid[owned]
+        ty[:n_own] = mesh.el_fa_type[owned]
+        part = Part(p, lo, hi, owned.astype(np.int64), int(is_send.sum()), ghosts.astype(np.int64), el_fa_el,
+                    fid, vid, ty)
         # A neighbour reads face (element, its own face id) of this element's face buffer, so the
         # send list holds (owned element, face) pairs whose face neighbour lives in the peer, and the
         # peer stores them at (its ghost copy of the element, the same face). Both sides list the
@@ -85,7 +97,7 @@ def plan(mesh, n_parts):
             i, f = np.nonzero(inner[lo:hi] & (nb >= qlo) & (nb < qhi))
             if len(i):
                 order = np.lexsort((f, i))
-                part.send[q] = np.stack([i[order], f[order]], 1).astype(np.int32)
+                part.send[q] = np.stack([loc_of[i[order]], f[order]], 1).astype(np.int32)
             j, g = np.nonzero(inner[qlo:qhi] & (ne[qlo:qhi] >= lo) & (ne[qlo:qhi] < hi))
             if len(j):
                 order = np.lexsort((g, j))
@@ -121,6 +133,7 @@ class PartSolver:
         self.part, self.prob = part, local
         self.solver = Solver(local, precision=precision, stream=stream, device=device)
         self.solver._chk(lib().edge_b200_set_owned(self.solver._h, part.n_owned), "set_owned")
+        self.solver._chk(lib().edge_b200_set_send_count(self.solver._h, part.n_send), "set_send_count")
         self.block = lib().edge_b200_face_block_bytes(self.solver._h)
         dev = torch.device("cuda", device)
         slots = lambda lst: torch.from_numpy((lst[:, 0].astype(np.int64) * 4 + lst[:, 1]).astype(np.int32)).to(dev)
@@ -131,16 +144,34 @@ class PartSolver:
 
     def upload_owned(self, dofs_e_global):
         e = np.zeros((self.part.n_local,) + dofs_e_global.shape[1:], dofs_e_global.dtype)
-        e[:self.part.n_owned] = dofs_e_global[self.part.lo:self.part.hi]
+        e[:self.part.n_owned] = dofs_e_global[self.part.owned]
         self.solver.upload_dofs(e)
 
     def download_owned(self):
+        """DOFs of the owned elements in global order (elements lo .. hi)."""
         e, a = self.solver.download_dofs()
-        return e[:self.part.n_owned], None if a is None else a[:self.part.n_owned]
+        idx = self.part.owned - self.part.lo
+        out_e = np.empty_like(e[:self.part.n_owned])
+        out_e[idx] = e[:self.part.n_owned]
+        out_a = None
+        if a is not None:
+            out_a = np.empty_like(a[:self.part.n_owned])
+            out_a[idx] = a[:self.part.n_owned]
+        return out_e, out_a
 
     def phase0(self, t, dt):
         from ._lib import lib
         self.solver._chk(lib().edge_b200_step_phase(self.solver._h, t, dt, 0), "step_phase 0")
+
+    def phase_send(self, t, dt):
+        """Receivers and the local step of the send elements (their face rows can then be packed)."""
+        from ._lib import lib
+        self.solver._chk(lib().edge_b200_step_phase(self.solver._h, t, dt, 2), "step_phase 2")
+
+    def phase_inner(self, t, dt):
+        """The local step of the other owned elements and the sources (overlapping the exchange)."""
+        from ._lib import lib
+        self.solver._chk(lib().edge_b200_step_phase(self.solver._h, t, dt, 3), "step_phase 3")
 
     def phase1(self, t, dt):
         from ._lib import lib
@@ -163,13 +194,32 @@ class PartSolver:
         self.solver.close()
 
 
-def exchange_nccl(ps):
+def exchange_nccl(ps, wait=True):
     """Moves this rank's packed send buffers to their peers' receive buffers (torch.distributed
     send / recv, NCCL between GPUs); every rank calls it once per step after pack(). The part's
-    solver must run on torch's current stream (stream=None), which NCCL orders its copies after."""
+    solver must run on torch's current stream (stream=None), which NCCL orders its copies after.
+    wait=False returns the pending works: work queued on the stream after this call (the inner
+    elements' local step) overlaps the transfer; wait on them before unpack()."""
     import torch.distributed as dist
     ops = [dist.P2POp(dist.isend, b, q) for q, b in sorted(ps.send_buf.items())]
     ops += [dist.P2POp(dist.irecv, b, q) for q, b in sorted(ps.recv_buf.items())]
-    if ops:
-        for r in dist.batch_isend_irecv(ops):
+    works = dist.batch_isend_irecv(ops) if ops else []
+    if wait:
+        for r in works:
             r.wait()
+        return []
+    return works
+
+
+def step_overlapped(ps, t, dt):
+    """One GTS step of a part with the halo exchange behind the inner elements' local step: send
+    elements' local step, pack, NCCL transfer started, inner elements' local step (and sources),
+    wait for the transfer, unpack into the ghosts' face slots, neighbour step."""
+    ps.phase_send(t, dt)
+    ps.pack()
+    works = exchange_nccl(ps, wait=False)
+    ps.phase_inner(t, dt)
+    for r in works:
+        r.wait()
+    ps.unpack()
+    ps.phase1(t, dt)

@@ -243,8 +243,14 @@ int edge_b200_wavefield(edge_b200_ctx *ctx, float *out);
  * [9][R][GF] of n face slots (slots[i] = element * 4 + face, a device int32 array) to / from the
  * device buffer out / in ([n] blocks of edge_b200_face_block_bytes each, GF = F rounded up to 16
  * bytes), ordered on the context stream; slots outside the mesh are skipped. Time groups need the
- * whole mesh owned. */
+ * whole mesh owned. To overlap the exchange with work, as the reference's inner / send regions do
+ * (src/impl/seismic/setup.inc:337-399), number the owned elements with a face neighbour in another
+ * part first and give their count to edge_b200_set_send_count: phase 2 runs the receivers and the
+ * local step of those [0, n_send), phase 3 the local step of the others [n_send, n_owned) and the
+ * sources; phases 2 and 3 together equal phase 0, and the send faces can be packed and sent between
+ * them. */
 int edge_b200_set_owned(edge_b200_ctx *ctx, int64_t n_owned);
+int edge_b200_set_send_count(edge_b200_ctx *ctx, int64_t n_send);
 int edge_b200_step_phase(edge_b200_ctx *ctx, double t, double dt, int phase);
 int64_t edge_b200_face_block_bytes(const edge_b200_ctx *ctx);
 int edge_b200_pack_faces(edge_b200_ctx *ctx, int n, const int32_t *slots, void *out);

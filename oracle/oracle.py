@@ -203,3 +203,43 @@ def lts_cycles(prob, state, group_first, t, dt_fun, n_cycles, flags, rel, recv=N
     oracle's LTS work regions."""
     lts_schedule(lambda lo, n, ft, tk, dt: lts_local(prob, state, lo, n, ft, tk, dt, flags, recv, src),
                  lambda lo, n, ft: lts_neigh(prob, state, lo, n, ft, rel), group_first, t, dt_fun, n_cycles)
+
+
+# ------------------------------------------------------------------------------------------------
+# halo exchange of pre-mixed face rows (numpy restatement, test infrastructure)
+# ------------------------------------------------------------------------------------------------
+def face_orientations(fluxL, fluxN):
+    """O[v] (F x F) with fluxN[4 v + f] = fluxL[f] . O[v] for every local face f: the neighbour
+    flux matrices of SurfIntVanilla::neigh (SurfIntVanilla.hpp:274-357, matrix 4 + 4 vId + fId)
+    are the local projections followed by the face-vertex orientation. Returns (O [3][F][F], the
+    largest residual of the factorisation over all v, f)."""
+    O, res = [], 0.0
+    for v in range(3):
+        o = np.linalg.lstsq(fluxL[0], fluxN[4 * v], rcond=None)[0]
+        O.append(o)
+        for f in range(4):
+            res = max(res, float(np.abs(fluxL[f] @ o - fluxN[4 * v + f]).max() / np.abs(fluxN[4 * v + f]).max()))
+    return np.array(O), res
+
+
+def face_rows_premixed(prob, tDofs, send):
+    """The face rows a part sends for its faces `send` [n][2] = (element, face): the element's
+    time-integrated DOFs projected on the face (tDofs . fluxL_face, the face-projected data EDGE's
+    MPI path ships, AderDg.hpp:419-473) and mixed with the flux solver of the element that reads
+    them (fsE[1] of the face neighbour at its own face id). Returns [n][9][F][R]."""
+    fl, fs1 = prob["fluxL"], prob["fsE"][1]
+    out = []
+    for e, f in send:
+        ne, fo = int(prob["elFaEl"][e, f]), int(prob["fIdElFaEl"][e, f])
+        proj = np.einsum("qbr,bf->qfr", tDofs[e], fl[f])
+        out.append(np.einsum("qp,pfr->qfr", fs1[ne, fo].reshape(9, 9), proj))
+    return np.array(out)
+
+
+def neigh_premixed_faces(prob, dofsE, faces, rows, O):
+    """Adds the lifted fluxes of received pre-mixed face rows (SurfIntVanilla::neigh with the mix
+    done by the sender): for face (element, face) with row P, dofs += (P . O[vId]) . fluxT_face."""
+    ft = prob["fluxT"]
+    for (e, f), P in zip(faces, rows):
+        s1 = np.einsum("qfr,fg->qgr", P, O[int(prob["vIdElFaEl"][e, f])])
+        dofsE[e] += np.einsum("qfr,fb->qbr", s1, ft[f])

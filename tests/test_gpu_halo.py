@@ -1,6 +1,8 @@
 """Halo exchange on the device: the parts of a partition as separate contexts on one GPU, their
 face rows moved by pack / device copy / unpack between the two halves of every step, against the
-one-domain run (the device half of the multi-GPU form; the transport between GPUs is NCCL)."""
+one-domain run (the device half of the multi-GPU form; the transport between GPUs is NCCL). Every
+other step runs the overlapped order: the send elements' local step, the pack, then the inner
+elements' local step before the exchanged rows are unpacked."""
 import numpy as np
 import pytest
 
@@ -28,10 +30,18 @@ def test_parts_match_one_domain(n_parts, precision, order, runs):
         for ps in parts:
             ps.upload_owned(e0.astype(dtype))
         t = 0.0
-        for _ in range(6):
+        for step in range(6):
+            # odd steps: the send elements' local step, the pack, then the inner elements' local
+            # step (the overlapped order); even steps: the whole local step first
             for ps in parts:
-                ps.phase0(t, prob.dt)
+                if step % 2:
+                    ps.phase_send(t, prob.dt)
+                else:
+                    ps.phase0(t, prob.dt)
             sent = {ps.part.rank: ps.pack() for ps in parts}
+            if step % 2:
+                for ps in parts:
+                    ps.phase_inner(t, prob.dt)
             for ps in parts:
                 for q, buf in ps.recv_buf.items():
                     buf.copy_(sent[q][ps.part.rank])
@@ -44,3 +54,35 @@ def test_parts_match_one_domain(n_parts, precision, order, runs):
         for ps in parts:
             ps.close()
     assert np.array_equal(got, want) or rel_l2(got, want) < 1e-14
+
+
+def test_send_then_inner_equals_whole_local_step():
+    """Phases 2 + 3 (send elements, then the rest with the sources) equal phase 0 bit for bit, with
+    sources and receivers on."""
+    prob = host.build_problem(3, 4, 1, jitter=0.1, seed=4, n_receivers=3, source="explosive", n_steps=8)
+    e0, _ = random_dofs(prob, seed=2, scale=1e-2)
+    out = []
+    for split in (False, True):
+        s = Solver(prob, precision=64)
+        try:
+            from edge_b200._lib import lib
+            s._chk(lib().edge_b200_set_owned(s._h, prob.n_el), "set_owned")
+            s._chk(lib().edge_b200_set_send_count(s._h, prob.n_el // 3), "set_send_count")
+            s.upload_dofs(e0)
+            t = 0.0
+            for _ in range(4):
+                if split:
+                    s._chk(lib().edge_b200_step_phase(s._h, t, prob.dt, 2), "phase 2")
+                    s._chk(lib().edge_b200_step_phase(s._h, t, prob.dt, 3), "phase 3")
+                else:
+                    s._chk(lib().edge_b200_step_phase(s._h, t, prob.dt, 0), "phase 0")
+                s._chk(lib().edge_b200_step_phase(s._h, t, prob.dt, 1), "phase 1")
+                t += prob.dt
+            e, _ = s.download_dofs()
+            rb, rt, rc = s.receivers()
+            out.append((e, rb, rc))
+        finally:
+            s.close()
+    assert np.array_equal(out[0][0], out[1][0])
+    assert np.array_equal(out[0][2], out[1][2]) and int(out[0][2][0]) > 0
+    assert np.array_equal(out[0][1], out[1][1])

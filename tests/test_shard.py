@@ -1,10 +1,12 @@
 """Halo partitions (edge_b200.shard): index tables on one process, and multi-rank gloo runs of the
 oracle's local / neighbour work regions with the per-step exchange, against the one-domain run.
 
-The device form exchanges face projections of the send faces between GPUs; this CPU test
-exchanges the whole time-integrated DOFs of the same send elements (what the oracle's neighbour
-step reads), so the partition, the local numbering, the ghost mapping and the step order are
-checked bit for bit without a GPU.
+The ranks exchange what the device form exchanges: the face rows of the send faces, projected on
+the face and pre-mixed with the reading element's flux solver (oracle.face_rows_premixed), sent
+after the send elements' local step and before the inner elements' one, and lifted by the
+reader with the face orientation and fluxT. So the partition, the local numbering (send elements
+first), the ghost mapping, the exchange format and the overlapped step order are checked on the
+CPU against the one-domain oracle.
 """
 import os
 import socket
@@ -33,16 +35,21 @@ def test_plan_covers_every_inner_face_once(n_parts):
         # local connectivity maps back to the global one on owned rows
         loc = q.el_fa_el[:q.n_owned]
         glob = np.where(loc >= 0, gid[np.maximum(loc, 0)], -1)
-        expect = np.where(m.el_fa_type[q.lo:q.hi] == host.FACE_INNER, m.el_fa_el[q.lo:q.hi], -1)
+        expect = np.where(m.el_fa_type[q.owned] == host.FACE_INNER, m.el_fa_el[q.owned], -1)
         assert np.array_equal(glob, expect)
+        assert sorted(q.owned) == list(range(q.lo, q.hi))
+        # send elements first: exactly the owned elements with a face neighbour in another part
+        remote = (loc >= q.n_owned).any(axis=1)
+        assert remote[:q.n_send].all() and not remote[q.n_send:].any()
         for peer, lst in q.send.items():
             rec = parts[peer].recv[q.rank]
             assert len(rec) == len(lst)
+            assert (lst[:, 0] < q.n_send).all()
             # the receiver's ghost is the sender's element, at the same face
-            assert np.array_equal(parts[peer].global_ids()[rec[:, 0]], lst[:, 0] + q.lo)
+            assert np.array_equal(parts[peer].global_ids()[rec[:, 0]], q.owned[lst[:, 0]])
             assert np.array_equal(rec[:, 1], lst[:, 1])
             for e, f in lst:
-                key = (int(e) + q.lo, int(f))
+                key = (int(q.owned[e]), int(f))
                 assert key not in sent
                 sent[key] = peer
     # every face between two parts is sent exactly once, to the part of the neighbour
@@ -63,6 +70,9 @@ def _free_port():
 
 
 def _rank_main(rank, world, port, order, n_steps, out_dir):
+    """One rank: the oracle's local step of the send elements, the pre-mixed face rows of the send
+    faces to the peers (gloo), the local step of the inner elements, the neighbour step with the
+    received rows for the ghost faces -- the device form's step order and exchange format."""
     import torch
 
     import oracle
@@ -75,36 +85,55 @@ def _rank_main(rank, world, port, order, n_steps, out_dir):
         part = shard.plan(p.mesh, world)[rank]
         ids = part.global_ids()
         full = p.oracle_dict()
+        O, _ = oracle.face_orientations(full["fluxL"], full["fluxN"])
         d = dict(full)
         d.update(nEl=part.n_local, starE=np.ascontiguousarray(full["starE"][ids]),
                  fsE=np.ascontiguousarray(full["fsE"][:, ids]),
                  elFaEl=np.ascontiguousarray(part.el_fa_el), fIdElFaEl=np.ascontiguousarray(part.fid),
                  vIdElFaEl=np.ascontiguousarray(part.vid), faType=np.ascontiguousarray(part.el_fa_type))
+        # the neighbour step skips the ghost faces; their rows come from the peers
+        ghost_face = (part.el_fa_el >= part.n_owned)
+        dn = dict(d, faType=np.ascontiguousarray(np.where(ghost_face, 2, part.el_fa_type).astype(np.uint8)))
+        ghost_faces = [(int(e), int(f)) for e, f in zip(*np.nonzero(ghost_face[:part.n_owned]))]
         st = dict(dofsE=np.ascontiguousarray(e0[ids]), dofsA=None,
                   tDofs=np.zeros((part.n_local, 9, p.B, 1)))
         t = 0.0
         for _ in range(n_steps):
-            oracle.lts_local(d, st, 0, part.n_owned, True, t, p.dt, None)
-            # exchange: the send elements' time integrals into the peers' ghost rows
-            reqs, bufs = [], []
+            oracle.lts_local(d, st, 0, part.n_send, True, t, p.dt, None)
+            reqs, got = [], {}
             for peer in sorted(set(part.send) | set(part.recv)):
                 if peer in part.send:
-                    el = np.unique(part.send[peer][:, 0])
-                    reqs.append(dist.isend(torch.from_numpy(np.ascontiguousarray(st["tDofs"][el])), peer))
+                    rows = oracle.face_rows_premixed(d, st["tDofs"], part.send[peer])
+                    reqs.append(dist.isend(torch.from_numpy(np.ascontiguousarray(rows)), peer))
                 if peer in part.recv:
-                    el = np.unique(part.recv[peer][:, 0])
-                    b = torch.zeros((len(el), 9, p.B, 1), dtype=torch.float64)
+                    b = torch.zeros((len(part.recv[peer]), 9, p.order * (p.order + 1) // 2, 1), dtype=torch.float64)
                     reqs.append(dist.irecv(b, peer))
-                    bufs.append((el, b))
+                    got[peer] = b
+            # the inner elements' local step while the rows travel
+            oracle.lts_local(d, st, part.n_send, part.n_owned - part.n_send, True, t, p.dt, None)
             for r in reqs:
                 r.wait()
-            for el, b in bufs:
-                st["tDofs"][el] = b.numpy()
-            oracle.lts_neigh(d, st, 0, part.n_owned, True, None)
+            slot = {}
+            for peer, b in got.items():
+                for (g, f), row in zip(part.recv[peer], b.numpy()):
+                    slot[(int(g), int(f))] = row
+            oracle.lts_neigh(dn, st, 0, part.n_owned, True, None)
+            rows = [slot[(int(part.el_fa_el[e, f]), int(part.fid[e, f]))] for e, f in ghost_faces]
+            oracle.neigh_premixed_faces(d, st["dofsE"], ghost_faces, rows, O)
             t += p.dt
-        np.save(os.path.join(out_dir, f"part{rank}.npy"), st["dofsE"][:part.n_owned])
+        out = np.empty_like(st["dofsE"][:part.n_owned])
+        out[part.owned - part.lo] = st["dofsE"][:part.n_owned]
+        np.save(os.path.join(out_dir, f"part{rank}.npy"), out)
     finally:
         dist.destroy_process_group()
+
+
+def test_face_orientation_factorisation():
+    import oracle
+    for order in (2, 3, 4, 5):
+        d = _prob(order=order, n=2).oracle_dict()
+        _, res = oracle.face_orientations(d["fluxL"], d["fluxN"])
+        assert res < 1e-12, (order, res)
 
 
 @pytest.mark.parametrize("world", [2, 3])
@@ -118,4 +147,7 @@ def test_ranks_with_exchange_match_one_domain(tmp_path, world):
     ref = OracleRun(p, e0)
     ref.step(n_steps)
     got = np.concatenate([np.load(os.path.join(tmp_path, f"part{r}.npy")) for r in range(world)])
-    assert np.array_equal(got, ref.state["dofsE"])
+    # (the ghost faces' fluxes are added after the other faces, with fluxL . O for fluxN: the same
+    # sums in another order)
+    rel = np.linalg.norm(got - ref.state["dofsE"]) / np.linalg.norm(ref.state["dofsE"])
+    assert rel < 1e-12, rel
