@@ -45,9 +45,9 @@ def parse():
     ap.add_argument("--serve-requests", type=int, default=160,
                     help="requests of the serving run (Poisson arrivals); 0 skips it")
     ap.add_argument("--serve-rate", type=float, default=20.0, help="mean arrivals per second")
-    ap.add_argument("--lts-report", action="store_true",
-                    help="also time rate-2 LTS against GTS on a layered box (adds about a minute)")
-    ap.add_argument("--batch-sims", type=int, default=32,
+    ap.add_argument("--lts-report", action=argparse.BooleanOptionalAction, default=True,
+                    help="also time rate-2 LTS against GTS on a layered box")
+    ap.add_argument("--batch-sims", type=int, default=64,
                     help="simulations of the uneven-batch run (graph-captured batch steps); 0 skips it")
     return ap.parse_args()
 
@@ -169,6 +169,19 @@ def algorithmic(prob, prec, premix=False, fs_pair=84, fused=False):
         local_bytes += face + dofs + 4 * (4 + 1 + 1 + 1)
         local_flops += neigh_flops
     return dict(local_bytes=local_bytes, neigh_bytes=neigh_bytes, local_flops=local_flops, neigh_flops=neigh_flops)
+
+
+def compulsory_step_bytes(prob, prec):
+    """Compulsory bytes of one element step with every array touched once: DOFs (elastic and
+    anelastic) read and written, the time-integrated DOFs written and read once, the FP64 star
+    matrices (3 x 24), both flux-solver sets (2 x 4 x 81) and, with attenuation, the anelastic
+    sources, star matrices and flux solvers, plus 24 bytes of connectivity."""
+    from edge_b200.host import n_modes
+    B, R, rm, p = n_modes(prob.order), prob.runs, prob.rm, (8 if prec == 64 else 4)
+    b = 2 * (9 + 6 * rm) * B * R * p + 2 * 9 * B * R * p + 3 * 24 * 8 + 2 * 4 * 81 * 8 + 24
+    if rm:
+        b += 12 * 8 * rm + 3 * 9 * 8 + 2 * 4 * 54 * 8
+    return b
 
 
 def measured_peaks():
@@ -475,76 +488,144 @@ def run_tc_probe(local_ms, n_el, order, runs, device, clock_mhz):
                     "everything"}
 
 
-# compiled FP32 configurations the uneven batch draws from: (order, runs, mechanisms)
-BATCH_CFGS = [(o, r, 0) for o in (3, 4, 5) for r in (1, 4, 8, 16)] + [(6, r, 0) for r in (4, 8, 16)] + \
-    [(3, 8, 3), (4, 8, 3)]
+# FP32 configurations the uneven batch draws from: orders 3-6, fused runs 1 / 4 / 8 / 16, elastic
+# or 3 mechanisms (order, runs, mechanisms)
+BATCH_CFGS = [(o, r, rm) for o in (3, 4, 5, 6) for r in (1, 4, 8, 16) for rm in (0, 3)]
+# four seeded boxes of the batch configuration's sizes: (cubes per axis, vertex jitter)
+BATCH_BOXES = [(10, 0.0), (19, 0.05), (29, 0.1), (44, 0.2)]
 
 
-def run_batch(n_sims, device, seed=3343, mem_fraction=0.6):
-    """Uneven batch in the shape of the 64-simulation batch configuration, scaled to a bounded run:
-    n_sims simulations over four seeded jittered boxes (9^3 .. 21^3 cubes x 6 = 4,374 .. 55,566 tets,
-    jitter 0 / 5 / 10 / 20%), each with its own order, fused runs and physics (compiled FP32
-    configurations, viscoelastic at 8 runs, orders 3-4), own random sources and 20-100 steps,
-    stepped together by graph-captured batch steps with autotuned launch shapes. Reported against
-    the same simulations run one after another through edge_b200_step (FP32), and against each
-    simulation alone on the plain FP64 path (one run per fused run; FP64 ms per step measured per
-    mesh, order and physics, times runs x steps)."""
+def _batch_sims(n_sims, seed, step_range):
+    """The seeded simulations of the uneven batch: (mesh index, order, runs, mechanisms, steps)."""
+    import numpy as np
+    rng = np.random.default_rng(seed)
+    out = []
+    for _ in range(n_sims):
+        mi = int(rng.integers(len(BATCH_BOXES)))
+        o, r, rm = BATCH_CFGS[int(rng.integers(len(BATCH_CFGS)))]
+        out.append((mi, o, r, rm, int(rng.integers(step_range[0], step_range[1] + 1))))
+    return out
+
+
+def run_batch(n_sims, device, seed=3343, mem_fraction=0.6, step_range=(20, 100)):
+    """The uneven batch configuration: n_sims simulations over four seeded boxes of 6,000, 41,154,
+    146,334 and 511,104 tets (jitter 0 / 5 / 10 / 20%), each with its own order (3-6), fused runs
+    (1, 4, 8, 16), physics (elastic or 3 mechanisms), random sources and step count (step_range; the
+    configuration's 200-1000 steps scaled by 1/10 to bound the run). Simulations are admitted in
+    waves by an HBM budget (mem_fraction of the free memory). Every wave runs three ways, timed on the
+    wall clock after a device sync: each simulation alone after another (its own fused multi-step
+    calls), the graph-captured batch steps of edge_b200_batch_* (a stream per context), and the
+    merged form (edge_b200.merged: one context and one persistent launch per kernel and step for
+    each configuration family, the families on streams of their own). Also against each simulation
+    alone on the plain FP64 path (one run per fused run; FP64 ms per step measured per mesh, order and
+    physics; viscoelastic orders 5-6 have no FP64 path and are left out of that sum)."""
     import time
 
     import numpy as np
     import torch
     from edge_b200 import host
     from edge_b200.batch import Batch
+    from edge_b200.merged import MergedFamily, family_key
     from edge_b200.solver import Solver
-    rng = np.random.default_rng(seed)
-    boxes = [(9, 0.0), (13, 0.05), (17, 0.1), (21, 0.2)]
-    meshes = [host.Mesh.box(n, (1e4, 1e4, 1e4), jitter=j, seed=seed + i) for i, (n, j) in enumerate(boxes)]
-    free, _ = torch.cuda.mem_get_info(device)
-    budget, used = free * mem_fraction, 0.0
-    sims = []
-    for k in range(n_sims):
-        mi = int(rng.integers(len(meshes)))
-        o, r, rm = BATCH_CFGS[int(rng.integers(len(BATCH_CFGS)))]
-        steps = int(rng.integers(20, 101))
-        mesh = meshes[mi]
+    meshes = [host.Mesh.box(n, (1e4, 1e4, 1e4), jitter=j, seed=seed + i) for i, (n, j) in enumerate(BATCH_BOXES)]
+    base = {}
+
+    def elem(mi, rm):
+        if (mi, rm) not in base:
+            m = meshes[mi]
+            rng = np.random.default_rng(seed + 7 * mi + rm)
+            rho, lam, mu = host.materials(m, 1e4, rng=rng)
+            qp = rng.uniform(50.0, 200.0, m.n_el) if rm else None
+            qs = rng.uniform(50.0, 200.0, m.n_el) if rm else None
+            base[(mi, rm)] = (rho, host.element_data(m, rho, lam, mu, rm, qp, qs))
+        return base[(mi, rm)]
+
+    def problem(k, mi, o, r, rm, steps):
+        rho, d = elem(mi, rm)
+        m = meshes[mi]
+        dt = host.dt_cfl(m, o, rho, d["lam"], d["mu"])
+        rng = np.random.default_rng(seed + 17 * k)
+        pos = rng.uniform(1e3, 9e3, (r, 3))
+        scal = np.concatenate([rng.normal(0.0, 1.0, (r, 6)) * 1e15, np.zeros((r, 3))], axis=1)
+        dts = dt / 10.0
+        src = host.make_sources(m, o, r, pos, scal, 1.5, 0.8, dts, int(np.ceil(steps * dt / dts)) + 4)
+        return host.Problem(order=o, runs=r, rm=rm, mesh=m, rho=rho, lam=d["lam"], mu=d["mu"], starE=d["starE"],
+                            fsE=d["fsE"], dt=dt, starA=d["starA"], srcA=d["srcA"], fsA=d["fsA"], omega=d["omega"],
+                            sources=src, name=f"sim{k}")
+
+    sims = _batch_sims(n_sims, seed, step_range)
+    budget = torch.cuda.mem_get_info(device)[0] * mem_fraction
+    waves, cur, used = [], [], 0.0
+    for k, (mi, o, r, rm, steps) in enumerate(sims):
         B, F = host.n_modes(o), o * (o + 1) // 2
-        need = mesh.n_el * r * 4 * ((9 + 6 * rm) * (B + 4) * 2 + 36 * (F + 4)) + mesh.n_el * 4000
-        if used + need > budget:
-            continue
-        prob = host.build_problem(0, o, r, rm=rm, mesh=mesh, seed=seed + 17 * k, source="random", n_receivers=0,
-                                  n_steps=steps, f0=1.5)
-        e0, a0 = prob.zero_dofs()
-        s = Solver(prob, precision=32, device=device)
-        s.upload_dofs(e0, a0)
-        sims.append((mi, o, r, rm, steps, prob, s))
+        need = meshes[mi].n_el * (r * 4 * ((9 + 6 * rm) * (B + 4) * 3 + 2 * 36 * (F + 4)) + 8000)
+        if cur and used + need > budget:
+            waves.append(cur)
+            cur, used = [], 0.0
+        cur.append(k)
         used += need
-    solvers = [x[6] for x in sims]
-    steps = [x[4] for x in sims]
-    upd = sum(x[5].n_el * x[2] * x[4] for x in sims)
-    torch.cuda.synchronize()
-    b = Batch(solvers, autotune=True)
-    b.run(1)  # captures the graph once outside the timing
-    t0 = time.perf_counter()
-    segs = b.run(steps)
-    t_batch = time.perf_counter() - t0
-    b.close()
-    # the same simulations one after another, each through its own steps
-    torch.cuda.synchronize()
-    t0 = time.perf_counter()
-    for s, k in zip(solvers, steps):
-        s.step(k)
-    torch.cuda.synchronize()
-    t_seq = time.perf_counter() - t0
+    if cur:
+        waves.append(cur)
+    t_seq = t_batch = t_merged = 0.0
+    upd = 0
+    merged_launches = seq_launches = 0
+    fams_total = 0
+    for wave in waves:
+        probs = {k: problem(k, *sims[k]) for k in wave}
+        steps = [sims[k][4] for k in wave]
+        upd += sum(probs[k].n_el * sims[k][2] * sims[k][4] for k in wave)
+        solvers = []
+        for k in wave:
+            sv = Solver(probs[k], precision=32, device=device)
+            e0, a0 = probs[k].zero_dofs(np.float32)
+            sv.upload_dofs(e0, a0)
+            solvers.append(sv)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for sv, n in zip(solvers, steps):
+            sv.step(n)
+            seq_launches += sv.launches()
+        torch.cuda.synchronize()
+        t_seq += time.perf_counter() - t0
+        b = Batch(solvers, autotune=False)
+        b.run(1)  # captures the graph once outside the timing
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        b.run(steps)
+        t_batch += time.perf_counter() - t0
+        b.close()
+        for sv in solvers:
+            sv.close()
+        del solvers
+        # merged families, each on a stream of its own
+        fams = {}
+        for k in wave:
+            fams.setdefault(family_key(probs[k], 32), []).append(k)
+        objs = []
+        for key, ks in fams.items():
+            st = torch.cuda.Stream(device=device)
+            fam = MergedFamily([probs[k] for k in ks], [sims[k][4] for k in ks], precision=32, device=device,
+                               stream=st.cuda_stream)
+            objs.append((fam, st))
+        fams_total += len(objs)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for fam, _ in objs:
+            merged_launches += fam.launch()
+        torch.cuda.synchronize()
+        t_merged += time.perf_counter() - t0
+        for fam, _ in objs:
+            fam.close()
+        del objs
     # plain FP64, one run: ms per step per (mesh, order, mechanisms)
     ms64 = {}
-    for mi, o, r, rm, k, prob, s in sims:
+    for k, (mi, o, r, rm, n) in enumerate(sims):
         key = (mi, o, rm)
-        if key in ms64:
+        if key in ms64 or (rm and o > 4):
             continue
-        p = host.build_problem(0, o, 1, rm=rm, mesh=meshes[mi], seed=seed, source=None, n_receivers=0)
+        p = problem(k, mi, o, 1, rm, 4)
+        p.sources = {}
         s64 = Solver(p, precision=64, device=device)
-        z, za = p.zero_dofs()
-        s64.upload_dofs(z, za)
         s64.step(2)
         s64.sync()
         t1 = time.perf_counter()
@@ -552,17 +633,21 @@ def run_batch(n_sims, device, seed=3343, mem_fraction=0.6):
         s64.sync()
         ms64[key] = (time.perf_counter() - t1) / 10 * 1e3
         s64.close()
-    t64 = sum(ms64[(mi, o, rm)] * r * k for mi, o, r, rm, k, _, _ in sims) / 1e3
-    for s in solvers:
-        s.close()
-    return {"simulations": len(sims), "tets": [m.n_el for m in meshes],
-            "configs": sorted({(o, r, rm) for _, o, r, rm, _, _, _ in sims}),
-            "element_updates": upd, "graph_segments": len(segs), "batch_s": t_batch,
-            "element_updates_per_s": upd / t_batch, "one_after_another_fp32_s": t_seq,
-            "speedup_vs_one_after_another_fp32": t_seq / t_batch, "plain_fp64_alone_s": t64,
-            "speedup_vs_plain_fp64_alone": t64 / t_batch,
-            "note": "wall clock (host timer after a device sync); FP64 extrapolated from 10 timed steps per "
-                    "mesh / order / physics"}
+    have64 = [x for x in sims if (x[0], x[1], x[3]) in ms64]
+    t64 = sum(ms64[(mi, o, rm)] * r * n for mi, o, r, rm, n in have64) / 1e3
+    frac64 = sum(meshes[x[0]].n_el * x[2] * x[4] for x in have64) / max(upd, 1)
+    return {"simulations": len(sims), "waves": len(waves), "tets": [m.n_el for m in meshes],
+            "configs": sorted({(o, r, rm) for _, o, r, rm, _ in sims}), "configuration_families": fams_total,
+            "steps_range": list(step_range), "element_updates": upd,
+            "one_after_another_fp32_s": t_seq, "graph_batch_s": t_batch, "merged_s": t_merged,
+            "element_updates_per_s": upd / t_merged,
+            "speedup_vs_one_after_another_fp32": t_seq / t_merged,
+            "graph_batch_speedup_vs_one_after_another_fp32": t_seq / t_batch,
+            "kernel_launches": {"one_after_another": seq_launches, "merged": merged_launches},
+            "plain_fp64_alone_s_covered": t64, "fp64_covered_fraction_of_updates": frac64,
+            "speedup_vs_plain_fp64_alone": t64 / (t_merged * frac64) if frac64 > 0 else None,
+            "note": "wall clock (host timer after a device sync); the FP64 comparison covers the simulations "
+                    "with an FP64 configuration and scales the merged time by their share of the updates"}
 
 
 def run_lts(device, n_cubes=48, order=5, runs=16, n_groups=3, cycles=2):
@@ -696,14 +781,27 @@ def main():
     alg = algorithmic(prob, prec, premix=bool(kc[1]), fs_pair=int(kc[2]), fused=bool(kc[5]))
     top = int(np.argmax(kms[:2]))
     avg_ms = kms[top] / max(kn[top], 1)
-    bytes_launch = (alg["local_bytes"] if top == 0 else alg["neigh_bytes"]) * prob.n_el
+    # algorithmic bytes: the path's compulsory bytes of one element step (every array touched once:
+    # DOFs read + written, time-integrated DOFs written + read once, FP64 star matrices and flux
+    # solvers, connectivity) times the elements of the launch. The fused local kernel runs a whole
+    # step per launch (this step's local update and the previous step's neighbour update); without
+    # fusion the step's two kernels are timed together.
+    fused = bool(kc[5])
+    step_bytes = compulsory_step_bytes(prob, prec)
+    bytes_launch = step_bytes * prob.n_el
+    launch_ms = avg_ms if (fused and top == 0) else (kms[0] / max(kn[0], 1) + kms[1] / max(kn[1], 1))
+    design_bytes = (alg["local_bytes"] if top == 0 else alg["neigh_bytes"]) * prob.n_el
     flops_launch = (alg["local_flops"] if top == 0 else alg["neigh_flops"]) * prob.n_el
     peak, peak_src = measured_peaks()
-    achieved = bytes_launch / (avg_ms / 1e3) / 1e9
+    achieved = bytes_launch / (launch_ms / 1e3) / 1e9
     traffic = traffic_from_profiles(a.workload)
-    roofline = {"bound": "hbm", "kernel": names[top], "achieved": achieved, "peak": peak, "unit": "GB/s",
+    roofline = {"bound": "hbm", "kernel": names[top] if (fused and top == 0) else "local+neighbour",
+                "achieved": achieved, "peak": peak, "unit": "GB/s",
                 "frac": achieved / peak, "peak_source": peak_src, "traffic": traffic,
-                "algorithmic_bytes_per_launch": bytes_launch,
+                "algorithmic_bytes_per_launch": bytes_launch, "algorithmic_bytes_per_element_step": step_bytes,
+                "launch_ms": launch_ms,
+                "design_bytes_per_launch": design_bytes,
+                "frac_design_bytes": design_bytes / (avg_ms / 1e3) / 1e9 / peak,
                 "achieved_tflops": flops_launch / (avg_ms / 1e3) / 1e12,
                 "kernel_avg_ms": {names[i]: float(kms[i] / kn[i]) for i in range(4) if kn[i]},
                 "kernel_share": shares}

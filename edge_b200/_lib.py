@@ -66,6 +66,9 @@ _SIGS = {
     "edge_b200_wavefield": (C.c_int, [vp, vp]),
     "edge_b200_error_norms": (C.c_int, [vp, dbl, C.c_int, vp, C.c_int, vp, vp, vp, vp, vp, vp]),
     "edge_b200_set_owned": (C.c_int, [vp, i64]),
+    "edge_b200_set_group_dt": (C.c_int, [vp, vp]),
+    "edge_b200_set_source_clocks": (C.c_int, [vp, vp, vp]),
+    "edge_b200_set_active_elements": (C.c_int, [vp, i64]),
     "edge_b200_set_send_count": (C.c_int, [vp, i64]),
     "edge_b200_step_phase": (C.c_int, [vp, dbl, dbl, C.c_int]),
     "edge_b200_face_block_bytes": (i64, [vp]),

@@ -225,6 +225,14 @@ struct edge_b200_ctx {
   // sources
   SrcArgs src{};
   DevBuf srcMem[10];
+  // per-source clocks and per-group time steps of merged simulations (edge_b200_set_source_clocks,
+  // edge_b200_set_group_dt); srcStep counts the steps since the clocks were set
+  DevBuf srcClk0, srcClkDt, grpDt;
+  bool srcClocks = false, grpDtOn = false;
+  int64_t srcStep = 0;
+  int nSrc = 0;
+  // merged simulations still running: elements [0, nActive) (the rest share no face with them)
+  int64_t nActive = INT64_MAX;
   // receivers
   int nRecv = 0, nRecvGrp = 0, maxBuf = 0;
   double recvTime = 0, period = 0;
@@ -449,9 +457,10 @@ struct edge_b200_ctx {
     a.vId = vId;
     a.faType = faType;
     a.fsLR = (ks->premix() && !fsLRStale) ? fsLR.p : nullptr;
+    a.grpDt = grpDtOn ? grpDt.as<double>() : nullptr;
     a.nEl = nEl;
     a.elFirst = 0;
-    a.elCount = nOwned;
+    a.elCount = std::min(nOwned, nActive);
     a.dt = dt;
     for (int i = 0; i < 3; i++) a.omega[i] = omega[i];
     return a;
@@ -720,6 +729,8 @@ int edge_b200_set_sources(edge_b200_ctx *ctx, int n, const int64_t *el, const in
   if (!ctx || n < 0) return EDGE_B200_EINVAL;
   ctx->src = SrcArgs{};
   ctx->hSrcGrpEl.clear();
+  ctx->nSrc = 0;
+  ctx->srcClocks = false;  // clocks belong to a source list
   if (n == 0) return EDGE_B200_OK;
   if (!el || !run || !scal || !b_eval || !t0 || !dt || !ts_off || !n_pts || !ts) return EDGE_B200_EINVAL;
   std::vector<int32_t> off{0};
@@ -757,7 +768,51 @@ int edge_b200_set_sources(edge_b200_ctx *ctx, int n, const int64_t *el, const in
   ctx->src.nPts = m[8].as<int64_t>();
   ctx->src.ts = m[9].as<double>();
   ctx->src.tol = kTolTime;
+  ctx->nSrc = n;
   EDGE_CUDA(cudaStreamSynchronize(s), "sources");
+  return EDGE_B200_OK;
+}
+
+int edge_b200_set_source_clocks(edge_b200_ctx *ctx, const double *t0, const double *dt) {
+  if (!ctx) return EDGE_B200_EINVAL;
+  ctx->srcStep = 0;
+  if (!t0 || !dt) {
+    ctx->srcClocks = false;
+    return EDGE_B200_OK;
+  }
+  const int n = ctx->nSrc;
+  if (n == 0) return EDGE_B200_EINVAL;
+  for (int i = 0; i < n; i++)
+    if (!(dt[i] > 0)) return EDGE_B200_EINVAL;
+  EDGE_CUDA(ctx->srcClk0.put(t0, n * sizeof(double), ctx->stream), "source clocks");
+  EDGE_CUDA(ctx->srcClkDt.put(dt, n * sizeof(double), ctx->stream), "source clocks");
+  EDGE_CUDA(cudaStreamSynchronize(ctx->stream), "source clocks");
+  ctx->srcClocks = true;
+  return EDGE_B200_OK;
+}
+
+int edge_b200_set_active_elements(edge_b200_ctx *ctx, int64_t n_active) {
+  if (!ctx || n_active < 0 || n_active > ctx->nEl || ctx->nTg > 1) return EDGE_B200_EINVAL;
+  // the pending neighbour step of a fused call covers the old range
+  EDGE_CUDA(ctx->flush(), "pending neighbour step");
+  ctx->nActive = n_active;
+  return EDGE_B200_OK;
+}
+
+int edge_b200_set_group_dt(edge_b200_ctx *ctx, const double *dt_group) {
+  if (!ctx) return EDGE_B200_EINVAL;
+  if (!dt_group) {
+    ctx->grpDtOn = false;
+    return EDGE_B200_OK;
+  }
+  if (ctx->nTg > 1) return EDGE_B200_EINVAL;  // GTS only
+  const int64_t E = ctx->ks->elementsPerCta(), n = (ctx->nEl + E - 1) / E;
+  for (int64_t g = 0; g < n; g++)
+    if (!(dt_group[g] > 0)) return EDGE_B200_EINVAL;
+  EDGE_CUDA(ctx->flush(), "pending neighbour step");
+  EDGE_CUDA(ctx->grpDt.put(dt_group, n * sizeof(double), ctx->stream), "group time steps");
+  EDGE_CUDA(cudaStreamSynchronize(ctx->stream), "group time steps");
+  ctx->grpDtOn = true;
   return EDGE_B200_OK;
 }
 
@@ -898,11 +953,18 @@ static int runSteps(edge_b200_ctx *ctx, double t, double dt, int n_steps, int ph
       if (ctx->src.nGrp > 0 && ctx->rangeSrc) {
         SrcArgs sa = ctx->src;
         sa.t = ts;
+        sa.elLimit = std::min(ctx->nOwned, ctx->nActive);
+        if (ctx->srcClocks) {
+          sa.clk0 = ctx->srcClk0.as<double>();
+          sa.clkDt = ctx->srcClkDt.as<double>();
+          sa.step = ctx->srcStep;
+        }
         sa.dt = dt;
         EDGE_CUDA(ctx->launch(2, [&] { return ctx->ks->sources(ctx->dofsE, sa, s); }), "source kernel");
         ctx->launches++;
       }
     }
+    if ((phases & 1) && ctx->rangeSrc) ctx->srcStep++;
     if (fused) {
       ctx->faceCur ^= 1;
       ctx->pending = true;
@@ -985,7 +1047,7 @@ int edge_b200_unpack_faces(edge_b200_ctx *ctx, int n, const int32_t *slots, cons
 
 int edge_b200_set_time_groups(edge_b200_ctx *ctx, int n_groups, const int64_t *group_first) {
   if (!ctx || !ctx->meshSet || n_groups < 1 || n_groups > 16 || !group_first) return EDGE_B200_EINVAL;
-  if (ctx->nOwned != ctx->nEl) return EDGE_B200_EINVAL;  // time groups cover the whole mesh
+  if (ctx->nOwned != ctx->nEl || ctx->nActive < ctx->nEl) return EDGE_B200_EINVAL;  // time groups cover the whole mesh
   if (group_first[0] != 0 || group_first[n_groups] != ctx->nEl) return EDGE_B200_EINVAL;
   for (int g = 0; g < n_groups; g++)
     if (group_first[g + 1] < group_first[g]) return EDGE_B200_EINVAL;
@@ -1391,6 +1453,10 @@ struct edge_b200_batch {
     if (ctx->src.nGrp > 0) {
       SrcArgs sa = ctx->src;
       sa.t = t0[k] + tOff;
+      if (ctx->srcClocks) {
+        sa.clk0 = ctx->srcClk0.as<double>();
+        sa.clkDt = ctx->srcClkDt.as<double>();
+      }
       sa.dt = dt[k];
       sa.stepDev = steps + k;
       if ((c = ctx->ks->sources(ctx->dofsE, sa, s))) return c;

@@ -41,6 +41,7 @@ class KernelSetImpl final : public KernelSet {
     b.firstTs = a.firstTs;
     b.fsLR = static_cast<const T *>(a.fsLR);
     b.faceIn = static_cast<const T *>(a.faceIn);
+    b.grpDt = a.grpDt;
     return b;
   }
   static constexpr size_t smemLocal() { return G::smemLocalGts; }

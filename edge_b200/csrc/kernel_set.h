@@ -29,6 +29,8 @@ struct StepArgsRaw {
   const void *fsLR = nullptr;
   // fused GTS steps: the previous step's face projections whose neighbour step is still pending
   const void *faceIn = nullptr;
+  // per element group time steps of the GTS local step (merged simulations), or null
+  const double *grpDt = nullptr;
 };
 
 class KernelSet {

@@ -60,6 +60,9 @@ struct StepArgs {
   // whose neighbour fluxes are added to the DOF rows before the recursion (the previous step's
   // neighbour step runs here), or null when none are pending
   const T *faceIn;
+  // GTS local step with a time step per element group (g = 0 .. of the launch range: E elements
+  // each) instead of dt, or null: several simulations merged into one context step together
+  const double *grpDt;
 };
 enum { LTS_HAS_LARGER = 1, LTS_HAS_SMALLER = 2 };
 enum { LTS_EQ = 0, LTS_GT = 1, LTS_LT = 2 };
@@ -1278,7 +1281,7 @@ __global__ void __launch_bounds__(Geo<T, O, R, RM>::NT, LTS == 2 ? 1 : Geo<T, O,
   const int q = threadIdx.x >> 5, l = threadIdx.x & 31;
   const int eo = l / R, r = l % R;
   const int64_t nGroups = (a.elCount + E - 1) / E;
-  const T dt = T(a.dt);
+  const T dt0 = T(a.dt);
   if constexpr (AS) {
     // the first group's DOF rows (and flux-solver blocks of its first face)
     const int64_t g0 = blockIdx.x;
@@ -1304,6 +1307,7 @@ __global__ void __launch_bounds__(Geo<T, O, R, RM>::NT, LTS == 2 ? 1 : Geo<T, O,
     const int64_t e = a.elFirst + g * E + eo;
     const bool valid = g * E + eo < a.elCount;
     const int64_t ev = valid ? e : 0;
+    const T dt = (LTS == 0 && a.grpDt) ? T(a.grpDt[g]) : dt0;
     T tIr[G::tiSmem ? 1 : B];
     T tIAr[(G::tiSmem || RM == 0) ? 1 : RM][B];
     // DOFs -> X, dt * DOFs -> TI (and the anelastic counterparts)
@@ -1999,6 +2003,12 @@ struct SrcArgs {
   // replayed launches (a captured batch step): the step starts at t + (*stepDev) * dt, the step
   // counter advancing on the device after each step; null: at t
   const int64_t *stepDev;
+  // per-source clocks (merged simulations with their own time steps), or null: source i's step k
+  // (k = *stepDev, or `step`) covers [clk0[i] + k clkDt[i], clk0[i] + (k + 1) clkDt[i]]
+  const double *clk0 = nullptr, *clkDt = nullptr;
+  int64_t step = 0;
+  // sources in elements at or beyond elLimit (not stepped) are skipped
+  int64_t elLimit = 0x7fffffffffffffffLL;
 };
 
 __device__ inline double seriesIntegral(double dx, double xStart, int64_t nPts, const double *vals, double x1,
@@ -2034,11 +2044,15 @@ __global__ void kSources(T *dofsE, SrcArgs s) {
   constexpr int B = nModes(O);
   const int g = blockIdx.x;
   if (g >= s.nGrp) return;
-  const double t1 = s.stepDev ? s.t + double(*s.stepDev) * s.dt : s.t;
+  const double k = s.stepDev ? double(*s.stepDev) : double(s.step);
+  const double t1 = s.stepDev ? s.t + k * s.dt : s.t;
+  if (s.el[s.grpOff[g]] >= s.elLimit) return;
   for (int t = threadIdx.x; t < 9 * B; t += blockDim.x) {
     const int q = t / B, md = t % B;
     for (int i = s.grpOff[g]; i < s.grpOff[g + 1]; i++) {
-      const double in = seriesIntegral(s.dts[i], s.t0[i], s.nPts[i], s.ts + s.tsOff[i], t1, t1 + s.dt, s.tol);
+      const double a1 = s.clk0 ? s.clk0[i] + k * s.clkDt[i] : t1;
+      const double a2 = s.clk0 ? a1 + s.clkDt[i] : t1 + s.dt;
+      const double in = seriesIntegral(s.dts[i], s.t0[i], s.nPts[i], s.ts + s.tsOff[i], a1, a2, s.tol);
       const double sc = in * s.scal[i * 9 + q];
       T *p = dofsE + ((s.el[i] * 9 + q) * R + s.run[i]) * int64_t(padGlobal<T>(B)) + md;
       *p = T(double(*p) + sc * s.bEval[i * B + md]);

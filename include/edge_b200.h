@@ -206,6 +206,22 @@ int edge_b200_set_sources(edge_b200_ctx *ctx, int n, const int64_t *el, const in
                           const double *scal, const double *b_eval, const double *t0,
                           const double *dt, const int64_t *ts_off, const int64_t *n_pts,
                           int64_t n_ts, const double *ts);
+/* Several simulations of one configuration (order, fused runs, mechanisms, precision, relaxation
+ * frequencies) merged into one context: their meshes side by side as disjoint element ranges, each
+ * padded to a multiple of the 32 / n_runs elements of a kernel group, so that one persistent launch
+ * per kernel steps all of them. edge_b200_set_group_dt gives every element group its own time
+ * step (dt_group[ceil(nEl / (32 / n_runs))]; NULL: the step's dt for all; GTS only), and
+ * edge_b200_set_source_clocks every point source its own clock (in the order of
+ * edge_b200_set_sources; NULL: the step's time): step k after the call integrates source i over
+ * [t0[i] + k dt[i], t0[i] + (k + 1) dt[i]]. Simulations that stop are dropped by ordering them last
+ * and lowering edge_b200_set_active_elements to the end of the ones still running: the kernels then
+ * step elements [0, n_active) only (multi-step calls still fuse their neighbour steps; the elements
+ * behind must share no face with those before) and sources beyond are skipped. No counterpart in
+ * the reference (one solver per process; uneven batches of one configuration family in one
+ * launch). */
+int edge_b200_set_group_dt(edge_b200_ctx *ctx, const double *dt_group);
+int edge_b200_set_source_clocks(edge_b200_ctx *ctx, const double *t0, const double *dt);
+int edge_b200_set_active_elements(edge_b200_ctx *ctx, int64_t n_active);
 /* Receivers grouped by element (el ascending; equal elements adjacent), basis[n][B] plain basis
  * values, first output time t_first and sampling period (Receivers::init / getRecvTimeRel /
  * writeRecvAll, io/Receivers.cpp:33-290). Up to max_buf samples are buffered per receiver. */
