@@ -463,9 +463,13 @@ def run_tc_probe(local_ms, n_el, order, runs, device, clock_mhz):
     from edge_b200 import tcprobe
     from edge_b200.host import n_face_modes, n_modes
     errs = {f"{n}x{k}x{it}": tcprobe.check(n, k, it) for n, k, it in ((16, 8, 1), (64, 32, 1), (128, 32, 3))}
-    cyc = {}
+    # cycles per instruction with one accumulator (each waits for the previous sum) and with three
+    # (the three row tiles of an element group, whose instructions overlap); the estimate uses three
+    cyc1, cyc = {}, {}
     for n in (16, 32, 48, 64, 96, 128):
-        ms, per_cta = tcprobe.time_shape(n)
+        ms, per_cta = tcprobe.time_shape(n, acc=1)
+        cyc1[n] = ms * 1e-3 * clock_mhz * 1e6 / per_cta
+        ms, per_cta = tcprobe.time_shape(n, acc=3)
         cyc[n] = ms * 1e-3 * clock_mhz * 1e6 / per_cta
     pad = lambda x, q: (x + q - 1) // q * q
     Bm = lambda o: n_modes(o) if o > 0 else 0
@@ -480,7 +484,8 @@ def run_tc_probe(local_ms, n_el, order, runs, device, clock_mhz):
         c = cyc[min(x for x in cyc if x >= nn)] if nn <= 128 else cyc[128] * nn / 128
         est[name] = groups_per_sm * tiles * split * (kk // 8) * c / (clock_mhz * 1e3)
     total = sum(est.values())
-    return {"check_rel_err": errs, "cycles_per_instruction_128xNx8": cyc, "clock_mhz": clock_mhz,
+    return {"check_rel_err": errs, "cycles_per_instruction_128xNx8": cyc,
+            "cycles_per_instruction_128xNx8_one_accumulator": cyc1, "clock_mhz": clock_mhz,
             "products": [{"name": a, "N": b, "K": c} for a, b, c in prods],
             "tensor_ms_per_step_by_product": est, "tensor_ms_per_step": total,
             "fused_local_kernel_ms": local_ms, "ratio_tensor_products_to_whole_fp32_kernel": total / local_ms,

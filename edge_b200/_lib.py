@@ -58,6 +58,7 @@ _SIGS = {
     "edge_b200_keep_tdofs": (C.c_int, [vp, C.c_int]),
     "edge_b200_set_run_dofs": (C.c_int, [vp, C.c_int, vp, vp]),
     "edge_b200_copy_run": (C.c_int, [vp, C.c_int, vp, C.c_int]),
+    "edge_b200_share_element_data": (C.c_int, [vp, vp]),
     "edge_b200_rewind_receivers": (C.c_int, [vp, dbl]),
     "edge_b200_set_sources": (C.c_int, [vp, C.c_int, vp, vp, vp, vp, vp, vp, vp, vp, i64, vp]),
     "edge_b200_set_receivers": (C.c_int, [vp, C.c_int, vp, vp, dbl, dbl, C.c_int]),

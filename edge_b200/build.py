@@ -32,19 +32,39 @@ def nvcc():
     raise RuntimeError("nvcc not found")
 
 
-def _deps_mtime():
-    hdrs = glob.glob(os.path.join(CSRC, "**", "*.h"), recursive=True)
-    hdrs += glob.glob(os.path.join(CSRC, "**", "*.cuh"), recursive=True)
-    hdrs += glob.glob(os.path.join(CSRC, "**", "*.inc"), recursive=True)
-    hdrs += [os.path.join(ROOT, "include", "edge_b200.h")]
-    return max(os.path.getmtime(h) for h in hdrs)
+def _includes(path, seen=None):
+    """The quoted #include files a source pulls in, transitively (searched beside the including
+    file, in csrc and in include/)."""
+    seen = set() if seen is None else seen
+    try:
+        text = open(path).read()
+    except OSError:
+        return seen
+    for line in text.splitlines():
+        line = line.strip()
+        if not line.startswith("#include \""):
+            continue
+        name = line.split('"')[1]
+        for d in (os.path.dirname(path), CSRC, os.path.join(ROOT, "include")):
+            cand = os.path.normpath(os.path.join(d, name))
+            if os.path.exists(cand):
+                if cand not in seen:
+                    seen.add(cand)
+                    _includes(cand, seen)
+                break
+    return seen
+
+
+def _deps_mtime(src):
+    return max([os.path.getmtime(h) for h in _includes(src)] + [0.0])
 
 
 def sources():
     return sorted(glob.glob(os.path.join(CSRC, "*.cu")) + glob.glob(os.path.join(CSRC, "*.cpp")))
 
 
-def _compile(src, force, hdr_mtime):
+def _compile(src, force):
+    hdr_mtime = _deps_mtime(src)
     obj = os.path.join(BUILD, os.path.basename(src) + ".o")
     if (not force and os.path.exists(obj) and os.path.getmtime(obj) >= os.path.getmtime(src)
             and os.path.getmtime(obj) >= hdr_mtime):
@@ -60,13 +80,12 @@ def _compile(src, force, hdr_mtime):
 
 def build(force=False, jobs=None, verbose=False):
     os.makedirs(BUILD, exist_ok=True)
-    hdr = _deps_mtime()
     srcs = sources()
     jobs = jobs or min(len(srcs), os.cpu_count() or 4)
     changed = False
     objs = []
     with cf.ThreadPoolExecutor(jobs) as ex:
-        for obj, ch in ex.map(lambda s: _compile(s, force, hdr), srcs):
+        for obj, ch in ex.map(lambda s: _compile(s, force), srcs):
             objs.append(obj)
             changed |= ch
     if changed or force or not os.path.exists(LIB) or os.path.getmtime(LIB) < max(os.path.getmtime(o) for o in objs):

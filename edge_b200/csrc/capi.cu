@@ -465,9 +465,13 @@ struct edge_b200_ctx {
     for (int i = 0; i < 3; i++) a.omega[i] = omega[i];
     return a;
   }
+  // element data borrowed from another context (edge_b200_share_element_data): not freed here
+  bool sharedData = false;
   ~edge_b200_ctx() {
     dfree(dofsE); dfree(dofsA); dfree(tDofs); dfree(face);
-    dfree(starE); dfree(starA); dfree(srcA); dfree(fsE); dfree(fsA);
+    if (!sharedData) {
+      dfree(starE); dfree(starA); dfree(srcA); dfree(fsE); dfree(fsA);
+    }
     dfree(elFaEl); dfree(fId); dfree(vId); dfree(faType);
     dfree(dTau); dfree(dSlot); dfree(stage);
     for (int i = 0; i < kSlots; i++) dfree(slotIn[i]);
@@ -586,6 +590,10 @@ int edge_b200_upload_element_data(edge_b200_ctx *ctx, const double *star_e, cons
   if (rm && (!star_a || !src_a || !fs_a || !omega)) return EDGE_B200_EINVAL;
   cudaStream_t s = ctx->stream;
   const size_t n = ctx->nEl;
+  if (ctx->sharedData) {  // stop borrowing: this context gets arrays of its own
+    ctx->starE = ctx->starA = ctx->srcA = ctx->fsE = ctx->fsA = nullptr;
+    ctx->sharedData = false;
+  }
   EDGE_CUDA(upload(ctx->starE, star_e, n * 72 * sizeof(double), s), "upload starE");
   EDGE_CUDA(upload(ctx->fsE, fs_e, n * 2 * 4 * 81 * sizeof(double), s), "upload fsE");
   if (rm) {
@@ -595,6 +603,28 @@ int edge_b200_upload_element_data(edge_b200_ctx *ctx, const double *star_e, cons
     for (int m = 0; m < rm; m++) ctx->omega[m] = omega[m];
   }
   EDGE_CUDA(cudaStreamSynchronize(s), "upload element data");
+  ctx->dataSet = true;
+  ctx->fsLRStale = true;
+  return EDGE_B200_OK;
+}
+
+int edge_b200_share_element_data(edge_b200_ctx *dst, const edge_b200_ctx *src) {
+  if (!dst || !src || dst == src || !src->dataSet) return EDGE_B200_EINVAL;
+  if (dst->nEl != src->nEl || dst->cfg.n_rms != src->cfg.n_rms || dst->cfg.device != src->cfg.device)
+    return EDGE_B200_EINVAL;
+  edge_b200_ctx *ctx = dst;
+  EDGE_CUDA(ctx->flush(), "pending neighbour step");
+  EDGE_CUDA(cudaStreamSynchronize(ctx->stream), "share element data");
+  if (!ctx->sharedData) {
+    dfree(ctx->starE); dfree(ctx->starA); dfree(ctx->srcA); dfree(ctx->fsE); dfree(ctx->fsA);
+  }
+  ctx->starE = src->starE;
+  ctx->starA = src->starA;
+  ctx->srcA = src->srcA;
+  ctx->fsE = src->fsE;
+  ctx->fsA = src->fsA;
+  for (int m = 0; m < 3; m++) ctx->omega[m] = src->omega[m];
+  ctx->sharedData = true;
   ctx->dataSet = true;
   ctx->fsLRStale = true;
   return EDGE_B200_OK;

@@ -108,33 +108,40 @@ class MeshCache:
                             fsA=d["fsA"], omega=d["omega"], name=f"pool_{key}_o{order}_m{rm}")
 
 
-def pool_bytes(n_el, order, runs, precision, rm=0):
+def element_data_bytes(n_el, rm=0):
+    """Device memory of a mesh's FP64 element data (star matrices, flux solvers, anelastic data)."""
+    return n_el * ((72 + 648) + (rm * 12 + 27 + 2 * 4 * 54) * (rm > 0)) * 8
+
+
+def pool_bytes(n_el, order, runs, precision, rm=0, shared=False):
     """Device memory of a pool context (DOF and anelastic rows, two face-projection buffers of the
-    fused steps, staging, element data: star matrices, flux solvers, the flux-solver pairs of the
-    pre-mixed face projections and the anelastic data)."""
+    fused steps, staging, the flux-solver pairs of the pre-mixed face projections and, unless
+    borrowed from the mesh's anchor context (shared), the element data)."""
     p = 8 if precision == 64 else 4
     w = 16 // p
     gb = math.ceil(host.n_modes(order) / w) * w
     gf = math.ceil(host.n_face_modes(order) / w) * w
     nq = 9 + 6 * rm
-    return n_el * (nq * runs * gb * p * 2 + 2 * 36 * runs * gf * p + nq * host.n_modes(order) * runs * p
-                   + (72 + 648) * 8 + 4 * 2 * 84 * p + 28 + (rm * 12 + 27 + 2 * 4 * 54) * 8 * (rm > 0))
+    own = n_el * (nq * runs * gb * p * 2 + 2 * 36 * runs * gf * p + nq * host.n_modes(order) * runs * p
+                  + 4 * 2 * 84 * p + 28)
+    return own + (0 if shared else element_data_bytes(n_el, rm))
 
 
 class Pool:
-    def __init__(self, key, order, meshes, runs=16, precision=32, chunk=20, device=0, rm=0):
+    def __init__(self, key, order, meshes, runs=16, precision=32, chunk=20, device=0, rm=0, anchor=None):
         import torch
         self.key, self.order, self.runs, self.chunk, self.rm = key, order, runs, chunk, rm
         self.prob = meshes.problem(key, order, runs, rm)
         m = self.prob.mesh
         self.stream = torch.cuda.Stream(device=device)
-        # (a new context's DOFs start at zero)
-        self.solver = Solver(self.prob, precision=precision, stream=self.stream.cuda_stream, device=device)
+        # (a new context's DOFs start at zero; its element data come from the mesh's anchor context)
+        self.solver = Solver(self.prob, precision=precision, stream=self.stream.cuda_stream, device=device,
+                             share_from=anchor)
         self.slots = [None] * runs
         self.t = 0.0
         self.dirty = True
         self.entries = []     # union receiver list: (request, receiver index)
-        self.bytes = pool_bytes(m.n_el, order, runs, precision, rm)
+        self.bytes = pool_bytes(m.n_el, order, runs, precision, rm, shared=anchor is not None)
         self.launched = 0
 
     def busy(self):
@@ -300,6 +307,10 @@ class Server:
         self.pools = {}
         self.pools_opened = 0
         self.max_pools = 0
+        # per (mesh, mechanisms): a small context holding the mesh's element data once on the device,
+        # which every pool of the mesh borrows (pools open without uploading them)
+        self.anchors = {}
+        self.share_element_data = True
 
     def _size_for(self, n):
         for x in self.sizes:
@@ -307,19 +318,46 @@ class Server:
                 return x
         return self.sizes[-1]
 
+    def _anchor(self, mesh, rm):
+        if not self.share_element_data or self.pool_cls is not Pool:
+            return None
+        if (mesh, rm) not in self.anchors:
+            p = self.meshes.problem(mesh, 3, 1, rm)
+            s = Solver(p, precision=32, device=self.device)
+            s.bytes = element_data_bytes(p.n_el, rm) + pool_bytes(p.n_el, 3, 1, 32, rm, shared=True)
+            self.anchors[(mesh, rm)] = s
+        return self.anchors[(mesh, rm)]
+
+    def _used(self):
+        return (self.base_used + sum(q.bytes for q in self.pools.values())
+                + sum(a.bytes for a in self.anchors.values()))
+
     def _fits(self, req, runs):
         m = self.meshes.data(req.mesh, req.rm)["mesh"]
-        need = pool_bytes(m.n_el, req.order, runs, self.precision, req.rm)
-        used = self.base_used + sum(q.bytes for q in self.pools.values())
+        shared = self.share_element_data and self.pool_cls is Pool
+        need = pool_bytes(m.n_el, req.order, runs, self.precision, req.rm, shared=shared)
+        if shared and (req.mesh, req.rm) not in self.anchors:
+            need += element_data_bytes(m.n_el, req.rm) + pool_bytes(m.n_el, 3, 1, 32, req.rm, shared=True)
+        used = self._used()
         if used + need > self.budget:
             # close idle pools to make room
             for k in [k for k, q in self.pools.items() if not q.busy()]:
                 self.pools.pop(k).close()
-            used = self.base_used + sum(q.bytes for q in self.pools.values())
+            # and the anchors of meshes without an open pool (other than the one asked for)
+            live = {(k[0], k[2]) for k in self.pools}
+            for k in [k for k in self.anchors if k not in live and k != (req.mesh, req.rm)]:
+                self.anchors.pop(k).close()
+            used = self._used()
         return used + need <= self.budget
 
     def _open(self, req, runs):
-        p = self.pool_cls(req.mesh, req.order, self.meshes, runs, self.precision, self.chunk, self.device, req.rm)
+        anchor = self._anchor(req.mesh, req.rm)
+        if anchor is not None:
+            p = self.pool_cls(req.mesh, req.order, self.meshes, runs, self.precision, self.chunk, self.device,
+                              req.rm, anchor=anchor)
+        else:
+            p = self.pool_cls(req.mesh, req.order, self.meshes, runs, self.precision, self.chunk, self.device,
+                              req.rm)
         self.pools_opened += 1
         return p
 
@@ -481,6 +519,9 @@ class Server:
         for p in self.pools.values():
             p.close()
         self.pools = {}
+        for a in self.anchors.values():
+            a.close()
+        self.anchors = {}
 
 
 def latency_stats(reqs):

@@ -13,7 +13,7 @@ from ._lib import Cfg, check, lib, ptr
 
 
 class Solver:
-    def __init__(self, prob, precision=64, stream=None, device=0):
+    def __init__(self, prob, precision=64, stream=None, device=0, share_from=None):
         self.prob = prob
         self.precision = precision
         self.dtype = np.float64 if precision == 64 else np.float32
@@ -31,9 +31,14 @@ class Solver:
                                           ptr(np.ascontiguousarray(m.fid)),
                                           ptr(np.ascontiguousarray(m.vid)),
                                           ptr(np.ascontiguousarray(m.el_fa_type))), "upload_mesh")
-        c = lambda a: None if a is None else np.ascontiguousarray(a, np.float64)
-        self._keep = [c(prob.starE), c(prob.fsE), c(prob.starA), c(prob.srcA), c(prob.fsA), c(prob.omega)]
-        self._chk(L.edge_b200_upload_element_data(h, *[ptr(a) for a in self._keep]), "upload_element_data")
+        if share_from is not None:
+            # element data borrowed from another context of the same mesh (kept alive with this one)
+            self._share = share_from
+            self._chk(L.edge_b200_share_element_data(h, share_from._h), "share_element_data")
+        else:
+            c = lambda a: None if a is None else np.ascontiguousarray(a, np.float64)
+            self._keep = [c(prob.starE), c(prob.fsE), c(prob.starA), c(prob.srcA), c(prob.fsA), c(prob.omega)]
+            self._chk(L.edge_b200_upload_element_data(h, *[ptr(a) for a in self._keep]), "upload_element_data")
         s = prob.sources
         if s and s.get("n", 0):
             self._chk(L.edge_b200_set_sources(h, s["n"], ptr(s["el"]), ptr(s["run"]), ptr(s["scal"]),

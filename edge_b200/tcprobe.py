@@ -17,8 +17,8 @@ def lib():
             raise RuntimeError("libedge_b200_probe.so is not built (python -m edge_b200.build)")
         _lib = C.CDLL(path)
         vp = C.c_void_p
-        _lib.edge_b200_probe_tc.argtypes = [vp, vp, vp, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, vp,
-                                            C.POINTER(C.c_float)]
+        _lib.edge_b200_probe_tc.argtypes = [vp, vp, vp, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int,
+                                            vp, C.POINTER(C.c_float)]
     return _lib
 
 
@@ -37,7 +37,7 @@ def check(n, k, iters=1, seed=0):
     D = torch.full((128, n), float("nan"), device="cuda")
     st = torch.zeros(1, dtype=torch.int32, device="cuda")
     ms = C.c_float()
-    rc = lib().edge_b200_probe_tc(A.data_ptr(), B.data_ptr(), D.data_ptr(), 128, n, k, iters, 1, st.data_ptr(),
+    rc = lib().edge_b200_probe_tc(A.data_ptr(), B.data_ptr(), D.data_ptr(), 128, n, k, iters, 1, 1, st.data_ptr(),
                                   C.byref(ms))
     if rc != 0 or int(st.item()) != 0:
         raise RuntimeError(f"probe failed: rc {rc}, status {int(st.item())}")
@@ -45,17 +45,17 @@ def check(n, k, iters=1, seed=0):
     return float(((D.double() - ref).abs().max() / ref.abs().max()).item())
 
 
-def time_shape(n, k=32, iters=4096, blocks=148):
-    """Milliseconds for `blocks` CTAs each issuing iters x k / 8 MMAs of 128 x n x 8 (tf32), and
-    the derived cycles per instruction at the given SM clock (MHz) are left to the caller."""
+def time_shape(n, k=32, iters=4096, blocks=148, acc=1):
+    """(milliseconds, instructions per CTA) for `blocks` CTAs each issuing iters x k / 8 MMAs of
+    128 x n x 8 (tf32) round robin into `acc` independent accumulators."""
     import torch
     A = torch.randn(128, k, device="cuda")
     B = torch.randn(n, k, device="cuda")
     st = torch.zeros(blocks, dtype=torch.int32, device="cuda")
     ms = C.c_float()
     for _ in range(2):  # the first launch sets the shared-memory attribute and warms the clocks
-        rc = lib().edge_b200_probe_tc(A.data_ptr(), B.data_ptr(), None, 128, n, k, iters, blocks, st.data_ptr(),
-                                      C.byref(ms))
+        rc = lib().edge_b200_probe_tc(A.data_ptr(), B.data_ptr(), None, 128, n, k, iters, acc, blocks,
+                                      st.data_ptr(), C.byref(ms))
         if rc != 0 or int(st.sum().item()) != 0:
             raise RuntimeError(f"probe failed: rc {rc}")
     return ms.value, iters * (k // 8)

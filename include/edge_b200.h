@@ -163,6 +163,12 @@ int edge_b200_upload_mesh(edge_b200_ctx *ctx, const int32_t *el_fa_el, const uin
 int edge_b200_upload_element_data(edge_b200_ctx *ctx, const double *star_e, const double *fs_e,
                                   const double *star_a, const double *src_a, const double *fs_a,
                                   const double *omega);
+/* Element data (star matrices, flux solvers, anelastic data, relaxation frequencies) borrowed from
+ * another context of the same mesh size, mechanisms and device instead of uploaded: the two share
+ * one device copy, src must outlive dst, and a later edge_b200_upload_element_data on dst gives dst
+ * arrays of its own again. Used by pools of one mesh at different orders or run counts (element
+ * data do not depend on either). No counterpart in the reference (one solver per mesh). */
+int edge_b200_share_element_data(edge_b200_ctx *dst, const edge_b200_ctx *src);
 /* DOFs in the context precision (double for 64, float for 32); dofs_a may be NULL without
  * mechanisms. */
 int edge_b200_upload_dofs(edge_b200_ctx *ctx, const void *dofs_e, const void *dofs_a);
