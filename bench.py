@@ -638,6 +638,38 @@ def run_batch(n_sims, device, seed=3343, mem_fraction=0.6, step_range=(20, 100))
         s64.sync()
         ms64[key] = (time.perf_counter() - t1) / 10 * 1e3
         s64.close()
+    # one configuration family of many small simulations (the case merging is for): 32 simulations
+    # of order 4, 8 runs, elastic on the 6,000-tet box with their own sources and 20-100 steps, alone
+    # after another against one merged context
+    fam_sims = [(0, 4, 8, 0, int(n)) for n in np.random.default_rng(seed + 5).integers(step_range[0],
+                                                                                          step_range[1] + 1, 32)]
+    fprobs = [problem(1000 + k, *x) for k, x in enumerate(fam_sims)]
+    fsteps = [x[4] for x in fam_sims]
+    fupd = sum(p.n_el * 8 * n for p, n in zip(fprobs, fsteps))
+    solvers = []
+    for p in fprobs:
+        sv = Solver(p, precision=32, device=device)
+        e0, _ = p.zero_dofs(np.float32)
+        sv.upload_dofs(e0)
+        solvers.append(sv)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for sv, n in zip(solvers, fsteps):
+        sv.step(n)
+    torch.cuda.synchronize()
+    f_seq = time.perf_counter() - t0
+    for sv in solvers:
+        sv.close()
+    fam = MergedFamily(fprobs, fsteps, precision=32, device=device)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    fam.launch()
+    torch.cuda.synchronize()
+    f_merged = time.perf_counter() - t0
+    fam.close()
+    small_family = {"simulations": len(fam_sims), "tets": fprobs[0].n_el, "order": 4, "runs": 8,
+                    "element_updates": fupd, "one_after_another_fp32_s": f_seq, "merged_s": f_merged,
+                    "speedup_vs_one_after_another_fp32": f_seq / f_merged}
     have64 = [x for x in sims if (x[0], x[1], x[3]) in ms64]
     t64 = sum(ms64[(mi, o, rm)] * r * n for mi, o, r, rm, n in have64) / 1e3
     frac64 = sum(meshes[x[0]].n_el * x[2] * x[4] for x in have64) / max(upd, 1)
@@ -651,6 +683,7 @@ def run_batch(n_sims, device, seed=3343, mem_fraction=0.6, step_range=(20, 100))
             "kernel_launches": {"one_after_another": seq_launches, "merged": merged_launches},
             "plain_fp64_alone_s_covered": t64, "fp64_covered_fraction_of_updates": frac64,
             "speedup_vs_plain_fp64_alone": t64 / (t_merged * frac64) if frac64 > 0 else None,
+            "small_family": small_family,
             "note": "wall clock (host timer after a device sync); the FP64 comparison covers the simulations "
                     "with an FP64 configuration and scales the merged time by their share of the updates"}
 

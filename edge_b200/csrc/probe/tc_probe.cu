@@ -76,14 +76,18 @@ __device__ __forceinline__ bool waitParity(uint32_t bar, uint32_t parity) {
   return false;
 }
 
-// One CTA per block: A [m][k] and B [n][k] (row-major in global memory, k <= kMaxK) staged into
-// the canonical layout, `iters` passes of k / 8 instructions accumulating round robin into `acc`
-// independent accumulators [m][n] in tensor memory (acc = 1: every instruction waits for the
-// previous one's sum; more: their latencies overlap, as the row tiles of an element group would);
-// accumulator 0 is written back to D (block 0 only) so the host can check it against the FP32
-// product. status[blockIdx.x]: 0 ok, 1 the completion wait gave up.
+// One CTA per block: A [m][k] and B [n][k] (row-major in global memory, k = 8 KB <= kMaxK) staged
+// into the canonical layout; `iters` passes, each issuing for every K block one instruction into
+// each of ACC independent accumulators [m][n] in tensor memory (ACC = 1: every instruction waits
+// for the previous one's sum; more: their latencies overlap, as the row tiles of an element group
+// would). Descriptors are computed once and the issue loop is unrolled, so the single issuing
+// thread adds little beyond the instructions themselves. Accumulator 0 is written back to D (block
+// 0 only) so the host can check it against the FP32 product. status[blockIdx.x]: 0 ok, 1 the
+// completion wait gave up.
+template <int ACC, int KB>
 __global__ void __launch_bounds__(kThreads, 1)
-    kTcProbe(const float *A, const float *B, float *D, int m, int n, int k, int iters, int acc, int *status) {
+    kTcProbe(const float *A, const float *B, float *D, int m, int n, int iters, int *status) {
+  constexpr int k = 8 * KB;
   extern __shared__ __align__(128) float dyn[];
   float *sA = dyn, *sB = dyn + kMaxRows * kMaxK;
   __shared__ __align__(8) uint64_t bar;
@@ -100,7 +104,7 @@ __global__ void __launch_bounds__(kThreads, 1)
   const uint32_t barAddr = smemAddr(&bar);
   const uint32_t stride = ((uint32_t)n + 31) / 32 * 32;  // accumulators on 32-column boundaries
   uint32_t cols = 32;
-  while (cols < stride * (uint32_t)acc) cols <<= 1;
+  while (cols < stride * (uint32_t)ACC) cols <<= 1;
   if (tid == 0) {
     asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" ::"r"(barAddr) : "memory");
     asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
@@ -121,13 +125,21 @@ __global__ void __launch_bounds__(kThreads, 1)
     const uint32_t idesc = instrDesc(m, n);
     const uint32_t aBase = smemAddr(sA), bBase = smemAddr(sB);
     const uint32_t aLbo = (uint32_t)(m / 8) * 128, bLbo = (uint32_t)(n / 8) * 128;
-    int idx = 0;
-    for (int it = 0; it < iters; it++)
-      for (int kb = 0; kb < k / 8; kb++, idx++) {
-        const uint64_t ad = smemDesc(aBase + 2 * kb * aLbo, aLbo, 128);
-        const uint64_t bd = smemDesc(bBase + 2 * kb * bLbo, bLbo, 128);
-        mmaTf32(tmem + (uint32_t)(idx % acc) * stride, ad, bd, idesc, idx >= acc ? 1u : 0u);
-      }
+    uint64_t ad[KB], bd[KB];
+    uint32_t dc[ACC];
+#pragma unroll
+    for (int kb = 0; kb < KB; kb++) {
+      ad[kb] = smemDesc(aBase + 2 * kb * aLbo, aLbo, 128);
+      bd[kb] = smemDesc(bBase + 2 * kb * bLbo, bLbo, 128);
+    }
+#pragma unroll
+    for (int a = 0; a < ACC; a++) dc[a] = tmem + (uint32_t)a * stride;
+    for (int it = 0; it < iters; it++) {
+#pragma unroll
+      for (int kb = 0; kb < KB; kb++)
+#pragma unroll
+        for (int a = 0; a < ACC; a++) mmaTf32(dc[a], ad[kb], bd[kb], idesc, (it > 0 || kb > 0) ? 1u : 0u);
+    }
     asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];\n" ::"r"(barAddr)
                  : "memory");
   }
@@ -160,23 +172,24 @@ __global__ void __launch_bounds__(kThreads, 1)
 
 extern "C" {
 
-// Runs the probe: `blocks` CTAs, each `iters` x (k / 8) tf32 MMAs of shape m x n x 8 on its own
-// operand copies (A [m][k], B [n][k] device arrays; D [m][n] device array or NULL, accumulator 0)
-// into acc (1..4) independent accumulators. m = 128, n a multiple of 16 in [16, 128], k a multiple
-// of 8 in [8, 32]. Returns 0, -1 for invalid shapes,
-// -3 for a CUDA error; *ms receives the kernel time (CUDA events), status[blocks] the per-CTA
-// completion flags (device array).
+// Runs the probe: `blocks` CTAs, each `iters` x (k / 8) x acc tf32 MMAs of shape m x n x 8 on its
+// own operand copies (A [m][k], B [n][k] device arrays; D [m][n] device array or NULL: accumulator
+// 0) into acc (1 or 3) independent accumulators. m = 128, n a multiple of 16 in [16, 128], k 8 or
+// 32. Returns 0, -1 for invalid shapes, -3 for a CUDA error; *ms receives the kernel time (CUDA
+// events), status[blocks] the per-CTA completion flags (device array).
 int edge_b200_probe_tc(const float *A, const float *B, float *D, int m, int n, int k, int iters, int acc,
                        int blocks, int *status, float *ms) {
-  if (m != 128 || n < 16 || n > kMaxRows || n % 16 || k < 8 || k > kMaxK || k % 8 || iters < 1 || blocks < 1 ||
-      acc < 1 || acc > 4 || !A || !B || !status || !ms)
+  if (m != 128 || n < 16 || n > kMaxRows || n % 16 || (k != 8 && k != 32) || iters < 1 || blocks < 1 ||
+      (acc != 1 && acc != 3) || !A || !B || !status || !ms)
     return -1;
-  if (cudaFuncSetAttribute(kTcProbe, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemBytes) != cudaSuccess)
+  void (*kern)(const float *, const float *, float *, int, int, int, int *) =
+      acc == 1 ? (k == 8 ? kTcProbe<1, 1> : kTcProbe<1, 4>) : (k == 8 ? kTcProbe<3, 1> : kTcProbe<3, 4>);
+  if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemBytes) != cudaSuccess)
     return -3;
   cudaEvent_t e0, e1;
   if (cudaEventCreate(&e0) != cudaSuccess || cudaEventCreate(&e1) != cudaSuccess) return -3;
   cudaEventRecord(e0);
-  kTcProbe<<<blocks, kThreads, kSmemBytes>>>(A, B, D, m, n, k, iters, acc, status);
+  kern<<<blocks, kThreads, kSmemBytes>>>(A, B, D, m, n, iters, status);
   cudaEventRecord(e1);
   cudaError_t err = cudaEventSynchronize(e1);
   if (err == cudaSuccess) err = cudaGetLastError();

@@ -58,4 +58,4 @@ def time_shape(n, k=32, iters=4096, blocks=148, acc=1):
                                       st.data_ptr(), C.byref(ms))
         if rc != 0 or int(st.sum().item()) != 0:
             raise RuntimeError(f"probe failed: rc {rc}")
-    return ms.value, iters * (k // 8)
+    return ms.value, iters * (k // 8) * acc
