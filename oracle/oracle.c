@@ -30,6 +30,7 @@
  *                      (AderDg.hpp:384-417 and 620-674, TimeGroupStatic.cpp:46-111)
  */
 #include <math.h>
+#include <stdint.h>
 #include <stdlib.h>
 #include <string.h>
 
@@ -43,6 +44,30 @@ static const int SR_R[12] = {0,0,0,1,1,1,2,2,2,3,4,5};
 static const int SR_C[12] = {0,1,2,0,1,2,0,1,2,3,4,5};
 
 static int nmodes(int o) { return o <= 0 ? 0 : o * (o + 1) * (o + 2) / 6; }
+
+/* Operand rounding of the products with the global DG matrices (mm_ac), for measuring what tensor
+ * cores would do to the results: 0 none (FP64), 1 both operands rounded to tf32 (10-bit mantissa,
+ * round to nearest with ties away from zero, as cvt.rna.tf32.f32 does after the FP32 value), 2 the
+ * three-product split a_hi b_hi + a_hi b_lo + a_lo b_hi of tf32 parts. The star and flux-solver
+ * mixes (mm_bc) stay exact. Test infrastructure only. */
+static int g_mmMode = 0;
+void oracle_set_mm_mode(int mode) { g_mmMode = mode; }
+
+static double tf32(double x) {
+  float f = (float)x;
+  uint32_t u;
+  memcpy(&u, &f, 4);
+  if ((u & 0x7f800000u) != 0x7f800000u) u = (u + 0x1000u) & 0xffffe000u;
+  memcpy(&f, &u, 4);
+  return (double)f;
+}
+
+static double mmProd(double a, double b) {
+  if (g_mmMode == 1) return tf32(a) * tf32(b);
+  const double ah = tf32(a), bh = tf32(b);
+  const double al = tf32((double)((float)a - (float)ah)), bl = tf32((double)((float)b - (float)bh));
+  return ah * bh + (ah * bl + al * bh);
+}
 
 /* C[m][n][r] (+)= sum_k A[m][k][r] * B[k][n]   (MmVanilla fused-AC, Matrix.h:296-330) */
 static void mm_ac(int R, int M, int N, int K, int ldA, int ldB, int ldC, double beta,
@@ -58,6 +83,11 @@ static void mm_ac(int R, int M, int N, int K, int ldA, int ldB, int ldC, double 
       for (int n = 0; n < N; n++) {
         double b = Bm[(size_t)k * ldB + n];
         if (b == 0.0) continue; /* exact: adding a zero product changes nothing */
+        if (g_mmMode) {
+          for (int r = 0; r < R; r++)
+            C[((size_t)m * ldC + n) * R + r] += mmProd(A[((size_t)m * ldA + k) * R + r], b);
+          continue;
+        }
         for (int r = 0; r < R; r++)
           C[((size_t)m * ldC + n) * R + r] += A[((size_t)m * ldA + k) * R + r] * b;
       }

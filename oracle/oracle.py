@@ -243,3 +243,9 @@ def neigh_premixed_faces(prob, dofsE, faces, rows, O):
     for (e, f), P in zip(faces, rows):
         s1 = np.einsum("qfr,fg->qgr", P, O[int(prob["vIdElFaEl"][e, f])])
         dofsE[e] += np.einsum("qfr,fb->qbr", s1, ft[f])
+
+
+def set_mm_mode(mode):
+    """Operand rounding of the oracle's products with the DG matrices: 0 none, 1 tf32 operands,
+    2 the three-product tf32 split (oracle.c g_mmMode; for measuring tensor-core arithmetic)."""
+    lib().oracle_set_mm_mode(C.c_int(mode))
