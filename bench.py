@@ -453,44 +453,64 @@ def run_serve(n_req, rate, device, seed=3343, n_check=12):
 
 def run_tc_probe(local_ms, n_el, order, runs, device, clock_mhz):
     """The tensor-core alternative for the local kernel's DG products, measured: tcgen05.mma
-    kind::tf32 (operands in shared memory, accumulator in tensor memory, one CTA per SM) timed per
-    instruction of 128 x N x 8 for the N the products would have, then the instructions one local
-    step needs in the tensor formulation -- rows (quantity, element, run) on M in tiles of 128 (the
-    288 rows of an element group in three tiles), output modes on N (padded to 16), input modes x 3
-    derivative directions (or x 4 faces) on K, each product three times for FP32 accuracy from tf32
-    (split operands) -- at the measured cycles. Only the products: the star and flux-solver mixes,
-    loads, stores and tensor-memory read-back come on top."""
+    (kind::tf32, and kind::f16 with bf16 operands; operands in shared memory, accumulator in tensor
+    memory) timed per instruction of 128 x N x K (K = 8 tf32, 16 bf16) for the N the products would
+    have, with one and two issuing CTAs per SM, then the instructions one local step needs in the
+    tensor formulation -- rows (quantity, element, run) on M in tiles of 128 (the 288 rows of an
+    element group in three tiles), output modes on N (padded to 16), input modes x 3 derivative
+    directions (or x 4 faces) on K, each product three times for FP32-level accuracy (split
+    operands: 3xtf32 or 3xbf16) -- at the measured cycles. Only the products: the star and
+    flux-solver mixes, the operand splits, loads, stores and tensor-memory read-back come on top."""
     from edge_b200 import tcprobe
     from edge_b200.host import n_face_modes, n_modes
-    errs = {f"{n}x{k}x{it}": tcprobe.check(n, k, it) for n, k, it in ((16, 8, 1), (64, 32, 1), (128, 32, 3))}
-    # cycles per instruction with one accumulator (each waits for the previous sum) and with three
-    # (the three row tiles of an element group, whose instructions overlap); the estimate uses three
-    cyc1, cyc = {}, {}
-    for n in (16, 32, 48, 64, 96, 128):
-        ms, per_cta = tcprobe.time_shape(n, acc=1)
-        cyc1[n] = ms * 1e-3 * clock_mhz * 1e6 / per_cta
-        ms, per_cta = tcprobe.time_shape(n, acc=3)
-        cyc[n] = ms * 1e-3 * clock_mhz * 1e6 / per_cta
+    errs = {f"{kind}_{n}x{k}x{it}": tcprobe.check(n, k, it, kind=kind)
+            for kind, n, k, it in (("tf32", 16, 8, 1), ("tf32", 64, 32, 1), ("tf32", 128, 32, 3),
+                                   ("bf16", 16, 16, 1), ("bf16", 128, 64, 3))}
+    ns = (16, 32, 48, 64, 96, 128)
+
+    def cycles(kind, acc, per_sm):
+        # cycles per instruction of one SM; two CTAs per SM only where their tensor memory fits
+        out = {}
+        for n in ns:
+            if per_sm == 2 and acc == 3 and n > 64:
+                continue
+            ms, per_sm_instr = tcprobe.time_shape(n, acc=acc, kind=kind, per_sm=per_sm)
+            out[n] = ms * 1e-3 * clock_mhz * 1e6 / per_sm_instr
+        return out
+
+    meas = {"tf32_acc1": cycles("tf32", 1, 1), "tf32_acc3": cycles("tf32", 3, 1),
+            "tf32_acc3_2cta": cycles("tf32", 3, 2), "bf16_acc3": cycles("bf16", 3, 1),
+            "bf16_acc3_2cta": cycles("bf16", 3, 2)}
     pad = lambda x, q: (x + q - 1) // q * q
     Bm = lambda o: n_modes(o) if o > 0 else 0
     F = n_face_modes(order)
-    prods = [("ck%d" % d, pad(Bm(order - d), 16), pad(3 * Bm(order - d + 1), 8)) for d in range(1, order)]
-    prods += [("volume", pad(Bm(order), 16), pad(3 * Bm(order - 1), 8)), ("fluxL", pad(4 * F, 16), pad(Bm(order), 8)),
-              ("fluxT", pad(Bm(order), 16), pad(4 * F, 8))]
+    prods = [("ck%d" % d, pad(Bm(order - d), 16), 3 * Bm(order - d + 1)) for d in range(1, order)]
+    prods += [("volume", pad(Bm(order), 16), 3 * Bm(order - 1)), ("fluxL", pad(4 * F, 16), Bm(order)),
+              ("fluxT", pad(Bm(order), 16), 4 * F)]
     groups_per_sm = n_el * runs / 32 / 148
     tiles, split = 3, 3
-    est = {}
-    for name, nn, kk in prods:
-        c = cyc[min(x for x in cyc if x >= nn)] if nn <= 128 else cyc[128] * nn / 128
-        est[name] = groups_per_sm * tiles * split * (kk // 8) * c / (clock_mhz * 1e3)
-    total = sum(est.values())
-    return {"check_rel_err": errs, "cycles_per_instruction_128xNx8": cyc,
-            "cycles_per_instruction_128xNx8_one_accumulator": cyc1, "clock_mhz": clock_mhz,
+
+    def estimate(kind, cyc, cyc_wide):
+        kq = tcprobe.K_INSTR[kind]
+        est = {}
+        for name, nn, kk in prods:
+            table = cyc if nn in cyc else cyc_wide  # N beyond the two-CTA range: one CTA per SM
+            c = table[min(x for x in table if x >= nn)]
+            est[name] = groups_per_sm * tiles * split * (pad(kk, kq) // kq) * c / (clock_mhz * 1e3)
+        return est
+
+    options = {"3xtf32": estimate("tf32", meas["tf32_acc3"], meas["tf32_acc3"]),
+               "3xtf32_2cta": estimate("tf32", meas["tf32_acc3_2cta"], meas["tf32_acc3"]),
+               "3xbf16": estimate("bf16", meas["bf16_acc3"], meas["bf16_acc3"]),
+               "3xbf16_2cta": estimate("bf16", meas["bf16_acc3_2cta"], meas["bf16_acc3"])}
+    totals = {k: sum(v.values()) for k, v in options.items()}
+    best = min(totals, key=totals.get)
+    return {"check_rel_err": errs, "cycles_per_instruction_per_sm_128xNxK": meas, "clock_mhz": clock_mhz,
             "products": [{"name": a, "N": b, "K": c} for a, b, c in prods],
-            "tensor_ms_per_step_by_product": est, "tensor_ms_per_step": total,
-            "fused_local_kernel_ms": local_ms, "ratio_tensor_products_to_whole_fp32_kernel": total / local_ms,
-            "note": "3xTF32 products only, at the measured per-instruction rate; the FP32 kernel's time includes "
-                    "everything"}
+            "tensor_ms_per_step_by_product": options, "tensor_ms_per_step": totals, "best": best,
+            "fused_local_kernel_ms": local_ms, "ratio_best_tensor_products_to_whole_fp32_kernel": totals[best] / local_ms,
+            "note": "split-operand products only, at the measured per-instruction rate; the FP32 kernel's time "
+                    "includes everything"}
 
 
 # FP32 configurations the uneven batch draws from: orders 3-6, fused runs 1 / 4 / 8 / 16, elastic

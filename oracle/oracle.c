@@ -48,8 +48,9 @@ static int nmodes(int o) { return o <= 0 ? 0 : o * (o + 1) * (o + 2) / 6; }
 /* Operand rounding of the products with the global DG matrices (mm_ac), for measuring what tensor
  * cores would do to the results: 0 none (FP64), 1 both operands rounded to tf32 (10-bit mantissa,
  * round to nearest with ties away from zero, as cvt.rna.tf32.f32 does after the FP32 value), 2 the
- * three-product split a_hi b_hi + a_hi b_lo + a_lo b_hi of tf32 parts. The star and flux-solver
- * mixes (mm_bc) stay exact. Test infrastructure only. */
+ * three-product split a_hi b_hi + a_hi b_lo + a_lo b_hi of tf32 parts, 3 both operands rounded to
+ * bf16 (8-bit mantissa, round to nearest even, as cvt.rn.bf16.f32), 4 the three-product split of
+ * bf16 parts. The star and flux-solver mixes (mm_bc) stay exact. Test infrastructure only. */
 static int g_mmMode = 0;
 void oracle_set_mm_mode(int mode) { g_mmMode = mode; }
 
@@ -62,10 +63,20 @@ static double tf32(double x) {
   return (double)f;
 }
 
+static double bf16(double x) {
+  float f = (float)x;
+  uint32_t u;
+  memcpy(&u, &f, 4);
+  if ((u & 0x7f800000u) != 0x7f800000u) u = (u + 0x7fffu + ((u >> 16) & 1u)) & 0xffff0000u;
+  memcpy(&f, &u, 4);
+  return (double)f;
+}
+
 static double mmProd(double a, double b) {
-  if (g_mmMode == 1) return tf32(a) * tf32(b);
-  const double ah = tf32(a), bh = tf32(b);
-  const double al = tf32((double)((float)a - (float)ah)), bl = tf32((double)((float)b - (float)bh));
+  double (*rnd)(double) = g_mmMode >= 3 ? bf16 : tf32;
+  if (g_mmMode == 1 || g_mmMode == 3) return rnd(a) * rnd(b);
+  const double ah = rnd(a), bh = rnd(b);
+  const double al = rnd((double)((float)a - (float)ah)), bl = rnd((double)((float)b - (float)bh));
   return ah * bh + (ah * bl + al * bh);
 }
 

@@ -247,5 +247,6 @@ def neigh_premixed_faces(prob, dofsE, faces, rows, O):
 
 def set_mm_mode(mode):
     """Operand rounding of the oracle's products with the DG matrices: 0 none, 1 tf32 operands,
-    2 the three-product tf32 split (oracle.c g_mmMode; for measuring tensor-core arithmetic)."""
+    2 the three-product tf32 split, 3 bf16 operands, 4 the three-product bf16 split (oracle.c
+    g_mmMode; for measuring tensor-core arithmetic)."""
     lib().oracle_set_mm_mode(C.c_int(mode))

@@ -24,11 +24,15 @@ def test_tf32_products_error_against_fp64():
     prob = small_problem(n=3, order=5, runs=1, jitter=0.1, n_steps=200, source="explosive", n_receivers=8)
     ref_b, ref_d = _run(0, prob)
     assert np.abs(ref_b).max() > 0
-    one_b, one_d = _run(1, prob)
-    three_b, three_d = _run(2, prob)
-    e1, e3 = rel_l2(one_b, ref_b), rel_l2(three_b, ref_b)
-    d1, d3 = rel_l2(one_d, ref_d), rel_l2(three_d, ref_d)
-    print(f"tf32 products: receivers {e1:.3e}, DOFs {d1:.3e}; 3xtf32: receivers {e3:.3e}, DOFs {d3:.3e}")
-    # the split recovers FP32-level products; plain tf32 is three orders of magnitude coarser
-    assert e3 < 1e-5 and d3 < 1e-5
-    assert e1 > 100 * e3
+    err = {}
+    for mode, name in ((1, "tf32"), (2, "3xtf32"), (3, "bf16"), (4, "3xbf16")):
+        b, d = _run(mode, prob)
+        err[name] = (rel_l2(b, ref_b), rel_l2(d, ref_d))
+    print("; ".join(f"{k}: receivers {e:.3e}, DOFs {d:.3e}" for k, (e, d) in err.items()))
+    # the tf32 split recovers FP32-level products; plain tf32 is three orders of magnitude coarser
+    assert err["3xtf32"][0] < 1e-5 and err["3xtf32"][1] < 1e-5
+    assert err["tf32"][0] > 100 * err["3xtf32"][0]
+    # plain bf16 is coarser than tf32 (8 against 11 significant bits); the bf16 split keeps about
+    # 16 bits, between the two
+    assert err["bf16"][0] > err["tf32"][0]
+    assert err["3xtf32"][0] < err["3xbf16"][0] < err["tf32"][0]
