@@ -34,7 +34,8 @@ def nvcc():
 
 def _includes(path, seen=None):
     """The quoted #include files a source pulls in, transitively (searched beside the including
-    file, in csrc and in include/)."""
+    file, in csrc and in include/), and the configuration list an inst_oN.cu names for its
+    computed include (#define EDGE_B200_INC "...")."""
     seen = set() if seen is None else seen
     try:
         text = open(path).read()
@@ -42,7 +43,7 @@ def _includes(path, seen=None):
         return seen
     for line in text.splitlines():
         line = line.strip()
-        if not line.startswith("#include \""):
+        if not (line.startswith("#include \"") or line.startswith("#define EDGE_B200_INC \"")):
             continue
         name = line.split('"')[1]
         for d in (os.path.dirname(path), CSRC, os.path.join(ROOT, "include")):
@@ -59,17 +60,33 @@ def _deps_mtime(src):
     return max([os.path.getmtime(h) for h in _includes(src)] + [0.0])
 
 
+INST_PARTS = 4  # objects per order's kernel-set instantiations (kInstParts in inst_order.cuh)
+
+
 def sources():
     return sorted(glob.glob(os.path.join(CSRC, "*.cu")) + glob.glob(os.path.join(CSRC, "*.cpp")))
 
 
-def _compile(src, force):
+def units():
+    """(source, part) per object: the order files inst_oN.cu once per part, the rest once."""
+    out = []
+    for s in sources():
+        if os.path.basename(s).startswith("inst_o"):
+            out += [(s, p) for p in range(INST_PARTS)]
+        else:
+            out.append((s, None))
+    # the slowest objects first, so that they start before the short ones
+    return sorted(out, key=lambda u: (u[1] is None, -int(os.path.basename(u[0])[6]) if u[1] is not None else 0))
+
+
+def _compile(unit, force):
+    src, part = unit
     hdr_mtime = _deps_mtime(src)
-    obj = os.path.join(BUILD, os.path.basename(src) + ".o")
+    obj = os.path.join(BUILD, os.path.basename(src) + (f".p{part}" if part is not None else "") + ".o")
     if (not force and os.path.exists(obj) and os.path.getmtime(obj) >= os.path.getmtime(src)
             and os.path.getmtime(obj) >= hdr_mtime):
         return obj, False
-    cmd = [nvcc()] + NVCC_FLAGS + ["-c", src, "-o", obj]
+    cmd = [nvcc()] + NVCC_FLAGS + (["-DEDGE_B200_PART=%d" % part] if part is not None else []) + ["-c", src, "-o", obj]
     if src.endswith(".cpp"):
         cmd = [nvcc(), "-x", "cu"] + NVCC_FLAGS + ["-c", src, "-o", obj]
     r = subprocess.run(cmd, capture_output=True, text=True)
@@ -80,12 +97,12 @@ def _compile(src, force):
 
 def build(force=False, jobs=None, verbose=False):
     os.makedirs(BUILD, exist_ok=True)
-    srcs = sources()
-    jobs = jobs or min(len(srcs), os.cpu_count() or 4)
+    us = units()
+    jobs = jobs or min(len(us), os.cpu_count() or 4)
     changed = False
     objs = []
     with cf.ThreadPoolExecutor(jobs) as ex:
-        for obj, ch in ex.map(lambda s: _compile(s, force), srcs):
+        for obj, ch in ex.map(lambda u: _compile(u, force), us):
             objs.append(obj)
             changed |= ch
     if changed or force or not os.path.exists(LIB) or os.path.getmtime(LIB) < max(os.path.getmtime(o) for o in objs):

@@ -95,6 +95,93 @@ __global__ void kBuildFsLR(const double *fsE, const int32_t *elFaEl, const uint8
   }
 }
 
+// characteristic factors of the same pairs (Geo::charMix): per element face the stacked flux
+// solvers S = [fsE[0]; the reader's fsE[1]] (18 x 9, zeros for an outflow reader) have rank 3 --
+// the waves leaving the element through the face -- so S = U V^T with U 18 x 3 and V 9 x 3. The
+// columns of S (inputs: stresses and velocities, whose scales differ by the impedances) are
+// scaled to unit maximum, c; Gram-Schmidt with pivoting over the 18 scaled rows (each new
+// direction orthogonalised twice) gives Q (3 orthonormal directions); then U = (S / c) Q^T and
+// V = c Q. out[nEl][4][2][P]: V [9][4] (column 3 zero), then per quantity q {U0[q][0..2],
+// U1[q][0..2], 0, 0}, the rest zero; a face whose scaled rows keep more than 1e-9 of the largest
+// row's norm outside the three directions counts in *bad (its pair is not of rank 3).
+template <typename T>
+__global__ void kBuildFsChar(const double *fsE, const int32_t *elFaEl, const uint8_t *fId, const uint8_t *faType,
+                             int64_t nEl, int P, T *out, int *bad) {
+  for (int64_t ef = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; ef < nEl * 4;
+       ef += int64_t(gridDim.x) * blockDim.x) {
+    const double *A = fsE + ef * 81;
+    const double *Bm = nullptr;
+    const int ty = faType[ef];
+    if (ty == EDGE_FACE_INNER)
+      Bm = fsE + ((nEl + elFaEl[ef]) * 4 + fId[ef]) * 81;
+    else if (ty == EDGE_FACE_FREE_SURFACE)
+      Bm = fsE + (nEl * 4 + ef) * 81;
+    auto entry = [&](int i, int j) { return i < 9 ? A[i * 9 + j] : (Bm ? Bm[(i - 9) * 9 + j] : 0.0); };
+    double c[9];
+    for (int j = 0; j < 9; j++) {
+      double m = 0;
+      for (int i = 0; i < 18; i++) m = fmax(m, fabs(entry(i, j)));
+      c[j] = m > 0 ? m : 1.0;
+    }
+    double rs[18][9], nrm0 = 0;
+    for (int i = 0; i < 18; i++) {
+      double n2 = 0;
+      for (int j = 0; j < 9; j++) {
+        rs[i][j] = entry(i, j) / c[j];
+        n2 += rs[i][j] * rs[i][j];
+      }
+      nrm0 = fmax(nrm0, n2);
+    }
+    double Q[3][9];
+    for (int k = 0; k < 3; k++) {
+      int piv = 0;
+      double best = -1;
+      for (int i = 0; i < 18; i++) {
+        double n2 = 0;
+        for (int j = 0; j < 9; j++) n2 += rs[i][j] * rs[i][j];
+        if (n2 > best) {
+          best = n2;
+          piv = i;
+        }
+      }
+      double v[9];
+      for (int j = 0; j < 9; j++) v[j] = rs[piv][j];
+      for (int pass = 0; pass < 2; pass++)
+        for (int kk = 0; kk < k; kk++) {
+          double d = 0;
+          for (int j = 0; j < 9; j++) d += v[j] * Q[kk][j];
+          for (int j = 0; j < 9; j++) v[j] -= d * Q[kk][j];
+        }
+      double n2 = 0;
+      for (int j = 0; j < 9; j++) n2 += v[j] * v[j];
+      const double inv = n2 > 1e-60 * nrm0 && n2 > 0 ? 1.0 / sqrt(n2) : 0.0;
+      for (int j = 0; j < 9; j++) Q[k][j] = v[j] * inv;
+      for (int i = 0; i < 18; i++) {
+        double d = 0;
+        for (int j = 0; j < 9; j++) d += rs[i][j] * Q[k][j];
+        for (int j = 0; j < 9; j++) rs[i][j] -= d * Q[k][j];
+      }
+    }
+    double res = 0;
+    for (int i = 0; i < 18; i++) {
+      double n2 = 0;
+      for (int j = 0; j < 9; j++) n2 += rs[i][j] * rs[i][j];
+      res = fmax(res, n2);
+    }
+    if (res > 1e-18 * nrm0) atomicAdd(bad, 1);
+    T *o = out + ef * 2 * P;
+    for (int j = 0; j < 2 * P; j++) o[j] = T(0);
+    for (int j = 0; j < 9; j++)
+      for (int k = 0; k < 3; k++) o[4 * j + k] = T(c[j] * Q[k][j]);
+    for (int i = 0; i < 18; i++)
+      for (int k = 0; k < 3; k++) {
+        double u = 0;
+        for (int j = 0; j < 9; j++) u += entry(i, j) / c[j] * Q[k][j];
+        o[36 + (i % 9) * 8 + (i / 9) * 3 + k] = T(u);
+      }
+  }
+}
+
 // halo exchange: blocks [9][R][GF] of face slots (element * 4 + face) to / from a packed buffer,
 // 16 bytes per thread; slots outside the face buffer are skipped
 __global__ void kFacePack(uint4 *face, uint4 *buf, const int32_t *slots, int n, int64_t blk16, int64_t nSlots,
@@ -214,6 +301,8 @@ struct edge_b200_ctx {
   // rebuilt before the next GTS step after the mesh or the element data changed
   DevBuf fsLR;
   bool fsLRStale = true;
+  bool fsLRChar = false;      // fsLR holds the characteristic factors of the pairs
+  bool charRejected = false;  // some face's pair is not of rank 3 (until the element data changes)
   // fused GTS steps (pre-mixing configurations, no halo): within one multi-step call each local
   // step also runs the previous step's neighbour step, so the face projections alternate between
   // two buffers (faceCur holds the last written); the last step's neighbour step runs on its own at
@@ -421,11 +510,41 @@ struct edge_b200_ctx {
     return cudaSuccess;
   }
 
-  cudaError_t ensureFsLR() {
-    if (!ks->premix() || !fsLRStale) return cudaSuccess;
+  // the flux-solver pairs of the pre-mixed projections, as characteristic factors for GTS steps of
+  // a configuration that mixes through them (unless some face's pair is not of rank 3, found when
+  // the factors are built: the pairs themselves from then on until the element data changes), as
+  // the pairs themselves for LTS steps
+  cudaError_t ensureFsLR(bool lts = false) {
+    if (!ks->premix()) return cudaSuccess;
+    const bool wantChar = !lts && ks->charMix() && !charRejected;
+    if (!fsLRStale && fsLRChar == wantChar) return cudaSuccess;
     const int P = ks->fsPairStride();
     cudaError_t e = fsLR.fit(size_t(nEl) * 4 * 2 * P * realSize);
     if (e) return e;
+    if (wantChar) {
+      int *bad = nullptr;
+      int nBad = 0;
+      if ((e = cudaMalloc(&bad, sizeof(int)))) return e;
+      e = cudaMemsetAsync(bad, 0, sizeof(int), stream);
+      if (!e) {
+        const int grid = (int)std::min<int64_t>((nEl * 4 + 127) / 128, 148 * 8);
+        if (cfg.precision == 64)
+          kBuildFsChar<double><<<grid, 128, 0, stream>>>(fsE, elFaEl, fId, faType, nEl, P, fsLR.as<double>(), bad);
+        else
+          kBuildFsChar<float><<<grid, 128, 0, stream>>>(fsE, elFaEl, fId, faType, nEl, P, fsLR.as<float>(), bad);
+        e = cudaGetLastError();
+      }
+      if (!e) e = cudaMemcpyAsync(&nBad, bad, sizeof(int), cudaMemcpyDeviceToHost, stream);
+      if (!e) e = cudaStreamSynchronize(stream);
+      cudaFree(bad);
+      if (e) return e;
+      if (nBad == 0) {
+        fsLRStale = false;
+        fsLRChar = true;
+        return cudaSuccess;
+      }
+      charRejected = true;
+    }
     const int64_t total = nEl * 4 * 2 * P;
     const int grid = (int)std::min<int64_t>((total + 255) / 256, 148 * 16);
     if (cfg.precision == 64)
@@ -434,6 +553,7 @@ struct edge_b200_ctx {
       kBuildFsLR<float><<<grid, 256, 0, stream>>>(fsE, elFaEl, fId, faType, nEl, P, fsLR.as<float>());
     if ((e = cudaGetLastError())) return e;
     fsLRStale = false;
+    fsLRChar = false;
     return cudaSuccess;
   }
 
@@ -457,6 +577,7 @@ struct edge_b200_ctx {
     a.vId = vId;
     a.faType = faType;
     a.fsLR = (ks->premix() && !fsLRStale) ? fsLR.p : nullptr;
+    a.fsChar = (a.fsLR && fsLRChar) ? 1 : 0;
     a.grpDt = grpDtOn ? grpDt.as<double>() : nullptr;
     a.nEl = nEl;
     a.elFirst = 0;
@@ -579,6 +700,7 @@ int edge_b200_upload_mesh(edge_b200_ctx *ctx, const int32_t *el_fa_el, const uin
   ctx->hFaType.assign(el_fa_type, el_fa_type + n);
   ctx->meshSet = true;
   ctx->fsLRStale = true;
+  ctx->charRejected = false;
   return EDGE_B200_OK;
 }
 
@@ -605,6 +727,7 @@ int edge_b200_upload_element_data(edge_b200_ctx *ctx, const double *star_e, cons
   EDGE_CUDA(cudaStreamSynchronize(s), "upload element data");
   ctx->dataSet = true;
   ctx->fsLRStale = true;
+  ctx->charRejected = false;
   return EDGE_B200_OK;
 }
 
@@ -627,6 +750,7 @@ int edge_b200_share_element_data(edge_b200_ctx *dst, const edge_b200_ctx *src) {
   ctx->sharedData = true;
   ctx->dataSet = true;
   ctx->fsLRStale = true;
+  ctx->charRejected = false;
   return EDGE_B200_OK;
 }
 
@@ -1138,7 +1262,7 @@ int edge_b200_step_lts(edge_b200_ctx *ctx, double t, double dt_fun, int n_cycles
   if (!ctx->meshSet || !ctx->dataSet) return EDGE_B200_EINVAL;
   if (!ctx->ks->ltsSupported()) return EDGE_B200_ENOTSUP;
   EDGE_CUDA(ctx->flush(), "pending neighbour step");
-  EDGE_CUDA(ctx->ensureFsLR(), "flux-solver pairs");
+  EDGE_CUDA(ctx->ensureFsLR(true), "flux-solver pairs");
   ctx->lastLts = true;
   const int G = ctx->nTg;
   const int64_t nFun = int64_t(1) << (G - 1);  // fundamental steps per cycle (largest group's step)

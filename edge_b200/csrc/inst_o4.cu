@@ -1,22 +1,5 @@
-// Compiled configurations of order 4 (precision, fused runs, relaxation mechanisms).
-#include "kernel_impl.cuh"
-
-namespace edge_b200 {
-KernelSet *makeKernelSet_o4(int precision, int order, int runs, int rms) {
-#include "inst_o4.inc"
-  return nullptr;
-}
-
-// process-wide instances, one per device, for callers that must not allocate
-// (edge_b200_step_noalloc); device < kStaticDevices
-KernelSet *staticKernelSet_o4(int precision, int order, int runs, int rms, int device) {
-#undef EDGE_B200_CFG
-#define EDGE_B200_CFG(T, O, R, RM, prec)                          \
-  if (precision == prec && order == O && runs == R && rms == RM) { \
-    static KernelSetImpl<T, O, R, RM> inst[kStaticDevices];       \
-    return &inst[device];                                         \
-  }
-#include "inst_o4.inc"
-  return nullptr;
-}
-}  // namespace edge_b200
+// Compiled configurations of order 4 (precision, fused runs, relaxation mechanisms: inst_o4.inc),
+// one of four parts per object (inst_order.cuh).
+#define EDGE_B200_ORDER 4
+#define EDGE_B200_INC "inst_o4.inc"
+#include "inst_order.cuh"

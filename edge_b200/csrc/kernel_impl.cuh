@@ -40,6 +40,7 @@ class KernelSetImpl final : public KernelSet {
     b.halfIdx = a.halfIdx;
     b.firstTs = a.firstTs;
     b.fsLR = static_cast<const T *>(a.fsLR);
+    b.fsChar = a.fsChar;
     b.faceIn = static_cast<const T *>(a.faceIn);
     b.grpDt = a.grpDt;
     return b;
@@ -62,6 +63,14 @@ class KernelSetImpl final : public KernelSet {
       return e;
     if constexpr (G::premix) {
       if ((e = cudaFuncSetAttribute(kLocal<T, O, R, RM, 0, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    (int)smemLocal())))
+        return e;
+    }
+    if constexpr (G::charMix) {
+      if ((e = cudaFuncSetAttribute(kLocal<T, O, R, RM, 0, false, true>,
+                                    cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smemLocal())))
+        return e;
+      if ((e = cudaFuncSetAttribute(kLocal<T, O, R, RM, 0, true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                     (int)smemLocal())))
         return e;
     }
@@ -107,12 +116,24 @@ class KernelSetImpl final : public KernelSet {
 
   cudaError_t local(const StepArgsRaw &a, cudaStream_t s) override {
     if (a.elCount < 1) return cudaSuccess;
+    if constexpr (G::charMix) {
+      if (a.fsChar) {
+        kLocal<T, O, R, RM, 0, false, true><<<grid(a.elCount, ctasLocal()), G::NT, smemLocal(), s>>>(cast(a));
+        return cudaGetLastError();
+      }
+    }
     kLocal<T, O, R, RM, 0><<<grid(a.elCount, ctasLocal()), G::NT, smemLocal(), s>>>(cast(a));
     return cudaGetLastError();
   }
   cudaError_t localFused(const StepArgsRaw &a, cudaStream_t s) override {
     if constexpr (G::premix) {
       if (a.elCount < 1) return cudaSuccess;
+      if constexpr (G::charMix) {
+        if (a.fsChar) {
+          kLocal<T, O, R, RM, 0, true, true><<<grid(a.elCount, ctasLocal()), G::NT, smemLocal(), s>>>(cast(a));
+          return cudaGetLastError();
+        }
+      }
       kLocal<T, O, R, RM, 0, true><<<grid(a.elCount, ctasLocal()), G::NT, smemLocal(), s>>>(cast(a));
       return cudaGetLastError();
     } else {
@@ -141,6 +162,7 @@ class KernelSetImpl final : public KernelSet {
   bool ltsSupported() const override { return G::ltsOk; }
   bool premix() const override { return G::premix; }
   int fsPairStride() const override { return G::FSP; }
+  bool charMix() const override { return G::charMix; }
   cudaError_t neigh(const StepArgsRaw &a, cudaStream_t s) override {
     if (a.elCount < 1) return cudaSuccess;
     kNeigh<T, O, R, RM, G::premix><<<grid(a.elCount, ctasNeigh()), G::NT, smemNeigh(), s>>>(cast(a));

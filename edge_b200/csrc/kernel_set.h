@@ -25,8 +25,10 @@ struct StepArgsRaw {
   const int32_t *sumIdx = nullptr, *halfIdx = nullptr;
   int firstTs = 0;
   // per element face fsE[0] and the face reader's fsE[1] in the configuration's precision, each
-  // padded to 16 bytes: [nEl][4][2][fsPairStride()] (premix)
+  // padded to 16 bytes: [nEl][4][2][fsPairStride()] (premix); fsChar: their characteristic
+  // factors instead (charMix)
   const void *fsLR = nullptr;
+  int fsChar = 0;
   // fused GTS steps: the previous step's face projections whose neighbour step is still pending
   const void *faceIn = nullptr;
   // per element group time steps of the GTS local step (merged simulations), or null
@@ -49,6 +51,9 @@ class KernelSet {
   // GTS face projections leave the local kernel mixed with the reader's flux solver (fsLR)
   virtual bool premix() const = 0;
   virtual int fsPairStride() const = 0;
+  // the GTS local kernel mixes face projections through the rank-3 factors of the flux-solver
+  // pairs when fsLR holds them (StepArgsRaw::fsChar)
+  virtual bool charMix() const = 0;
   virtual cudaError_t neigh(const StepArgsRaw &a, cudaStream_t s) = 0;
   // the neighbour step over the buffers the LTS local kernels wrote (pre-mixed where those
   // kernels have room for it)

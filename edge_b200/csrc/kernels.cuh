@@ -54,8 +54,10 @@ struct StepArgs {
   // elastic GTS (Geo::premix): per element face the element's own flux solver fsE[0] and the one
   // its face reader applies (fsE[1] of the face neighbour at its face, or the element's own for a
   // free surface; zeros for outflow) in T, each padded to 16 bytes (Geo::FSP): [nEl][4][2][FSP];
-  // null: gathered through the connectivity
+  // null: gathered through the connectivity. fsChar: fsLR holds the characteristic factors of
+  // those pairs instead (Geo::charMix: V [9][4], then per quantity {U0[q][0..2], U1[q][0..2], 0, 0})
   const T *fsLR;
+  int fsChar;
   // fused GTS steps (kLocal<..., FUSED>, kRecv): the previous step's pre-mixed face projections,
   // whose neighbour fluxes are added to the DOF rows before the recursion (the previous step's
   // neighbour step runs here), or null when none are pending
@@ -347,7 +349,19 @@ struct Geo {
   static constexpr size_t fsExtraOff = srcOff + srcBytes;
   static constexpr size_t tilesOff = (fsExtraOff + fsLocalBytes + 15) / 16 * 16;
   static constexpr bool projSplit = srcSplit && tilesOff + 2 * nS0 * sizeof(T) <= localBudget;
-  static constexpr size_t smemLocalGts = premix      ? smemLocal + premixBytes
+  // characteristic mix (elastic GTS, pre-mixing): the two flux solvers a face projection P meets
+  // -- fsE[0] of the element and the reader's fsE[1] -- stacked (18 x 9) have rank 3, the three
+  // waves that leave the element through the face: [fsE0; fsE1] = [U0; U1] V^T. The nine warps
+  // first compute the three characteristic rows W = V^T P (a four-mode chunk each), then every
+  // warp its two output rows from W: 3 x 9 + 2 x 9 x 3 products per face mode instead of 2 x 81.
+  // W [3][32][SF] lives in X behind the face rows it holds during the faces, or behind the
+  // flux-solver buffers
+  static constexpr size_t nW = size_t(3) * 32 * SF;
+  static constexpr bool wInX = nW <= nX - nS0;
+  static constexpr bool charMix =
+      premix && (F + 3) / 4 <= 9 && (wInX || smemLocal + premixBytes + nW * sizeof(T) <= localBudget);
+  static constexpr size_t smemLocalGts = premix      ? smemLocal + premixBytes +
+                                                      (charMix && !wInX ? nW * sizeof(T) : 0)
                                          : projSplit ? tilesOff + 2 * nS0 * sizeof(T)
                                          : srcSplit  ? srcOff + srcBytes
                                          : fsLocal  ? smemLocal + fsLocalBytes + (coefSmem ? coefBytes : 0)
@@ -838,7 +852,75 @@ template <typename T>
 struct MixFs {
   T *buf;  // two buffers [2][E][2][FSP]
   int64_t g, nGroups;
+  T *w = nullptr;  // characteristic rows [3][32][SF] (Geo::charMix)
 };
+
+// characteristic rows of a face (Geo::charMix), first half: warp q < ceil(F / 4) computes modes
+// [4q, 4q + 4) of W[k] = sum_i V[i][k] S0[i] (k < 3) into Wt; fb = this lane's element's factors
+// (V [9][4] first). Modes past F read whatever the row holds there and count as zero.
+template <typename T, int F, int SF>
+__device__ __forceinline__ void charRows(const T *S0, const T *fb, int q, int l, T *Wt) {
+  if (q >= (F + 3) / 4) return;
+  const int j0 = 4 * q;
+  T w[3][4];
+#pragma unroll
+  for (int k = 0; k < 3; k++)
+#pragma unroll
+    for (int u = 0; u < 4; u++) w[k][u] = T(0);
+#pragma unroll
+  for (int i = 0; i < 9; i++) {
+    T v[4], vk[4];
+    ld4<T>(rowPtr<T, SF>(S0, i, l) + j0, v);
+    ld4<T>(fb + 4 * i, vk);
+#pragma unroll
+    for (int u = 0; u < 4; u++) {
+      const T x = j0 + u < F ? v[u] : T(0);
+#pragma unroll
+      for (int k = 0; k < 3; k++) w[k][u] = fmaT(vk[k], x, w[k][u]);
+    }
+  }
+#pragma unroll
+  for (int k = 0; k < 3; k++) st4<T>(rowPtr<T, SF>(Wt, k, l) + j0, w[k]);
+}
+
+// second half: s[j] = sum_k uu[k] W[k][j] into registers, t[j] = sum_k uu[3 + k] W[k][j] written to
+// tRow[0, G) chunk by chunk; W is zero past F, so is t
+template <typename T, int F, int SF, int G>
+__device__ __forceinline__ void charMix2(const T *Wt, int l, const T *uu, T *s, T *tRow) {
+  T u[8];
+  {
+    T a[4], b[4];
+    ld4<T>(uu, a);
+    ld4<T>(uu + 4, b);
+#pragma unroll
+    for (int i = 0; i < 4; i++) {
+      u[i] = a[i];
+      u[4 + i] = b[i];
+    }
+  }
+#pragma unroll
+  for (int j0 = 0; j0 < F; j0 += 4) {
+    T w0[4], w1[4], w2[4], o[4], p[4];
+    ld4<T>(rowPtr<T, SF>(Wt, 0, l) + j0, w0);
+    ld4<T>(rowPtr<T, SF>(Wt, 1, l) + j0, w1);
+    ld4<T>(rowPtr<T, SF>(Wt, 2, l) + j0, w2);
+#pragma unroll
+    for (int v = 0; v < 4; v++) {
+      o[v] = fmaT(u[2], w2[v], fmaT(u[1], w1[v], u[0] * w0[v]));
+      p[v] = fmaT(u[5], w2[v], fmaT(u[4], w1[v], u[3] * w0[v]));
+    }
+#pragma unroll
+    for (int v = 0; v < 4; v++)
+      if (j0 + v < F) s[j0 + v] = o[v];
+    if (j0 + 4 <= G) {
+      st4<T>(tRow + j0, p);
+    } else {
+#pragma unroll
+      for (int v = 0; v < 4; v++)
+        if (j0 + v < G) tRow[j0 + v] = p[v];
+    }
+  }
+}
 template <typename T, int O, int R, int RM, int FA>
 __device__ __forceinline__ void issueMixFs(const StepArgs<T> &a, T *buf, int64_t g, int64_t nGroups) {
   using G = Geo<T, O, R, RM>;
@@ -996,7 +1078,8 @@ __device__ __forceinline__ void neighFluxDirect(const StepArgs<T> &a, const T *f
 // projections of elements with a smaller neighbour (needs TIh)
 // pre-mixed projections (LTS 0, Geo::premix): S0alt is a tile free for this warp's own rows,
 // through which the mixed projection leaves as coalesced stores; mf the flux-solver buffers
-template <typename T, int O, int R, int RM, int FA, int LTS = 0, bool TAIL = true>
+// CHAR: the pre-mixed projections mix through the characteristic factors in mf.buf (Geo::charMix)
+template <typename T, int O, int R, int RM, int FA, int LTS = 0, bool TAIL = true, bool CHAR = false>
 __device__ __forceinline__ void localFace(const StepArgs<T> &a, const T *TI, T *S0, int q, int l, int64_t e,
                                           int r, bool valid, T *acc, T *upA, const T *TIh = nullptr,
                                           T *S0alt = nullptr, const MixFs<T> &mf = MixFs<T>{nullptr, 0, 0},
@@ -1075,14 +1158,29 @@ __device__ __forceinline__ void localFace(const StepArgs<T> &a, const T *TI, T *
     else
       issueMixFs<T, O, R, RM, 0>(a, mf.buf, mf.g + gridDim.x, mf.nGroups);
     cpAsyncCommit();
+    const T *fbE = mf.buf + (FA % 2) * (E * 2 * FSP) + (l / R) * (2 * FSP);
+    static_assert(!CHAR || (LTS == 0 && G::charMix), "characteristic mix: GTS configurations with room for it");
+    if constexpr (CHAR) {
+      // the characteristic rows of all warps' projections, then both mixes from them; the mixed
+      // projection leaves through this warp's own row of S0 (no warp reads S0 after the barrier)
+      charRows<T, F, SF>(S0, fbE, q, l, mf.w);
+      __syncthreads();
+      T *tRow = rowPtr<T, SF>(S0, q, l);
+      charMix2<T, F, SF, G::GF>(mf.w, l, fbE + 36 + q * 8, s, tRow);
+      __syncwarp();
+      if (ty != FT_OUTFLOW)
+        storeRowsCoalesced<T, R, G::GF, SF>(S0, a.face + ((e * 4 + FA) * 9 + q) * int64_t(R * G::GF), q, l / R,
+                                            l % R);
+      __syncwarp();
+      FluxTMul<O, FA>::template run<T>(s, acc);
+      if constexpr (TAIL) __syncthreads();
+      return;
+    }
     T fr[9], fr1[9];
-    {
-      const T *fb = mf.buf + (FA % 2) * (E * 2 * FSP) + (l / R) * (2 * FSP) + q * 9;
 #pragma unroll
-      for (int i = 0; i < 9; i++) {
-        fr[i] = fb[i];
-        fr1[i] = fb[FSP + i];
-      }
+    for (int i = 0; i < 9; i++) {
+      fr[i] = fbE[q * 9 + i];
+      fr1[i] = fbE[FSP + q * 9 + i];
     }
     T *tRow = rowPtr<T, SF>(S0alt, q, l);
     faceMix2<T, F, SF, G::GF>(S0, l, fr, fr1, s, tRow);
@@ -1235,7 +1333,7 @@ __device__ __forceinline__ void facesSplit(const StepArgs<T> &a, const T *TI, T 
 // 1 runs on the elements of a time group without a smaller neighbour
 // FUSED (GTS, pre-mixing configurations): the previous step's neighbour fluxes (a.faceIn, when
 // pending) are added to each group's DOF rows first, and the completed rows stored back
-template <typename T, int O, int R, int RM, int LTS, bool FUSED = false>
+template <typename T, int O, int R, int RM, int LTS, bool FUSED = false, bool CHAR = false>
 __global__ void __launch_bounds__(Geo<T, O, R, RM>::NT, LTS == 2 ? 1 : Geo<T, O, R, RM>::minCtasLocal)
     kLocal(StepArgs<T> a) {
   using G = Geo<T, O, R, RM>;
@@ -1454,7 +1552,10 @@ __global__ void __launch_bounds__(Geo<T, O, R, RM>::NT, LTS == 2 ? 1 : Geo<T, O,
     }
     // local surface integral (SurfIntVanilla::local, SurfIntVanilla.hpp:212-262) + face projections
     if constexpr (AS) {
-      const MixFs<T> mf{fsb, g, nGroups};
+      // characteristic rows: behind the face rows of X, or behind the flux-solver buffers
+      T *const wTile =
+          CHAR ? (G::wInX ? X + G::nS0 : reinterpret_cast<T *>(smem + G::smemLocal + G::premixBytes)) : nullptr;
+      const MixFs<T> mf{fsb, g, nGroups, wTile};
       const LocalFs lf{fsl, g, nGroups};
       if constexpr (PSP) {
         T *const tiles[4] = {S0, X, reinterpret_cast<T *>(smem + G::tilesOff),
@@ -1469,11 +1570,12 @@ __global__ void __launch_bounds__(Geo<T, O, R, RM>::NT, LTS == 2 ? 1 : Geo<T, O,
         issueLocalFs<T, O, R, RM, 3>(a, fsExtra + E * G::NFL, gn, nGroups);
         cpAsyncCommit();
       } else {
-        localFace<T, O, R, RM, 0, LTS, false>(a, TI, S0, q, l, ev, r, valid, acc, upA, TIh, X, mf, Sh, lf);
-        localFace<T, O, R, RM, 1, LTS, false>(a, TI, X, q, l, ev, r, valid, acc, upA, TIh, S0, mf, Sh, lf);
-        localFace<T, O, R, RM, 2, LTS, false>(a, TI, S0, q, l, ev, r, valid, acc, upA, TIh, X, mf, Sh, lf);
-        // the barrier after the last face orders its readers of X before the next group writes X
-        localFace<T, O, R, RM, 3, LTS, true>(a, TI, X, q, l, ev, r, valid, acc, upA, TIh, S0, mf, Sh, lf);
+        localFace<T, O, R, RM, 0, LTS, false, CHAR>(a, TI, S0, q, l, ev, r, valid, acc, upA, TIh, X, mf, Sh, lf);
+        localFace<T, O, R, RM, 1, LTS, false, CHAR>(a, TI, X, q, l, ev, r, valid, acc, upA, TIh, S0, mf, Sh, lf);
+        localFace<T, O, R, RM, 2, LTS, false, CHAR>(a, TI, S0, q, l, ev, r, valid, acc, upA, TIh, X, mf, Sh, lf);
+        // the barrier after the last face orders its readers of X (and of the characteristic rows
+        // behind its face rows) before the next group writes X
+        localFace<T, O, R, RM, 3, LTS, true, CHAR>(a, TI, X, q, l, ev, r, valid, acc, upA, TIh, S0, mf, Sh, lf);
       }
       if constexpr (SS)
         if (q < 6) addSrcRows<T, B, SB>(srcBuf, q, l, acc);
