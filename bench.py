@@ -35,7 +35,7 @@ def parse():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="edge", choices=["edge", "reference"])
     ap.add_argument("--workload", default="box48_o5_r16_fp32", choices=sorted(WORKLOADS))
-    ap.add_argument("--e2e-steps", type=int, default=10)
+    ap.add_argument("--e2e-steps", type=int, default=20)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-fp64", action="store_true")
     ap.add_argument("--tc-probe", action=argparse.BooleanOptionalAction, default=True,
