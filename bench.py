@@ -913,10 +913,38 @@ def main():
     torch.cuda.synchronize()
     e2e_ms = max_over_ranks(x0.elapsed_time(x1), ws)
     dof_bytes = pin_e.numel() * pin_e.element_size() + (pin_a.numel() * pin_a.element_size() if pin_a is not None else 0)
+    # the copies' own bound on this host: 1 GiB each way at once between the same pinned buffers
+    # and the device (CUDA events on two streams), after the timed region
+    nb = min(1 << 30, pin_e.numel() * pin_e.element_size())
+    hb = pin_e.view(-1).view(torch.uint8)[:nb]
+    ob = out_e.view(-1).view(torch.uint8)[:nb]
+    dev_a = torch.empty(nb, dtype=torch.uint8, device=local)
+    dev_b = torch.empty(nb, dtype=torch.uint8, device=local)
+    s_up, s_dn = torch.cuda.Stream(device=local), torch.cuda.Stream(device=local)
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(4)]
+    for rep in range(2):  # the first pass warms the copy engines
+        torch.cuda.synchronize()
+        ev[0].record(s_up)
+        ev[2].record(s_dn)
+        with torch.cuda.stream(s_up):
+            dev_a.copy_(hb, non_blocking=True)
+        with torch.cuda.stream(s_dn):
+            ob.copy_(dev_b, non_blocking=True)
+        ev[1].record(s_up)
+        ev[3].record(s_dn)
+        torch.cuda.synchronize()
+    h2d_gbs = nb / (ev[0].elapsed_time(ev[1]) / 1e3) / 1e9
+    d2h_gbs = nb / (ev[2].elapsed_time(ev[3]) / 1e3) / 1e9
+    del dev_a, dev_b
+    bound_s = max(dof_bytes / (h2d_gbs * 1e9), dof_bytes / (d2h_gbs * 1e9))
     e2e = {"value": units_per_step * ke * ws / (e2e_ms / 1e3), "unit": UNIT, "h2d_bytes_per_step": dof_bytes,
-           "d2h_bytes_per_step": dof_bytes,
+           "d2h_bytes_per_step": dof_bytes, "steps": ke,
+           "pcie_gbs_both_directions_at_once": {"h2d": h2d_gbs, "d2h": d2h_gbs},
+           "copy_bound_value": units_per_step / bound_s,
+           "frac_of_copy_bound": (units_per_step * ke / (e2e_ms / 1e3)) / (units_per_step / bound_s),
            "note": "per step: pinned host->device DOFs, one GTS step, device->host DOFs (the drop-in for "
-                   "host-resident DOFs), asynchronous copies overlapping across steps"}
+                   "host-resident DOFs), asynchronous copies overlapping across steps; copy_bound_value: the "
+                   "rate if each step took only its DOFs' copies at the measured bandwidth"}
 
     # plain FP64 path on the same mesh (one run) for the batched-FP32 vs plain-FP64 ratio
     fp64 = None

@@ -101,9 +101,11 @@ __global__ void kBuildFsLR(const double *fsE, const int32_t *elFaEl, const uint8
 // columns of S (inputs: stresses and velocities, whose scales differ by the impedances) are
 // scaled to unit maximum, c; Gram-Schmidt with pivoting over the 18 scaled rows (each new
 // direction orthogonalised twice) gives Q (3 orthonormal directions); then U = (S / c) Q^T and
-// V = c Q. out[nEl][4][2][P]: V [9][4] (column 3 zero), then per quantity q {U0[q][0..2],
-// U1[q][0..2], 0, 0}, the rest zero; a face whose scaled rows keep more than 1e-9 of the largest
-// row's norm outside the three directions counts in *bad (its pair is not of rank 3).
+// V = c Q. out[nEl][4][2][P] (zeroed before): V [9][4] and U0 [9][4] of the face at the face, and
+// U1 [9][4] at the face of its reader (the face neighbour's face for an inner face, the face
+// itself for a free surface; none for outflow) as that face's Uin, each with column 3 zero; a face
+// whose scaled rows keep more than 1e-9 of the largest row's norm outside the three directions
+// counts in *bad (its pair is not of rank 3).
 template <typename T>
 __global__ void kBuildFsChar(const double *fsE, const int32_t *elFaEl, const uint8_t *fId, const uint8_t *faType,
                              int64_t nEl, int P, T *out, int *bad) {
@@ -170,15 +172,20 @@ __global__ void kBuildFsChar(const double *fsE, const int32_t *elFaEl, const uin
     }
     if (res > 1e-18 * nrm0) atomicAdd(bad, 1);
     T *o = out + ef * 2 * P;
-    for (int j = 0; j < 2 * P; j++) o[j] = T(0);
+    const int64_t reader = ty == EDGE_FACE_INNER ? int64_t(elFaEl[ef]) * 4 + fId[ef]
+                           : ty == EDGE_FACE_FREE_SURFACE ? ef
+                                                          : -1;
     for (int j = 0; j < 9; j++)
       for (int k = 0; k < 3; k++) o[4 * j + k] = T(c[j] * Q[k][j]);
-    for (int i = 0; i < 18; i++)
+    for (int i = 0; i < 18; i++) {
+      if (i >= 9 && reader < 0) break;
+      T *dst = i < 9 ? o + 36 + i * 4 : out + reader * 2 * P + 72 + (i - 9) * 4;
       for (int k = 0; k < 3; k++) {
         double u = 0;
         for (int j = 0; j < 9; j++) u += entry(i, j) / c[j] * Q[k][j];
-        o[36 + (i % 9) * 8 + (i / 9) * 3 + k] = T(u);
+        dst[k] = T(u);
       }
+    }
   }
 }
 
@@ -526,6 +533,7 @@ struct edge_b200_ctx {
       int nBad = 0;
       if ((e = cudaMalloc(&bad, sizeof(int)))) return e;
       e = cudaMemsetAsync(bad, 0, sizeof(int), stream);
+      if (!e) e = cudaMemsetAsync(fsLR.p, 0, size_t(nEl) * 4 * 2 * P * realSize, stream);
       if (!e) {
         const int grid = (int)std::min<int64_t>((nEl * 4 + 127) / 128, 148 * 8);
         if (cfg.precision == 64)
