@@ -143,14 +143,16 @@ def host_n_modes(order):
     return order * (order + 1) * (order + 2) // 6
 
 
-def algorithmic(prob, prec, premix=False, fs_pair=84, fused=False):
+def algorithmic(prob, prec, premix=False, fs_pair=84, fused=False, char=False):
     """Per-element algorithmic bytes and flops of one step (dense-in-modes counts as in the
     roofline model of the path) for each kernel. premix: the local kernel mixes the face
     projections with the reading element's flux solver and reads per face the padded pair
     [2][fs_pair] of flux solvers in the compute precision instead of its own fsE[0] block; the
-    neighbour kernel then reads no flux solvers. fused: the local kernel also runs the previous step's
-    neighbour step (reads the four neighbour projections and the connectivity, adds their lifted
-    fluxes and stores the completed DOF rows once more)."""
+    neighbour kernel then reads no flux solvers. char: the faces leave as three characteristic rows
+    instead of nine pre-mixed ones; the local kernel reads 72 factor values per face, the reader 36
+    (its factor of the pair) and mixes the rows back. fused: the local kernel also runs the previous
+    step's neighbour step (reads the four neighbour projections and the connectivity, adds their
+    lifted fluxes and stores the completed DOF rows once more)."""
     from edge_b200.host import n_face_modes, n_modes
     O, R, rm = prob.order, prob.runs, prob.rm
     B, F, p = n_modes(O), n_face_modes(O), (8 if prec == 64 else 4)
@@ -159,14 +161,17 @@ def algorithmic(prob, prec, premix=False, fs_pair=84, fused=False):
     vol = 3 * (2 * 9 * B * Bm(O - 1) + 2 * 24 * B)
     surf = 4 * (2 * 9 * F * B + 2 * 81 * F + 2 * 9 * B * F)
     dofs = (9 + 6 * rm) * B * R * p
-    face = 4 * 9 * F * R * p
-    fs_local = 4 * 2 * fs_pair * p if premix else 4 * 81 * 8
+    face = 4 * (3 if char else 9) * F * R * p
+    fs_local = 4 * 72 * p if char else (4 * 2 * fs_pair * p if premix else 4 * 81 * 8)
+    uin = 4 * 36 * p if char else 0
     local_bytes = 2 * dofs + face + 3 * 24 * 8 + fs_local + (rm * 12 * 8 + 27 * 8 + 4 * 54 * 8 if rm else 0)
-    neigh_bytes = 2 * dofs + face + (0 if premix else 4 * 81 * 8) + 4 * (4 + 1 + 1 + 1) + (4 * 54 * 8 if rm else 0)
-    mix = 4 * 2 * 81 * F if premix else 0
-    local_flops, neigh_flops = (ck + vol + surf + mix) * R, (surf - mix) * R
+    neigh_bytes = (2 * dofs + face + uin + (0 if premix else 4 * 81 * 8) + 4 * (4 + 1 + 1 + 1) +
+                   (4 * 54 * 8 if rm else 0))
+    mix = (4 * (2 * 27 * F) if char else 4 * 2 * 81 * F) if premix else 0
+    local_flops = (ck + vol + surf + mix) * R
+    neigh_flops = (surf - 4 * 2 * 81 * F + (4 * 2 * 27 * F if char else 0)) * R if premix else surf * R
     if fused:
-        local_bytes += face + dofs + 4 * (4 + 1 + 1 + 1)
+        local_bytes += face + uin + dofs + 4 * (4 + 1 + 1 + 1)
         local_flops += neigh_flops
     return dict(local_bytes=local_bytes, neigh_bytes=neigh_bytes, local_flops=local_flops, neigh_flops=neigh_flops)
 
@@ -840,7 +845,7 @@ def main():
     shares = {names[i]: float(kms[i] / kms.sum()) for i in range(4) if kn[i]}
     kc = np.zeros(6, np.int32)
     L.edge_b200_kernel_config(sv._h, _lib.ptr(kc))
-    alg = algorithmic(prob, prec, premix=bool(kc[1]), fs_pair=int(kc[2]), fused=bool(kc[5]))
+    alg = algorithmic(prob, prec, premix=bool(kc[1]), fs_pair=int(kc[2]), fused=bool(kc[5]), char=int(kc[1]) == 2)
     top = int(np.argmax(kms[:2]))
     avg_ms = kms[top] / max(kn[top], 1)
     # algorithmic bytes: the path's compulsory bytes of one element step (every array touched once:

@@ -903,14 +903,17 @@ __device__ __forceinline__ void charMix(const T *Wt, int l, const T *uq, T *s) {
       if (j0 + v < F) s[j0 + v] = fmaT(u[2], w2[v], fmaT(u[1], w1[v], u[0] * w0[v]));
   }
 }
-template <typename T, int O, int R, int RM, int FA>
+// CHAR: only the characteristic factors the local step reads (V and U0: the first 72 values)
+template <typename T, int O, int R, int RM, int FA, bool CHAR = false>
 __device__ __forceinline__ void issueMixFs(const StepArgs<T> &a, T *buf, int64_t g, int64_t nGroups) {
   using G = Geo<T, O, R, RM>;
   constexpr int E = G::E, FSP = G::FSP, W = 16 / int(sizeof(T)), NC = FSP / W;
+  constexpr int NCP = CHAR ? 72 / W : 2 * NC;  // chunks copied per element face
+  static_assert(72 % W == 0, "factor blocks of whole chunks");
   if (g >= nGroups) return;
   if (a.fsLR) {
-    for (int i = threadIdx.x; i < E * 2 * NC; i += G::NT) {
-      const int eo = i / (2 * NC), k = i % (2 * NC);
+    for (int i = threadIdx.x; i < E * NCP; i += G::NT) {
+      const int eo = i / NCP, k = i % NCP;
       if (g * E + eo >= a.elCount) continue;
       const int64_t e = a.elFirst + g * E + eo;
       cpAsync16(buf + eo * 2 * FSP + k * W, a.fsLR + (e * 4 + FA) * (2 * FSP) + k * W);
@@ -1160,9 +1163,9 @@ __device__ __forceinline__ void localFace(const StepArgs<T> &a, const T *TI, T *
     // the next face's blocks into the other buffer, whose readers (two faces back) all passed the
     // barrier; after the last face the next group's first
     if constexpr (FA < 3)
-      issueMixFs<T, O, R, RM, FA + 1>(a, mf.buf + ((FA + 1) % 2) * (E * 2 * FSP), mf.g, mf.nGroups);
+      issueMixFs<T, O, R, RM, FA + 1, CHAR>(a, mf.buf + ((FA + 1) % 2) * (E * 2 * FSP), mf.g, mf.nGroups);
     else
-      issueMixFs<T, O, R, RM, 0>(a, mf.buf, mf.g + gridDim.x, mf.nGroups);
+      issueMixFs<T, O, R, RM, 0, CHAR>(a, mf.buf, mf.g + gridDim.x, mf.nGroups);
     cpAsyncCommit();
     const T *fbE = mf.buf + (FA % 2) * (E * 2 * FSP) + (l / R) * (2 * FSP);
     static_assert(!CHAR || (LTS == 0 && G::charMix), "characteristic mix: GTS configurations with room for it");
@@ -1394,7 +1397,7 @@ __global__ void __launch_bounds__(Geo<T, O, R, RM>::NT, LTS == 2 ? 1 : Geo<T, O,
         for (int m = 0; m < RM; m++)
           copyRows<T, R, G::GB, SB>(TIA, a.dofsA, a.elFirst + g0 * E + eo, RM * 6, m * 6 + q - 9, eo, r);
     }
-    if constexpr (PM) issueMixFs<T, O, R, RM, 0>(a, fsb, g0, nGroups);
+    if constexpr (PM) issueMixFs<T, O, R, RM, 0, CHAR>(a, fsb, g0, nGroups);
     if constexpr (FL) issueLocalFs<T, O, R, RM, 0>(a, fsl, g0, nGroups);
     if constexpr (PSP) {
       issueLocalFs<T, O, R, RM, 1>(a, fsl + E * G::NFL, g0, nGroups);
