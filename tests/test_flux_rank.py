@@ -5,11 +5,12 @@ stacked into an 18 x 9 matrix, have rank 3 -- the three waves (P, S, S) that lea
 through the face. The device then mixes each face projection through three characteristic rows
 instead of two 9 x 9 blocks. Checked here on the host-built flux solvers (pinned to the reference's
 Elasticity code in test_host_setup.py) for heterogeneous, layered, jittered meshes with every face
-type, with a restatement of the factorisation the device builds (column-scaled Gram-Schmidt with
-pivoting, each direction orthogonalised twice)."""
+type, with the oracle's restatement of the factorisation the device builds (column-scaled
+Gram-Schmidt with pivoting, each direction orthogonalised twice)."""
 import numpy as np
 import pytest
 
+import oracle
 from edge_b200 import host
 from helpers import small_problem
 
@@ -30,24 +31,6 @@ def _pairs(p):
             yield t, np.vstack([a, b])
 
 
-def _factor(S):
-    """U (18 x 3), V (9 x 3) with S = U V^T, as the device builds them."""
-    c = np.abs(S).max(axis=0)
-    c[c == 0] = 1.0
-    St = S / c
-    R = St.copy()
-    Q = np.zeros((3, 9))
-    for k in range(3):
-        v = R[np.argmax((R * R).sum(axis=1))].copy()
-        for _ in range(2):
-            for kk in range(k):
-                v -= (v @ Q[kk]) * Q[kk]
-        n = np.sqrt(v @ v)
-        Q[k] = v / n if n > 0 else 0.0
-        R -= np.outer(R @ Q[k], Q[k])
-    return St @ Q.T, c[:, None] * Q.T, np.sqrt((R * R).sum(axis=1).max() / (St * St).sum(axis=1).max())
-
-
 @pytest.mark.parametrize("bc_sides", [host.FACE_OUTFLOW, host.FACE_FREE_SURFACE])
 def test_stacked_flux_solvers_have_rank_three(bc_sides):
     p = small_problem(n=3, order=3, runs=1, jitter=0.2, seed=5, n_steps=2, source=None, n_receivers=0,
@@ -58,8 +41,8 @@ def test_stacked_flux_solvers_have_rank_three(bc_sides):
         s = np.linalg.svd(S, compute_uv=False)
         assert s[2] > 1e-3 * s[0]  # three waves
         assert s[3] < 1e-12 * s[0]  # and no more
-        U, V, res = _factor(S)
-        assert res < 1e-12
+        V, U0, U1 = oracle.flux_char_factors(S[:9], S[9:] if np.any(S[9:]) else None)
+        U = np.vstack([U0, U1])
         # every entry reproduced to rounding relative to its row and its column
         scale = np.minimum(np.abs(S).max(axis=1)[:, None], np.abs(S).max(axis=0)[None, :])
         assert np.all(np.abs(U @ V.T - S) <= 1e-12 * scale + 1e-300)
