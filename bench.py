@@ -148,11 +148,11 @@ def algorithmic(prob, prec, premix=False, fs_pair=84, fused=False, char=False):
     roofline model of the path) for each kernel. premix: the local kernel mixes the face
     projections with the reading element's flux solver and reads per face the padded pair
     [2][fs_pair] of flux solvers in the compute precision instead of its own fsE[0] block; the
-    neighbour kernel then reads no flux solvers. char: the faces leave as three characteristic rows
-    instead of nine pre-mixed ones; the local kernel reads 72 factor values per face, the reader 36
-    (its factor of the pair) and mixes the rows back. fused: the local kernel also runs the previous
-    step's neighbour step (reads the four neighbour projections and the connectivity, adds their
-    lifted fluxes and stores the completed DOF rows once more)."""
+    neighbour kernel then reads no flux solvers. char: the local kernel mixes through the rank-3
+    factors of each face's flux-solver pair (3 x 9 + 2 x 9 x 3 products per face mode for both
+    mixes instead of 2 x 81) and reads 108 factor values per face instead of the pair. fused: the
+    local kernel also runs the previous step's neighbour step (reads the four neighbour projections
+    and the connectivity, adds their lifted fluxes and stores the completed DOF rows once more)."""
     from edge_b200.host import n_face_modes, n_modes
     O, R, rm = prob.order, prob.runs, prob.rm
     B, F, p = n_modes(O), n_face_modes(O), (8 if prec == 64 else 4)
@@ -161,17 +161,17 @@ def algorithmic(prob, prec, premix=False, fs_pair=84, fused=False, char=False):
     vol = 3 * (2 * 9 * B * Bm(O - 1) + 2 * 24 * B)
     surf = 4 * (2 * 9 * F * B + 2 * 81 * F + 2 * 9 * B * F)
     dofs = (9 + 6 * rm) * B * R * p
-    face = 4 * (3 if char else 9) * F * R * p
-    fs_local = 4 * 72 * p if char else (4 * 2 * fs_pair * p if premix else 4 * 81 * 8)
-    uin = 4 * 36 * p if char else 0
+    face = 4 * 9 * F * R * p
+    fs_local = 4 * 108 * p if char else (4 * 2 * fs_pair * p if premix else 4 * 81 * 8)
     local_bytes = 2 * dofs + face + 3 * 24 * 8 + fs_local + (rm * 12 * 8 + 27 * 8 + 4 * 54 * 8 if rm else 0)
-    neigh_bytes = (2 * dofs + face + uin + (0 if premix else 4 * 81 * 8) + 4 * (4 + 1 + 1 + 1) +
-                   (4 * 54 * 8 if rm else 0))
-    mix = (4 * (2 * 27 * F) if char else 4 * 2 * 81 * F) if premix else 0
+    neigh_bytes = 2 * dofs + face + (0 if premix else 4 * 81 * 8) + 4 * (4 + 1 + 1 + 1) + (4 * 54 * 8 if rm else 0)
+    # the face mixes: surf counts one 9 x 9 mix per face; pre-mixing adds the second, and the
+    # factors replace both by 3 x 9 + 2 x 9 x 3 products per face mode
+    mix = (4 * 2 * (81 + 54 - 2 * 81) * F if char else 0) + (4 * 2 * 81 * F if premix else 0)
     local_flops = (ck + vol + surf + mix) * R
-    neigh_flops = (surf - 4 * 2 * 81 * F + (4 * 2 * 27 * F if char else 0)) * R if premix else surf * R
+    neigh_flops = (surf - 4 * 2 * 81 * F) * R if premix else surf * R
     if fused:
-        local_bytes += face + uin + dofs + 4 * (4 + 1 + 1 + 1)
+        local_bytes += face + dofs + 4 * (4 + 1 + 1 + 1)
         local_flops += neigh_flops
     return dict(local_bytes=local_bytes, neigh_bytes=neigh_bytes, local_flops=local_flops, neigh_flops=neigh_flops)
 

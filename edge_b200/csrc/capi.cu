@@ -101,109 +101,84 @@ __global__ void kBuildFsLR(const double *fsE, const int32_t *elFaEl, const uint8
 // columns of S (inputs: stresses and velocities, whose scales differ by the impedances) are
 // scaled to unit maximum, c; Gram-Schmidt with pivoting over the 18 scaled rows (each new
 // direction orthogonalised twice) gives Q (3 orthonormal directions); then U = (S / c) Q^T and
-// V = c Q. Returns false when the scaled rows keep more than 1e-9 of the largest row's norm
-// outside the three directions (the pair is not of rank 3). fs1 null: no reader. Not inlined: the
-// writer and the reader of a face factor the same pair through the same instructions, so their
-// factors agree to the bit.
-__device__ __noinline__ bool charFactors(const double *fs0, const double *fs1, double V[9][3], double U[18][3]) {
-  auto entry = [&](int i, int j) { return i < 9 ? fs0[i * 9 + j] : (fs1 ? fs1[(i - 9) * 9 + j] : 0.0); };
-  double c[9];
-  for (int j = 0; j < 9; j++) {
-    double m = 0;
-    for (int i = 0; i < 18; i++) m = fmax(m, fabs(entry(i, j)));
-    c[j] = m > 0 ? m : 1.0;
-  }
-  double rs[18][9], nrm0 = 0;
-  for (int i = 0; i < 18; i++) {
-    double n2 = 0;
-    for (int j = 0; j < 9; j++) {
-      rs[i][j] = entry(i, j) / c[j];
-      n2 += rs[i][j] * rs[i][j];
-    }
-    nrm0 = fmax(nrm0, n2);
-  }
-  double Q[3][9];
-  for (int k = 0; k < 3; k++) {
-    int piv = 0;
-    double best = -1;
-    for (int i = 0; i < 18; i++) {
-      double n2 = 0;
-      for (int j = 0; j < 9; j++) n2 += rs[i][j] * rs[i][j];
-      if (n2 > best) {
-        best = n2;
-        piv = i;
-      }
-    }
-    double v[9];
-    for (int j = 0; j < 9; j++) v[j] = rs[piv][j];
-    for (int pass = 0; pass < 2; pass++)
-      for (int kk = 0; kk < k; kk++) {
-        double d = 0;
-        for (int j = 0; j < 9; j++) d += v[j] * Q[kk][j];
-        for (int j = 0; j < 9; j++) v[j] -= d * Q[kk][j];
-      }
-    double n2 = 0;
-    for (int j = 0; j < 9; j++) n2 += v[j] * v[j];
-    const double inv = n2 > 1e-60 * nrm0 && n2 > 0 ? 1.0 / sqrt(n2) : 0.0;
-    for (int j = 0; j < 9; j++) Q[k][j] = v[j] * inv;
-    for (int i = 0; i < 18; i++) {
-      double d = 0;
-      for (int j = 0; j < 9; j++) d += rs[i][j] * Q[k][j];
-      for (int j = 0; j < 9; j++) rs[i][j] -= d * Q[k][j];
-    }
-  }
-  double res = 0;
-  for (int i = 0; i < 18; i++) {
-    double n2 = 0;
-    for (int j = 0; j < 9; j++) n2 += rs[i][j] * rs[i][j];
-    res = fmax(res, n2);
-  }
-  for (int j = 0; j < 9; j++)
-    for (int k = 0; k < 3; k++) V[j][k] = c[j] * Q[k][j];
-  for (int i = 0; i < 18; i++)
-    for (int k = 0; k < 3; k++) {
-      double u = 0;
-      for (int j = 0; j < 9; j++) u += entry(i, j) / c[j] * Q[k][j];
-      U[i][k] = u;
-    }
-  return res <= 1e-18 * nrm0;
-}
-
-// per element face out[nEl][4][2][P]: V [9][4] and U0 [9][4] of the face's own pair (it writes),
-// then Uin [9][4]: U1 of the pair of the face it reads (the face neighbour's face for an inner
-// face, its own for a free surface; zeros for outflow), each with column 3 zero and the rest of the
-// entry zero. Every face computes both factorisations itself, so a reader next to a ghost (a halo
-// part) gets the factor the ghost's owner used for the rows it sends. Faces whose pair is not of
-// rank 3 count in *bad.
+// V = c Q. out[nEl][4][2][P]: V [9][4] (column 3 zero), then per quantity q {U0[q][0..2],
+// U1[q][0..2], 0, 0}, the rest zero; a face whose scaled rows keep more than 1e-9 of the largest
+// row's norm outside the three directions counts in *bad (its pair is not of rank 3).
 template <typename T>
 __global__ void kBuildFsChar(const double *fsE, const int32_t *elFaEl, const uint8_t *fId, const uint8_t *faType,
                              int64_t nEl, int P, T *out, int *bad) {
   for (int64_t ef = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; ef < nEl * 4;
        ef += int64_t(gridDim.x) * blockDim.x) {
+    const double *A = fsE + ef * 81;
+    const double *Bm = nullptr;
     const int ty = faType[ef];
-    // the face this one's rows reach (its reader), which is also the face it reads from
-    const int64_t other = ty == EDGE_FACE_INNER ? int64_t(elFaEl[ef]) * 4 + fId[ef]
-                          : ty == EDGE_FACE_FREE_SURFACE ? ef
-                                                         : -1;
-    const double *own0 = fsE + ef * 81;
-    const double *own1 = fsE + (nEl * 4 + ef) * 81;
-    double V[9][3], U[18][3];
+    if (ty == EDGE_FACE_INNER)
+      Bm = fsE + ((nEl + elFaEl[ef]) * 4 + fId[ef]) * 81;
+    else if (ty == EDGE_FACE_FREE_SURFACE)
+      Bm = fsE + (nEl * 4 + ef) * 81;
+    auto entry = [&](int i, int j) { return i < 9 ? A[i * 9 + j] : (Bm ? Bm[(i - 9) * 9 + j] : 0.0); };
+    double c[9];
+    for (int j = 0; j < 9; j++) {
+      double m = 0;
+      for (int i = 0; i < 18; i++) m = fmax(m, fabs(entry(i, j)));
+      c[j] = m > 0 ? m : 1.0;
+    }
+    double rs[18][9], nrm0 = 0;
+    for (int i = 0; i < 18; i++) {
+      double n2 = 0;
+      for (int j = 0; j < 9; j++) {
+        rs[i][j] = entry(i, j) / c[j];
+        n2 += rs[i][j] * rs[i][j];
+      }
+      nrm0 = fmax(nrm0, n2);
+    }
+    double Q[3][9];
+    for (int k = 0; k < 3; k++) {
+      int piv = 0;
+      double best = -1;
+      for (int i = 0; i < 18; i++) {
+        double n2 = 0;
+        for (int j = 0; j < 9; j++) n2 += rs[i][j] * rs[i][j];
+        if (n2 > best) {
+          best = n2;
+          piv = i;
+        }
+      }
+      double v[9];
+      for (int j = 0; j < 9; j++) v[j] = rs[piv][j];
+      for (int pass = 0; pass < 2; pass++)
+        for (int kk = 0; kk < k; kk++) {
+          double d = 0;
+          for (int j = 0; j < 9; j++) d += v[j] * Q[kk][j];
+          for (int j = 0; j < 9; j++) v[j] -= d * Q[kk][j];
+        }
+      double n2 = 0;
+      for (int j = 0; j < 9; j++) n2 += v[j] * v[j];
+      const double inv = n2 > 1e-60 * nrm0 && n2 > 0 ? 1.0 / sqrt(n2) : 0.0;
+      for (int j = 0; j < 9; j++) Q[k][j] = v[j] * inv;
+      for (int i = 0; i < 18; i++) {
+        double d = 0;
+        for (int j = 0; j < 9; j++) d += rs[i][j] * Q[k][j];
+        for (int j = 0; j < 9; j++) rs[i][j] -= d * Q[k][j];
+      }
+    }
+    double res = 0;
+    for (int i = 0; i < 18; i++) {
+      double n2 = 0;
+      for (int j = 0; j < 9; j++) n2 += rs[i][j] * rs[i][j];
+      res = fmax(res, n2);
+    }
+    if (res > 1e-18 * nrm0) atomicAdd(bad, 1);
     T *o = out + ef * 2 * P;
     for (int j = 0; j < 2 * P; j++) o[j] = T(0);
-    // the pair this face writes: its fsE[0] and the reader's fsE[1]
-    bool ok = charFactors(own0, other >= 0 ? fsE + (nEl * 4 + other) * 81 : nullptr, V, U);
     for (int j = 0; j < 9; j++)
+      for (int k = 0; k < 3; k++) o[4 * j + k] = T(c[j] * Q[k][j]);
+    for (int i = 0; i < 18; i++)
       for (int k = 0; k < 3; k++) {
-        o[4 * j + k] = T(V[j][k]);
-        o[36 + 4 * j + k] = T(U[j][k]);
+        double u = 0;
+        for (int j = 0; j < 9; j++) u += entry(i, j) / c[j] * Q[k][j];
+        o[36 + (i % 9) * 8 + (i / 9) * 3 + k] = T(u);
       }
-    // the pair it reads: the writer's fsE[0] and this face's fsE[1]
-    if (other >= 0) {
-      ok &= charFactors(fsE + other * 81, own1, V, U);
-      for (int j = 0; j < 9; j++)
-        for (int k = 0; k < 3; k++) o[72 + 4 * j + k] = T(U[9 + j][k]);
-    }
-    if (!ok) atomicAdd(bad, 1);
   }
 }
 

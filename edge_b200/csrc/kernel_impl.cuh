@@ -67,12 +67,6 @@ class KernelSetImpl final : public KernelSet {
         return e;
     }
     if constexpr (G::charMix) {
-      if ((e = cudaFuncSetAttribute(kNeigh<T, O, R, RM, true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                    (int)smemNeigh())))
-        return e;
-      if ((e = cudaFuncSetAttribute(kRecv<T, O, R, RM, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                    (int)smemRecv())))
-        return e;
       if ((e = cudaFuncSetAttribute(kLocal<T, O, R, RM, 0, false, true>,
                                     cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smemLocal())))
         return e;
@@ -171,12 +165,6 @@ class KernelSetImpl final : public KernelSet {
   bool charMix() const override { return G::charMix; }
   cudaError_t neigh(const StepArgsRaw &a, cudaStream_t s) override {
     if (a.elCount < 1) return cudaSuccess;
-    if constexpr (G::charMix) {
-      if (a.fsChar) {
-        kNeigh<T, O, R, RM, true, true><<<grid(a.elCount, ctasNeigh()), G::NT, smemNeigh(), s>>>(cast(a));
-        return cudaGetLastError();
-      }
-    }
     kNeigh<T, O, R, RM, G::premix><<<grid(a.elCount, ctasNeigh()), G::NT, smemNeigh(), s>>>(cast(a));
     return cudaGetLastError();
   }
@@ -188,12 +176,6 @@ class KernelSetImpl final : public KernelSet {
   cudaError_t recv(const StepArgsRaw &a, const RecvArgs &r, cudaStream_t s) override {
     const int g = (r.nGrp + G::E - 1) / G::E;
     if (g == 0) return cudaSuccess;
-    if constexpr (G::charMix) {
-      if (a.fsChar) {
-        kRecv<T, O, R, RM, true><<<g, G::NT, smemRecv(), s>>>(cast(a), r);
-        return cudaGetLastError();
-      }
-    }
     kRecv<T, O, R, RM><<<g, G::NT, smemRecv(), s>>>(cast(a), r);
     return cudaGetLastError();
   }

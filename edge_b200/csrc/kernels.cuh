@@ -55,10 +55,7 @@ struct StepArgs {
   // its face reader applies (fsE[1] of the face neighbour at its face, or the element's own for a
   // free surface; zeros for outflow) in T, each padded to 16 bytes (Geo::FSP): [nEl][4][2][FSP];
   // null: gathered through the connectivity. fsChar: fsLR holds the characteristic factors of
-  // those pairs instead (Geo::charMix: [nEl][4][2][FSP] with V [9][4], U0 [9][4] and Uin [9][4],
-  // each with column 3 zero: the face's own projection mixes as U0 V^T, and the three
-  // characteristic rows W = V^T P its reader receives mix on arrival as Uin W, Uin being the
-  // writer's U1 stored at the reader's face), and the face buffers hold W (rows 0-2 of each block)
+  // those pairs instead (Geo::charMix: V [9][4], then per quantity {U0[q][0..2], U1[q][0..2], 0, 0})
   const T *fsLR;
   int fsChar;
   // fused GTS steps (kLocal<..., FUSED>, kRecv): the previous step's pre-mixed face projections,
@@ -886,30 +883,51 @@ __device__ __forceinline__ void charRows(const T *S0, const T *fb, int q, int l,
   for (int k = 0; k < 3; k++) st4<T>(rowPtr<T, SF>(Wt, k, l) + j0, w[k]);
 }
 
-// second half: s[j] = sum_k u[k] W[k][j] (the face's own flux term) into registers; u = this lane's
-// U0[q] (or, on arrival, Uin[q])
-template <typename T, int F, int SF>
-__device__ __forceinline__ void charMix(const T *Wt, int l, const T *uq, T *s) {
-  T u[4];
-  ld4<T>(uq, u);
+// second half: s[j] = sum_k uu[k] W[k][j] into registers, t[j] = sum_k uu[3 + k] W[k][j] written to
+// tRow[0, G) chunk by chunk; W is zero past F, so is t
+template <typename T, int F, int SF, int G>
+__device__ __forceinline__ void charMix2(const T *Wt, int l, const T *uu, T *s, T *tRow) {
+  T u[8];
+  {
+    T a[4], b[4];
+    ld4<T>(uu, a);
+    ld4<T>(uu + 4, b);
+#pragma unroll
+    for (int i = 0; i < 4; i++) {
+      u[i] = a[i];
+      u[4 + i] = b[i];
+    }
+  }
 #pragma unroll
   for (int j0 = 0; j0 < F; j0 += 4) {
-    T w0[4], w1[4], w2[4];
+    T w0[4], w1[4], w2[4], o[4], p[4];
     ld4<T>(rowPtr<T, SF>(Wt, 0, l) + j0, w0);
     ld4<T>(rowPtr<T, SF>(Wt, 1, l) + j0, w1);
     ld4<T>(rowPtr<T, SF>(Wt, 2, l) + j0, w2);
 #pragma unroll
+    for (int v = 0; v < 4; v++) {
+      o[v] = fmaT(u[2], w2[v], fmaT(u[1], w1[v], u[0] * w0[v]));
+      p[v] = fmaT(u[5], w2[v], fmaT(u[4], w1[v], u[3] * w0[v]));
+    }
+#pragma unroll
     for (int v = 0; v < 4; v++)
-      if (j0 + v < F) s[j0 + v] = fmaT(u[2], w2[v], fmaT(u[1], w1[v], u[0] * w0[v]));
+      if (j0 + v < F) s[j0 + v] = o[v];
+    if (j0 + 4 <= G) {
+      st4<T>(tRow + j0, p);
+    } else {
+#pragma unroll
+      for (int v = 0; v < 4; v++)
+        if (j0 + v < G) tRow[j0 + v] = p[v];
+    }
   }
 }
-// CHAR: only the characteristic factors the local step reads (V and U0: the first 72 values)
+// CHAR: only the characteristic factors (the first 108 values: V [9][4], then {U0, U1} [9][8])
 template <typename T, int O, int R, int RM, int FA, bool CHAR = false>
 __device__ __forceinline__ void issueMixFs(const StepArgs<T> &a, T *buf, int64_t g, int64_t nGroups) {
   using G = Geo<T, O, R, RM>;
   constexpr int E = G::E, FSP = G::FSP, W = 16 / int(sizeof(T)), NC = FSP / W;
-  constexpr int NCP = CHAR ? 72 / W : 2 * NC;  // chunks copied per element face
-  static_assert(72 % W == 0, "factor blocks of whole chunks");
+  constexpr int NCP = CHAR ? 108 / W : 2 * NC;  // chunks copied per element face
+  static_assert(108 % W == 0 && 108 <= 2 * FSP, "factor entries of whole chunks within the pair stride");
   if (g >= nGroups) return;
   if (a.fsLR) {
     for (int i = threadIdx.x; i < E * NCP; i += G::NT) {
@@ -1017,40 +1035,16 @@ __device__ __forceinline__ int neighOri(const FaceMeta &m) {
 // the neighbour flux of face FA through pre-mixed projections read straight from global memory
 // (this warp's quantity row, this lane's run): the arithmetic of the neighbour kernel's
 // neighApplyMixed, for kernels that fold a pending neighbour step into their DOF rows
-// the arriving rows of face FA as this warp's quantity row: CHAR, the three characteristic rows of
-// the writer mixed with this face's Uin[q] (fsLR); else the writer's pre-mixed row q
-template <typename T, int O, int R, int RM, bool CHAR>
-__device__ __forceinline__ void arrivingRow(const T *faceIn, const T *fsLR, int64_t src, int64_t e, int FA, int q,
-                                            int r, T *x) {
-  using G = Geo<T, O, R, RM>;
-  constexpr int F = G::F;
-  if constexpr (CHAR) {
-    T u[4], w[F];
-    ld4<T>(fsLR + (e * 4 + FA) * (2 * G::FSP) + 72 + q * 4, u);
-    ldRowG<T, F>(gRow<T, R, G::GF>(faceIn, src, 9, 0, r), w, true);
-#pragma unroll
-    for (int j = 0; j < F; j++) x[j] = u[0] * w[j];
-#pragma unroll
-    for (int k = 1; k < 3; k++) {
-      ldRowG<T, F>(gRow<T, R, G::GF>(faceIn, src, 9, k, r), w, true);
-#pragma unroll
-      for (int j = 0; j < F; j++) x[j] = fmaT(u[k], w[j], x[j]);
-    }
-  } else {
-    ldRowG<T, F>(gRow<T, R, G::GF>(faceIn, src, 9, q, r), x, true);
-  }
-}
-
-template <typename T, int O, int R, int RM, int FA, bool CHAR = false>
-__device__ __forceinline__ void neighFluxFace(const StepArgs<T> &a, const T *faceIn, const FaceMeta &m, int64_t e,
-                                              int q, int r, bool valid, T *acc) {
+template <typename T, int O, int R, int RM, int FA>
+__device__ __forceinline__ void neighFluxFace(const T *faceIn, const FaceMeta &m, int64_t e, int q, int r,
+                                              bool valid, T *acc) {
   using G = Geo<T, O, R, RM>;
   constexpr int F = G::F;
   const int ty = m.type(FA);
   if (!valid || ty == FT_OUTFLOW || q >= 9) return;
   const int64_t src = ty == FT_INNER ? int64_t(m.src[FA]) : e * 4 + FA;
   T x[F];
-  arrivingRow<T, O, R, RM, CHAR>(faceIn, a.fsLR, src, e, FA, q, r, x);
+  ldRowG<T, F>(gRow<T, R, G::GF>(faceIn, src, 9, q, r), x, true);
   if (ty == FT_INNER) {
     T o[F];
 #pragma unroll
@@ -1067,15 +1061,15 @@ __device__ __forceinline__ void neighFluxFace(const StepArgs<T> &a, const T *fac
     FluxTMul<O, FA>::template run<T>(x, acc);
   }
 }
-template <typename T, int O, int R, int RM, bool CHAR = false>
+template <typename T, int O, int R, int RM>
 __device__ __forceinline__ void neighFluxDirect(const StepArgs<T> &a, const T *faceIn, int64_t e, int q, int r,
                                                 bool valid, T *acc) {
   FaceMeta m;
   m.load(a, e, valid);
-  neighFluxFace<T, O, R, RM, 0, CHAR>(a, faceIn, m, e, q, r, valid, acc);
-  neighFluxFace<T, O, R, RM, 1, CHAR>(a, faceIn, m, e, q, r, valid, acc);
-  neighFluxFace<T, O, R, RM, 2, CHAR>(a, faceIn, m, e, q, r, valid, acc);
-  neighFluxFace<T, O, R, RM, 3, CHAR>(a, faceIn, m, e, q, r, valid, acc);
+  neighFluxFace<T, O, R, RM, 0>(faceIn, m, e, q, r, valid, acc);
+  neighFluxFace<T, O, R, RM, 1>(faceIn, m, e, q, r, valid, acc);
+  neighFluxFace<T, O, R, RM, 2>(faceIn, m, e, q, r, valid, acc);
+  neighFluxFace<T, O, R, RM, 3>(faceIn, m, e, q, r, valid, acc);
 }
 
 // ------------------------------------------------------------------------------------------------
@@ -1170,14 +1164,17 @@ __device__ __forceinline__ void localFace(const StepArgs<T> &a, const T *TI, T *
     const T *fbE = mf.buf + (FA % 2) * (E * 2 * FSP) + (l / R) * (2 * FSP);
     static_assert(!CHAR || (LTS == 0 && G::charMix), "characteristic mix: GTS configurations with room for it");
     if constexpr (CHAR) {
-      // the characteristic rows of all warps' projections, then this face's own flux term from
-      // them; the reader receives the rows themselves (warps 0-2 store rows 0-2 of the block)
+      // the characteristic rows of all warps' projections, then both mixes from them; the mixed
+      // projection leaves through this warp's own row of S0 (no warp reads S0 after the barrier)
       charRows<T, F, SF>(S0, fbE, q, l, mf.w);
       __syncthreads();
-      charMix<T, F, SF>(mf.w, l, fbE + 36 + q * 4, s);
-      if (q < 3 && ty != FT_OUTFLOW)
-        storeRowsCoalesced<T, R, G::GF, SF>(mf.w, a.face + ((e * 4 + FA) * 9 + q) * int64_t(R * G::GF), q, l / R,
+      T *tRow = rowPtr<T, SF>(S0, q, l);
+      charMix2<T, F, SF, G::GF>(mf.w, l, fbE + 36 + q * 8, s, tRow);
+      __syncwarp();
+      if (ty != FT_OUTFLOW)
+        storeRowsCoalesced<T, R, G::GF, SF>(S0, a.face + ((e * 4 + FA) * 9 + q) * int64_t(R * G::GF), q, l / R,
                                             l % R);
+      __syncwarp();
       FluxTMul<O, FA>::template run<T>(s, acc);
       if constexpr (TAIL) __syncthreads();
       return;
@@ -1427,7 +1424,7 @@ __global__ void __launch_bounds__(Geo<T, O, R, RM>::NT, LTS == 2 ? 1 : Geo<T, O,
           for (int n = 0; n < B; n++) v[n] = T(0);
         if constexpr (FUSED) {
           if (a.faceIn) {
-            neighFluxDirect<T, O, R, RM, CHAR>(a, a.faceIn, ev, q, r, valid, v);
+            neighFluxDirect<T, O, R, RM>(a, a.faceIn, ev, q, r, valid, v);
             // the completed rows back to the DOFs (the volume integral reads them again)
             T *p = rowPtr<T, SB>(X, q, l);
             stRow<T, B>(p, v);
@@ -1729,15 +1726,15 @@ struct NeighSlots {
   }
 
   // copies of item (group g, face FA) into `slot`; m = connectivity of this lane's element; PM: the
-  // rows are pre-mixed (no flux-solver blocks); CHAR: the three characteristic rows (warps 0-2)
-  template <int FA, bool PM, bool CHAR = false>
+  // rows are pre-mixed (no flux-solver blocks)
+  template <int FA, bool PM>
   __device__ __forceinline__ static void issue(const StepArgs<T> &a, unsigned char *base, int slot, int q, int l,
                                                int64_t g, bool groupValid, const FaceMeta &m) {
     if (groupValid) {
       const int eo = l / R, r = l % R;
       const int64_t e = a.elFirst + g * E + eo;
       const int ty = m.type(FA);
-      if (q < (CHAR ? 3 : 9) && g * E + eo < a.elCount && ty != FT_OUTFLOW) {
+      if (q < 9 && g * E + eo < a.elCount && ty != FT_OUTFLOW) {
         // inner faces: the neighbour's projection over this element's step (its own face buffer,
         // or with LTS its two-step sum / half-step buffer); free surface: this element's own
         const T *buf = a.face;
@@ -1847,59 +1844,15 @@ __device__ __forceinline__ void neighApplyMixed(const T *S, int q, int l, bool v
   }
 }
 
-// characteristic rows: the writer's three rows of the slot mixed with this face's Uin[q], rotated
-// into this element's face orientation (inner faces), then fluxT
-template <typename T, int O, int R, int RM, int FA>
-__device__ __forceinline__ void neighApplyChar(const StepArgs<T> &a, const T *S, int q, int l, int64_t e,
-                                               bool valid, const FaceMeta &m, T *acc) {
-  using G = Geo<T, O, R, RM>;
-  constexpr int F = G::F, SF = G::SF;
-  const int ty = m.type(FA);
-  if (!valid || ty == FT_OUTFLOW || q >= 9) return;
-  T x[F];
-  charMix<T, F, SF>(S, l, a.fsLR + (e * 4 + FA) * (2 * G::FSP) + 72 + q * 4, x);
-  if (ty == FT_INNER) {
-    T o[F];
-#pragma unroll
-    for (int j = 0; j < F; j++) o[j] = T(0);
-    const int v = neighOri<O, FA>(m);
-    if (v == 0)
-      OriMul<O, 0>::template run<T>(x, o);
-    else if (v == 1)
-      OriMul<O, 1>::template run<T>(x, o);
-    else
-      OriMul<O, 2>::template run<T>(x, o);
-    FluxTMul<O, FA>::template run<T>(o, acc);
-  } else {
-    FluxTMul<O, FA>::template run<T>(x, acc);
-  }
-}
-
 // item (local group k, face FA): item index i = 4k + FA lives in slot i % NSN; after the barrier the
 // item i + NSN - 1 is issued into slot (i - 1) % NSN, which the barrier has released. PM: every warp
-// touches only its own quantity rows, so a warp-level order replaces the barrier. CHAR: warps 0-2
-// bring the three characteristic rows every warp reads, so the barrier stays.
-template <typename T, int O, int R, int RM, int FA, bool PM, bool CHAR = false>
+// touches only its own quantity rows, so a warp-level order replaces the barrier.
+template <typename T, int O, int R, int RM, int FA, bool PM>
 __device__ __forceinline__ void neighItem(const StepArgs<T> &a, unsigned char *base, int q, int l, int64_t e,
                                           bool valid, const FaceMeta &cur, const FaceMeta &nxt, int64_t g,
                                           bool nextValid, int64_t k, T *acc, T *upA) {
   using NS = NeighSlots<T, O, R, RM>;
   constexpr int NSN = Geo<T, O, R, RM>::NSN;
-  if constexpr (CHAR) {
-    static_assert(PM, "characteristic rows replace pre-mixed ones");
-    cpAsyncWait<NSN - 2>();
-    __syncthreads();
-    const int64_t item = k * 4 + FA;
-    const int slot = int(item % NSN);
-    constexpr int AHEAD = FA + NSN - 1;
-    const int slotNext = int((item + NSN - 1) % NSN);
-    if constexpr (AHEAD < 4)
-      NS::template issue<AHEAD, true, true>(a, base, slotNext, q, l, g, true, cur);
-    else
-      NS::template issue<AHEAD - 4, true, true>(a, base, slotNext, q, l, g + gridDim.x, nextValid, nxt);
-    neighApplyChar<T, O, R, RM, FA>(a, NS::rows(base, slot), q, l, e, valid, cur, acc);
-    return;
-  }
   if constexpr (PM) {
     cpAsyncWait<NSN - 2>();
     __syncwarp();
@@ -1937,8 +1890,7 @@ __device__ __forceinline__ void neighItem(const StepArgs<T> &a, unsigned char *b
 // PM: the face buffers hold projections pre-mixed with this element's flux solvers (the local
 // kernels write them so where their buffers fit); otherwise the mix happens here (attenuation,
 // configurations without room for pre-mixing)
-// CHAR: the face buffers hold the writers' characteristic rows (StepArgs::fsChar)
-template <typename T, int O, int R, int RM, bool PM, bool CHAR = false>
+template <typename T, int O, int R, int RM, bool PM>
 __global__ void __launch_bounds__(Geo<T, O, R, RM>::NT, Geo<T, O, R, RM>::minCtasNeigh) kNeigh(StepArgs<T> a) {
   using G = Geo<T, O, R, RM>;
   using NS = NeighSlots<T, O, R, RM>;
@@ -1953,9 +1905,9 @@ __global__ void __launch_bounds__(Geo<T, O, R, RM>::NT, Geo<T, O, R, RM>::minCta
   // prologue: the first group's DOF rows and items 0 .. NSN-2 (its first faces)
   NS::issueDofs(a, smem, q, l, g, g < nGroups);
   NS::issueDofsA(a, smem, q, l, g, g < nGroups);
-  NS::template issue<0, PM, CHAR>(a, smem, 0, q, l, g, g < nGroups, cur);
-  if constexpr (NSN > 2) NS::template issue<1, PM, CHAR>(a, smem, 1, q, l, g, g < nGroups, cur);
-  if constexpr (NSN > 3) NS::template issue<2, PM, CHAR>(a, smem, 2, q, l, g, g < nGroups, cur);
+  NS::template issue<0, PM>(a, smem, 0, q, l, g, g < nGroups, cur);
+  if constexpr (NSN > 2) NS::template issue<1, PM>(a, smem, 1, q, l, g, g < nGroups, cur);
+  if constexpr (NSN > 3) NS::template issue<2, PM>(a, smem, 2, q, l, g, g < nGroups, cur);
   for (int64_t k = 0; g < nGroups; g += gridDim.x, k++) {
     const int64_t e = a.elFirst + g * E + eo;
     const bool valid = g * E + eo < a.elCount;
@@ -1986,10 +1938,10 @@ __global__ void __launch_bounds__(Geo<T, O, R, RM>::NT, Geo<T, O, R, RM>::minCta
 #pragma unroll
       for (int n = 0; n < B; n++) upA[n] = T(0);
     }
-    neighItem<T, O, R, RM, 0, PM, CHAR>(a, smem, q, l, e, valid, cur, nxt, g, nextValid, k, acc, upA);
-    neighItem<T, O, R, RM, 1, PM, CHAR>(a, smem, q, l, e, valid, cur, nxt, g, nextValid, k, acc, upA);
-    neighItem<T, O, R, RM, 2, PM, CHAR>(a, smem, q, l, e, valid, cur, nxt, g, nextValid, k, acc, upA);
-    neighItem<T, O, R, RM, 3, PM, CHAR>(a, smem, q, l, e, valid, cur, nxt, g, nextValid, k, acc, upA);
+    neighItem<T, O, R, RM, 0, PM>(a, smem, q, l, e, valid, cur, nxt, g, nextValid, k, acc, upA);
+    neighItem<T, O, R, RM, 1, PM>(a, smem, q, l, e, valid, cur, nxt, g, nextValid, k, acc, upA);
+    neighItem<T, O, R, RM, 2, PM>(a, smem, q, l, e, valid, cur, nxt, g, nextValid, k, acc, upA);
+    neighItem<T, O, R, RM, 3, PM>(a, smem, q, l, e, valid, cur, nxt, g, nextValid, k, acc, upA);
     if constexpr (RM > 0) {
       if (q >= 9) {
         if (valid) {
@@ -2083,8 +2035,7 @@ __device__ __forceinline__ void recvAll(T *X, T *TI, T *XA, T *TIA, int q, int l
   }
 }
 
-// CHAR: a pending neighbour step arrives as characteristic rows (StepArgs::fsChar)
-template <typename T, int O, int R, int RM, bool CHAR = false>
+template <typename T, int O, int R, int RM>
 __global__ void __launch_bounds__(Geo<T, O, R, RM>::NT) kRecv(StepArgs<T> a, RecvArgs rv) {
   using G = Geo<T, O, R, RM>;
   constexpr int B = G::B, E = G::E, SB = G::SB;
@@ -2110,7 +2061,7 @@ __global__ void __launch_bounds__(Geo<T, O, R, RM>::NT) kRecv(StepArgs<T> a, Rec
     ldRowG<T, B>(gRow<T, R, G::GB>(a.dofsE, ev, 9, q, r), v, valid);
     // a pending neighbour step (fused GTS steps) completes the rows first
     if constexpr (RM == 0)
-      if (a.faceIn) neighFluxDirect<T, O, R, RM, CHAR>(a, a.faceIn, ev, q, r, valid, v);
+      if (a.faceIn) neighFluxDirect<T, O, R, RM>(a, a.faceIn, ev, q, r, valid, v);
     stRow<T, B>(rowPtr<T, SB>(X, q, l), v);
     if constexpr (G::tiSmem)
       stRow<T, B>(rowPtr<T, SB>(TI, q, l), zero);

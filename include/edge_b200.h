@@ -322,10 +322,10 @@ int edge_b200_kernel_times(edge_b200_ctx *ctx, double *ms, int64_t *launches);
  * kernels run one element per thread team): info[0] elements per CTA, info[1] 1 when GTS face
  * projections leave the local kernel pre-mixed with the reading element's flux solver (the local
  * kernel then reads per element face the padded pair [2][info[2]] of flux solvers in the
- * configuration's precision, the neighbour kernel none), 2 when they leave as the three
- * characteristic rows of the face's flux-solver pair instead (the local kernel reads 72 factor
- * values per face, the reader 36 more and three rows instead of nine; the form of the next GTS
- * step once its factors are built), info[3] / info[4] persistent CTAs of the
+ * configuration's precision, the neighbour kernel none), 2 when the local kernel does both of those
+ * mixes through the rank-3 factors of the face's flux-solver pair (it then reads 108 factor values
+ * per face instead of the pair; the form of the next GTS step once its factors are built),
+ * info[3] / info[4] persistent CTAs of the
  * local / neighbour kernel, info[5] 1 when multi-step calls fuse each neighbour step into the next
  * local kernel (edge_b200_set_fused). */
 int edge_b200_kernel_config(const edge_b200_ctx *ctx, int32_t info[6]);

@@ -246,31 +246,25 @@ def flux_char_factors(fs0, fs1):
     return c[:, None] * Q.T, U[:9], U[9:]
 
 
-def face_rows_char(prob, tDofs, send):
-    """The face rows a part sends for its faces `send` [n][2] = (element, face) in the device's
-    characteristic form: the element's time-integrated DOFs projected on the face (tDofs . fluxL,
-    the face-projected data of EDGE's MPI path, AderDg.hpp:419-473) reduced to the three
-    characteristic rows W = V^T P of the face's flux-solver pair (flux_char_factors with the
-    reader's fsE[1]: the face neighbour's at its own face id). Returns [n][3][F][R]."""
-    fl, fs0, fs1 = prob["fluxL"], prob["fsE"][0], prob["fsE"][1]
+def face_rows_premixed(prob, tDofs, send):
+    """The face rows a part sends for its faces `send` [n][2] = (element, face): the element's
+    time-integrated DOFs projected on the face (tDofs . fluxL_face, the face-projected data EDGE's
+    MPI path ships, AderDg.hpp:419-473) and mixed with the flux solver of the element that reads
+    them (fsE[1] of the face neighbour at its own face id). Returns [n][9][F][R]."""
+    fl, fs1 = prob["fluxL"], prob["fsE"][1]
     out = []
     for e, f in send:
         ne, fo = int(prob["elFaEl"][e, f]), int(prob["fIdElFaEl"][e, f])
-        V, _, _ = flux_char_factors(fs0[e, f], fs1[ne, fo])
         proj = np.einsum("qbr,bf->qfr", tDofs[e], fl[f])
-        out.append(np.einsum("qk,qfr->kfr", V, proj))
+        out.append(np.einsum("qp,pfr->qfr", fs1[ne, fo].reshape(9, 9), proj))
     return np.array(out)
 
 
-def neigh_char_faces(prob, dofsE, faces, rows, O, writers):
-    """Adds the lifted fluxes of received characteristic rows: for reader face (element, face) with
-    rows W from writer face (element', face') [given in `writers`], the reader's factor U1 of the
-    writer's pair mixes them back to nine rows, P = U1 W, and dofs += (P . O[vId]) . fluxT_face (the
-    neighbour step of SurfIntVanilla::neigh with the flux solver applied through the factors)."""
-    ft, fs0, fs1 = prob["fluxT"], prob["fsE"][0], prob["fsE"][1]
-    for (e, f), (we, wf), W in zip(faces, writers, rows):
-        _, _, U1 = flux_char_factors(fs0[we, wf], fs1[e, f])
-        P = np.einsum("qk,kfr->qfr", U1, W)
+def neigh_premixed_faces(prob, dofsE, faces, rows, O):
+    """Adds the lifted fluxes of received pre-mixed face rows (SurfIntVanilla::neigh with the mix
+    done by the sender): for face (element, face) with row P, dofs += (P . O[vId]) . fluxT_face."""
+    ft = prob["fluxT"]
+    for (e, f), P in zip(faces, rows):
         s1 = np.einsum("qfr,fg->qgr", P, O[int(prob["vIdElFaEl"][e, f])])
         dofsE[e] += np.einsum("qfr,fb->qbr", s1, ft[f])
 

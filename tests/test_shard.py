@@ -2,10 +2,9 @@
 oracle's local / neighbour work regions with the per-step exchange, against the one-domain run.
 
 The ranks exchange what the device form exchanges: the face rows of the send faces, projected on
-the face and reduced to the three characteristic rows of the face's flux-solver pair
-(oracle.face_rows_char), sent after the send elements' local step and before the inner elements'
-one, mixed back by the reader with its factor of the pair and lifted with the face orientation
-and fluxT (oracle.neigh_char_faces). So the partition, the local numbering (send elements
+the face and pre-mixed with the reading element's flux solver (oracle.face_rows_premixed), sent
+after the send elements' local step and before the inner elements' one, and lifted by the
+reader with the face orientation and fluxT. So the partition, the local numbering (send elements
 first), the ghost mapping, the exchange format and the overlapped step order are checked on the
 CPU against the one-domain oracle.
 """
@@ -104,10 +103,10 @@ def _rank_main(rank, world, port, order, n_steps, out_dir):
             reqs, got = [], {}
             for peer in sorted(set(part.send) | set(part.recv)):
                 if peer in part.send:
-                    rows = oracle.face_rows_char(d, st["tDofs"], part.send[peer])
+                    rows = oracle.face_rows_premixed(d, st["tDofs"], part.send[peer])
                     reqs.append(dist.isend(torch.from_numpy(np.ascontiguousarray(rows)), peer))
                 if peer in part.recv:
-                    b = torch.zeros((len(part.recv[peer]), 3, p.order * (p.order + 1) // 2, 1), dtype=torch.float64)
+                    b = torch.zeros((len(part.recv[peer]), 9, p.order * (p.order + 1) // 2, 1), dtype=torch.float64)
                     reqs.append(dist.irecv(b, peer))
                     got[peer] = b
             # the inner elements' local step while the rows travel
@@ -119,9 +118,8 @@ def _rank_main(rank, world, port, order, n_steps, out_dir):
                 for (g, f), row in zip(part.recv[peer], b.numpy()):
                     slot[(int(g), int(f))] = row
             oracle.lts_neigh(dn, st, 0, part.n_owned, True, None)
-            writers = [(int(part.el_fa_el[e, f]), int(part.fid[e, f])) for e, f in ghost_faces]
-            rows = [slot[w] for w in writers]
-            oracle.neigh_char_faces(d, st["dofsE"], ghost_faces, rows, O, writers)
+            rows = [slot[(int(part.el_fa_el[e, f]), int(part.fid[e, f]))] for e, f in ghost_faces]
+            oracle.neigh_premixed_faces(d, st["dofsE"], ghost_faces, rows, O)
             t += p.dt
         out = np.empty_like(st["dofsE"][:part.n_owned])
         out[part.owned - part.lo] = st["dofsE"][:part.n_owned]
