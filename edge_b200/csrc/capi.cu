@@ -302,6 +302,7 @@ struct edge_b200_ctx {
   DevBuf fsLR;
   bool fsLRStale = true;
   bool fsLRChar = false;      // fsLR holds the characteristic factors of the pairs
+  DevBuf charBad;             // device counter of the factor build's rank check
   bool charRejected = false;  // some face's pair is not of rank 3 (until the element data changes)
   // fused GTS steps (pre-mixing configurations, no halo): within one multi-step call each local
   // step also runs the previous step's neighbour step, so the face projections alternate between
@@ -522,9 +523,11 @@ struct edge_b200_ctx {
     cudaError_t e = fsLR.fit(size_t(nEl) * 4 * 2 * P * realSize);
     if (e) return e;
     if (wantChar) {
-      int *bad = nullptr;
+      // the count of faces whose pair is not of rank 3, read back once (no allocation or device-wide
+      // synchronisation on the way: pools of a server set themselves up while others run)
+      if ((e = charBad.fit(sizeof(int)))) return e;
+      int *bad = charBad.as<int>();
       int nBad = 0;
-      if ((e = cudaMalloc(&bad, sizeof(int)))) return e;
       e = cudaMemsetAsync(bad, 0, sizeof(int), stream);
       if (!e) {
         const int grid = (int)std::min<int64_t>((nEl * 4 + 127) / 128, 148 * 8);
@@ -536,7 +539,6 @@ struct edge_b200_ctx {
       }
       if (!e) e = cudaMemcpyAsync(&nBad, bad, sizeof(int), cudaMemcpyDeviceToHost, stream);
       if (!e) e = cudaStreamSynchronize(stream);
-      cudaFree(bad);
       if (e) return e;
       if (nBad == 0) {
         fsLRStale = false;
