@@ -39,6 +39,7 @@ def load(order=4, runs=1, rm=0):
     L.ref_trafo.argtypes = [vp] * 5
     L.ref_fs.argtypes = [C.c_double] * 6 + [vp] * 3 + [C.c_int, vp, vp]
     L.ref_frequencies.argtypes = [C.c_int, C.c_double, C.c_double, vp]
+    L.ref_locate_eval.argtypes = [vp] * 5
     _cache[key] = L
     return L
 

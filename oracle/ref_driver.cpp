@@ -24,6 +24,9 @@
 #include "impl/seismic/setups/ViscoElasticity.h"
 #include "impl/seismic/common.hpp"
 #include "linalg/Series.hpp"
+#include "linalg/Mappings.hpp"
+#include "linalg/Matrix.h"
+#include "dg/Basis.h"
 #include "data/Dynamic.h"
 
 #include "edge_b200/csrc/gen/dg_tet.h"
@@ -200,6 +203,19 @@ void ref_fs(double rhoL, double rhoR, double lamL, double lamR, double muL, doub
 
 void ref_frequencies(int n, double fc, double fr, double *out) {
   edge::seismic::setups::ViscoElasticity::frequencies(n, fc, fr, out);
+}
+
+// a point in a tet's reference coordinates (linalg::Mappings::phyToRefTet4; ves [3 dims][4 vertices]),
+// the element basis there (dg::Basis::evalBasis) and the determinant of the element's Jacobian
+// (Mappings::evalJac, Matrix::det): the steps receivers and point sources take to their basis
+// values (Receivers.cpp:127-143; PointSources.hpp:458-495, which also scales by the inverse mass
+// matrix and divides by the determinant)
+void ref_locate_eval(const double *ves, const double *x, double *ref, double *basis, double *jacDet) {
+  edge::linalg::Mappings::phyToRefTet4((const double (*)[4])ves, x, ref);
+  for (int md = 0; md < B; md++) basis[md] = edge::dg::Basis::evalBasis(md, TET4, ref[0], ref[1], ref[2]);
+  double jac[3][3];
+  edge::linalg::Mappings::evalJac(TET4, ves, jac[0]);
+  *jacDet = edge::linalg::Matrix::det(3, jac[0]);
 }
 
 double ref_series_int(double dx, double x0, long n, const double *vals, double x1, double x2) {
