@@ -373,7 +373,7 @@ int edge_b200_step_noalloc(const edge_b200_cfg *cfg, int64_t n_el, double dt, in
  * upload DOFs and element data before creating the batch, and call edge_b200_batch_sync before
  * using a context on its own again. Contexts with receivers, halo parts or kernel timing on are
  * refused (EDGE_B200_ENOTSUP): those run through edge_b200_step. No counterpart in the reference
- * (one solver per process; cfg4-style uneven batches). */
+ * (one solver per process; here uneven batches of simulations on one GPU). */
 typedef struct edge_b200_batch edge_b200_batch;
 int edge_b200_batch_create(edge_b200_ctx *const *ctxs, int n, const double *t0, const double *dt,
                            edge_b200_batch **out);

@@ -1,6 +1,6 @@
 """Shared test helpers: build small problems and run the CPU oracle the way the device path runs.
 
-The oracle (oracle/oracle.c) is the checker only; the device results come from edge_b200.solver.
+The oracle (oracle/oracle.c) only checks; the device results come from edge_b200.solver.
 """
 import numpy as np
 

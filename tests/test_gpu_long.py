@@ -1,6 +1,6 @@
 """Long runs on the GPU.
 
-* The plain-method configuration as BASELINE names it: 10 km box, 12^3 cubes x 6 = 10,368 tets,
+* The plain-method configuration: 10 km box, 12^3 cubes x 6 = 10,368 tets,
   order 4, FP64, one run, free surface on top and outflow elsewhere, explosive source at the centre
   (2 Hz Ricker), 8 seeded receivers, 200 steps at CFL 0.5: DOFs and receivers within rel-L2 1e-12 of
   the oracle.
