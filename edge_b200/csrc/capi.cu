@@ -511,13 +511,13 @@ struct edge_b200_ctx {
     return cudaSuccess;
   }
 
-  // the flux-solver pairs of the pre-mixed projections, as characteristic factors for GTS steps of
-  // a configuration that mixes through them (unless some face's pair is not of rank 3, found when
-  // the factors are built: the pairs themselves from then on until the element data changes), as
-  // the pairs themselves for LTS steps
+  // the flux-solver pairs of the pre-mixed projections, as characteristic factors for the steps of
+  // a configuration whose kernels (GTS, or LTS for lts) mix through them (unless some face's pair is
+  // not of rank 3, found when the factors are built: the pairs themselves from then on until the
+  // element data changes), else as the pairs themselves
   cudaError_t ensureFsLR(bool lts = false) {
     if (!ks->premix()) return cudaSuccess;
-    const bool wantChar = !lts && ks->charMix() && !charRejected;
+    const bool wantChar = (lts ? ks->charMixLts() : ks->charMix()) && !charRejected;
     if (!fsLRStale && fsLRChar == wantChar) return cudaSuccess;
     const int P = ks->fsPairStride();
     cudaError_t e = fsLR.fit(size_t(nEl) * 4 * 2 * P * realSize);

@@ -96,6 +96,14 @@ class KernelSetImpl final : public KernelSet {
                                                              G::smemLocalSums)))
         return e;
       occLocalSum_ = occLocalSum_ < 1 ? 1 : occLocalSum_;
+      if constexpr (G::charMixLts) {
+        if ((e = cudaFuncSetAttribute(kLocal<T, O, R, RM, 2, false, true>,
+                                      cudaFuncAttributeMaxDynamicSharedMemorySize, (int)G::smemLocalLts)))
+          return e;
+        if ((e = cudaFuncSetAttribute(kLocal<T, O, R, RM, 1, false, true>,
+                                      cudaFuncAttributeMaxDynamicSharedMemorySize, (int)G::smemLocalSums)))
+          return e;
+      }
     }
     occLocal_ = occLocal_ < 1 ? 1 : occLocal_;
     occNeigh_ = occNeigh_ < 1 ? 1 : occNeigh_;
@@ -144,6 +152,13 @@ class KernelSetImpl final : public KernelSet {
   cudaError_t localLts(const StepArgsRaw &a, cudaStream_t s) override {
     if constexpr (G::ltsOk) {
       if (a.elCount < 1) return cudaSuccess;
+      if constexpr (G::charMixLts) {
+        if (a.fsChar) {
+          kLocal<T, O, R, RM, 2, false, true>
+              <<<grid(a.elCount, numSms_ * occLocalLts_), G::NT, G::smemLocalLts, s>>>(cast(a));
+          return cudaGetLastError();
+        }
+      }
       kLocal<T, O, R, RM, 2><<<grid(a.elCount, numSms_ * occLocalLts_), G::NT, G::smemLocalLts, s>>>(cast(a));
       return cudaGetLastError();
     } else {
@@ -153,6 +168,13 @@ class KernelSetImpl final : public KernelSet {
   cudaError_t localLtsSums(const StepArgsRaw &a, cudaStream_t s) override {
     if constexpr (G::ltsOk) {
       if (a.elCount < 1) return cudaSuccess;
+      if constexpr (G::charMixLts) {
+        if (a.fsChar) {
+          kLocal<T, O, R, RM, 1, false, true>
+              <<<grid(a.elCount, numSms_ * occLocalSum_), G::NT, G::smemLocalSums, s>>>(cast(a));
+          return cudaGetLastError();
+        }
+      }
       kLocal<T, O, R, RM, 1><<<grid(a.elCount, numSms_ * occLocalSum_), G::NT, G::smemLocalSums, s>>>(cast(a));
       return cudaGetLastError();
     } else {
@@ -163,6 +185,7 @@ class KernelSetImpl final : public KernelSet {
   bool premix() const override { return G::premix; }
   int fsPairStride() const override { return G::FSP; }
   bool charMix() const override { return G::charMix; }
+  bool charMixLts() const override { return G::charMixLts; }
   cudaError_t neigh(const StepArgsRaw &a, cudaStream_t s) override {
     if (a.elCount < 1) return cudaSuccess;
     kNeigh<T, O, R, RM, G::premix><<<grid(a.elCount, ctasNeigh()), G::NT, smemNeigh(), s>>>(cast(a));

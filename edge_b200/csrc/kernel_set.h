@@ -54,6 +54,8 @@ class KernelSet {
   // the GTS local kernel mixes face projections through the rank-3 factors of the flux-solver
   // pairs when fsLR holds them (StepArgsRaw::fsChar)
   virtual bool charMix() const = 0;
+  // the LTS local kernels do the same (both of their tiles of characteristic rows fit)
+  virtual bool charMixLts() const = 0;
   virtual cudaError_t neigh(const StepArgsRaw &a, cudaStream_t s) = 0;
   // the neighbour step over the buffers the LTS local kernels wrote (pre-mixed where those
   // kernels have room for it)

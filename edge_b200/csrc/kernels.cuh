@@ -360,6 +360,9 @@ struct Geo {
   static constexpr bool wInX = nW <= nX - nS0;
   static constexpr bool charMix =
       premix && (F + 3) / 4 <= 9 && (wInX || smemLocal + premixBytes + nW * sizeof(T) <= localBudget);
+  // LTS local kernels: the characteristic rows (and, in mode 2, those of the half-step projections)
+  // behind X's face rows, where both tiles fit there
+  static constexpr bool w2InX = 2 * nW <= nX - nS0;
   static constexpr size_t smemLocalGts = premix      ? smemLocal + premixBytes +
                                                       (charMix && !wInX ? nW * sizeof(T) : 0)
                                          : projSplit ? tilesOff + 2 * nS0 * sizeof(T)
@@ -386,6 +389,7 @@ struct Geo {
   // the LTS local kernel without half-step integrals (mode 1)
   static constexpr size_t smemLocalSums = smemLocal + (premixLts ? premixBytes : 0);
   static constexpr bool ltsOk = tiSmem && smemLocalLts <= 227 * 1024;
+  static constexpr bool charMixLts = premixLts && charMix && ltsOk && w2InX;
   // neighbour kernel: a ring of NSN slots, each [9][32][SF] face rows and, for E <= 4, the E
   // elements' flux-solver blocks (81 + 54 doubles); as many slots (2..4) as fit the shared memory
   // of minCtasNeigh CTAs per SM (228 KB, 1 KB reserved per CTA)
@@ -845,6 +849,22 @@ __device__ __forceinline__ void faceMix2(const T *S0, int l, const T (&fr)[9], c
   }
 }
 
+// one mix of the characteristic rows: h[j] = sum_k u[k] W[k][j] for j < F (u: three values)
+template <typename T, int F, int SF>
+__device__ __forceinline__ void charMixOne(const T *Wt, int l, const T *u, T *h) {
+  const T u0 = u[0], u1 = u[1], u2 = u[2];
+#pragma unroll
+  for (int j0 = 0; j0 < F; j0 += 4) {
+    T w0[4], w1[4], w2[4];
+    ld4<T>(rowPtr<T, SF>(Wt, 0, l) + j0, w0);
+    ld4<T>(rowPtr<T, SF>(Wt, 1, l) + j0, w1);
+    ld4<T>(rowPtr<T, SF>(Wt, 2, l) + j0, w2);
+#pragma unroll
+    for (int v = 0; v < 4; v++)
+      if (j0 + v < F) h[j0 + v] = fmaT(u2, w2[v], fmaT(u1, w1[v], u0 * w0[v]));
+  }
+}
+
 // the flux-solver blocks of face FA of group g's elements (pre-mixed projections) into buf
 // [E][2][FSP]: 16-byte copies from fsLR, or (without it) loads gathered through the connectivity
 // and stored in T, visible after the next barrier like the copies
@@ -852,7 +872,8 @@ template <typename T>
 struct MixFs {
   T *buf;  // two buffers [2][E][2][FSP]
   int64_t g, nGroups;
-  T *w = nullptr;  // characteristic rows [3][32][SF] (Geo::charMix)
+  T *w = nullptr;   // characteristic rows [3][32][SF] (Geo::charMix)
+  T *wh = nullptr;  // those of the half-step projections (LTS mode 2, Geo::charMixLts)
 };
 
 // characteristic rows of a face (Geo::charMix), first half: warp q < ceil(F / 4) computes modes
@@ -1162,34 +1183,32 @@ __device__ __forceinline__ void localFace(const StepArgs<T> &a, const T *TI, T *
       issueMixFs<T, O, R, RM, 0, CHAR>(a, mf.buf, mf.g + gridDim.x, mf.nGroups);
     cpAsyncCommit();
     const T *fbE = mf.buf + (FA % 2) * (E * 2 * FSP) + (l / R) * (2 * FSP);
-    static_assert(!CHAR || (LTS == 0 && G::charMix), "characteristic mix: GTS configurations with room for it");
+    static_assert(!CHAR || (LTS == 0 ? G::charMix : G::charMixLts),
+                  "characteristic mix: configurations with room for its rows");
+    // the mixed projection t of this warp's row: through the characteristic rows of all warps'
+    // projections (CHAR; it leaves through this warp's own row of S0, which no warp reads after the
+    // second barrier), else through the pair blocks (through the warp's row of S0alt)
+    T *tile = CHAR ? S0 : S0alt;
+    T *tRow = rowPtr<T, SF>(tile, q, l);
+    T fr1[CHAR ? 1 : 9];
     if constexpr (CHAR) {
-      // the characteristic rows of all warps' projections, then both mixes from them; the mixed
-      // projection leaves through this warp's own row of S0 (no warp reads S0 after the barrier)
       charRows<T, F, SF>(S0, fbE, q, l, mf.w);
+      // with half-step projections (LTS 2) their characteristic rows too
+      if constexpr (LTS == 2) charRows<T, F, SF>(ShF, fbE, q, l, mf.wh);
       __syncthreads();
-      T *tRow = rowPtr<T, SF>(S0, q, l);
       charMix2<T, F, SF, G::GF>(mf.w, l, fbE + 36 + q * 8, s, tRow);
-      __syncwarp();
-      if (ty != FT_OUTFLOW)
-        storeRowsCoalesced<T, R, G::GF, SF>(S0, a.face + ((e * 4 + FA) * 9 + q) * int64_t(R * G::GF), q, l / R,
-                                            l % R);
-      __syncwarp();
-      FluxTMul<O, FA>::template run<T>(s, acc);
-      if constexpr (TAIL) __syncthreads();
-      return;
-    }
-    T fr[9], fr1[9];
+    } else {
+      T fr[9];
 #pragma unroll
-    for (int i = 0; i < 9; i++) {
-      fr[i] = fbE[q * 9 + i];
-      fr1[i] = fbE[FSP + q * 9 + i];
+      for (int i = 0; i < 9; i++) {
+        fr[i] = fbE[q * 9 + i];
+        fr1[i] = fbE[FSP + q * 9 + i];
+      }
+      faceMix2<T, F, SF, G::GF>(S0, l, fr, fr1, s, tRow);
     }
-    T *tRow = rowPtr<T, SF>(S0alt, q, l);
-    faceMix2<T, F, SF, G::GF>(S0, l, fr, fr1, s, tRow);
     __syncwarp();
     if (ty != FT_OUTFLOW)
-      storeRowsCoalesced<T, R, G::GF, SF>(S0alt, a.face + ((e * 4 + FA) * 9 + q) * int64_t(R * G::GF), q, l / R,
+      storeRowsCoalesced<T, R, G::GF, SF>(tile, a.face + ((e * 4 + FA) * 9 + q) * int64_t(R * G::GF), q, l / R,
                                           l % R);
     if constexpr (LTS) {
       // the LTS buffers of the (pre-mixed) projection t: its sum over the two steps of a pair for a
@@ -1207,7 +1226,10 @@ __device__ __forceinline__ void localFace(const StepArgs<T> &a, const T *TI, T *
         }
         if (LTS == 2 && half) {
           T h[F], t[F];
-          faceMix<T, F, SF>(ShF, l, fr1, h);
+          if constexpr (CHAR)
+            charMixOne<T, F, SF>(mf.wh, l, fbE + 36 + q * 8 + 3, h);
+          else
+            faceMix<T, F, SF>(ShF, l, fr1, h);
           const int64_t slot = int64_t(a.halfIdx[e]) * 4 + FA;
           stRowG<T, F>(gRow<T, R, G::GF>(a.faceHalf1, slot, 9, q, r), h);
           ldRow<T, F>(tRow, t);
@@ -1558,7 +1580,7 @@ __global__ void __launch_bounds__(Geo<T, O, R, RM>::NT, LTS == 2 ? 1 : Geo<T, O,
       // characteristic rows: behind the face rows of X, or behind the flux-solver buffers
       T *const wTile =
           CHAR ? (G::wInX ? X + G::nS0 : reinterpret_cast<T *>(smem + G::smemLocal + G::premixBytes)) : nullptr;
-      const MixFs<T> mf{fsb, g, nGroups, wTile};
+      const MixFs<T> mf{fsb, g, nGroups, wTile, (CHAR && LTS == 2) ? X + G::nS0 + G::nW : nullptr};
       const LocalFs lf{fsl, g, nGroups};
       if constexpr (PSP) {
         T *const tiles[4] = {S0, X, reinterpret_cast<T *>(smem + G::tilesOff),
